@@ -1,0 +1,441 @@
+"""Case generation and the reference's case-file formats.
+
+A case is a single structured block of hexahedral elements with a high-order
+grid, a flow state at the nodal solution DOFs, and the run parameters. This
+module writes the three files the reference solver reads for such a case:
+
+* ``param.cfg``  -- "keyword: value" parameter file plus the subface table
+  (parser: src/InputParamClass.cpp:155-444, 1441-1580);
+* the PLOT3D grid -- Fortran unformatted records, single block, i fastest,
+  x block then y block then z block (reader: src/SolverClass.cpp:2893-3032);
+* the SU2 restart -- header {535532, nVar, nDOFs, 1, 8}, 33-byte variable
+  names, then per element (i fastest) and per nodal DOF (i fastest) the values
+  x, y, z, rho, rho u, rho v, rho w, rho E in dimensional form, then one int
+  and 8 doubles of metadata (reader: src/SolverClass.cpp:3040-3376 and
+  include/SolverClass.hpp:679-740; writer: src/SolverClass.cpp:4375-4808).
+
+The same arrays are handed to the GPU path directly, so both solvers start
+from identical grids and states. The analytic initial states (isentropic
+vortex, Taylor-Green vortex, Gaussian pressure pulse) are evaluated here in
+dimensional variables with the reference conditions of
+InputParamClass::ComputeReferenceConditions (src/InputParamClass.cpp:605-761).
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+import os
+import struct
+from typing import Optional, Sequence, Tuple
+
+import numpy as np
+
+GAMMA = 1.4
+R_GAS = 287.058
+MU_DIM = 1.716e-5
+SU2_MAGIC = 535532
+NAME_LEN = 33
+
+
+def lgl_points(n: int) -> np.ndarray:
+    """Gauss-Lobatto-Legendre points on [-1, 1] (n points).
+
+    Closed forms for n <= 7 as used by LocationDOFs1D
+    (src/StandAloneFunctions.cpp:182-327); Newton iteration on
+    (1 - x^2) P'_{n-1}(x) otherwise.
+    """
+    if n == 1:
+        return np.zeros(1)
+    if n == 2:
+        return np.array([-1.0, 1.0])
+    if n == 3:
+        return np.array([-1.0, 0.0, 1.0])
+    if n == 4:
+        a = math.sqrt(1.0 / 5.0)
+        return np.array([-1.0, -a, a, 1.0])
+    if n == 5:
+        a = math.sqrt(3.0 / 7.0)
+        return np.array([-1.0, -a, 0.0, a, 1.0])
+    if n == 6:
+        t1 = 2.0 * math.sqrt(7.0) / 21.0
+        t2 = math.sqrt(1.0 / 3.0 + t1)
+        t3 = math.sqrt(1.0 / 3.0 - t1)
+        return np.array([-1.0, -t2, -t3, t3, t2, 1.0])
+    if n == 7:
+        t1 = 2.0 * math.sqrt(5.0 / 3.0) / 11.0
+        t2 = math.sqrt(5.0 / 11.0 + t1)
+        t3 = math.sqrt(5.0 / 11.0 - t1)
+        return np.array([-1.0, -t2, -t3, 0.0, t3, t2, 1.0])
+    N = n - 1
+    x = -np.cos(np.pi * np.arange(n) / N)
+    for _ in range(100):
+        P0, P1 = np.ones_like(x), x.copy()
+        for k in range(2, N + 1):
+            P0, P1 = P1, ((2 * k - 1) * x * P1 - (k - 1) * P0) / k
+        dx = (x * P1 - P0) / (n * P1)
+        x = x - dx
+        if np.max(np.abs(dx)) < 1e-16:
+            break
+    x[0], x[-1] = -1.0, 1.0
+    return x
+
+
+def equidistant_points(n: int) -> np.ndarray:
+    return np.array([-1.0 + i * 2.0 / (n - 1) for i in range(n)]) if n > 1 else np.zeros(1)
+
+
+@dataclasses.dataclass
+class CaseSpec:
+    """Everything that defines one case (grid, physics, discretisation)."""
+
+    name: str = "case"
+    kind: str = "vortex"                 # vortex | tgv | pulse | uniform
+    n_elem: Tuple[int, int, int] = (8, 8, 8)
+    p: int = 3                           # polynomial degree of the solution
+    p_grid: Optional[int] = None         # polynomial degree of the grid (default p)
+    n_poly_int: Optional[int] = None     # integration rule degree (default 3p)
+    lo: Tuple[float, float, float] = (0.0, 0.0, 0.0)
+    hi: Tuple[float, float, float] = (10.0, 10.0, 10.0)
+    mach: float = 0.5
+    reynolds: float = 1.0e4
+    reynolds_length: float = 1.0
+    t_inf: float = 288.15
+    vel_dir: Tuple[float, float, float] = (1.0, 0.0, 0.0)
+    riemann: str = "IsmailRoe"           # IsmailRoe | Roe
+    theta_sym: float = 1.0
+    penalty: float = 1.0
+    cfl: float = 0.5
+    # Grid deformation: "sine" = x_i + amp sin(pi x_j/h) sin(pi x_k/h) with h = L/2,
+    # "random" = seeded uniform node perturbation of amp * element size,
+    # applied to nodes not on the block boundary; "none" = uniform grid.
+    grid_map: str = "sine"
+    grid_amp: float = 0.05
+    seed: int = 1
+    # Isentropic vortex strength and centre.
+    beta: float = 5.0
+    center: Tuple[float, float, float] = (5.0, 5.0, 5.0)
+    # Pressure pulse amplitude (relative) and width.
+    pulse_amp: float = 1.0e-3
+    pulse_width: float = 0.5
+
+    def __post_init__(self):
+        if self.p_grid is None:
+            self.p_grid = self.p
+        if self.n_poly_int is None:
+            self.n_poly_int = 3 * self.p
+        self.n_elem = tuple(int(v) for v in self.n_elem)
+
+    @property
+    def n_dofs_1d(self) -> int:
+        return self.p + 1
+
+    @property
+    def n_elements(self) -> int:
+        return self.n_elem[0] * self.n_elem[1] * self.n_elem[2]
+
+    @property
+    def n_dofs(self) -> int:
+        return self.n_elements * self.n_dofs_1d ** 3
+
+
+@dataclasses.dataclass
+class RefConditions:
+    """Reference state for a case with only periodic faces.
+
+    Follows the far-field branch of ComputeReferenceConditions
+    (src/InputParamClass.cpp:605-761): v_inf = M sqrt(gamma R T),
+    rho_ref = Re mu / (L v_inf), p_ref = rho_ref R T, u_ref = sqrt(p_ref/rho_ref),
+    and the non-dimensional viscosity mu u_ref / p_ref.
+    """
+
+    p_ref: float
+    rho_ref: float
+    u_ref: float
+    mu_nondim: float
+    v_inf: float
+    vel_dir: Tuple[float, float, float]
+
+
+def reference_conditions(spec: CaseSpec) -> RefConditions:
+    v_inf = spec.mach * math.sqrt(GAMMA * R_GAS * spec.t_inf)
+    rho_ref = spec.reynolds * MU_DIM / (spec.reynolds_length * v_inf)
+    p_ref = rho_ref * R_GAS * spec.t_inf
+    u_ref = math.sqrt(p_ref / rho_ref)
+    d = np.asarray(spec.vel_dir, dtype=float)
+    d = d / math.sqrt(float(d @ d))
+    return RefConditions(p_ref, rho_ref, u_ref, MU_DIM * u_ref / p_ref, v_inf, tuple(d))
+
+
+# ---------------------------------------------------------------------------
+# Grid
+# ---------------------------------------------------------------------------
+
+def _nodes_1d(n_elem: int, p: int, lo: float, hi: float) -> np.ndarray:
+    """Block node coordinates along one index direction: LGL nodes per element."""
+    r = lgl_points(p + 1)
+    h = (hi - lo) / n_elem
+    out = np.empty(n_elem * p + 1)
+    for e in range(n_elem):
+        out[e * p:(e + 1) * p + 1] = lo + h * (e + 0.5 * (r + 1.0))
+    out[-1] = hi
+    return out
+
+
+def make_grid(spec: CaseSpec) -> np.ndarray:
+    """Block grid nodes, shape (3, kl, jl, il): x, y, z with i fastest."""
+    pg = spec.p_grid
+    xs = [_nodes_1d(spec.n_elem[d], pg, spec.lo[d], spec.hi[d]) for d in range(3)]
+    Z, Y, X = np.meshgrid(xs[2], xs[1], xs[0], indexing="ij")
+    if spec.grid_map == "sine":
+        h = [0.5 * (spec.hi[d] - spec.lo[d]) for d in range(3)]
+        a = spec.grid_amp
+        sx = np.sin(np.pi * (X - spec.lo[0]) / h[0])
+        sy = np.sin(np.pi * (Y - spec.lo[1]) / h[1])
+        sz = np.sin(np.pi * (Z - spec.lo[2]) / h[2])
+        Xn, Yn, Zn = X + a * sy * sz, Y + a * sx * sz, Z + a * sx * sy
+        X, Y, Z = Xn, Yn, Zn
+    elif spec.grid_map == "random":
+        rng = np.random.default_rng(spec.seed)
+        dh = [(spec.hi[d] - spec.lo[d]) / spec.n_elem[d] for d in range(3)]
+        pert = rng.uniform(-1.0, 1.0, size=(3,) + X.shape)
+        interior = np.zeros(X.shape, dtype=bool)
+        interior[1:-1, 1:-1, 1:-1] = True
+        X = X + np.where(interior, spec.grid_amp * dh[0] * pert[0], 0.0)
+        Y = Y + np.where(interior, spec.grid_amp * dh[1] * pert[1], 0.0)
+        Z = Z + np.where(interior, spec.grid_amp * dh[2] * pert[2], 0.0)
+    elif spec.grid_map != "none":
+        raise ValueError(f"unknown grid_map {spec.grid_map!r}")
+    return np.stack([X, Y, Z])
+
+
+def element_nodes(grid: np.ndarray, n_elem: Sequence[int], p: int) -> np.ndarray:
+    """Per-element grid nodes, shape (nElem, 3, (p+1)^3); elements and nodes i fastest.
+
+    Same gathering as SolverClass::ReadGrid (src/SolverClass.cpp:2993-3032).
+    """
+    nI, nJ, nK = n_elem
+    n1 = p + 1
+    out = np.empty((nK, nJ, nI, 3, n1, n1, n1))
+    for k in range(nK):
+        for j in range(nJ):
+            for i in range(nI):
+                out[k, j, i] = grid[:, k * p:k * p + n1, j * p:j * p + n1, i * p:i * p + n1]
+    return out.reshape(nI * nJ * nK, 3, n1 ** 3)
+
+
+# ---------------------------------------------------------------------------
+# Initial states (dimensional primitive -> conservative at the nodal DOFs)
+# ---------------------------------------------------------------------------
+
+def primitive_state(spec: CaseSpec, xyz: np.ndarray, ref: RefConditions):
+    """Dimensional (rho, u, v, w, p) at points xyz (shape (3, ...))."""
+    x, y, z = xyz[0], xyz[1], xyz[2]
+    rho_inf, p_inf, c_u = ref.rho_ref, ref.p_ref, ref.u_ref
+    u_inf = [ref.v_inf * d for d in ref.vel_dir]
+    if spec.kind == "uniform":
+        ones = np.ones_like(x)
+        return rho_inf * ones, u_inf[0] * ones, u_inf[1] * ones, u_inf[2] * ones, p_inf * ones
+    if spec.kind == "vortex":
+        # Shu's isentropic vortex about the z axis: velocity perturbation scaled by
+        # sqrt(p_inf/rho_inf), temperature T/T_inf = 1 - (g-1) b^2/(8 g pi^2) e^(1-r^2).
+        dx, dy = x - spec.center[0], y - spec.center[1]
+        r2 = dx * dx + dy * dy
+        b = spec.beta
+        f = b / (2.0 * np.pi) * np.exp(0.5 * (1.0 - r2))
+        T = 1.0 - (GAMMA - 1.0) * b * b / (8.0 * GAMMA * np.pi ** 2) * np.exp(1.0 - r2)
+        rho = rho_inf * T ** (1.0 / (GAMMA - 1.0))
+        p = p_inf * T ** (GAMMA / (GAMMA - 1.0))
+        u = u_inf[0] - c_u * f * dy
+        v = u_inf[1] + c_u * f * dx
+        w = u_inf[2] + 0.0 * x
+        return rho, u, v, w, p
+    if spec.kind == "tgv":
+        # Taylor-Green vortex with V0 = v_inf, rho0 = rho_ref, p0 = p_ref, unit length.
+        V0 = ref.v_inf
+        u = V0 * np.sin(x) * np.cos(y) * np.cos(z)
+        v = -V0 * np.cos(x) * np.sin(y) * np.cos(z)
+        w = 0.0 * x
+        p = p_inf + rho_inf * V0 * V0 / 16.0 * (np.cos(2 * x) + np.cos(2 * y)) * (np.cos(2 * z) + 2.0)
+        rho = p / (R_GAS * spec.t_inf)
+        return rho, u, v, w, p
+    if spec.kind == "pulse":
+        # Gaussian pressure pulse p = p_inf (1 + a exp(-r^2/(2 w^2))), isentropic density.
+        r2 = sum((c - spec.center[d]) ** 2 for d, c in enumerate((x, y, z)))
+        p = p_inf * (1.0 + spec.pulse_amp * np.exp(-r2 / (2.0 * spec.pulse_width ** 2)))
+        rho = rho_inf * (p / p_inf) ** (1.0 / GAMMA)
+        ones = np.ones_like(x)
+        return rho, u_inf[0] * ones, u_inf[1] * ones, u_inf[2] * ones, p
+    raise ValueError(f"unknown case kind {spec.kind!r}")
+
+
+def conservative_state(spec: CaseSpec, xyz: np.ndarray, ref: RefConditions) -> np.ndarray:
+    """Dimensional conservative variables, shape (5,) + xyz.shape[1:]."""
+    rho, u, v, w, p = primitive_state(spec, xyz, ref)
+    rE = p / (GAMMA - 1.0) + 0.5 * rho * (u * u + v * v + w * w)
+    return np.stack([rho, rho * u, rho * v, rho * w, rE])
+
+
+def solution_dof_coordinates(spec: CaseSpec, elem_nodes: np.ndarray) -> np.ndarray:
+    """Coordinates of the nodal solution DOFs per element, shape (nElem, 3, K^3).
+
+    The generated grids place the grid nodes of every element at the LGL points
+    of the element, and the solution DOFs are LGL points of the same degree, so
+    the DOFs coincide with the grid nodes (the reference interpolates the grid
+    with Lagrange polynomials to the DOFs, ElementClass::ComputeCoorNodalSolDOFs).
+    """
+    if spec.p_grid != spec.p:
+        raise NotImplementedError("generated cases use grid degree == solution degree")
+    return elem_nodes
+
+
+# ---------------------------------------------------------------------------
+# File formats
+# ---------------------------------------------------------------------------
+
+def write_plot3d(path: str, grid: np.ndarray) -> None:
+    """Single-block PLOT3D file with Fortran record markers (double precision)."""
+    _, kl, jl, il = grid.shape
+    n = il * jl * kl
+    with open(path, "wb") as f:
+        f.write(struct.pack("<iii", 4, 1, 4))
+        f.write(struct.pack("<iiiii", 12, il, jl, kl, 12))
+        f.write(struct.pack("<i", 24 * n))
+        f.write(np.ascontiguousarray(grid, dtype="<f8").tobytes())
+        f.write(struct.pack("<i", 24 * n))
+
+
+def read_plot3d(path: str) -> np.ndarray:
+    with open(path, "rb") as f:
+        data = f.read()
+    if struct.unpack_from("<i", data, 0)[0] == 4:
+        off = 12
+    else:
+        off = 0
+    _, il, jl, kl, _ = struct.unpack_from("<iiiii", data, off)
+    off += 20 + 4
+    n = il * jl * kl
+    arr = np.frombuffer(data, dtype="<f8", count=3 * n, offset=off)
+    return arr.reshape(3, kl, jl, il).copy()
+
+
+def write_su2_restart(path: str, dof_xyz: np.ndarray, cons: np.ndarray) -> None:
+    """SU2 restart: per element, per DOF: x y z rho rhou rhov rhow rhoE (doubles).
+
+    dof_xyz has shape (nElem, 3, nDOFs); cons has shape (nElem, 5, nDOFs).
+    """
+    n_elem, _, n_dofs = dof_xyz.shape
+    names = ["x", "y", "z", "Density", "Momentum_x", "Momentum_y", "Momentum_z", "Energy"]
+    body = np.concatenate([dof_xyz, cons], axis=1).transpose(0, 2, 1)  # elem, dof, var
+    with open(path, "wb") as f:
+        f.write(struct.pack("<5i", SU2_MAGIC, len(names), n_elem * n_dofs, 1, 8))
+        for nm in names:
+            f.write(nm.encode().ljust(NAME_LEN, b"\0")[:NAME_LEN])
+        f.write(np.ascontiguousarray(body, dtype="<f8").tobytes())
+        f.write(struct.pack("<i", 0))
+        f.write(np.zeros(8, dtype="<f8").tobytes())
+
+
+def read_su2_restart(path: str, n_elem: int, n_dofs: int):
+    with open(path, "rb") as f:
+        data = f.read()
+    hdr = struct.unpack_from("<5i", data, 0)
+    if hdr[0] != SU2_MAGIC:
+        raise ValueError("not an SU2 restart file")
+    nvar = hdr[1]
+    off = 20 + nvar * NAME_LEN
+    body = np.frombuffer(data, dtype="<f8", count=n_elem * n_dofs * nvar, offset=off)
+    body = body.reshape(n_elem, n_dofs, nvar).transpose(0, 2, 1)
+    return body[:, :3].copy(), body[:, 3:8].copy()
+
+
+def _periodic_subfaces(spec: CaseSpec) -> str:
+    nI, nJ, nK = spec.n_elem
+    L = [spec.hi[d] - spec.lo[d] for d in range(3)]
+    I, J, K = nI + 1, nJ + 1, nK + 1
+    rows = [
+        (f"1 1 1 {J} 1 {K}", f"{I} {I} 1 {J} 1 {K}", (L[0], 0.0, 0.0)),
+        (f"{I} {I} 1 {J} 1 {K}", f"1 1 1 {J} 1 {K}", (-L[0], 0.0, 0.0)),
+        (f"1 {I} 1 1 1 {K}", f"1 {I} {J} {J} 1 {K}", (0.0, L[1], 0.0)),
+        (f"1 {I} {J} {J} 1 {K}", f"1 {I} 1 1 1 {K}", (0.0, -L[1], 0.0)),
+        (f"1 {I} 1 {J} 1 1", f"1 {I} 1 {J} {K} {K}", (0.0, 0.0, L[2])),
+        (f"1 {I} 1 {J} {K} {K}", f"1 {I} 1 {J} 1 1", (0.0, 0.0, -L[2])),
+    ]
+    out = []
+    for face, (own, donor, t) in enumerate(rows, start=1):
+        out.append(f"    {face}    1")
+        out.append(f"        Periodic1to1Trans  {own}   {donor}   1 2 3   "
+                   f"{t[0]!r} {t[1]!r} {t[2]!r}")
+    return "\n".join(out)
+
+
+def param_cfg_text(spec: CaseSpec, grid_file="grid.xyz", restart_file="restart.dat",
+                   restart=True) -> str:
+    d = spec.vel_dir
+    return f"""# Generated case {spec.name} ({spec.kind})
+Polynomial degree grid: {spec.p_grid}
+Polynomial degree solution: {spec.p}
+Polynomial degree integration rule: {spec.n_poly_int}
+Location of the DOFs: LGL
+Grid file name: {grid_file}
+Solution file name: data/Solution
+Restart file name: {restart_file}
+Restart: {"yes" if restart else "no"}
+Paraview visualization file name: anim/Solution.vtk
+Space average data file name: proc/SpaceAverage.vtk
+SU2 grid file name: proc/GridSU2.su2
+Write SU2 grid file: no
+Save solution every: 100000000
+Write time history info every: 1
+FEM working variables: Entropy
+Riemann solver: {spec.riemann}
+Subgrid scale model: None
+Wall modeling: No wall model
+Theta parameter symmetrizing terms: {spec.theta_sym!r}
+Relative penalty parameter: {spec.penalty!r}
+Mach number: {spec.mach!r}
+Reynolds number: {spec.reynolds!r}
+Reynolds length: {spec.reynolds_length!r}
+Free stream temperature: {spec.t_inf!r}
+Free stream velocity direction: {d[0]!r} {d[1]!r} {d[2]!r}
+Fluctuations to add to initial solution: No fluctuations
+Monitor forces: no
+Number of synchronization time steps: 1
+Synchronization time step: 1.0
+CFL number: {spec.cfl!r}
+Compute average solution: no
+
+Subface information
+{_periodic_subfaces(spec)}
+"""
+
+
+@dataclasses.dataclass
+class CaseData:
+    spec: CaseSpec
+    ref: RefConditions
+    grid: np.ndarray           # (3, kl, jl, il)
+    elem_nodes: np.ndarray     # (nElem, 3, K^3)
+    dof_xyz: np.ndarray        # (nElem, 3, K^3)
+    cons: np.ndarray           # (nElem, 5, K^3) dimensional conservative
+
+
+def build_case(spec: CaseSpec) -> CaseData:
+    ref = reference_conditions(spec)
+    grid = make_grid(spec)
+    nodes = element_nodes(grid, spec.n_elem, spec.p_grid)
+    xyz = solution_dof_coordinates(spec, nodes)
+    cons = conservative_state(spec, xyz.transpose(1, 0, 2), ref).transpose(1, 0, 2)
+    return CaseData(spec, ref, grid, nodes, xyz, np.ascontiguousarray(cons))
+
+
+def write_case(case: CaseData, directory: str) -> str:
+    """Write param.cfg, grid.xyz and restart.dat into directory; returns the cfg path."""
+    os.makedirs(directory, exist_ok=True)
+    for sub in ("data", "anim", "proc"):
+        os.makedirs(os.path.join(directory, sub), exist_ok=True)
+    write_plot3d(os.path.join(directory, "grid.xyz"), case.grid)
+    write_su2_restart(os.path.join(directory, "restart.dat"), case.dof_xyz, case.cons)
+    cfg = os.path.join(directory, "param.cfg")
+    with open(cfg, "w") as f:
+        f.write(param_cfg_text(case.spec))
+    return cfg
