@@ -1,0 +1,164 @@
+/*
+ * vcp3d_b200.h -- C ABI of the B200 (sm_100a) implementation of the VCP3D
+ * explicit DG residual and time step.
+ *
+ * The library replaces the per-element work inside the reference solver's
+ * residual and Runge-Kutta stage calls:
+ *
+ *   SolverClass::Residual(su2double *monitoringData, bool)      include/SolverClass.hpp:72-73
+ *   SolverClass::ExecuteTimeSynchronizationStep(su2double *)    include/SolverClass.hpp:50
+ *   ElementClass::ComputeTimeStep(...)                          include/ElementClass.hpp:312-317
+ *
+ * Everything crosses the boundary as plain pointers and sizes. A handle owns
+ * all device memory and one CUDA stream; the solution stays resident on the
+ * device between calls and host pointers are only borrowed for the duration
+ * of a call. Every entry point returns VCPG_OK (0) or one of the error codes
+ * below; vcpg_last_error() gives the message. The reference aborts the
+ * process in these situations (Terminate, src/StandAloneFunctions.cpp:628-674);
+ * a host shim that wants that behaviour maps a non-zero code to Terminate.
+ *
+ * Array conventions (all double precision, row-major, no padding):
+ *   K = n_poly + 1 (DOFs per direction), M = n_int_1d (integration points per
+ *   direction). Elements are numbered i fastest, then j, then k. Within an
+ *   element, DOFs and volume integration points are numbered i fastest; face
+ *   integration points follow the reference's face layout (i-faces: j fastest
+ *   then k; j-faces: i fastest then k; k-faces: i fastest then j).
+ *   Solution and residual: [n_elem][5][K^3], modal coefficients of the
+ *   entropy variables (the reference's mSol / mRes without padding).
+ */
+#ifndef VCP3D_B200_H
+#define VCP3D_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum vcpg_status {
+  VCPG_OK = 0,
+  VCPG_E_CUDA = 1,            /* a CUDA runtime call failed                      */
+  VCPG_E_CG_NOCONV = 2,       /* mass-matrix CG hit its iteration cap (100)      */
+  VCPG_E_NEG_A2 = 3,          /* negative speed of sound squared in the time step */
+  VCPG_E_NONFINITE = 4,       /* a non-finite value appeared in the state         */
+  VCPG_E_OOM = 5,             /* device allocation failed                         */
+  VCPG_E_UNSUPPORTED_KM = 6,  /* (K, M) pair without a compiled kernel            */
+  VCPG_E_ADMISSION = 7,       /* request does not fit the device memory budget    */
+  VCPG_E_INVALID = 8          /* invalid argument                                 */
+};
+
+enum vcpg_riemann { VCPG_ROE = 0, VCPG_ISMAIL_ROE = 1 };
+enum vcpg_precision { VCPG_FP64 = 0, VCPG_MIXED = 1 };
+enum vcpg_scheme { VCPG_SSPRK3 = 0, VCPG_LSRK4 = 1 };
+
+/* Face numbering used by every per-face array: 0 iMin, 1 iMax, 2 jMin, 3 jMax, 4 kMin, 5 kMax. */
+
+typedef struct vcpg_params {
+  int32_t n_elem[3];          /* elements in i, j, k                                 */
+  int32_t n_poly;             /* polynomial degree of the solution, K = n_poly + 1    */
+  int32_t n_int_1d;           /* integration points per direction, M                  */
+  int32_t riemann;            /* enum vcpg_riemann                                   */
+  int32_t metric_index_compat;/* 1: gradient and symmetrizing-flux transforms index
+                                 the metric by the variable index as the reference
+                                 does (src/ElementClass.cpp:3865-3873,
+                                 src/FluxesFace.cpp:272-282, 325-332); 0: by point */
+  int32_t precision;          /* enum vcpg_precision                                 */
+  double theta_sym;           /* "Theta parameter symmetrizing terms"                */
+  double rel_penalty;         /* "Relative penalty parameter"                        */
+  double cfl;                 /* "CFL number"                                        */
+  double mu;                  /* non-dimensional laminar viscosity                   */
+  double p_ref, u_ref, rho_ref; /* reference conditions (dimensional)                */
+} vcpg_params;
+
+/* Standard-element operators (StandardElementClass, src/StandardElementClass.cpp:105-911). */
+typedef struct vcpg_operators {
+  const double *leg_int;      /* [K][M] orthonormal Legendre basis at the 1-D Gauss points */
+  const double *dleg_int;     /* [K][M] its derivative                                     */
+  const double *leg_face;     /* [2][K] basis at r = -1 (min face) and r = +1 (max face)    */
+  const double *dleg_face;    /* [2][K] derivative at r = -1 and r = +1                     */
+  const double *w_int;        /* [M]    1-D Gauss weights                                   */
+  const double *leg_dofs;     /* [K][K] basis at the 1-D nodal DOFs (time-step conversion)  */
+  const double *basis_center; /* [K^3]  3-D basis at the element centre (CG preconditioner) */
+} vcpg_operators;
+
+/* Per-element geometry (ElementClass::ComputeMetricTerms, src/ElementClass.cpp:1027-1407). */
+typedef struct vcpg_geometry {
+  const double *vol_metric;   /* [n_elem][10][M^3]: J, dr/dx dr/dy dr/dz ds/dx ... dt/dz   */
+  const double *face_metric;  /* [n_elem][6][13][M^2]: unit normal (3), area, 9 terms      */
+  const double *elem_scalars; /* [n_elem][15]: lenI lenJ lenK lenLES lenVol volElem,
+                                 averaged unit normals of the i, j, k directions (9)       */
+  const int32_t *neighbors;   /* [n_elem][6]: neighbour element per face, -1 = boundary    */
+} vcpg_geometry;
+
+typedef struct vcpg_handle vcpg_handle;
+
+/* Creates a solver on the current CUDA device; uploads operators and geometry. */
+int vcpg_create(const vcpg_params *params, const vcpg_operators *ops,
+                const vcpg_geometry *geom, vcpg_handle **out);
+int vcpg_destroy(vcpg_handle *h);
+const char *vcpg_last_error(const vcpg_handle *h);
+
+/* Host-side set-up from a high-order grid (the product's own restatement of the
+ * reference's operator and metric pre-processing). grid_nodes is the per-element
+ * grid, [n_elem][3][(p_grid+1)^3], nodes at LGL (dof_location = 1) or
+ * equidistant (0) parametric positions. Fills caller-allocated arrays with the
+ * shapes documented in vcpg_operators / vcpg_geometry; neighbors are filled for
+ * a block that is periodic in every direction listed in periodic[3]. */
+int vcpg_setup_geometry(const vcpg_params *params, int32_t p_grid, int32_t dof_location,
+                        const int32_t periodic[3], const double *grid_nodes,
+                        double *leg_int, double *dleg_int, double *leg_face,
+                        double *dleg_face, double *w_int, double *leg_dofs,
+                        double *basis_center, double *vol_metric, double *face_metric,
+                        double *elem_scalars, int32_t *neighbors);
+
+/* Converts dimensional conservative variables at the nodal DOFs
+ * ([n_elem][5][K^3]) to modal entropy-variable coefficients, as
+ * SolverClass::ReadRestartSolution does (src/SolverClass.cpp:3310-3366).
+ * vand_inv is the [K][K] inverse 1-D Vandermonde matrix of the nodal DOFs,
+ * vand_inv[c * K + o] mapping nodal value c to mode o; NULL selects the LGL
+ * nodal DOFs. */
+int vcpg_nodal_conservative_to_modal(const vcpg_params *params, const double *vand_inv,
+                                     const double *cons, double *modal, int64_t n_elem);
+
+/* State transfer (host <-> device), [n_elem][5][K^3]. */
+int vcpg_set_state(vcpg_handle *h, const double *modal);
+int vcpg_get_state(vcpg_handle *h, double *modal);
+int vcpg_get_residual(vcpg_handle *h, double *res);
+
+/* One residual evaluation of the current state: volume + face terms followed
+ * by the generalised mass-matrix solve (SolverClass::Residual). monitoring
+ * receives the reference's 8 monitoring values when non-NULL. The residual
+ * before the mass-matrix solve is kept when keep_raw is non-zero and can be
+ * read with vcpg_get_raw_residual. */
+int vcpg_residual(vcpg_handle *h, double *monitoring, int32_t keep_raw);
+int vcpg_get_raw_residual(vcpg_handle *h, double *res);
+
+/* Global CFL time step (minimum of ElementClass::ComputeTimeStep, non-dimensional). */
+int vcpg_time_step(vcpg_handle *h, double *dt);
+
+/* n_steps full time steps with the given scheme (SSP-RK3 as in
+ * ExecuteTimeSynchronizationStep, or five-stage low-storage RK4). If
+ * fixed_dt > 0 it is used as the non-dimensional step, otherwise the CFL step
+ * is recomputed on the device at the start of every step. The residual of the
+ * current state must be valid (vcpg_residual) before the first step, as in the
+ * reference main program (src/VCP3D_CurviLinear.cpp:94). dt_history, when
+ * non-NULL, receives the n_steps time steps. The step sequence is captured in
+ * a CUDA graph on first use. */
+int vcpg_step(vcpg_handle *h, int32_t scheme, int32_t n_steps, double fixed_dt,
+              double *dt_history);
+
+/* Synchronises the handle's stream and reports the first device-side error
+ * (CG cap, negative a^2) recorded since the last call. */
+int vcpg_sync(vcpg_handle *h);
+
+/* The handle's CUDA stream (cudaStream_t) for callers that time or order work. */
+void *vcpg_stream(vcpg_handle *h);
+
+/* Number of this library's kernel launches issued since creation. */
+int64_t vcpg_launch_count(const vcpg_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VCP3D_B200_H */

@@ -1,0 +1,100 @@
+"""ctypes binding of the C ABI declared in include/vcp3d_b200.h.
+
+The shared library is built in-tree (vcp3d_open_b200/libvcp3d_b200.so, see
+build.py). Loading fails loudly when it is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libvcp3d_b200.so")
+
+VCPG_OK = 0
+ERRORS = {1: "VCPG_E_CUDA", 2: "VCPG_E_CG_NOCONV", 3: "VCPG_E_NEG_A2", 4: "VCPG_E_NONFINITE",
+          5: "VCPG_E_OOM", 6: "VCPG_E_UNSUPPORTED_KM", 7: "VCPG_E_ADMISSION", 8: "VCPG_E_INVALID"}
+ROE, ISMAIL_ROE = 0, 1
+FP64, MIXED = 0, 1
+SSPRK3, LSRK4 = 0, 1
+
+# Every symbol include/vcp3d_b200.h declares.
+EXPORTED = [
+    "vcpg_create", "vcpg_destroy", "vcpg_last_error", "vcpg_setup_geometry",
+    "vcpg_nodal_conservative_to_modal", "vcpg_set_state", "vcpg_get_state",
+    "vcpg_get_residual", "vcpg_residual", "vcpg_get_raw_residual", "vcpg_time_step",
+    "vcpg_step", "vcpg_sync", "vcpg_stream", "vcpg_launch_count",
+]
+
+
+class Params(C.Structure):
+    _fields_ = [("n_elem", C.c_int32 * 3), ("n_poly", C.c_int32), ("n_int_1d", C.c_int32),
+                ("riemann", C.c_int32), ("metric_index_compat", C.c_int32),
+                ("precision", C.c_int32), ("theta_sym", C.c_double),
+                ("rel_penalty", C.c_double), ("cfl", C.c_double), ("mu", C.c_double),
+                ("p_ref", C.c_double), ("u_ref", C.c_double), ("rho_ref", C.c_double)]
+
+
+class Operators(C.Structure):
+    _fields_ = [(n, C.POINTER(C.c_double)) for n in
+                ("leg_int", "dleg_int", "leg_face", "dleg_face", "w_int", "leg_dofs",
+                 "basis_center")]
+
+
+class Geometry(C.Structure):
+    _fields_ = [("vol_metric", C.POINTER(C.c_double)), ("face_metric", C.POINTER(C.c_double)),
+                ("elem_scalars", C.POINTER(C.c_double)), ("neighbors", C.POINTER(C.c_int32))]
+
+
+class VcpgError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Loads the library once; raises if it was not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with python -m vcp3d_open_b200.build")
+    lib = C.CDLL(LIB_PATH)
+    dp, ip = C.POINTER(C.c_double), C.POINTER(C.c_int32)
+    hp = C.c_void_p
+    lib.vcpg_create.argtypes = [C.POINTER(Params), C.POINTER(Operators), C.POINTER(Geometry),
+                                C.POINTER(C.c_void_p)]
+    lib.vcpg_destroy.argtypes = [hp]
+    lib.vcpg_last_error.argtypes = [hp]
+    lib.vcpg_last_error.restype = C.c_char_p
+    lib.vcpg_setup_geometry.argtypes = [C.POINTER(Params), C.c_int32, C.c_int32, ip, dp, dp, dp,
+                                        dp, dp, dp, dp, dp, dp, dp, dp, ip]
+    lib.vcpg_nodal_conservative_to_modal.argtypes = [C.POINTER(Params), dp, dp, dp, C.c_int64]
+    for name in ("vcpg_set_state", "vcpg_get_state", "vcpg_get_residual", "vcpg_get_raw_residual"):
+        getattr(lib, name).argtypes = [hp, dp]
+    lib.vcpg_residual.argtypes = [hp, dp, C.c_int32]
+    lib.vcpg_time_step.argtypes = [hp, dp]
+    lib.vcpg_step.argtypes = [hp, C.c_int32, C.c_int32, C.c_double, dp]
+    lib.vcpg_sync.argtypes = [hp]
+    lib.vcpg_stream.argtypes = [hp]
+    lib.vcpg_stream.restype = C.c_void_p
+    lib.vcpg_launch_count.argtypes = [hp]
+    lib.vcpg_launch_count.restype = C.c_int64
+    _lib = lib
+    return lib
+
+
+def ptr(a: np.ndarray):
+    """Pointer to a C-contiguous float64 or int32 array."""
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"], "array must be C-contiguous"
+    if a.dtype == np.float64:
+        return a.ctypes.data_as(C.POINTER(C.c_double))
+    if a.dtype == np.int32:
+        return a.ctypes.data_as(C.POINTER(C.c_int32))
+    raise TypeError(f"unsupported dtype {a.dtype}")

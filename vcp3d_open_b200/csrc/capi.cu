@@ -1,0 +1,370 @@
+// C ABI of the library (include/vcp3d_b200.h): handle management, uploads,
+// one residual, the CFL time step and CUDA-graph-captured time steps.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/vcp3d_b200.h"
+#include "dg_residual.cuh"
+#include "host_setup.h"
+#include "kernels.h"
+
+
+using namespace vcpg;
+
+struct vcpg_handle {
+  vcpg_params prm{};
+  int K = 0, M = 0, KD = 0, MD = 0, M2 = 0;
+  int64_t nE = 0;
+  cudaStream_t stream = nullptr;
+  double *d_sol = nullptr, *d_solOld = nullptr, *d_res = nullptr, *d_resRaw = nullptr;
+  double *d_vol = nullptr, *d_face = nullptr, *d_sc = nullptr;
+  int *d_nbr = nullptr;
+  unsigned long long *d_dtbits = nullptr, *d_mach2 = nullptr;
+  double *d_dt = nullptr, *d_fixed = nullptr, *d_hist = nullptr;
+  int *d_status = nullptr, *d_counter = nullptr;
+  int hist_cap = 0;
+  cudaGraph_t graph[2] = {nullptr, nullptr};
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  int graph_launches[2] = {0, 0};
+  int64_t launches = 0;
+  std::string err;
+};
+
+namespace {
+
+const double kLsA[5] = {0.0, -567301805773.0 / 1357537059087.0, -2404267990393.0 / 2016746695238.0,
+                        -3550918686646.0 / 2091501179385.0, -1275806237668.0 / 842570457699.0};
+const double kLsB[5] = {1432997174477.0 / 9575080441755.0, 5161836677717.0 / 13612068292357.0,
+                        1720146321549.0 / 2090206949498.0, 3134564353537.0 / 4481467310338.0,
+                        2277821191437.0 / 14882151754819.0};
+
+int Fail(vcpg_handle *h, int code, const std::string &msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+int CudaFail(vcpg_handle *h, cudaError_t e, const char *what) {
+  return Fail(h, VCPG_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define VCPG_CUDA(h, call)                                   \
+  do {                                                       \
+    cudaError_t e_ = (call);                                 \
+    if (e_ != cudaSuccess) return CudaFail((h), e_, #call); \
+  } while (0)
+
+ResidualArgs MakeResidualArgs(vcpg_handle *h, double *rawOut, unsigned long long *mach) {
+  ResidualArgs a{};
+  a.sol = h->d_sol;
+  a.res = h->d_res;
+  a.res_raw = rawOut;
+  a.vol_metric = h->d_vol;
+  a.face_metric = h->d_face;
+  a.elem_scalars = h->d_sc;
+  a.nbr = h->d_nbr;
+  a.n_elem = (int)h->nE;
+  a.mu = h->prm.mu;
+  a.tau_num = (double)((h->prm.n_poly + 1) * (h->prm.n_poly + 1)) * h->prm.rel_penalty;
+  a.theta_sym = h->prm.theta_sym;
+  a.riemann = h->prm.riemann;
+  a.metric_compat = h->prm.metric_index_compat;
+  a.mach2max = mach;
+  a.status = h->d_status;
+  return a;
+}
+
+TimeStepArgs MakeTimeStepArgs(vcpg_handle *h) {
+  TimeStepArgs t{};
+  t.sol = h->d_sol;
+  t.elem_scalars = h->d_sc;
+  t.n_elem = (int)h->nE;
+  t.n_poly = h->prm.n_poly;
+  t.cfl = h->prm.cfl;
+  t.mu = h->prm.mu;
+  t.p_ref = h->prm.p_ref;
+  t.u_ref = h->prm.u_ref;
+  t.rho_ref = h->prm.rho_ref;
+  t.dt_bits = h->d_dtbits;
+  t.status = h->d_status;
+  return t;
+}
+
+// Reads and clears the device status words; maps them to an error code.
+int CheckStatus(vcpg_handle *h) {
+  int st[4] = {0, 0, 0, 0};
+  VCPG_CUDA(h, cudaMemcpyAsync(st, h->d_status, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
+  VCPG_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (st[0] || st[1] || st[2] || st[3])
+    VCPG_CUDA(h, cudaMemsetAsync(h->d_status, 0, sizeof(st), h->stream));
+  if (st[0]) return Fail(h, VCPG_E_CG_NOCONV, "mass-matrix CG reached 100 iterations in " +
+                                                  std::to_string(st[0]) + " element solve(s)");
+  if (st[2]) return Fail(h, VCPG_E_NEG_A2, "negative square speed of sound in the time step");
+  if (st[1]) return Fail(h, VCPG_E_INVALID, "physical boundary face without a boundary condition");
+  return VCPG_OK;
+}
+
+int EnqueueStep(vcpg_handle *h, int scheme) {
+  const size_t n = (size_t)h->nE * 5 * h->KD;
+  TimeStepArgs t = MakeTimeStepArgs(h);
+  VCPG_CUDA(h, LaunchTimeStep(h->K, h->M, t, h->stream));
+  // The fixed step lives in device memory (d_fixed); a non-positive value selects the CFL step.
+  VCPG_CUDA(h, LaunchFinalizeDt(h->d_dtbits, h->d_fixed, h->d_dt, h->d_hist, h->hist_cap, h->d_counter,
+                                h->stream));
+  ResidualArgs a = MakeResidualArgs(h, nullptr, nullptr);
+  if (scheme == VCPG_SSPRK3) {
+    const double alphaRK[] = {1.0, 3.0 / 4.0, 1.0 / 3.0};
+    const double betaRK[] = {1.0, 1.0 / 4.0, 2.0 / 3.0};
+    for (int s = 0; s < 3; ++s) {
+      VCPG_CUDA(h, LaunchSspStage(h->d_sol, h->d_solOld, h->d_res, h->d_dt, alphaRK[s], betaRK[s],
+                                  s == 0, n, h->stream));
+      VCPG_CUDA(h, LaunchResidual(h->K, h->M, a, h->stream));
+    }
+  } else {
+    for (int s = 0; s < 5; ++s) {
+      VCPG_CUDA(h, LaunchLsrkStage(h->d_sol, h->d_solOld, h->d_res, h->d_dt, kLsA[s], kLsB[s], n,
+                                   h->stream));
+      VCPG_CUDA(h, LaunchResidual(h->K, h->M, a, h->stream));
+    }
+  }
+  return VCPG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *vcpg_last_error(const vcpg_handle *h) { return h ? h->err.c_str() : "null handle"; }
+
+int vcpg_destroy(vcpg_handle *h) {
+  if (!h) return VCPG_OK;
+  for (int s = 0; s < 2; ++s) {
+    if (h->exec[s]) cudaGraphExecDestroy(h->exec[s]);
+    if (h->graph[s]) cudaGraphDestroy(h->graph[s]);
+  }
+  void *bufs[] = {h->d_sol, h->d_solOld, h->d_res, h->d_resRaw, h->d_vol, h->d_face, h->d_sc,
+                  h->d_nbr, h->d_dtbits, h->d_mach2, h->d_dt, h->d_fixed, h->d_hist,
+                  h->d_status, h->d_counter};
+  for (void *p : bufs)
+    if (p) cudaFree(p);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return VCPG_OK;
+}
+
+int vcpg_create(const vcpg_params *params, const vcpg_operators *ops, const vcpg_geometry *geom,
+                vcpg_handle **out) {
+  if (!params || !ops || !geom || !out) return VCPG_E_INVALID;
+  *out = nullptr;
+  vcpg_handle *h = new vcpg_handle();
+  h->prm = *params;
+  h->K = params->n_poly + 1;
+  h->M = params->n_int_1d;
+  h->KD = h->K * h->K * h->K;
+  h->MD = h->M * h->M * h->M;
+  h->M2 = h->M * h->M;
+  h->nE = (int64_t)params->n_elem[0] * params->n_elem[1] * params->n_elem[2];
+  if (h->nE <= 0 || h->nE > (int64_t)2147483647) {
+    int rc = Fail(h, VCPG_E_INVALID, "invalid element count");
+    *out = h;
+    return rc;
+  }
+  if (!Supported(h->K, h->M) || h->K > kKMax || h->M > kMMax) {
+    int rc = Fail(h, VCPG_E_UNSUPPORTED_KM, "no kernel for K=" + std::to_string(h->K) +
+                                                " M=" + std::to_string(h->M));
+    *out = h;
+    return rc;
+  }
+  if (params->precision != VCPG_FP64) {
+    int rc = Fail(h, VCPG_E_INVALID, "mixed precision is selected per handle at build time only");
+    *out = h;
+    return rc;
+  }
+  *out = h;
+  const int K = h->K, M = h->M;
+  // Operator table into the (K, M) constant slot.
+  OpTable t;
+  std::memset(&t, 0, sizeof(t));
+  for (int k = 0; k < K; ++k)
+    for (int m = 0; m < M; ++m) {
+      t.leg[k * M + m] = ops->leg_int[k * M + m];
+      t.dleg[k * M + m] = ops->dleg_int[k * M + m];
+    }
+  for (int i = 0; i < 2 * K; ++i) {
+    t.face[i] = ops->leg_face[i];
+    t.dface[i] = ops->dleg_face[i];
+  }
+  for (int m = 0; m < M; ++m) t.w[m] = ops->w_int[m];
+  for (int i = 0; i < K * K; ++i) t.legdof[i] = ops->leg_dofs[i];
+  for (int i = 0; i < h->KD; ++i) t.center[i] = ops->basis_center[i];
+  VCPG_CUDA(h, UploadOpTable(SlotOf(K, M), t));
+
+  VCPG_CUDA(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  const size_t nState = (size_t)h->nE * 5 * h->KD;
+  auto alloc = [&](void **p, size_t bytes) -> int {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) return Fail(h, VCPG_E_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    return VCPG_OK;
+  };
+  int rc;
+  if ((rc = alloc((void **)&h->d_sol, nState * 8))) return rc;
+  if ((rc = alloc((void **)&h->d_solOld, nState * 8))) return rc;
+  if ((rc = alloc((void **)&h->d_res, nState * 8))) return rc;
+  if ((rc = alloc((void **)&h->d_vol, (size_t)h->nE * 10 * h->MD * 8))) return rc;
+  if ((rc = alloc((void **)&h->d_face, (size_t)h->nE * 6 * 13 * h->M2 * 8))) return rc;
+  if ((rc = alloc((void **)&h->d_sc, (size_t)h->nE * 15 * 8))) return rc;
+  if ((rc = alloc((void **)&h->d_nbr, (size_t)h->nE * 6 * sizeof(int)))) return rc;
+  if ((rc = alloc((void **)&h->d_dtbits, sizeof(unsigned long long)))) return rc;
+  if ((rc = alloc((void **)&h->d_mach2, sizeof(unsigned long long)))) return rc;
+  if ((rc = alloc((void **)&h->d_dt, sizeof(double)))) return rc;
+  if ((rc = alloc((void **)&h->d_fixed, sizeof(double)))) return rc;
+  if ((rc = alloc((void **)&h->d_status, 4 * sizeof(int)))) return rc;
+  if ((rc = alloc((void **)&h->d_counter, sizeof(int)))) return rc;
+  h->hist_cap = 1024;
+  if ((rc = alloc((void **)&h->d_hist, (size_t)h->hist_cap * 8))) return rc;
+  VCPG_CUDA(h, cudaMemcpyAsync(h->d_vol, geom->vol_metric, (size_t)h->nE * 10 * h->MD * 8,
+                               cudaMemcpyHostToDevice, h->stream));
+  VCPG_CUDA(h, cudaMemcpyAsync(h->d_face, geom->face_metric, (size_t)h->nE * 6 * 13 * h->M2 * 8,
+                               cudaMemcpyHostToDevice, h->stream));
+  VCPG_CUDA(h, cudaMemcpyAsync(h->d_sc, geom->elem_scalars, (size_t)h->nE * 15 * 8,
+                               cudaMemcpyHostToDevice, h->stream));
+  VCPG_CUDA(h, cudaMemcpyAsync(h->d_nbr, geom->neighbors, (size_t)h->nE * 6 * sizeof(int),
+                               cudaMemcpyHostToDevice, h->stream));
+  VCPG_CUDA(h, cudaMemsetAsync(h->d_sol, 0, nState * 8, h->stream));
+  VCPG_CUDA(h, cudaMemsetAsync(h->d_solOld, 0, nState * 8, h->stream));
+  VCPG_CUDA(h, cudaMemsetAsync(h->d_res, 0, nState * 8, h->stream));
+  VCPG_CUDA(h, cudaMemsetAsync(h->d_status, 0, 4 * sizeof(int), h->stream));
+  const double big = 1.e+10;
+  unsigned long long bits;
+  std::memcpy(&bits, &big, 8);
+  VCPG_CUDA(h, cudaMemcpyAsync(h->d_dtbits, &bits, 8, cudaMemcpyHostToDevice, h->stream));
+  VCPG_CUDA(h, cudaStreamSynchronize(h->stream));
+  return VCPG_OK;
+}
+
+int vcpg_set_state(vcpg_handle *h, const double *modal) {
+  if (!h || !modal) return VCPG_E_INVALID;
+  VCPG_CUDA(h, cudaMemcpyAsync(h->d_sol, modal, (size_t)h->nE * 5 * h->KD * 8,
+                               cudaMemcpyHostToDevice, h->stream));
+  VCPG_CUDA(h, cudaStreamSynchronize(h->stream));
+  return VCPG_OK;
+}
+
+int vcpg_get_state(vcpg_handle *h, double *modal) {
+  if (!h || !modal) return VCPG_E_INVALID;
+  VCPG_CUDA(h, cudaMemcpyAsync(modal, h->d_sol, (size_t)h->nE * 5 * h->KD * 8,
+                               cudaMemcpyDeviceToHost, h->stream));
+  VCPG_CUDA(h, cudaStreamSynchronize(h->stream));
+  return VCPG_OK;
+}
+
+int vcpg_get_residual(vcpg_handle *h, double *res) {
+  if (!h || !res) return VCPG_E_INVALID;
+  VCPG_CUDA(h, cudaMemcpyAsync(res, h->d_res, (size_t)h->nE * 5 * h->KD * 8,
+                               cudaMemcpyDeviceToHost, h->stream));
+  VCPG_CUDA(h, cudaStreamSynchronize(h->stream));
+  return VCPG_OK;
+}
+
+int vcpg_get_raw_residual(vcpg_handle *h, double *res) {
+  if (!h || !res) return VCPG_E_INVALID;
+  if (!h->d_resRaw) return Fail(h, VCPG_E_INVALID, "no raw residual kept");
+  VCPG_CUDA(h, cudaMemcpyAsync(res, h->d_resRaw, (size_t)h->nE * 5 * h->KD * 8,
+                               cudaMemcpyDeviceToHost, h->stream));
+  VCPG_CUDA(h, cudaStreamSynchronize(h->stream));
+  return VCPG_OK;
+}
+
+int vcpg_residual(vcpg_handle *h, double *monitoring, int32_t keep_raw) {
+  if (!h) return VCPG_E_INVALID;
+  if (keep_raw && !h->d_resRaw) {
+    cudaError_t e = cudaMalloc((void **)&h->d_resRaw, (size_t)h->nE * 5 * h->KD * 8);
+    if (e != cudaSuccess) return Fail(h, VCPG_E_OOM, "cudaMalloc raw residual");
+  }
+  if (monitoring) VCPG_CUDA(h, cudaMemsetAsync(h->d_mach2, 0, 8, h->stream));
+  ResidualArgs a = MakeResidualArgs(h, keep_raw ? h->d_resRaw : nullptr,
+                                    monitoring ? h->d_mach2 : nullptr);
+  VCPG_CUDA(h, LaunchResidual(h->K, h->M, a, h->stream));
+  h->launches += 1;
+  int rc = CheckStatus(h);
+  if (monitoring) {
+    unsigned long long bits = 0;
+    VCPG_CUDA(h, cudaMemcpy(&bits, h->d_mach2, 8, cudaMemcpyDeviceToHost));
+    double m2;
+    std::memcpy(&m2, &bits, 8);
+    // Periodic blocks carry no walls: force coefficients are zero and no SGS model is used.
+    for (int i = 0; i < 6; ++i) monitoring[i] = 0.0;
+    monitoring[6] = m2;
+    monitoring[7] = 0.0;
+  }
+  return rc;
+}
+
+int vcpg_time_step(vcpg_handle *h, double *dt) {
+  if (!h || !dt) return VCPG_E_INVALID;
+  TimeStepArgs t = MakeTimeStepArgs(h);
+  VCPG_CUDA(h, LaunchTimeStep(h->K, h->M, t, h->stream));
+  h->launches += 1;
+  unsigned long long bits = 0;
+  VCPG_CUDA(h, cudaMemcpyAsync(&bits, h->d_dtbits, 8, cudaMemcpyDeviceToHost, h->stream));
+  VCPG_CUDA(h, cudaStreamSynchronize(h->stream));
+  std::memcpy(dt, &bits, 8);
+  const double big = 1.e+10;
+  std::memcpy(&bits, &big, 8);
+  VCPG_CUDA(h, cudaMemcpyAsync(h->d_dtbits, &bits, 8, cudaMemcpyHostToDevice, h->stream));
+  return CheckStatus(h);
+}
+
+int vcpg_step(vcpg_handle *h, int32_t scheme, int32_t n_steps, double fixed_dt,
+              double *dt_history) {
+  if (!h || n_steps < 0 || (scheme != VCPG_SSPRK3 && scheme != VCPG_LSRK4)) return VCPG_E_INVALID;
+  if (n_steps == 0) return VCPG_OK;
+  if (n_steps > h->hist_cap) {
+    // Grow the history buffer; graphs hold the old pointer and are rebuilt.
+    for (int s = 0; s < 2; ++s) {
+      if (h->exec[s]) { cudaGraphExecDestroy(h->exec[s]); h->exec[s] = nullptr; }
+      if (h->graph[s]) { cudaGraphDestroy(h->graph[s]); h->graph[s] = nullptr; }
+    }
+    cudaFree(h->d_hist);
+    h->d_hist = nullptr;
+    h->hist_cap = n_steps;
+    cudaError_t e = cudaMalloc((void **)&h->d_hist, (size_t)h->hist_cap * 8);
+    if (e != cudaSuccess) return Fail(h, VCPG_E_OOM, "cudaMalloc dt history");
+  }
+  const double fx = fixed_dt > 0.0 ? fixed_dt : -1.0;
+  VCPG_CUDA(h, cudaMemcpyAsync(h->d_fixed, &fx, 8, cudaMemcpyHostToDevice, h->stream));
+  VCPG_CUDA(h, cudaMemsetAsync(h->d_counter, 0, sizeof(int), h->stream));
+  if (!h->exec[scheme]) {
+    VCPG_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = EnqueueStep(h, scheme);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) return CudaFail(h, e, "cudaStreamEndCapture");
+    h->graph[scheme] = g;
+    VCPG_CUDA(h, cudaGraphInstantiate(&h->exec[scheme], g, 0));
+    h->graph_launches[scheme] = 2 + (scheme == VCPG_SSPRK3 ? 3 : 5) * 2;
+  }
+  for (int s = 0; s < n_steps; ++s) VCPG_CUDA(h, cudaGraphLaunch(h->exec[scheme], h->stream));
+  h->launches += (int64_t)n_steps * h->graph_launches[scheme];
+  if (dt_history)
+    VCPG_CUDA(h, cudaMemcpyAsync(dt_history, h->d_hist, (size_t)n_steps * 8,
+                                 cudaMemcpyDeviceToHost, h->stream));
+  return CheckStatus(h);
+}
+
+int vcpg_sync(vcpg_handle *h) {
+  if (!h) return VCPG_E_INVALID;
+  return CheckStatus(h);
+}
+
+void *vcpg_stream(vcpg_handle *h) { return h ? (void *)h->stream : nullptr; }
+
+int64_t vcpg_launch_count(const vcpg_handle *h) { return h ? h->launches : 0; }
+
+}  // extern "C"

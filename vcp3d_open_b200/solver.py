@@ -1,0 +1,198 @@
+"""Host-side mirror of the reference solver's residual / time-step interface.
+
+The reference drives its hot path through SolverClass
+(include/SolverClass.hpp:40-124):
+
+    solver.Residual(monitoringData, computeMonitoring)      -> Solver.residual
+    solver.ExecuteTimeSynchronizationStep(monitoringData)   -> Solver.step
+    ElementClass::ComputeTimeStep (min over elements)       -> Solver.time_step
+
+Solver wraps one C-ABI handle (include/vcp3d_b200.h); every call goes through
+the CUDA library. Discretization holds the host-side inputs (operators and
+geometry) produced by vcpg_setup_geometry.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+from typing import Optional
+
+import numpy as np
+
+from . import capi
+from .cases import CaseData
+
+
+@dataclasses.dataclass
+class Discretization:
+    n_elem: tuple
+    n_poly: int
+    n_int_1d: int
+    leg_int: np.ndarray
+    dleg_int: np.ndarray
+    leg_face: np.ndarray
+    dleg_face: np.ndarray
+    w_int: np.ndarray
+    leg_dofs: np.ndarray
+    basis_center: np.ndarray
+    vol_metric: np.ndarray      # [nE][10][M^3]
+    face_metric: np.ndarray     # [nE][6][13][M^2]
+    elem_scalars: np.ndarray    # [nE][15]
+    neighbors: np.ndarray       # [nE][6] int32
+
+    @property
+    def n_elements(self) -> int:
+        return int(np.prod(self.n_elem))
+
+
+def make_params(case: CaseData, metric_compat: bool = True,
+                precision: int = capi.FP64) -> capi.Params:
+    s, r = case.spec, case.ref
+    p = capi.Params()
+    p.n_elem[:] = list(s.n_elem)
+    p.n_poly = s.p
+    p.n_int_1d = s.n_poly_int // 2 + 1
+    p.riemann = capi.ISMAIL_ROE if s.riemann.lower() == "ismailroe" else capi.ROE
+    p.metric_index_compat = 1 if metric_compat else 0
+    p.precision = precision
+    p.theta_sym = s.theta_sym
+    p.rel_penalty = s.penalty
+    p.cfl = s.cfl
+    p.mu = r.mu_nondim
+    p.p_ref, p.u_ref, p.rho_ref = r.p_ref, r.u_ref, r.rho_ref
+    return p
+
+
+def setup_discretization(case: CaseData, params: capi.Params,
+                         periodic=(1, 1, 1)) -> Discretization:
+    """Operators and metric terms from the case grid (host C++ in the library)."""
+    lib = capi.load()
+    s = case.spec
+    K, M, nE = s.p + 1, params.n_int_1d, s.n_elements
+    d = Discretization(
+        n_elem=tuple(s.n_elem), n_poly=s.p, n_int_1d=M,
+        leg_int=np.zeros((K, M)), dleg_int=np.zeros((K, M)), leg_face=np.zeros((2, K)),
+        dleg_face=np.zeros((2, K)), w_int=np.zeros(M), leg_dofs=np.zeros((K, K)),
+        basis_center=np.zeros(K ** 3), vol_metric=np.zeros((nE, 10, M ** 3)),
+        face_metric=np.zeros((nE, 6, 13, M * M)), elem_scalars=np.zeros((nE, 15)),
+        neighbors=np.zeros((nE, 6), dtype=np.int32))
+    per = np.asarray(periodic, dtype=np.int32)
+    nodes = np.ascontiguousarray(case.elem_nodes, dtype=np.float64)
+    rc = lib.vcpg_setup_geometry(
+        C.byref(params), s.p_grid, 1, capi.ptr(per), capi.ptr(nodes), capi.ptr(d.leg_int),
+        capi.ptr(d.dleg_int), capi.ptr(d.leg_face), capi.ptr(d.dleg_face), capi.ptr(d.w_int),
+        capi.ptr(d.leg_dofs), capi.ptr(d.basis_center), capi.ptr(d.vol_metric),
+        capi.ptr(d.face_metric), capi.ptr(d.elem_scalars), capi.ptr(d.neighbors))
+    if rc != capi.VCPG_OK:
+        raise capi.VcpgError(rc, "vcpg_setup_geometry failed")
+    return d
+
+
+def nodal_to_modal(case: CaseData, params: capi.Params) -> np.ndarray:
+    """Initial modal entropy-variable state from the case's nodal conservative state."""
+    lib = capi.load()
+    cons = np.ascontiguousarray(case.cons, dtype=np.float64)
+    out = np.zeros_like(cons)
+    rc = lib.vcpg_nodal_conservative_to_modal(C.byref(params), None, capi.ptr(cons),
+                                              capi.ptr(out), cons.shape[0])
+    if rc != capi.VCPG_OK:
+        raise capi.VcpgError(rc, "vcpg_nodal_conservative_to_modal failed")
+    return out
+
+
+class Solver:
+    """One GPU-resident case. All work runs in the CUDA library."""
+
+    def __init__(self, params: capi.Params, disc: Discretization):
+        self.lib = capi.load()
+        self.params = params
+        self.disc = disc
+        self._keep = [np.ascontiguousarray(a) for a in (
+            disc.leg_int, disc.dleg_int, disc.leg_face, disc.dleg_face, disc.w_int,
+            disc.leg_dofs, disc.basis_center, disc.vol_metric, disc.face_metric,
+            disc.elem_scalars)]
+        ops = capi.Operators(*[capi.ptr(a) for a in self._keep[:7]])
+        nbr = np.ascontiguousarray(disc.neighbors, dtype=np.int32)
+        self._keep.append(nbr)
+        geom = capi.Geometry(capi.ptr(self._keep[7]), capi.ptr(self._keep[8]),
+                             capi.ptr(self._keep[9]), capi.ptr(nbr))
+        h = C.c_void_p()
+        rc = self.lib.vcpg_create(C.byref(params), C.byref(ops), C.byref(geom), C.byref(h))
+        self.h = h
+        if rc != capi.VCPG_OK:
+            msg = self.lib.vcpg_last_error(h).decode() if h.value else "create failed"
+            self.close()
+            raise capi.VcpgError(rc, msg)
+        K = params.n_poly + 1
+        self.shape = (disc.n_elements, 5, K ** 3)
+
+    def _check(self, rc: int, what: str):
+        if rc != capi.VCPG_OK:
+            raise capi.VcpgError(rc, f"{what}: {self.lib.vcpg_last_error(self.h).decode()}")
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.lib.vcpg_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_state(self, modal: np.ndarray):
+        a = np.ascontiguousarray(modal, dtype=np.float64).reshape(self.shape)
+        self._check(self.lib.vcpg_set_state(self.h, capi.ptr(a)), "set_state")
+
+    def get_state(self) -> np.ndarray:
+        out = np.empty(self.shape)
+        self._check(self.lib.vcpg_get_state(self.h, capi.ptr(out)), "get_state")
+        return out
+
+    def residual(self, monitoring: bool = False, keep_raw: bool = False):
+        mon = np.zeros(8) if monitoring else None
+        self._check(self.lib.vcpg_residual(self.h, capi.ptr(mon), 1 if keep_raw else 0),
+                    "residual")
+        return mon
+
+    def get_residual(self) -> np.ndarray:
+        out = np.empty(self.shape)
+        self._check(self.lib.vcpg_get_residual(self.h, capi.ptr(out)), "get_residual")
+        return out
+
+    def get_raw_residual(self) -> np.ndarray:
+        out = np.empty(self.shape)
+        self._check(self.lib.vcpg_get_raw_residual(self.h, capi.ptr(out)), "get_raw_residual")
+        return out
+
+    def time_step(self) -> float:
+        dt = C.c_double()
+        self._check(self.lib.vcpg_time_step(self.h, C.byref(dt)), "time_step")
+        return dt.value
+
+    def step(self, n_steps: int, scheme: int = capi.SSPRK3,
+             fixed_dt: float = -1.0) -> np.ndarray:
+        hist = np.zeros(max(n_steps, 1))
+        self._check(self.lib.vcpg_step(self.h, scheme, n_steps, fixed_dt, capi.ptr(hist)), "step")
+        return hist[:n_steps]
+
+    def sync(self):
+        self._check(self.lib.vcpg_sync(self.h), "sync")
+
+    @property
+    def stream(self) -> int:
+        return self.lib.vcpg_stream(self.h)
+
+    @property
+    def launch_count(self) -> int:
+        return int(self.lib.vcpg_launch_count(self.h))
+
+
+def create(case: CaseData, metric_compat: bool = True) -> Solver:
+    """Set-up + handle + initial state for a generated case."""
+    params = make_params(case, metric_compat=metric_compat)
+    disc = setup_discretization(case, params)
+    s = Solver(params, disc)
+    s.set_state(nodal_to_modal(case, params))
+    return s
