@@ -157,6 +157,10 @@ void *vcpg_stream(vcpg_handle *h);
 /* Number of this library's kernel launches issued since creation. */
 int64_t vcpg_launch_count(const vcpg_handle *h);
 
+/* Cumulative mass-matrix CG statistics since creation: total iterations and
+ * element solves (the reference's per-element CG, src/CG_MassMatrix.cpp:395-492). */
+int vcpg_stats(vcpg_handle *h, int64_t *cg_iterations, int64_t *element_solves);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,43 @@
+"""Shared test set-up: the gpu marker and helpers for the golden fixtures."""
+from __future__ import annotations
+
+import glob
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+sys.path.insert(0, ROOT)
+sys.path.insert(0, GOLDEN)
+
+from make_golden import spec_from_json  # noqa: E402
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200); runs the CUDA library")
+
+
+def golden_files():
+    return sorted(glob.glob(os.path.join(GOLDEN, "case_*.npz")))
+
+
+def load_golden(path):
+    g = dict(np.load(path))
+    g["spec"] = spec_from_json(str(g["spec_json"]))
+    return g
+
+
+def rel_l2(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+
+@pytest.fixture(scope="session")
+def gpu_available():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return True

@@ -1,0 +1,109 @@
+"""Generates the golden fixtures under tests/golden/ by running the reference
+solver itself (oracle/_ref/vcp3d_ref, built from the reference sources by
+oracle/Makefile) on small generated cases.
+
+    make -C oracle && python tests/golden/make_golden.py
+
+Each fixture case_<name>.npz holds, for one case:
+  spec_json       the CaseSpec (JSON) that regenerates grid and initial state
+  sol0            initial modal entropy-variable state [nE][5][K^3] (reference's
+                  own restart-file conversion)
+  res_raw, res    residual before / after the mass-matrix solve of sol0
+  monitor         the 8 monitoring values of that residual
+  dt0             CFL time step of sol0
+  ssp_sol, ssp_dt state and time steps after N_STEPS SSP-RK3 steps
+  ls_sol, ls_dt   state and time steps after N_STEPS low-storage RK4 steps
+  metric_sums     per-array checksums of the reference's metric terms
+  vol_metric_e0, face_metric_e0  metric terms of element 0 (unpadded)
+"""
+from __future__ import annotations
+
+import dataclasses
+import json
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import records  # noqa: E402
+from vcp3d_open_b200 import cases  # noqa: E402
+
+N_STEPS = 3
+TWO_PI = 6.283185307179586
+
+GOLDEN_SPECS = {
+    # Isentropic vortex on the curvilinear periodic cube (config 1 family), reduced.
+    "vortex_p3_4x4x4": cases.CaseSpec(name="vortex_p3_4x4x4", kind="vortex", n_elem=(4, 4, 4),
+                                      p=3),
+    # Taylor-Green vortex, perturbed grid, degree 4 (config 3/4 family), reduced.
+    "tgv_p4_3x3x3": cases.CaseSpec(name="tgv_p4_3x3x3", kind="tgv", n_elem=(3, 3, 3), p=4,
+                                   hi=(TWO_PI,) * 3, mach=0.1, reynolds=1600.0,
+                                   grid_map="random", grid_amp=0.01, seed=1),
+    # Degree 2 with the Roe flux, anisotropic block.
+    "vortex_p2_roe_4x3x2": cases.CaseSpec(name="vortex_p2_roe_4x3x2", kind="vortex",
+                                          n_elem=(4, 3, 2), p=2, riemann="Roe",
+                                          hi=(10.0, 7.5, 5.0), center=(5.0, 3.75, 2.5)),
+    # Degree 5.
+    "tgv_p5_2x2x2": cases.CaseSpec(name="tgv_p5_2x2x2", kind="tgv", n_elem=(2, 2, 2), p=5,
+                                   hi=(TWO_PI,) * 3, mach=0.1, reynolds=1600.0,
+                                   grid_map="random", grid_amp=0.01, seed=3),
+}
+
+
+def spec_to_json(spec: cases.CaseSpec) -> str:
+    return json.dumps(dataclasses.asdict(spec))
+
+
+def spec_from_json(text: str) -> cases.CaseSpec:
+    d = json.loads(text)
+    for k in ("n_elem", "lo", "hi", "vel_dir", "center"):
+        d[k] = tuple(d[k])
+    return cases.CaseSpec(**d)
+
+
+def make(name: str, spec: cases.CaseSpec, out_dir: str) -> str:
+    K = spec.p + 1
+    KD = K ** 3
+    case = cases.build_case(spec)
+    with tempfile.TemporaryDirectory() as tmp:
+        cfg = cases.write_case(case, tmp)
+        f_dump, f_res = os.path.join(tmp, "dump.bin"), os.path.join(tmp, "res.bin")
+        f_ssp, f_ls = os.path.join(tmp, "ssp.bin"), os.path.join(tmp, "ls.bin")
+        records.run_reference(cfg, "dump", f_dump)
+        records.run_reference(cfg, "residual", f_res)
+        records.run_reference(cfg, "run", f_ssp, "--steps", str(N_STEPS), "--scheme", "ssprk3")
+        records.run_reference(cfg, "run", f_ls, "--steps", str(N_STEPS), "--scheme", "lsrk4")
+        d, r = records.read_records(f_dump), records.read_records(f_res)
+        s, l = records.read_records(f_ssp), records.read_records(f_ls)
+    M = int(d["params"][5])
+    MD, M2 = M ** 3, M * M
+    faces = ["surfIMin", "surfIMax", "surfJMin", "surfJMax", "surfKMin", "surfKMax"]
+    sums = [np.abs(d["volMetric"][:, :10, :MD]).sum()] + \
+           [np.abs(d[f][:, :13, :M2]).sum() for f in faces] + \
+           [np.abs(d["elemScalars"]).sum()]
+    path = os.path.join(out_dir, f"case_{name}.npz")
+    np.savez_compressed(
+        path, spec_json=np.array(spec_to_json(spec)), sol0=d["sol"][:, :, :KD],
+        res_raw=r["resRaw"][:, :, :KD], res=r["res"][:, :, :KD], monitor=r["monitor"],
+        dt0=r["dt"], ssp_sol=s["sol"][:, :, :KD], ssp_dt=s["dtHist"],
+        ls_sol=l["sol"][:, :, :KD], ls_dt=l["dtHist"], refcond=d["refcond"],
+        metric_sums=np.array(sums), vol_metric_e0=d["volMetric"][0, :10, :MD],
+        face_metric_e0=np.stack([d[f][0, :13, :M2] for f in faces]),
+        elem_scalars=d["elemScalars"], n_steps=np.array(N_STEPS))
+    return path
+
+
+def main():
+    if not records.have_reference_build():
+        raise SystemExit("build the oracle first: make -C oracle")
+    for name, spec in GOLDEN_SPECS.items():
+        print(make(name, spec, HERE))
+
+
+if __name__ == "__main__":
+    main()

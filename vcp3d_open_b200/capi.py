@@ -24,7 +24,7 @@ EXPORTED = [
     "vcpg_create", "vcpg_destroy", "vcpg_last_error", "vcpg_setup_geometry",
     "vcpg_nodal_conservative_to_modal", "vcpg_set_state", "vcpg_get_state",
     "vcpg_get_residual", "vcpg_residual", "vcpg_get_raw_residual", "vcpg_time_step",
-    "vcpg_step", "vcpg_sync", "vcpg_stream", "vcpg_launch_count",
+    "vcpg_step", "vcpg_sync", "vcpg_stream", "vcpg_launch_count", "vcpg_stats",
 ]
 
 
@@ -84,6 +84,7 @@ def load() -> C.CDLL:
     lib.vcpg_stream.restype = C.c_void_p
     lib.vcpg_launch_count.argtypes = [hp]
     lib.vcpg_launch_count.restype = C.c_int64
+    lib.vcpg_stats.argtypes = [hp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     _lib = lib
     return lib
 

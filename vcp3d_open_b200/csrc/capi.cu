@@ -28,6 +28,7 @@ struct vcpg_handle {
   unsigned long long *d_dtbits = nullptr, *d_mach2 = nullptr;
   double *d_dt = nullptr, *d_fixed = nullptr, *d_hist = nullptr;
   int *d_status = nullptr, *d_counter = nullptr;
+  unsigned long long *d_cgstats = nullptr;
   int hist_cap = 0;
   cudaGraph_t graph[2] = {nullptr, nullptr};
   cudaGraphExec_t exec[2] = {nullptr, nullptr};
@@ -76,6 +77,7 @@ ResidualArgs MakeResidualArgs(vcpg_handle *h, double *rawOut, unsigned long long
   a.metric_compat = h->prm.metric_index_compat;
   a.mach2max = mach;
   a.status = h->d_status;
+  a.cg_stats = h->d_cgstats;
   return a;
 }
 
@@ -149,7 +151,7 @@ int vcpg_destroy(vcpg_handle *h) {
   }
   void *bufs[] = {h->d_sol, h->d_solOld, h->d_res, h->d_resRaw, h->d_vol, h->d_face, h->d_sc,
                   h->d_nbr, h->d_dtbits, h->d_mach2, h->d_dt, h->d_fixed, h->d_hist,
-                  h->d_status, h->d_counter};
+                  h->d_status, h->d_counter, h->d_cgstats};
   for (void *p : bufs)
     if (p) cudaFree(p);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -225,6 +227,8 @@ int vcpg_create(const vcpg_params *params, const vcpg_operators *ops, const vcpg
   if ((rc = alloc((void **)&h->d_fixed, sizeof(double)))) return rc;
   if ((rc = alloc((void **)&h->d_status, 4 * sizeof(int)))) return rc;
   if ((rc = alloc((void **)&h->d_counter, sizeof(int)))) return rc;
+  if ((rc = alloc((void **)&h->d_cgstats, 2 * sizeof(unsigned long long)))) return rc;
+  VCPG_CUDA(h, cudaMemsetAsync(h->d_cgstats, 0, 2 * sizeof(unsigned long long), h->stream));
   h->hist_cap = 1024;
   if ((rc = alloc((void **)&h->d_hist, (size_t)h->hist_cap * 8))) return rc;
   VCPG_CUDA(h, cudaMemcpyAsync(h->d_vol, geom->vol_metric, (size_t)h->nE * 10 * h->MD * 8,
@@ -366,5 +370,15 @@ int vcpg_sync(vcpg_handle *h) {
 void *vcpg_stream(vcpg_handle *h) { return h ? (void *)h->stream : nullptr; }
 
 int64_t vcpg_launch_count(const vcpg_handle *h) { return h ? h->launches : 0; }
+
+int vcpg_stats(vcpg_handle *h, int64_t *cg_iterations, int64_t *element_solves) {
+  if (!h) return VCPG_E_INVALID;
+  unsigned long long st[2] = {0, 0};
+  VCPG_CUDA(h, cudaMemcpyAsync(st, h->d_cgstats, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
+  VCPG_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (cg_iterations) *cg_iterations = (int64_t)st[0];
+  if (element_solves) *element_solves = (int64_t)st[1];
+  return VCPG_OK;
+}
 
 }  // extern "C"

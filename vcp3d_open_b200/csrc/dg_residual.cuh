@@ -36,6 +36,7 @@ struct ResidualArgs {
   int metric_compat;           // 1: metric indexed by the variable index
   unsigned long long *mach2max;  // optional: bits of max Mach^2 (non-negative double)
   int *status;                 // [0] CG iteration cap hits, [1] boundary face without BC
+  unsigned long long *cg_stats;  // [0] CG iterations, [1] element solves (cumulative)
 };
 
 // Arguments of the CFL time-step kernel (kernels.cu).
@@ -537,7 +538,8 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
   for (int i = threadIdx.x; i < 5 * KD; i += NT) p[i] = z[i];
   __syncthreads();
 
-  for (int iter = 0;; ++iter) {
+  int iter = 0;
+  for (;; ++iter) {
     if (iter == 100) {
       if (threadIdx.x == 0) atomicAdd(a.status, 1);
       break;
@@ -595,6 +597,10 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
     const double beta = -alpha * BlockSum<NT>(part, s_red) / dotrz;
     for (int i = threadIdx.x; i < 5 * KD; i += NT) p[i] = beta * p[i] + z[i];
     __syncthreads();
+  }
+  if (threadIdx.x == 0 && a.cg_stats) {
+    atomicAdd(a.cg_stats, (unsigned long long)(iter + 1));
+    atomicAdd(a.cg_stats + 1, 1ull);
   }
 }
 

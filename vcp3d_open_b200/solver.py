@@ -156,6 +156,11 @@ class Solver:
                     "residual")
         return mon
 
+    def get_state_into(self, out: np.ndarray):
+        """Copies the device state into a caller-provided (e.g. pinned) array."""
+        assert out.dtype == np.float64 and out.flags["C_CONTIGUOUS"] and out.size == np.prod(self.shape)
+        self._check(self.lib.vcpg_get_state(self.h, capi.ptr(out)), "get_state")
+
     def get_residual(self) -> np.ndarray:
         out = np.empty(self.shape)
         self._check(self.lib.vcpg_get_residual(self.h, capi.ptr(out)), "get_residual")
@@ -183,6 +188,12 @@ class Solver:
     @property
     def stream(self) -> int:
         return self.lib.vcpg_stream(self.h)
+
+    def cg_stats(self):
+        """(total CG iterations, element solves) since creation."""
+        it, n = C.c_int64(), C.c_int64()
+        self._check(self.lib.vcpg_stats(self.h, C.byref(it), C.byref(n)), "stats")
+        return it.value, n.value
 
     @property
     def launch_count(self) -> int:
