@@ -63,9 +63,14 @@ def test_gpu_matches_restatement_on_identical_inputs(gpu_available, path, compat
         d = dn.from_discretization(disc, prm)
         s.set_state(g["sol0"])
         s.residual(keep_raw=True)
-        raw, res, _ = dn.residual(g["sol0"].reshape(-1, 5, K, K, K), d, compat=compat)
-        assert rel_l2(s.get_raw_residual(), raw.reshape(g["sol0"].shape)) < 1e-12
-        assert rel_l2(s.get_residual(), res.reshape(g["sol0"].shape)) < 1e-11
+        U = g["sol0"].reshape(-1, 5, K, K, K)
+        raw, res, _ = dn.residual(U, d, compat=compat)
+        # The residual is a small difference of large volume and face terms; the
+        # bound is 1e-13 relative to the volume term (summation-order rounding).
+        vol = dn.volume_residual(U, d, compat)[0]
+        scale = np.linalg.norm(vol.ravel()) / np.linalg.norm(raw.ravel())
+        assert rel_l2(s.get_raw_residual(), raw.reshape(g["sol0"].shape)) < 1e-13 * scale
+        assert rel_l2(s.get_residual(), res.reshape(g["sol0"].shape)) < 1e-13 * scale
     finally:
         s.close()
 
