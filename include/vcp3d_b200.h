@@ -161,6 +161,30 @@ int64_t vcpg_launch_count(const vcpg_handle *h);
  * element solves (the reference's per-element CG, src/CG_MassMatrix.cpp:395-492). */
 int vcpg_stats(vcpg_handle *h, int64_t *cg_iterations, int64_t *element_solves);
 
+/* Allocation-free CFL time step. This entry point has no counterpart in the
+ * reference solver. It is for callers that cannot call cudaMalloc: programs
+ * whose device memory all belongs to their own pool allocator (a framework's
+ * caching allocator, or a driver budgeting many resident cases) and that must
+ * not allocate or free behind that pool, whose accounting would not see it and
+ * whose work cudaMalloc/cudaFree could stall by synchronising the device.
+ * The caller passes device arrays it already owns: d_sol [n_elem][5][K^3],
+ * d_elem_scalars [n_elem][15] (as in vcpg_geometry) and d_dt (one double,
+ * receives the same global time step vcpg_time_step returns). No handle is
+ * used and nothing is allocated: the only scratch (one double per element and
+ * a status slot) is a static device array of the library sized for
+ * VCPG_NOALLOC_MAX_ELEMS elements (2 MiB), held by every GPU that loads the
+ * library until the process exits. Larger n_elem returns VCPG_E_ADMISSION
+ * before any device work. The first call on each device looks up the array's
+ * device address with that device current; make that first call before any
+ * stream capture. All calls share the array and overwrite it: calls that
+ * overlap on the GPU (different streams or host threads) race, so order them.
+ * The call synchronises `stream` (a cudaStream_t, NULL = legacy default stream)
+ * before returning; VCPG_E_NEG_A2 reports a negative speed of sound squared. */
+#define VCPG_NOALLOC_MAX_ELEMS 262144
+int vcpg_time_step_noalloc(const vcpg_params *params, const vcpg_operators *ops,
+                           const double *d_sol, const double *d_elem_scalars, double *d_dt,
+                           void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -25,6 +25,7 @@ EXPORTED = [
     "vcpg_nodal_conservative_to_modal", "vcpg_set_state", "vcpg_get_state",
     "vcpg_get_residual", "vcpg_residual", "vcpg_get_raw_residual", "vcpg_time_step",
     "vcpg_step", "vcpg_sync", "vcpg_stream", "vcpg_launch_count", "vcpg_stats",
+    "vcpg_time_step_noalloc",
 ]
 
 
@@ -85,6 +86,8 @@ def load() -> C.CDLL:
     lib.vcpg_launch_count.argtypes = [hp]
     lib.vcpg_launch_count.restype = C.c_int64
     lib.vcpg_stats.argtypes = [hp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    lib.vcpg_time_step_noalloc.argtypes = [C.POINTER(Params), C.POINTER(Operators), C.c_void_p,
+                                           C.c_void_p, C.c_void_p, C.c_void_p]
     _lib = lib
     return lib
 

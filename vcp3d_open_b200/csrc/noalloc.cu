@@ -1,0 +1,172 @@
+// Allocation-free CFL time step: vcpg_time_step_noalloc (include/vcp3d_b200.h).
+//
+// Who needs this: a host program that hands all of its device memory to its
+// own pool allocator (a framework's caching allocator, or a driver that budgets
+// the memory of many resident cases itself) must not call cudaMalloc/cudaFree
+// behind the pool's back -- the memory would be invisible to the pool's
+// accounting, and those calls can synchronise the device. Such a caller already
+// owns the state and the geometry on the device; this entry point computes the
+// global time step from them without allocating anything.
+//
+// Its only scratch -- one double per element for the per-element steps plus one
+// status slot -- is the static device array below, 2 MiB for the stated limit of
+// VCPG_NOALLOC_MAX_ELEMS elements. Every GPU that loads this library holds it
+// until the process exits. All calls share it and each call overwrites it, so
+// calls that overlap on the GPU (other streams, other host threads) race; the
+// caller must order them. The status slot is cleared at the start of every call.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <mutex>
+
+#include "../../include/vcp3d_b200.h"
+#include "dg_residual.cuh"
+#include "kernels.h"
+
+namespace {
+
+using namespace vcpg;
+
+constexpr int64_t kMaxElems = VCPG_NOALLOC_MAX_ELEMS;
+constexpr int64_t kStatusSlot = kMaxElems;  // 1.0 when a negative a^2 was seen
+
+static __device__ __align__(256) double g_noalloc_scratch[kMaxElems + 32];
+
+// Device address of g_noalloc_scratch per device; looked up once per device.
+std::mutex g_setup_mutex;
+double *g_scratch_ptr[256] = {};
+
+int ScratchForCurrentDevice(double **out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return VCPG_E_CUDA;
+  std::lock_guard<std::mutex> lock(g_setup_mutex);
+  if (!g_scratch_ptr[dev]) {
+    double *p = nullptr;
+    if (cudaGetSymbolAddress((void **)&p, g_noalloc_scratch) != cudaSuccess || !p)
+      return VCPG_E_CUDA;
+    g_scratch_ptr[dev] = p;
+  }
+  *out = g_scratch_ptr[dev];
+  return VCPG_OK;
+}
+
+// Per-element step into scratch[e] (the arithmetic of ElementClass::ComputeTimeStep,
+// src/ElementClass.cpp:1522-1644, as in TimeStepKernel).
+template <int K, int M, int NT>
+__global__ void __launch_bounds__(NT) NoAllocElementDtKernel(const double *sol,
+                                                             const double *scalars, int n_elem,
+                                                             int n_poly, double cfl, double mu,
+                                                             double p_ref, double u_ref,
+                                                             double rho_ref, double *scratch) {
+  constexpr int SLOT = Slot<K, M>::value;
+  constexpr int KD = K * K * K;
+  __shared__ double s_sol[5 * KD], s_t1[5 * KD], s_t2[5 * KD], s_red[64];
+  const int e = blockIdx.x;
+  if (e >= n_elem) return;
+  const double *src = sol + (size_t)e * 5 * KD;
+  for (int i = threadIdx.x; i < 5 * KD; i += NT) s_sol[i] = src[i];
+  __syncthreads();
+  Contract<NT, SLOT, K, M, kLegDof, 2, 5, K, K, K, K, K, false>(s_sol, s_t1);
+  __syncthreads();
+  Contract<NT, SLOT, K, M, kLegDof, 1, 5, K, K, K, K, K, false>(s_t1, s_t2);
+  __syncthreads();
+  Contract<NT, SLOT, K, M, kLegDof, 0, 5, K, K, K, K, K, false>(s_t2, s_t1);
+  __syncthreads();
+  const double *sc = scalars + (size_t)e * 15;
+  const double muDim = mu * p_ref / u_ref;
+  const double dliInv = 1.0 / sc[0], dljInv = 1.0 / sc[1], dlkInv = 1.0 / sc[2];
+  const double dLen2Inv = dliInv * dliInv + dljInv * dljInv + dlkInv * dlkInv;
+  const double radVisOverNuLam = fmax(fmax(1.0, 2.0 + kLamOverMu), kFactHFLam) * dLen2Inv;
+  double radInvMax = 0.0, radVisMax = 0.0, a2Min = 1.e+10;
+  for (int l = threadIdx.x; l < KD; l += NT) {
+    double rho, u, v, w, p, eKin;
+    EntropyToPrim(s_t1[l], s_t1[KD + l], s_t1[2 * KD + l], s_t1[3 * KD + l], s_t1[4 * KD + l],
+                  rho, u, v, w, p, eKin);
+    rho *= rho_ref; u *= u_ref; v *= u_ref; w *= u_ref; p *= p_ref;
+    const double rhoInv = 1.0 / rho;
+    const double a2 = kGam * p * rhoInv;
+    const double velI = u * sc[6] + v * sc[7] + w * sc[8];
+    const double velJ = u * sc[9] + v * sc[10] + w * sc[11];
+    const double velK = u * sc[12] + v * sc[13] + w * sc[14];
+    const double aa = sqrt(fabs(a2));
+    const double radInv = (fabs(velI) + aa) * dliInv + (fabs(velJ) + aa) * dljInv +
+                          (fabs(velK) + aa) * dlkInv;
+    const double radVis = rhoInv * (muDim * radVisOverNuLam + 0.0);
+    radInvMax = fmax(radInvMax, radInv);
+    radVisMax = fmax(radVisMax, radVis);
+    a2Min = fmin(a2Min, a2);
+  }
+  radInvMax = BlockMax<NT>(radInvMax, s_red);
+  radVisMax = BlockMax<NT>(radVisMax, s_red);
+  a2Min = -BlockMax<NT>(-a2Min, s_red);
+  if (threadIdx.x == 0) {
+    if (a2Min < 0.0) scratch[kStatusSlot] = 1.0;
+    const double f1[] = {2.0, 6.0, 12.0, 20.0, 28.0, 38.0, 50.0, 64.0, 80.0, 98.0};
+    const double f2[] = {6.0, 36.0, 150.0, 420.0, 980.0, 1975.0, 3575.0, 7000.0, 14000.0, 28000.0};
+    scratch[e] = cfl * u_ref / (f1[n_poly] * radInvMax + f2[n_poly] * radVisMax);
+  }
+}
+
+// Minimum of scratch[0, n) into *out (one block).
+__global__ void __launch_bounds__(1024) NoAllocMinKernel(const double *scratch, int n,
+                                                         double *out) {
+  __shared__ double s_red[64];
+  double m = 1.e+10;
+  for (int i = threadIdx.x; i < n; i += 1024) m = fmin(m, scratch[i]);
+  m = -BlockMax<1024>(-m, s_red);
+  if (threadIdx.x == 0) *out = m;
+}
+
+template <int K, int M>
+cudaError_t LaunchKM(const vcpg_params *p, const double *sol, const double *sc, int n,
+                     double *scratch, double *d_dt, cudaStream_t st) {
+  NoAllocElementDtKernel<K, M, 64><<<n, 64, 0, st>>>(sol, sc, n, p->n_poly, p->cfl, p->mu,
+                                                     p->p_ref, p->u_ref, p->rho_ref, scratch);
+  NoAllocMinKernel<<<1, 1024, 0, st>>>(scratch, n, d_dt);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+extern "C" int vcpg_time_step_noalloc(const vcpg_params *params, const vcpg_operators *ops,
+                                      const double *d_sol, const double *d_elem_scalars,
+                                      double *d_dt, void *stream) {
+  if (!params || !ops || !d_sol || !d_elem_scalars || !d_dt) return VCPG_E_INVALID;
+  const int K = params->n_poly + 1, M = params->n_int_1d;
+  const int64_t nE = (int64_t)params->n_elem[0] * params->n_elem[1] * params->n_elem[2];
+  if (nE <= 0) return VCPG_E_INVALID;
+  if (nE > kMaxElems) return VCPG_E_ADMISSION;  // beyond the static scratch array
+  if (!Supported(K, M) || K > kKMax || M > kMMax) return VCPG_E_UNSUPPORTED_KM;
+  double *scratch = nullptr;
+  int rc = ScratchForCurrentDevice(&scratch);
+  if (rc != VCPG_OK) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  // Operator table of this (K, M) pair into this file's constant memory.
+  OpTable t;
+  memset(&t, 0, sizeof(t));
+  for (int i = 0; i < K * M; ++i) { t.leg[i] = ops->leg_int[i]; t.dleg[i] = ops->dleg_int[i]; }
+  for (int i = 0; i < 2 * K; ++i) { t.face[i] = ops->leg_face[i]; t.dface[i] = ops->dleg_face[i]; }
+  for (int i = 0; i < M; ++i) t.w[i] = ops->w_int[i];
+  for (int i = 0; i < K * K; ++i) t.legdof[i] = ops->leg_dofs[i];
+  for (int i = 0; i < K * K * K; ++i) t.center[i] = ops->basis_center[i];
+  if (cudaMemcpyToSymbol(c_ops, &t, sizeof(OpTable), sizeof(OpTable) * (size_t)SlotOf(K, M),
+                         cudaMemcpyHostToDevice) != cudaSuccess)
+    return VCPG_E_CUDA;
+  if (cudaMemsetAsync(scratch + kStatusSlot, 0, sizeof(double), st) != cudaSuccess)
+    return VCPG_E_CUDA;
+  cudaError_t e = cudaErrorInvalidValue;
+  const int n = (int)nE;
+  if (K == 2 && M == 3) e = LaunchKM<2, 3>(params, d_sol, d_elem_scalars, n, scratch, d_dt, st);
+  else if (K == 3 && M == 4) e = LaunchKM<3, 4>(params, d_sol, d_elem_scalars, n, scratch, d_dt, st);
+  else if (K == 4 && M == 5) e = LaunchKM<4, 5>(params, d_sol, d_elem_scalars, n, scratch, d_dt, st);
+  else if (K == 5 && M == 7) e = LaunchKM<5, 7>(params, d_sol, d_elem_scalars, n, scratch, d_dt, st);
+  else if (K == 6 && M == 8) e = LaunchKM<6, 8>(params, d_sol, d_elem_scalars, n, scratch, d_dt, st);
+  if (e != cudaSuccess) return VCPG_E_CUDA;
+  double status = 0.0;
+  if (cudaMemcpyAsync(&status, scratch + kStatusSlot, sizeof(double), cudaMemcpyDeviceToHost,
+                      st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return VCPG_E_CUDA;
+  return status != 0.0 ? VCPG_E_NEG_A2 : VCPG_OK;
+}
