@@ -78,6 +78,28 @@ __device__ __forceinline__ double BlockMax(double v, double *red) {
   return s;
 }
 
+// Block-wide (sum a, sum b, max c) with one pair of barriers; red needs 3*NT/32.
+template <int NT>
+__device__ __forceinline__ void BlockReduce3(double &a, double &b, double &c, double *red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+    c = fmax(c, __shfl_xor_sync(0xffffffffu, c, o));
+  }
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) { red[w] = a; red[NT / 32 + w] = b; red[2 * (NT / 32) + w] = c; }
+  __syncthreads();
+  a = 0.0; b = 0.0; c = red[2 * (NT / 32)];
+#pragma unroll
+  for (int i = 0; i < NT / 32; ++i) {
+    a += red[i];
+    b += red[NT / 32 + i];
+    c = fmax(c, red[2 * (NT / 32) + i]);
+  }
+}
+
 // Shared-memory plan (doubles) of the fused kernel for a (K, M) pair.
 template <int K, int M> struct Plan {
   static constexpr int KD = K * K * K, MD = M * M * M, M2 = M * M;
@@ -87,16 +109,20 @@ template <int K, int M> struct Plan {
   static constexpr int VOL = TK + TJ + 20 * MD;
   // Face phase: per face-side trace (value + 3 derivatives) 20*M2, two sides,
   // three faces at a time, plus normal-evaluation and stage buffers.
-  static constexpr int TRACE = 20 * M2;
-  static constexpr int FACE_STAGE = 10 * K * K + 5 * K * M;
-  static constexpr int FACE = 6 * TRACE + FACE_STAGE + 5 * KD;
+  // Face phase: BN/BND 60 K^2, three fast-axis buffers 90 K M, traces 120 M^2.
+  static constexpr int FACE = 60 * K * K + 90 * K * M + 120 * M2;
   // CG phase: z, p, Ap, x, pInt and the contraction buffers.
   static constexpr int CG = 20 * KD + 5 * MD + TK + TJ;
   static constexpr int WORK = VOL > FACE ? (VOL > CG ? VOL : CG) : (FACE > CG ? FACE : CG);
-  // Persistent: sol, R, CG point data (8 per point), J*w, reduction scratch.
-  static constexpr int PERSIST = 10 * KD + 9 * MD + 64;
+  // Persistent: sol, R, CG point data (8 per point), J*w, reduction scratch,
+  // face vectors (basis and derivative at r = -1, +1).
+  static constexpr int PERSIST = 10 * KD + 9 * MD + 64 + 4 * kKMax;
   static constexpr int TOTAL = PERSIST + WORK;
   static constexpr size_t BYTES = sizeof(double) * (size_t)TOTAL;
+  // Threads per CTA and the CTAs per SM that the shared memory allows (227 KB).
+  static constexpr int NT = K >= 5 ? 256 : 128;
+  static constexpr int MIN_BLOCKS =
+      (int)(227 * 1024 / BYTES) < 1 ? 1 : ((int)(227 * 1024 / BYTES) > 4 ? 4 : (int)(227 * 1024 / BYTES));
 };
 
 
@@ -244,48 +270,81 @@ __device__ __forceinline__ void VolumePhase(const ResidualArgs &a, const int e,
 }
 
 // ---------------------------------------------------------------------------
-// Face trace of one element side (TPSAGI/J/K, include/TensorProductSolAndGrad
-// [IJK]Face.hpp): the value and the three parametric derivatives at the face
-// integration points, out = [U | d/dr | d/ds | d/dt], each [5][M][M].
+// Face phase. The faces are processed in two groups -- the Min faces of the
+// three directions, then the Max faces -- and every stage of a group runs over
+// all three faces and both sides of each face at once, so a group needs three
+// barriers for its six traces and three for its distributions.
+//
+// Trace t = 2 d + s: face direction d (0 i, 1 j, 2 k), s = 0 own side, s = 1
+// neighbour side. Face arrays are [slow][fast] with (slow, fast) = (k, j), (k, i),
+// (j, i) for d = 0, 1, 2, as in the reference's TPSAG[IJK] outputs. Trace
+// storage TR[q][t][v][M^2]: q = 0 value, 1 face-normal derivative, 2 fast-axis
+// derivative, 3 slow-axis derivative.
 // ---------------------------------------------------------------------------
-template <int NT, int K, int M, int DIR, bool GLOBAL_SRC>
-__device__ __forceinline__ void FaceTrace(const double *b, const int side, double *stage,
-                                          double *out) {
-  constexpr int SLOT = Slot<K, M>::value;
-  constexpr int M2 = M * M;
-  double *bn = stage, *bnd = stage + 5 * K * K, *t1 = stage + 10 * K * K;
-  // Parametric slots of the fast, slow and normal face axes.
-  constexpr int QN = DIR, QF = DIR == 0 ? 1 : 0, QS = DIR == 2 ? 1 : 2;
-  double *U = out, *dN = out + 5 * M2 * (1 + QN), *dF = out + 5 * M2 * (1 + QF),
-         *dS = out + 5 * M2 * (1 + QS);
-  FaceNormal<NT, SLOT, K, DIR, 5, GLOBAL_SRC>(b, side, bn, bnd);
-  __syncthreads();
-  Contract<NT, SLOT, K, M, kLeg, 0, 5, K, K, 1, K, M, false>(bn, t1);
-  __syncthreads();
-  Contract<NT, SLOT, K, M, kLeg, 1, 5, M, K, 1, K, M, false>(t1, U);
-  Contract<NT, SLOT, K, M, kDLeg, 1, 5, M, K, 1, K, M, false>(t1, dS);
-  __syncthreads();
-  Contract<NT, SLOT, K, M, kDLeg, 0, 5, K, K, 1, K, M, false>(bn, t1);
-  __syncthreads();
-  Contract<NT, SLOT, K, M, kLeg, 1, 5, M, K, 1, K, M, false>(t1, dF);
-  __syncthreads();
-  Contract<NT, SLOT, K, M, kLeg, 0, 5, K, K, 1, K, M, false>(bnd, t1);
-  __syncthreads();
-  Contract<NT, SLOT, K, M, kLeg, 1, 5, M, K, 1, K, M, false>(t1, dN);
-  __syncthreads();
+__device__ __forceinline__ int FastParam(const int d) { return d == 0 ? 1 : 0; }
+
+// Trace quantity q holding parametric derivative p (0 r, 1 s, 2 t) for direction d.
+__device__ __forceinline__ int DerivSlot(const int d, const int p) {
+  return p == d ? 1 : (p == FastParam(d) ? 2 : 3);
 }
 
-// Parametric -> Cartesian gradient of the five variables at face point pt
-// with face metric fm ([13][M2]); metric index per variable in compat mode.
+// Face-normal evaluation of the six sides of a group (first stage of TPSAG[IJK]).
+template <int NT, int SLOT, int K>
+__device__ __forceinline__ void FaceNormalBatch(const double *s_sol, const double *gsol,
+                                                const int nb0, const int nb1, const int nb2,
+                                                const int g, const double *s_fv, double *bn,
+                                                double *bnd) {
+  constexpr int KD = K * K * K, L = 5 * K * K;
+  for (int line = threadIdx.x; line < 6 * L; line += NT) {
+    const int t = line / L, r = line - t * L;
+    const int d = t >> 1, nbr = (t & 1);
+    const int side = nbr ? 1 - g : g;
+    const int v = r / (K * K), r2 = r - v * K * K, sl = r2 / K, f = r2 - sl * K;
+    int base, ns;
+    if (d == 0) { base = sl * K * K + f * K; ns = 1; }
+    else if (d == 1) { base = sl * K * K + f; ns = K; }
+    else { base = sl * K + f; ns = K * K; }
+    base += v * KD;
+    const double *fv = s_fv + side * K, *dfv = s_fv + (2 + side) * K;
+    double a0 = 0.0, d0 = 0.0;
+    if (nbr) {
+      const int nb = d == 0 ? nb0 : (d == 1 ? nb1 : nb2);
+      if (nb >= 0) {
+        const double *b = gsol + (size_t)nb * 5 * KD + base;
+#pragma unroll
+        for (int n = 0; n < K; ++n) {
+          const double x = __ldg(b + n * ns);
+          a0 = fma(fv[n], x, a0);
+          d0 = fma(dfv[n], x, d0);
+        }
+      }
+    } else {
+      const double *b = s_sol + base;
+#pragma unroll
+      for (int n = 0; n < K; ++n) {
+        const double x = b[n * ns];
+        a0 = fma(fv[n], x, a0);
+        d0 = fma(dfv[n], x, d0);
+      }
+    }
+    bn[line] = a0;
+    bnd[line] = d0;
+  }
+}
+
+// Parametric -> Cartesian gradient of one side at face point pt from TR.
 template <int M2>
-__device__ __forceinline__ void FaceCartesianGrad(const double *tr, const int pt,
-                                                  const double *fm, const int compat,
-                                                  double *gx, double *gy, double *gz) {
+__device__ __forceinline__ void TraceCartesianGrad(const double *TR, const int t, const int d,
+                                                   const int pt, const double *fm,
+                                                   const int compat, double *gx, double *gy,
+                                                   double *gz) {
+  const int qr = DerivSlot(d, 0), qs = DerivSlot(d, 1), qt = DerivSlot(d, 2);
 #pragma unroll
   for (int n = 0; n < 5; ++n) {
     const int mi = compat ? n : pt;
-    const double dvdr = tr[(1 * 5 + n) * M2 + pt], dvds = tr[(2 * 5 + n) * M2 + pt],
-                 dvdt = tr[(3 * 5 + n) * M2 + pt];
+    const double dvdr = TR[((qr * 6 + t) * 5 + n) * M2 + pt];
+    const double dvds = TR[((qs * 6 + t) * 5 + n) * M2 + pt];
+    const double dvdt = TR[((qt * 6 + t) * 5 + n) * M2 + pt];
     gx[n] = dvdr * __ldg(fm + 4 * M2 + mi) + dvds * __ldg(fm + 7 * M2 + mi) +
             dvdt * __ldg(fm + 10 * M2 + mi);
     gy[n] = dvdr * __ldg(fm + 5 * M2 + mi) + dvds * __ldg(fm + 8 * M2 + mi) +
@@ -295,27 +354,30 @@ __device__ __forceinline__ void FaceCartesianGrad(const double *tr, const int pt
   }
 }
 
-// Fluxes of an interior face point (FluxesInternalFace, src/FluxesFace.cpp:220-343)
-// seen from the own side. trL/trR are the traces of the left (Max-face) and
-// right (Min-face) elements with metrics fmL/fmR. ownIsLeft selects whose
-// symmetrizing fluxes are returned and the sign of the normal flux. The
-// result overwrites the own trace at this point: [flux | symR | symS | symT].
+// Fluxes of one interior face point (FluxesInternalFace, src/FluxesFace.cpp:220-343),
+// seen from the own side. Writes the own-side distribution inputs by role:
+// P1[role][d][v][M2] with role 0 fast-axis symmetrizing flux, 1 normal flux (with
+// the own side's sign), 2 face-normal symmetrizing flux; P2[d][v][M2] the
+// slow-axis symmetrizing flux.
 template <int K, int M>
-__device__ __forceinline__ void InteriorFacePoint(const ResidualArgs &a, const int pt,
-                                                  const double *trL, const double *trR,
-                                                  const double *fmL, const double *fmR,
-                                                  const double lenScale, const bool ownIsLeft,
-                                                  double *own) {
+__device__ __forceinline__ void GroupFacePoint(const ResidualArgs &a, const int g, const int d,
+                                               const int pt, const double *TR,
+                                               const double *fmOwn, const double *fmNb,
+                                               const double lenScale, double *P1, double *P2) {
   constexpr int SLOT = Slot<K, M>::value;
   constexpr int M2 = M * M;
+  const int tOwn = 2 * d, tNb = 2 * d + 1;
+  // g == 0: own Min face, the neighbour is the left state; g == 1: own Max face.
+  const int tL = g == 0 ? tNb : tOwn, tR = g == 0 ? tOwn : tNb;
+  const double *fmL = g == 0 ? fmNb : fmOwn, *fmR = g == 0 ? fmOwn : fmNb;
   double VL[5], VR[5], gxL[5], gyL[5], gzL[5], gxR[5], gyR[5], gzR[5];
 #pragma unroll
   for (int n = 0; n < 5; ++n) {
-    VL[n] = trL[n * M2 + pt];
-    VR[n] = trR[n * M2 + pt];
+    VL[n] = TR[(tL * 5 + n) * M2 + pt];
+    VR[n] = TR[(tR * 5 + n) * M2 + pt];
   }
-  FaceCartesianGrad<M2>(trL, pt, fmL, a.metric_compat, gxL, gyL, gzL);
-  FaceCartesianGrad<M2>(trR, pt, fmR, a.metric_compat, gxR, gyR, gzR);
+  TraceCartesianGrad<M2>(TR, tL, d, pt, fmL, a.metric_compat, gxL, gyL, gzL);
+  TraceCartesianGrad<M2>(TR, tR, d, pt, fmR, a.metric_compat, gxR, gyR, gzR);
   double gx[5], gy[5], gz[5];
 #pragma unroll
   for (int n = 0; n < 5; ++n) {
@@ -336,119 +398,106 @@ __device__ __forceinline__ void InteriorFacePoint(const ResidualArgs &a, const i
   double sx[5], sy[5], sz[5];
   ViscousPenaltySymFlux(VL, VR, gx, gy, gz, nx, ny, nz, 1.0, wf, area, a.mu,
                         a.tau_num / lenScale, a.theta_sym, flux, sx, sy, sz);
-  const double *fm = ownIsLeft ? fmL : fmR;
+  const double *fm = g == 0 ? fmR : fmL;  // the own side's metric
+  const int pFast = FastParam(d);
 #pragma unroll
   for (int n = 0; n < 5; ++n) {
     const int mi = a.metric_compat ? n : pt;
-    const double symR = sx[n] * __ldg(fm + 4 * M2 + mi) + sy[n] * __ldg(fm + 5 * M2 + mi) +
-                        sz[n] * __ldg(fm + 6 * M2 + mi);
-    const double symS = sx[n] * __ldg(fm + 7 * M2 + mi) + sy[n] * __ldg(fm + 8 * M2 + mi) +
-                        sz[n] * __ldg(fm + 9 * M2 + mi);
-    const double symT = sx[n] * __ldg(fm + 10 * M2 + mi) + sy[n] * __ldg(fm + 11 * M2 + mi) +
-                        sz[n] * __ldg(fm + 12 * M2 + mi);
-    own[(0 * 5 + n) * M2 + pt] = ownIsLeft ? flux[n] : -flux[n];
-    own[(1 * 5 + n) * M2 + pt] = symR;
-    own[(2 * 5 + n) * M2 + pt] = symS;
-    own[(3 * 5 + n) * M2 + pt] = symT;
+    double sym[3];
+#pragma unroll
+    for (int p = 0; p < 3; ++p)
+      sym[p] = sx[n] * __ldg(fm + (4 + 3 * p) * M2 + mi) +
+               sy[n] * __ldg(fm + (5 + 3 * p) * M2 + mi) +
+               sz[n] * __ldg(fm + (6 + 3 * p) * M2 + mi);
+    const int o = (d * 5 + n) * M2 + pt;
+    P1[1 * 15 * M2 + o] = g == 0 ? -flux[n] : flux[n];
+    P1[2 * 15 * M2 + o] = sym[d];
+    P1[0 * 15 * M2 + o] = sym[pFast];
+    P2[o] = sym[3 - d - pFast];
   }
-}
-
-// One TPR*F call (include/TensorProductRes[IJK]Face.hpp): slow axis, fast axis,
-// then expansion along the face normal into res.
-template <int NT, int K, int M, int DIR, int OPS, int OPF, bool DFACE>
-__device__ __forceinline__ void FaceResCall(const double *B, const int side, double *stage,
-                                            double *res) {
-  constexpr int SLOT = Slot<K, M>::value;
-  double *tS = stage, *tF = stage + 5 * K * M;
-  Contract<NT, SLOT, K, M, OPS, 1, 5, M, M, 1, M, K, false>(B, tS);
-  __syncthreads();
-  Contract<NT, SLOT, K, M, OPF, 0, 5, M, K, 1, M, K, false>(tS, tF);
-  __syncthreads();
-  FaceExpand<NT, SLOT, K, DIR, 5, DFACE>(tF, side, res);
-  __syncthreads();
-}
-
-// The four distributions of a face (normal flux, then the symmetrizing fluxes
-// of the r, s and t directions), as in IFaceResiduals (src/ElementClass.cpp:2752-2783).
-template <int NT, int K, int M, int DIR>
-__device__ __forceinline__ void FaceDistribute(const double *own, const int side, double *stage,
-                                               double *res) {
-  constexpr int M2 = M * M;
-  // Parametric direction q gets the derivative on its own axis.
-  FaceResCall<NT, K, M, DIR, kLegT, kLegT, false>(own, side, stage, res);
-  // q = r (i axis): normal for i-faces, fast axis otherwise.
-  if (DIR == 0) FaceResCall<NT, K, M, DIR, kLegT, kLegT, true>(own + 5 * M2, side, stage, res);
-  else FaceResCall<NT, K, M, DIR, kLegT, kDLegT, false>(own + 5 * M2, side, stage, res);
-  // q = s (j axis): fast for i-faces, normal for j-faces, slow for k-faces.
-  if (DIR == 0) FaceResCall<NT, K, M, DIR, kLegT, kDLegT, false>(own + 10 * M2, side, stage, res);
-  else if (DIR == 1) FaceResCall<NT, K, M, DIR, kLegT, kLegT, true>(own + 10 * M2, side, stage, res);
-  else FaceResCall<NT, K, M, DIR, kDLegT, kLegT, false>(own + 10 * M2, side, stage, res);
-  // q = t (k axis): slow for i- and j-faces, normal for k-faces.
-  if (DIR == 2) FaceResCall<NT, K, M, DIR, kLegT, kLegT, true>(own + 15 * M2, side, stage, res);
-  else FaceResCall<NT, K, M, DIR, kDLegT, kLegT, false>(own + 15 * M2, side, stage, res);
-}
-
-// ---------------------------------------------------------------------------
-// Face phase: Min faces of the three directions (accumulated into s_R in the
-// order i, j, k), then Max faces (each summed from zero, then added in the
-// order i, j, k, like the neighbours' mResIMin/JMin/KMin in the reference).
-// ---------------------------------------------------------------------------
-template <int NT, int K, int M, int DIR>
-__device__ __forceinline__ void FaceTracesDir(const ResidualArgs &a, const int e, const int g,
-                                              const double *s_sol, double *traces, double *stage) {
-  constexpr int KD = K * K * K, M2 = M * M;
-  const int nb = a.nbr[e * 6 + 2 * DIR + g];
-  double *own = traces + (2 * DIR) * 20 * M2, *oth = own + 20 * M2;
-  FaceTrace<NT, K, M, DIR, false>(s_sol, g, stage, own);
-  if (nb >= 0) FaceTrace<NT, K, M, DIR, true>(a.sol + (size_t)nb * 5 * KD, 1 - g, stage, oth);
 }
 
 template <int NT, int K, int M>
 __device__ __forceinline__ void FacePhase(const ResidualArgs &a, const int e, const double *s_sol,
-                                          double *s_R, double *work) {
-  constexpr int KD = K * K * K, M2 = M * M;
-  double *traces = work;                    // 6 x 20 M2
-  double *stage = work + 120 * M2;          // FACE_STAGE
-  double *s_T = stage + 10 * K * K + 5 * K * M;  // 5 KD
+                                          double *s_R, const double *s_fv, double *work) {
+  constexpr int SLOT = Slot<K, M>::value;
+  constexpr int KD = K * K * K, M2 = M * M, K2 = K * K;
+  static_assert(2 * M <= 3 * K && K <= 2 * M, "face-phase buffer aliasing");
+  double *BN = work, *BND = BN + 30 * K2;        // 60 K^2
+  double *T1a = BND + 30 * K2, *T1b = T1a + 30 * K * M, *T1c = T1b + 30 * K * M;  // 90 K M
+  double *TR = T1c + 30 * K * M;                 // 120 M^2
+  double *P1 = T1a, *P2 = T1a + 45 * M2;         // distribution inputs (in T1)
+  double *Q1 = TR, *Q2 = TR + 45 * K * M;        // after the slow-axis contraction (in TR)
+  double *RF = BN, *RFN = RF + 15 * K2, *RS = RFN + 30 * K2;  // after the fast axis (in BN)
   const double *sc = a.elem_scalars + (size_t)e * 15;
   for (int g = 0; g < 2; ++g) {
-    FaceTracesDir<NT, K, M, 0>(a, e, g, s_sol, traces, stage);
-    FaceTracesDir<NT, K, M, 1>(a, e, g, s_sol, traces, stage);
-    FaceTracesDir<NT, K, M, 2>(a, e, g, s_sol, traces, stage);
-    // Pointwise fluxes of the three faces of this group.
+    const int nb0 = a.nbr[e * 6 + 0 + g], nb1 = a.nbr[e * 6 + 2 + g], nb2 = a.nbr[e * 6 + 4 + g];
+    // Traces of the six sides (TPSAG[IJK]): normal, fast axis, slow axis.
+    FaceNormalBatch<NT, SLOT, K>(s_sol, a.sol, nb0, nb1, nb2, g, s_fv, BN, BND);
+    __syncthreads();
+    Contract<NT, SLOT, K, M, kLeg, 0, 30, K, K, 1, K, M, false>(BN, T1a);
+    Contract<NT, SLOT, K, M, kDLeg, 0, 30, K, K, 1, K, M, false>(BN, T1b);
+    Contract<NT, SLOT, K, M, kLeg, 0, 30, K, K, 1, K, M, false>(BND, T1c);
+    __syncthreads();
+    Contract<NT, SLOT, K, M, kLeg, 1, 30, M, K, 1, K, M, false>(T1a, TR);
+    Contract<NT, SLOT, K, M, kDLeg, 1, 30, M, K, 1, K, M, false>(T1a, TR + 3 * 30 * M2);
+    Contract<NT, SLOT, K, M, kLeg, 1, 30, M, K, 1, K, M, false>(T1b, TR + 2 * 30 * M2);
+    Contract<NT, SLOT, K, M, kLeg, 1, 30, M, K, 1, K, M, false>(T1c, TR + 1 * 30 * M2);
+    __syncthreads();
+    // Pointwise fluxes of the three faces.
     for (int idx = threadIdx.x; idx < 3 * M2; idx += NT) {
       const int d = idx / M2, pt = idx - d * M2;
-      const int nb = a.nbr[e * 6 + 2 * d + g];
-      double *own = traces + (2 * d) * 20 * M2, *oth = own + 20 * M2;
+      const int nb = d == 0 ? nb0 : (d == 1 ? nb1 : nb2);
       if (nb < 0) {
-        // Physical boundary faces are handled by the boundary-face path.
+        // Physical boundary faces are not part of this interior-face path.
         if (pt == 0) atomicAdd(a.status + 1, 1);
+        for (int n = 0; n < 5; ++n) {
+          const int o = (d * 5 + n) * M2 + pt;
+          P1[o] = P1[15 * M2 + o] = P1[30 * M2 + o] = P2[o] = 0.0;
+        }
         continue;
       }
       const double lenScale = fmin(sc[d], a.elem_scalars[(size_t)nb * 15 + d]);
       const double *fmOwn = a.face_metric + ((size_t)e * 6 + 2 * d + g) * 13 * M2;
       const double *fmNb = a.face_metric + ((size_t)nb * 6 + 2 * d + 1 - g) * 13 * M2;
-      if (g == 0)  // own Min face: the neighbour is the left state
-        InteriorFacePoint<K, M>(a, pt, oth, own, fmNb, fmOwn, lenScale, false, own);
-      else
-        InteriorFacePoint<K, M>(a, pt, own, oth, fmOwn, fmNb, lenScale, true, own);
+      GroupFacePoint<K, M>(a, g, d, pt, TR, fmOwn, fmNb, lenScale, P1, P2);
     }
     __syncthreads();
-    for (int d = 0; d < 3; ++d) {
-      const double *own = traces + (2 * d) * 20 * M2;
-      double *target = g == 0 ? s_R : s_T;
-      if (g == 1) {
-        for (int i = threadIdx.x; i < 5 * KD; i += NT) s_T[i] = 0.0;
-        __syncthreads();
+    // Distribution (TPR[IJK]F): slow axis, fast axis, then the face-normal expansion.
+    Contract<NT, SLOT, K, M, kLegT, 1, 45, M, M, 1, M, K, false>(P1, Q1);
+    Contract<NT, SLOT, K, M, kDLegT, 1, 15, M, M, 1, M, K, false>(P2, Q2);
+    __syncthreads();
+    Contract<NT, SLOT, K, M, kDLegT, 0, 15, M, K, 1, M, K, false>(Q1, RF);
+    Contract<NT, SLOT, K, M, kLegT, 0, 30, M, K, 1, M, K, false>(Q1 + 15 * K * M, RFN);
+    Contract<NT, SLOT, K, M, kLegT, 0, 15, M, K, 1, M, K, false>(Q2, RS);
+    __syncthreads();
+    const double *fv = s_fv + g * K, *dfv = s_fv + (2 + g) * K;
+    for (int idx = threadIdx.x; idx < 5 * KD; idx += NT) {
+      const int v = idx / KD, r = idx - v * KD;
+      const int k = r / K2, r2 = r - k * K2, j = r2 / K, i = r2 - j * K;
+      double acc = s_R[idx];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const int n = d == 0 ? i : (d == 1 ? j : k);
+        const int sf = d == 0 ? k * K + j : (d == 1 ? k * K + i : j * K + i);
+        const int o = (d * 5 + v) * K2 + sf;
+        const double aF = fv[n], aD = dfv[n];
+        const double tFlux = RFN[o], tN = RFN[15 * K2 + o], tFast = RF[o], tSlow = RS[o];
+        // Reference order: normal flux, then the r, s, t symmetrizing fluxes.
+        const int pFast = FastParam(d);
+        double c = g == 0 ? acc : 0.0;
+        c = fma(aF, tFlux, c);
+#pragma unroll
+        for (int p = 0; p < 3; ++p) {
+          if (p == d) c = fma(aD, tN, c);
+          else if (p == pFast) c = fma(aF, tFast, c);
+          else c = fma(aF, tSlow, c);
+        }
+        acc = g == 0 ? c : acc + c;
       }
-      if (d == 0) FaceDistribute<NT, K, M, 0>(own, g, stage, target);
-      else if (d == 1) FaceDistribute<NT, K, M, 1>(own, g, stage, target);
-      else FaceDistribute<NT, K, M, 2>(own, g, stage, target);
-      if (g == 1) {
-        for (int i = threadIdx.x; i < 5 * KD; i += NT) s_R[i] += s_T[i];
-        __syncthreads();
-      }
+      s_R[idx] = acc;
     }
+    __syncthreads();
   }
 }
 
@@ -535,8 +584,12 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
   };
   precond();
   __syncthreads();
-  for (int i = threadIdx.x; i < 5 * KD; i += NT) p[i] = z[i];
-  __syncthreads();
+  double part = 0.0;
+  for (int i = threadIdx.x; i < 5 * KD; i += NT) {
+    p[i] = z[i];
+    part = fma(r[i], z[i], part);
+  }
+  double dotrz = BlockSum<NT>(part, s_red);
 
   int iter = 0;
   for (;; ++iter) {
@@ -544,10 +597,6 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
       if (threadIdx.x == 0) atomicAdd(a.status, 1);
       break;
     }
-    double part = 0.0;
-    for (int i = threadIdx.x; i < 5 * KD; i += NT) part = fma(r[i], z[i], part);
-    const double dotrz = BlockSum<NT>(part, s_red);
-
     // Ap = Leg^T3 (w J dU/dV (Leg3 p)) (src/CG_MassMatrix.cpp:408-443).
     Contract<NT, SLOT, K, M, kLeg, 2, 5, K, K, K, K, M, false>(p, tK);
     __syncthreads();
@@ -580,21 +629,36 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
     __syncthreads();
     part = 0.0;
     for (int i = threadIdx.x; i < 5 * KD; i += NT) part = fma(p[i], Ap[i], part);
-    const double dotpAp = BlockSum<NT>(part, s_red);
-    const double alpha = dotrz / dotpAp;
-    m = 0.0;
-    for (int i = threadIdx.x; i < 5 * KD; i += NT) {
-      x[i] = fma(alpha, p[i], x[i]);
-      r[i] = fma(-alpha, Ap[i], r[i]);
-      m = fmax(m, fabs(r[i]));
+    const double alpha = dotrz / BlockSum<NT>(part, s_red);
+    // Each thread owns whole DOFs: update x and r, precondition, and form the
+    // partial sums of the three reductions that close the iteration.
+    double zAp = 0.0, rzNew = 0.0, rMax = 0.0;
+    for (int l = threadIdx.x; l < KD; l += NT) {
+      double rr[5];
+#pragma unroll
+      for (int q = 0; q < 5; ++q) {
+        x[q * KD + l] = fma(alpha, p[q * KD + l], x[q * KD + l]);
+        rr[q] = fma(-alpha, Ap[q * KD + l], r[q * KD + l]);
+        r[q * KD + l] = rr[q];
+        rMax = fmax(rMax, fabs(rr[q]));
+      }
+      const double zz[5] = {
+          D[0] * rr[0] + D[1] * rr[1] + D[2] * rr[2] + D[3] * rr[3] + D[4] * rr[4],
+          D[1] * rr[0] + D[5] * rr[1] + D[6] * rr[2] + D[7] * rr[3] + D[8] * rr[4],
+          D[2] * rr[0] + D[6] * rr[1] + D[9] * rr[2] + D[10] * rr[3] + D[11] * rr[4],
+          D[3] * rr[0] + D[7] * rr[1] + D[10] * rr[2] + D[12] * rr[3] + D[13] * rr[4],
+          D[4] * rr[0] + D[8] * rr[1] + D[11] * rr[2] + D[13] * rr[3] + D[14] * rr[4]};
+#pragma unroll
+      for (int q = 0; q < 5; ++q) {
+        z[q * KD + l] = zz[q];
+        zAp = fma(zz[q], Ap[q * KD + l], zAp);
+        rzNew = fma(rr[q], zz[q], rzNew);
+      }
     }
-    const double rMax = BlockMax<NT>(m, s_red);
+    BlockReduce3<NT>(zAp, rzNew, rMax, s_red);
     if (rMax < 1.e-10 * rInitMax) break;
-    precond();
-    __syncthreads();
-    part = 0.0;
-    for (int i = threadIdx.x; i < 5 * KD; i += NT) part = fma(z[i], Ap[i], part);
-    const double beta = -alpha * BlockSum<NT>(part, s_red) / dotrz;
+    const double beta = -alpha * zAp / dotrz;
+    dotrz = rzNew;
     for (int i = threadIdx.x; i < 5 * KD; i += NT) p[i] = beta * p[i] + z[i];
     __syncthreads();
   }
@@ -608,19 +672,23 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
 // The fused kernel.
 // ---------------------------------------------------------------------------
 template <int K, int M, int NT>
-__global__ void __launch_bounds__(NT) ResidualKernel(const ResidualArgs a) {
+__global__ void __launch_bounds__(NT, Plan<K, M>::MIN_BLOCKS) ResidualKernel(const ResidualArgs a) {
   using P = Plan<K, M>;
   constexpr int KD = P::KD, MD = P::MD;
   extern __shared__ double smem[];
   double *s_sol = smem, *s_R = s_sol + 5 * KD, *s_cgp = s_R + 5 * KD, *s_jw = s_cgp + 8 * MD;
-  double *s_red = s_jw + MD, *work = s_red + 64;
+  double *s_red = s_jw + MD, *s_fv = s_red + 64, *work = s_fv + 4 * kKMax;
   const int e = blockIdx.x;
   if (e >= a.n_elem) return;
   const double *src = a.sol + (size_t)e * 5 * KD;
   for (int i = threadIdx.x; i < 5 * KD; i += NT) s_sol[i] = src[i];
+  if (threadIdx.x < 2 * K) {
+    s_fv[threadIdx.x] = c_ops[Slot<K, M>::value].face[threadIdx.x];
+    s_fv[2 * K + threadIdx.x] = c_ops[Slot<K, M>::value].dface[threadIdx.x];
+  }
   __syncthreads();
   VolumePhase<NT, K, M>(a, e, s_sol, s_R, s_cgp, s_jw, work, s_red);
-  FacePhase<NT, K, M>(a, e, s_sol, s_R, work);
+  FacePhase<NT, K, M>(a, e, s_sol, s_R, s_fv, work);
   if (a.res_raw) {
     double *dst = a.res_raw + (size_t)e * 5 * KD;
     for (int i = threadIdx.x; i < 5 * KD; i += NT) dst[i] = s_R[i];

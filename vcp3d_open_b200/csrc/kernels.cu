@@ -108,7 +108,7 @@ __global__ void LsrkStageKernel(double *sol, double *du, const double *res, cons
 // ---------------------------------------------------------------------------
 template <int K, int M>
 static cudaError_t LaunchResidualKM(const ResidualArgs &a, cudaStream_t st) {
-  constexpr int NT = 128;
+  constexpr int NT = Plan<K, M>::NT;
   const size_t bytes = Plan<K, M>::BYTES;
   static bool configured = false;
   if (!configured) {
