@@ -62,7 +62,10 @@ typedef struct vcpg_params {
                                  the metric by the variable index as the reference
                                  does (src/ElementClass.cpp:3865-3873,
                                  src/FluxesFace.cpp:272-282, 325-332); 0: by point */
-  int32_t precision;          /* enum vcpg_precision                                 */
+  int32_t precision;          /* enum vcpg_precision. VCPG_MIXED: the residual
+                                 (contractions, fluxes, mass solve) computes in
+                                 FP32 with a 1e-5 CG tolerance; state, metrics,
+                                 time step and RK updates stay FP64            */
   double theta_sym;           /* "Theta parameter symmetrizing terms"                */
   double rel_penalty;         /* "Relative penalty parameter"                        */
   double cfl;                 /* "CFL number"                                        */
@@ -120,7 +123,8 @@ int vcpg_setup_geometry(const vcpg_params *params, int32_t p_grid, int32_t dof_l
 int vcpg_nodal_conservative_to_modal(const vcpg_params *params, const double *vand_inv,
                                      const double *cons, double *modal, int64_t n_elem);
 
-/* State transfer (host <-> device), [n_elem][5][K^3]. */
+/* State transfer (host <-> device), [n_elem][5][K^3]. vcpg_set_state marks the
+ * stored residual as stale. */
 int vcpg_set_state(vcpg_handle *h, const double *modal);
 int vcpg_get_state(vcpg_handle *h, double *modal);
 int vcpg_get_residual(vcpg_handle *h, double *res);
@@ -139,9 +143,10 @@ int vcpg_time_step(vcpg_handle *h, double *dt);
 /* n_steps full time steps with the given scheme (SSP-RK3 as in
  * ExecuteTimeSynchronizationStep, or five-stage low-storage RK4). If
  * fixed_dt > 0 it is used as the non-dimensional step, otherwise the CFL step
- * is recomputed on the device at the start of every step. The residual of the
- * current state must be valid (vcpg_residual) before the first step, as in the
- * reference main program (src/VCP3D_CurviLinear.cpp:94). dt_history, when
+ * is recomputed on the device at the start of every step. The first stage uses
+ * the residual of the current state, as in the reference main program
+ * (src/VCP3D_CurviLinear.cpp:94); when the state was set since the last
+ * residual, vcpg_step evaluates it first (one extra launch). dt_history, when
  * non-NULL, receives the n_steps time steps. The step sequence is captured in
  * a CUDA graph on first use. */
 int vcpg_step(vcpg_handle *h, int32_t scheme, int32_t n_steps, double fixed_dt,

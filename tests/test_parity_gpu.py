@@ -162,3 +162,21 @@ def test_launch_count_and_graph_reuse(gpu_available):
         assert s.launch_count - n0 == 4 * 8
     finally:
         s.close()
+
+
+def test_step_after_set_state_evaluates_the_residual_first(gpu_available):
+    """A step right after vcpg_set_state equals residual + step (one extra launch)."""
+    g = load_golden(golden_files()[0])
+    _, _, _, s = _make(g["spec"])
+    try:
+        s.set_state(g["sol0"])
+        s.residual()
+        s.step(2, capi.LSRK4)
+        want = s.get_state()
+        s.set_state(g["sol0"])
+        n0 = s.launch_count
+        s.step(2, capi.LSRK4)
+        assert s.launch_count - n0 == 1 + 2 * 12
+        np.testing.assert_array_equal(s.get_state(), want)
+    finally:
+        s.close()

@@ -40,6 +40,12 @@ def test_create_rejects_bad_arguments_without_touching_the_device():
     assert rc == 6
     assert b"no kernel" in lib.vcpg_last_error(h)
     lib.vcpg_destroy(h)
+    p.n_poly, p.n_int_1d = 3, 5
+    p.precision = 7                      # neither VCPG_FP64 nor VCPG_MIXED
+    rc = lib.vcpg_create(C.byref(p), C.byref(ops), C.byref(geo), C.byref(h))
+    assert rc == 8
+    assert b"precision" in lib.vcpg_last_error(h)
+    lib.vcpg_destroy(h)
     assert lib.vcpg_step(None, 0, 1, -1.0, None) == 8
 
 

@@ -34,6 +34,7 @@ struct vcpg_handle {
   cudaGraphExec_t exec[2] = {nullptr, nullptr};
   int graph_launches[2] = {0, 0};
   int64_t launches = 0;
+  bool res_valid = false;  // d_res holds the residual of d_sol
   std::string err;
 };
 
@@ -78,6 +79,10 @@ ResidualArgs MakeResidualArgs(vcpg_handle *h, double *rawOut, unsigned long long
   a.mach2max = mach;
   a.status = h->d_status;
   a.cg_stats = h->d_cgstats;
+  // The mixed form computes the residual in FP32; its mass-matrix CG stops at a
+  // tolerance FP32 can reach (1e-5 relative), the FP64 form at the reference's 1e-10.
+  a.mixed = h->prm.precision == VCPG_MIXED ? 1 : 0;
+  a.cg_tol = a.mixed ? 1.e-5 : 1.e-10;
   return a;
 }
 
@@ -182,8 +187,8 @@ int vcpg_create(const vcpg_params *params, const vcpg_operators *ops, const vcpg
     *out = h;
     return rc;
   }
-  if (params->precision != VCPG_FP64) {
-    int rc = Fail(h, VCPG_E_INVALID, "mixed precision is selected per handle at build time only");
+  if (params->precision != VCPG_FP64 && params->precision != VCPG_MIXED) {
+    int rc = Fail(h, VCPG_E_INVALID, "precision must be VCPG_FP64 or VCPG_MIXED");
     *out = h;
     return rc;
   }
@@ -204,6 +209,11 @@ int vcpg_create(const vcpg_params *params, const vcpg_operators *ops, const vcpg
   for (int m = 0; m < M; ++m) t.w[m] = ops->w_int[m];
   for (int i = 0; i < K * K; ++i) t.legdof[i] = ops->leg_dofs[i];
   for (int i = 0; i < h->KD; ++i) t.center[i] = ops->basis_center[i];
+  // FP32 copies, rounded once from the FP64 operators, for the mixed form.
+  for (int i = 0; i < K * M; ++i) { t.legf[i] = (float)t.leg[i]; t.dlegf[i] = (float)t.dleg[i]; }
+  for (int i = 0; i < 2 * K; ++i) { t.facef[i] = (float)t.face[i]; t.dfacef[i] = (float)t.dface[i]; }
+  for (int m = 0; m < M; ++m) t.wf[m] = (float)t.w[m];
+  for (int i = 0; i < h->KD; ++i) t.centerf[i] = (float)t.center[i];
   VCPG_CUDA(h, UploadOpTable(SlotOf(K, M), t));
 
   VCPG_CUDA(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
@@ -253,6 +263,7 @@ int vcpg_create(const vcpg_params *params, const vcpg_operators *ops, const vcpg
 
 int vcpg_set_state(vcpg_handle *h, const double *modal) {
   if (!h || !modal) return VCPG_E_INVALID;
+  h->res_valid = false;
   VCPG_CUDA(h, cudaMemcpyAsync(h->d_sol, modal, (size_t)h->nE * 5 * h->KD * 8,
                                cudaMemcpyHostToDevice, h->stream));
   VCPG_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -296,6 +307,7 @@ int vcpg_residual(vcpg_handle *h, double *monitoring, int32_t keep_raw) {
   VCPG_CUDA(h, LaunchResidual(h->K, h->M, a, h->stream));
   h->launches += 1;
   int rc = CheckStatus(h);
+  h->res_valid = rc == VCPG_OK;
   if (monitoring) {
     unsigned long long bits = 0;
     VCPG_CUDA(h, cudaMemcpy(&bits, h->d_mach2, 8, cudaMemcpyDeviceToHost));
@@ -340,6 +352,12 @@ int vcpg_step(vcpg_handle *h, int32_t scheme, int32_t n_steps, double fixed_dt,
     cudaError_t e = cudaMalloc((void **)&h->d_hist, (size_t)h->hist_cap * 8);
     if (e != cudaSuccess) return Fail(h, VCPG_E_OOM, "cudaMalloc dt history");
   }
+  if (!h->res_valid) {
+    // The first stage uses the residual of the current state: evaluate it once
+    // after a new state was set (later steps reuse the last stage's residual).
+    VCPG_CUDA(h, LaunchResidual(h->K, h->M, MakeResidualArgs(h, nullptr, nullptr), h->stream));
+    h->launches += 1;
+  }
   const double fx = fixed_dt > 0.0 ? fixed_dt : -1.0;
   VCPG_CUDA(h, cudaMemcpyAsync(h->d_fixed, &fx, 8, cudaMemcpyHostToDevice, h->stream));
   VCPG_CUDA(h, cudaMemsetAsync(h->d_counter, 0, sizeof(int), h->stream));
@@ -359,7 +377,9 @@ int vcpg_step(vcpg_handle *h, int32_t scheme, int32_t n_steps, double fixed_dt,
   if (dt_history)
     VCPG_CUDA(h, cudaMemcpyAsync(dt_history, h->d_hist, (size_t)n_steps * 8,
                                  cudaMemcpyDeviceToHost, h->stream));
-  return CheckStatus(h);
+  const int rc = CheckStatus(h);
+  h->res_valid = rc == VCPG_OK;
+  return rc;
 }
 
 int vcpg_sync(vcpg_handle *h) {

@@ -37,6 +37,8 @@ struct ResidualArgs {
   unsigned long long *mach2max;  // optional: bits of max Mach^2 (non-negative double)
   int *status;                 // [0] CG iteration cap hits, [1] boundary face without BC
   unsigned long long *cg_stats;  // [0] CG iterations, [1] element solves (cumulative)
+  double cg_tol;               // relative CG stopping tolerance (1e-10 in the FP64 form)
+  int mixed;                   // 1: FP32 compute (contractions, fluxes, mass solve)
 };
 
 // Arguments of the CFL time-step kernel (kernels.cu).
@@ -50,58 +52,58 @@ struct TimeStepArgs {
   int *status;  // [2]: negative a^2 seen
 };
 
-template <int NT>
-__device__ __forceinline__ double BlockSum(double v, double *red) {
+template <int NT, typename T>
+__device__ __forceinline__ T BlockSum(T v, T *red) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   __syncthreads();
   if (lane == 0) red[w] = v;
   __syncthreads();
-  double s = 0.0;
+  T s = T(0.0);
 #pragma unroll
   for (int i = 0; i < NT / 32; ++i) s += red[i];
   return s;
 }
 
-template <int NT>
-__device__ __forceinline__ double BlockMax(double v, double *red) {
+template <int NT, typename T>
+__device__ __forceinline__ T BlockMax(T v, T *red) {
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  for (int o = 16; o > 0; o >>= 1) v = Fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   __syncthreads();
   if (lane == 0) red[w] = v;
   __syncthreads();
-  double s = red[0];
+  T s = red[0];
 #pragma unroll
-  for (int i = 1; i < NT / 32; ++i) s = fmax(s, red[i]);
+  for (int i = 1; i < NT / 32; ++i) s = Fmax(s, red[i]);
   return s;
 }
 
 // Block-wide (sum a, sum b, max c) with one pair of barriers; red needs 3*NT/32.
-template <int NT>
-__device__ __forceinline__ void BlockReduce3(double &a, double &b, double &c, double *red) {
+template <int NT, typename T>
+__device__ __forceinline__ void BlockReduce3(T &a, T &b, T &c, T *red) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     a += __shfl_xor_sync(0xffffffffu, a, o);
     b += __shfl_xor_sync(0xffffffffu, b, o);
-    c = fmax(c, __shfl_xor_sync(0xffffffffu, c, o));
+    c = Fmax(c, __shfl_xor_sync(0xffffffffu, c, o));
   }
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   __syncthreads();
   if (lane == 0) { red[w] = a; red[NT / 32 + w] = b; red[2 * (NT / 32) + w] = c; }
   __syncthreads();
-  a = 0.0; b = 0.0; c = red[2 * (NT / 32)];
+  a = T(0.0); b = T(0.0); c = red[2 * (NT / 32)];
 #pragma unroll
   for (int i = 0; i < NT / 32; ++i) {
     a += red[i];
     b += red[NT / 32 + i];
-    c = fmax(c, red[2 * (NT / 32) + i]);
+    c = Fmax(c, red[2 * (NT / 32) + i]);
   }
 }
 
 // Shared-memory plan (doubles) of the fused kernel for a (K, M) pair.
-template <int K, int M> struct Plan {
+template <int K, int M, typename T = double> struct Plan {
   static constexpr int KD = K * K * K, MD = M * M * M, M2 = M * M;
   static constexpr int TK = 5 * K * K * M;      // first-stage buffer
   static constexpr int TJ = 5 * K * M * M;      // second-stage buffer
@@ -118,7 +120,7 @@ template <int K, int M> struct Plan {
   // face vectors (basis and derivative at r = -1, +1).
   static constexpr int PERSIST = 10 * KD + 9 * MD + 64 + 4 * kKMax;
   static constexpr int TOTAL = PERSIST + WORK;
-  static constexpr size_t BYTES = sizeof(double) * (size_t)TOTAL;
+  static constexpr size_t BYTES = sizeof(T) * (size_t)TOTAL;
   // Threads per CTA and the CTAs per SM that the shared memory allows (227 KB).
   static constexpr int NT = K >= 5 ? 256 : 128;
   static constexpr int MIN_BLOCKS =
@@ -132,15 +134,15 @@ template <int K, int M> struct Plan {
 // into s_R. Also stores the CG point data (rho, u, v, w, p, rhoE, dUdV(4,4))
 // and J*w.  Follows ElementClass::VolumeResidual, src/ElementClass.cpp:3809-4443.
 // ---------------------------------------------------------------------------
-template <int NT, int K, int M>
+template <int NT, int K, int M, typename T>
 __device__ __forceinline__ void VolumePhase(const ResidualArgs &a, const int e,
-                                            const double *s_sol, double *s_R, double *s_cgp,
-                                            double *s_jw, double *work, double *s_red) {
+                                            const T *s_sol, T *s_R, T *s_cgp,
+                                            T *s_jw, T *work, T *s_red) {
   constexpr int SLOT = Slot<K, M>::value;
-  using P = Plan<K, M>;
+  using P = Plan<K, M, T>;
   constexpr int MD = P::MD, KD = P::KD, M2 = P::M2;
-  double *tK = work, *tJ = work + P::TK, *Var = tJ + P::TJ;
-  double *dX = Var + 5 * MD, *dY = dX + 5 * MD, *dZ = dY + 5 * MD;
+  T *tK = work, *tJ = work + P::TK, *Var = tJ + P::TJ;
+  T *dX = Var + 5 * MD, *dY = dX + 5 * MD, *dZ = dY + 5 * MD;
 
   // TPSAGV (include/TensorProductSolAndGradVolume.hpp:5-249): k, then j, then i.
   Contract<NT, SLOT, K, M, kLeg, 2, 5, K, K, K, K, M, false>(s_sol, tK);
@@ -159,44 +161,44 @@ __device__ __forceinline__ void VolumePhase(const ResidualArgs &a, const int e,
   Contract<NT, SLOT, K, M, kLeg, 1, 5, K, K, M, K, M, false>(tK, tJ);
   __syncthreads();
   Contract<NT, SLOT, K, M, kLeg, 0, 5, K, M, M, K, M, false>(tJ, dZ);
-  for (int i = threadIdx.x; i < 5 * KD; i += NT) s_R[i] = 0.0;
+  for (int i = threadIdx.x; i < 5 * KD; i += NT) s_R[i] = T(0.0);
   __syncthreads();
 
   const double *vm = a.vol_metric + (size_t)e * 10 * MD;
-  const double gm1 = kGam - 1.0, ov1mg = -1.0 / gm1;
-  double mach2 = 0.0;
+  const T gm1 = T(kGam) - T(1.0), ov1mg = -T(1.0) / gm1;
+  T mach2 = T(0.0);
   for (int l = threadIdx.x; l < MD; l += NT) {
     const int i = l % M, j = (l / M) % M, k = l / M2;
     // Parametric -> Cartesian gradients (src/ElementClass.cpp:3856-3875). In the
     // compatibility mode the metric of point n is used for variable n.
-    double V[5], gx[5], gy[5], gz[5];
+    T V[5], gx[5], gy[5], gz[5];
 #pragma unroll
     for (int n = 0; n < 5; ++n) {
       const int mi = a.metric_compat ? n : l;
-      const double dvdr = dX[n * MD + l], dvds = dY[n * MD + l], dvdt = dZ[n * MD + l];
-      gx[n] = dvdr * __ldg(vm + 1 * MD + mi) + dvds * __ldg(vm + 4 * MD + mi) +
-              dvdt * __ldg(vm + 7 * MD + mi);
-      gy[n] = dvdr * __ldg(vm + 2 * MD + mi) + dvds * __ldg(vm + 5 * MD + mi) +
-              dvdt * __ldg(vm + 8 * MD + mi);
-      gz[n] = dvdr * __ldg(vm + 3 * MD + mi) + dvds * __ldg(vm + 6 * MD + mi) +
-              dvdt * __ldg(vm + 9 * MD + mi);
+      const T dvdr = dX[n * MD + l], dvds = dY[n * MD + l], dvdt = dZ[n * MD + l];
+      gx[n] = dvdr * LdT<T>(vm + 1 * MD + mi) + dvds * LdT<T>(vm + 4 * MD + mi) +
+              dvdt * LdT<T>(vm + 7 * MD + mi);
+      gy[n] = dvdr * LdT<T>(vm + 2 * MD + mi) + dvds * LdT<T>(vm + 5 * MD + mi) +
+              dvdt * LdT<T>(vm + 8 * MD + mi);
+      gz[n] = dvdr * LdT<T>(vm + 3 * MD + mi) + dvds * LdT<T>(vm + 6 * MD + mi) +
+              dvdt * LdT<T>(vm + 9 * MD + mi);
       V[n] = Var[n * MD + l];
     }
     // Entropy -> primitive variables, velocity and internal-energy gradients
     // (src/ElementClass.cpp:4183-4257).
-    double rho, u, v, w, p, eKin;
+    T rho, u, v, w, p, eKin;
     EntropyToPrim(V[0], V[1], V[2], V[3], V[4], rho, u, v, w, p, eKin);
-    const double V4Inv = 1.0 / V[4];
-    const double rE = -p * ov1mg + rho * eKin;
-    const double dudx = -V4Inv * (gx[1] + u * gx[4]), dudy = -V4Inv * (gy[1] + u * gy[4]),
+    const T V4Inv = T(1.0) / V[4];
+    const T rE = -p * ov1mg + rho * eKin;
+    const T dudx = -V4Inv * (gx[1] + u * gx[4]), dudy = -V4Inv * (gy[1] + u * gy[4]),
                  dudz = -V4Inv * (gz[1] + u * gz[4]);
-    const double dvdx = -V4Inv * (gx[2] + v * gx[4]), dvdy = -V4Inv * (gy[2] + v * gy[4]),
+    const T dvdx = -V4Inv * (gx[2] + v * gx[4]), dvdy = -V4Inv * (gy[2] + v * gy[4]),
                  dvdz = -V4Inv * (gz[2] + v * gz[4]);
-    const double dwdx = -V4Inv * (gx[3] + w * gx[4]), dwdy = -V4Inv * (gy[3] + w * gy[4]),
+    const T dwdx = -V4Inv * (gx[3] + w * gx[4]), dwdy = -V4Inv * (gy[3] + w * gy[4]),
                  dwdz = -V4Inv * (gz[3] + w * gz[4]);
-    const double fact = -V4Inv * V4Inv * ov1mg;
-    const double dedx = gx[4] * fact, dedy = gy[4] * fact, dedz = gz[4] * fact;
-    const double rH = rE + p;
+    const T fact = -V4Inv * V4Inv * ov1mg;
+    const T dedx = gx[4] * fact, dedy = gy[4] * fact, dedz = gz[4] * fact;
+    const T rH = rE + p;
     s_cgp[0 * MD + l] = rho;
     s_cgp[1 * MD + l] = u;
     s_cgp[2 * MD + l] = v;
@@ -204,37 +206,37 @@ __device__ __forceinline__ void VolumePhase(const ResidualArgs &a, const int e,
     s_cgp[4 * MD + l] = p;
     s_cgp[5 * MD + l] = rE;
     s_cgp[6 * MD + l] = rE * rH / rho + p * eKin;  // dUdV(4,4)
-    mach2 = fmax(mach2, rho * (u * u + v * v + w * w) / (kGam * p));
+    mach2 = Fmax(mach2, rho * (u * u + v * v + w * w) / (T(kGam) * p));
 
     // Inviscid + viscous fluxes times -J w and the metric (src/ElementClass.cpp:4320-4416).
-    const double Wl = c_ops[SLOT].w[i] * c_ops[SLOT].w[j] * c_ops[SLOT].w[k];
-    const double Jl = __ldg(vm + l);
+    const T Wl = Weight1D<SLOT, T>(i) * Weight1D<SLOT, T>(j) * Weight1D<SLOT, T>(k);
+    const T Jl = LdT<T>(vm + l);
     s_jw[l] = Wl * Jl;
-    const double weight = -Jl * Wl;
-    const double ru = rho * u, rv = rho * v, rw = rho * w;
-    const double muTot = a.mu + 0.0;
-    const double factHeatFluxTot = a.mu * kFactHFLam + 0.0 * kFactHFTurb;
-    const double divVelTerm = kLamOverMu * (dudx + dvdy + dwdz);
-    const double tauxx = muTot * (2.0 * dudx + divVelTerm);
-    const double tauyy = muTot * (2.0 * dvdy + divVelTerm);
-    const double tauzz = muTot * (2.0 * dwdz + divVelTerm);
-    const double tauxy = muTot * (dudy + dvdx);
-    const double tauxz = muTot * (dudz + dwdx);
-    const double tauyz = muTot * (dvdz + dwdy);
-    const double qx = -factHeatFluxTot * dedx, qy = -factHeatFluxTot * dedy,
+    const T weight = -Jl * Wl;
+    const T ru = rho * u, rv = rho * v, rw = rho * w;
+    const T muTot = a.mu + T(0.0);
+    const T factHeatFluxTot = a.mu * T(kFactHFLam) + T(0.0) * T(kFactHFTurb);
+    const T divVelTerm = T(kLamOverMu) * (dudx + dvdy + dwdz);
+    const T tauxx = muTot * (T(2.0) * dudx + divVelTerm);
+    const T tauyy = muTot * (T(2.0) * dvdy + divVelTerm);
+    const T tauzz = muTot * (T(2.0) * dwdz + divVelTerm);
+    const T tauxy = muTot * (dudy + dvdx);
+    const T tauxz = muTot * (dudz + dwdx);
+    const T tauyz = muTot * (dvdz + dwdy);
+    const T qx = -factHeatFluxTot * dedx, qy = -factHeatFluxTot * dedy,
                  qz = -factHeatFluxTot * dedz;
-    const double fx[5] = {ru, ru * u - tauxx + p, rv * u - tauxy, rw * u - tauxz,
+    const T fx[5] = {ru, ru * u - tauxx + p, rv * u - tauxy, rw * u - tauxz,
                           (rE + p) * u - (u * tauxx + v * tauxy + w * tauxz - qx)};
-    const double fy[5] = {rv, ru * v - tauxy, rv * v - tauyy + p, rw * v - tauyz,
+    const T fy[5] = {rv, ru * v - tauxy, rv * v - tauyy + p, rw * v - tauyz,
                           (rE + p) * v - (u * tauxy + v * tauyy + w * tauyz - qy)};
-    const double fz[5] = {rw, ru * w - tauxz, rv * w - tauyz, rw * w - tauzz + p,
+    const T fz[5] = {rw, ru * w - tauxz, rv * w - tauyz, rw * w - tauzz + p,
                           (rE + p) * w - (u * tauxz + v * tauyz + w * tauzz - qz)};
-    const double drdx = weight * __ldg(vm + 1 * MD + l), drdy = weight * __ldg(vm + 2 * MD + l),
-                 drdz = weight * __ldg(vm + 3 * MD + l);
-    const double dsdx = weight * __ldg(vm + 4 * MD + l), dsdy = weight * __ldg(vm + 5 * MD + l),
-                 dsdz = weight * __ldg(vm + 6 * MD + l);
-    const double dtdx = weight * __ldg(vm + 7 * MD + l), dtdy = weight * __ldg(vm + 8 * MD + l),
-                 dtdz = weight * __ldg(vm + 9 * MD + l);
+    const T drdx = weight * LdT<T>(vm + 1 * MD + l), drdy = weight * LdT<T>(vm + 2 * MD + l),
+                 drdz = weight * LdT<T>(vm + 3 * MD + l);
+    const T dsdx = weight * LdT<T>(vm + 4 * MD + l), dsdy = weight * LdT<T>(vm + 5 * MD + l),
+                 dsdz = weight * LdT<T>(vm + 6 * MD + l);
+    const T dtdx = weight * LdT<T>(vm + 7 * MD + l), dtdy = weight * LdT<T>(vm + 8 * MD + l),
+                 dtdz = weight * LdT<T>(vm + 9 * MD + l);
 #pragma unroll
     for (int n = 0; n < 5; ++n) {
       dX[n * MD + l] = fx[n] * drdx + fy[n] * drdy + fz[n] * drdz;
@@ -243,8 +245,8 @@ __device__ __forceinline__ void VolumePhase(const ResidualArgs &a, const int e,
     }
   }
   if (a.mach2max) {
-    const double m = BlockMax<NT>(mach2, s_red);
-    if (threadIdx.x == 0) atomicMax(a.mach2max, (unsigned long long)__double_as_longlong(m));
+    const T m = BlockMax<NT>(mach2, s_red);
+    if (threadIdx.x == 0) atomicMax(a.mach2max, (unsigned long long)__double_as_longlong((double)m));
   }
   __syncthreads();
 
@@ -289,11 +291,11 @@ __device__ __forceinline__ int DerivSlot(const int d, const int p) {
 }
 
 // Face-normal evaluation of the six sides of a group (first stage of TPSAG[IJK]).
-template <int NT, int SLOT, int K>
-__device__ __forceinline__ void FaceNormalBatch(const double *s_sol, const double *gsol,
+template <int NT, int SLOT, int K, typename T>
+__device__ __forceinline__ void FaceNormalBatch(const T *s_sol, const double *gsol,
                                                 const int nb0, const int nb1, const int nb2,
-                                                const int g, const double *s_fv, double *bn,
-                                                double *bnd) {
+                                                const int g, const T *s_fv, T *bn,
+                                                T *bnd) {
   constexpr int KD = K * K * K, L = 5 * K * K;
   for (int line = threadIdx.x; line < 6 * L; line += NT) {
     const int t = line / L, r = line - t * L;
@@ -305,26 +307,26 @@ __device__ __forceinline__ void FaceNormalBatch(const double *s_sol, const doubl
     else if (d == 1) { base = sl * K * K + f; ns = K; }
     else { base = sl * K + f; ns = K * K; }
     base += v * KD;
-    const double *fv = s_fv + side * K, *dfv = s_fv + (2 + side) * K;
-    double a0 = 0.0, d0 = 0.0;
+    const T *fv = s_fv + side * K, *dfv = s_fv + (2 + side) * K;
+    T a0 = T(0.0), d0 = T(0.0);
     if (nbr) {
       const int nb = d == 0 ? nb0 : (d == 1 ? nb1 : nb2);
       if (nb >= 0) {
         const double *b = gsol + (size_t)nb * 5 * KD + base;
 #pragma unroll
         for (int n = 0; n < K; ++n) {
-          const double x = __ldg(b + n * ns);
-          a0 = fma(fv[n], x, a0);
-          d0 = fma(dfv[n], x, d0);
+          const T x = LdT<T>(b + n * ns);
+          a0 = Fma(fv[n], x, a0);
+          d0 = Fma(dfv[n], x, d0);
         }
       }
     } else {
-      const double *b = s_sol + base;
+      const T *b = s_sol + base;
 #pragma unroll
       for (int n = 0; n < K; ++n) {
-        const double x = b[n * ns];
-        a0 = fma(fv[n], x, a0);
-        d0 = fma(dfv[n], x, d0);
+        const T x = b[n * ns];
+        a0 = Fma(fv[n], x, a0);
+        d0 = Fma(dfv[n], x, d0);
       }
     }
     bn[line] = a0;
@@ -333,24 +335,24 @@ __device__ __forceinline__ void FaceNormalBatch(const double *s_sol, const doubl
 }
 
 // Parametric -> Cartesian gradient of one side at face point pt from TR.
-template <int M2>
-__device__ __forceinline__ void TraceCartesianGrad(const double *TR, const int t, const int d,
+template <int M2, typename T>
+__device__ __forceinline__ void TraceCartesianGrad(const T *TR, const int t, const int d,
                                                    const int pt, const double *fm,
-                                                   const int compat, double *gx, double *gy,
-                                                   double *gz) {
+                                                   const int compat, T *gx, T *gy,
+                                                   T *gz) {
   const int qr = DerivSlot(d, 0), qs = DerivSlot(d, 1), qt = DerivSlot(d, 2);
 #pragma unroll
   for (int n = 0; n < 5; ++n) {
     const int mi = compat ? n : pt;
-    const double dvdr = TR[((qr * 6 + t) * 5 + n) * M2 + pt];
-    const double dvds = TR[((qs * 6 + t) * 5 + n) * M2 + pt];
-    const double dvdt = TR[((qt * 6 + t) * 5 + n) * M2 + pt];
-    gx[n] = dvdr * __ldg(fm + 4 * M2 + mi) + dvds * __ldg(fm + 7 * M2 + mi) +
-            dvdt * __ldg(fm + 10 * M2 + mi);
-    gy[n] = dvdr * __ldg(fm + 5 * M2 + mi) + dvds * __ldg(fm + 8 * M2 + mi) +
-            dvdt * __ldg(fm + 11 * M2 + mi);
-    gz[n] = dvdr * __ldg(fm + 6 * M2 + mi) + dvds * __ldg(fm + 9 * M2 + mi) +
-            dvdt * __ldg(fm + 12 * M2 + mi);
+    const T dvdr = TR[((qr * 6 + t) * 5 + n) * M2 + pt];
+    const T dvds = TR[((qs * 6 + t) * 5 + n) * M2 + pt];
+    const T dvdt = TR[((qt * 6 + t) * 5 + n) * M2 + pt];
+    gx[n] = dvdr * LdT<T>(fm + 4 * M2 + mi) + dvds * LdT<T>(fm + 7 * M2 + mi) +
+            dvdt * LdT<T>(fm + 10 * M2 + mi);
+    gy[n] = dvdr * LdT<T>(fm + 5 * M2 + mi) + dvds * LdT<T>(fm + 8 * M2 + mi) +
+            dvdt * LdT<T>(fm + 11 * M2 + mi);
+    gz[n] = dvdr * LdT<T>(fm + 6 * M2 + mi) + dvds * LdT<T>(fm + 9 * M2 + mi) +
+            dvdt * LdT<T>(fm + 12 * M2 + mi);
   }
 }
 
@@ -359,18 +361,18 @@ __device__ __forceinline__ void TraceCartesianGrad(const double *TR, const int t
 // P1[role][d][v][M2] with role 0 fast-axis symmetrizing flux, 1 normal flux (with
 // the own side's sign), 2 face-normal symmetrizing flux; P2[d][v][M2] the
 // slow-axis symmetrizing flux.
-template <int K, int M>
+template <int K, int M, typename T>
 __device__ __forceinline__ void GroupFacePoint(const ResidualArgs &a, const int g, const int d,
-                                               const int pt, const double *TR,
+                                               const int pt, const T *TR,
                                                const double *fmOwn, const double *fmNb,
-                                               const double lenScale, double *P1, double *P2) {
+                                               const T lenScale, T *P1, T *P2) {
   constexpr int SLOT = Slot<K, M>::value;
   constexpr int M2 = M * M;
   const int tOwn = 2 * d, tNb = 2 * d + 1;
   // g == 0: own Min face, the neighbour is the left state; g == 1: own Max face.
   const int tL = g == 0 ? tNb : tOwn, tR = g == 0 ? tOwn : tNb;
   const double *fmL = g == 0 ? fmNb : fmOwn, *fmR = g == 0 ? fmOwn : fmNb;
-  double VL[5], VR[5], gxL[5], gyL[5], gzL[5], gxR[5], gyR[5], gzR[5];
+  T VL[5], VR[5], gxL[5], gyL[5], gzL[5], gxR[5], gyR[5], gzR[5];
 #pragma unroll
   for (int n = 0; n < 5; ++n) {
     VL[n] = TR[(tL * 5 + n) * M2 + pt];
@@ -378,37 +380,37 @@ __device__ __forceinline__ void GroupFacePoint(const ResidualArgs &a, const int 
   }
   TraceCartesianGrad<M2>(TR, tL, d, pt, fmL, a.metric_compat, gxL, gyL, gzL);
   TraceCartesianGrad<M2>(TR, tR, d, pt, fmR, a.metric_compat, gxR, gyR, gzR);
-  double gx[5], gy[5], gz[5];
+  T gx[5], gy[5], gz[5];
 #pragma unroll
   for (int n = 0; n < 5; ++n) {
-    gx[n] = 0.5 * (gxL[n] + gxR[n]);
-    gy[n] = 0.5 * (gyL[n] + gyR[n]);
-    gz[n] = 0.5 * (gzL[n] + gzR[n]);
+    gx[n] = T(0.5) * (gxL[n] + gxR[n]);
+    gy[n] = T(0.5) * (gyL[n] + gyR[n]);
+    gz[n] = T(0.5) * (gzL[n] + gzR[n]);
   }
   const int f = pt % M, sl = pt / M;
-  const double wf = c_ops[SLOT].w[f] * c_ops[SLOT].w[sl];
-  const double nx = 1.0 * __ldg(fmL + 0 * M2 + pt), ny = 1.0 * __ldg(fmL + 1 * M2 + pt),
-               nz = 1.0 * __ldg(fmL + 2 * M2 + pt);
-  const double area = __ldg(fmL + 3 * M2 + pt);
-  double flux[5];
+  const T wf = Weight1D<SLOT, T>(f) * Weight1D<SLOT, T>(sl);
+  const T nx = T(1.0) * LdT<T>(fmL + 0 * M2 + pt), ny = T(1.0) * LdT<T>(fmL + 1 * M2 + pt),
+               nz = T(1.0) * LdT<T>(fmL + 2 * M2 + pt);
+  const T area = LdT<T>(fmL + 3 * M2 + pt);
+  T flux[5];
   if (a.riemann == 1)
     IsmailRoeFlux(VL, VR, nx, ny, nz, wf * area, flux);
   else
-    RoeFlux(VL, VR, nx, ny, nz, 0.5 * wf * area, flux);
-  double sx[5], sy[5], sz[5];
-  ViscousPenaltySymFlux(VL, VR, gx, gy, gz, nx, ny, nz, 1.0, wf, area, a.mu,
-                        a.tau_num / lenScale, a.theta_sym, flux, sx, sy, sz);
+    RoeFlux(VL, VR, nx, ny, nz, T(0.5) * wf * area, flux);
+  T sx[5], sy[5], sz[5];
+  ViscousPenaltySymFlux(VL, VR, gx, gy, gz, nx, ny, nz, T(1.0), wf, area, T(a.mu),
+                        T(a.tau_num) / lenScale, T(a.theta_sym), flux, sx, sy, sz);
   const double *fm = g == 0 ? fmR : fmL;  // the own side's metric
   const int pFast = FastParam(d);
 #pragma unroll
   for (int n = 0; n < 5; ++n) {
     const int mi = a.metric_compat ? n : pt;
-    double sym[3];
+    T sym[3];
 #pragma unroll
     for (int p = 0; p < 3; ++p)
-      sym[p] = sx[n] * __ldg(fm + (4 + 3 * p) * M2 + mi) +
-               sy[n] * __ldg(fm + (5 + 3 * p) * M2 + mi) +
-               sz[n] * __ldg(fm + (6 + 3 * p) * M2 + mi);
+      sym[p] = sx[n] * LdT<T>(fm + (4 + 3 * p) * M2 + mi) +
+               sy[n] * LdT<T>(fm + (5 + 3 * p) * M2 + mi) +
+               sz[n] * LdT<T>(fm + (6 + 3 * p) * M2 + mi);
     const int o = (d * 5 + n) * M2 + pt;
     P1[1 * 15 * M2 + o] = g == 0 ? -flux[n] : flux[n];
     P1[2 * 15 * M2 + o] = sym[d];
@@ -417,18 +419,18 @@ __device__ __forceinline__ void GroupFacePoint(const ResidualArgs &a, const int 
   }
 }
 
-template <int NT, int K, int M>
-__device__ __forceinline__ void FacePhase(const ResidualArgs &a, const int e, const double *s_sol,
-                                          double *s_R, const double *s_fv, double *work) {
+template <int NT, int K, int M, typename T>
+__device__ __forceinline__ void FacePhase(const ResidualArgs &a, const int e, const T *s_sol,
+                                          T *s_R, const T *s_fv, T *work) {
   constexpr int SLOT = Slot<K, M>::value;
   constexpr int KD = K * K * K, M2 = M * M, K2 = K * K;
   static_assert(2 * M <= 3 * K && K <= 2 * M, "face-phase buffer aliasing");
-  double *BN = work, *BND = BN + 30 * K2;        // 60 K^2
-  double *T1a = BND + 30 * K2, *T1b = T1a + 30 * K * M, *T1c = T1b + 30 * K * M;  // 90 K M
-  double *TR = T1c + 30 * K * M;                 // 120 M^2
-  double *P1 = T1a, *P2 = T1a + 45 * M2;         // distribution inputs (in T1)
-  double *Q1 = TR, *Q2 = TR + 45 * K * M;        // after the slow-axis contraction (in TR)
-  double *RF = BN, *RFN = RF + 15 * K2, *RS = RFN + 30 * K2;  // after the fast axis (in BN)
+  T *BN = work, *BND = BN + 30 * K2;        // 60 K^2
+  T *T1a = BND + 30 * K2, *T1b = T1a + 30 * K * M, *T1c = T1b + 30 * K * M;  // 90 K M
+  T *TR = T1c + 30 * K * M;                 // 120 M^2
+  T *P1 = T1a, *P2 = T1a + 45 * M2;         // distribution inputs (in T1)
+  T *Q1 = TR, *Q2 = TR + 45 * K * M;        // after the slow-axis contraction (in TR)
+  T *RF = BN, *RFN = RF + 15 * K2, *RS = RFN + 30 * K2;  // after the fast axis (in BN)
   const double *sc = a.elem_scalars + (size_t)e * 15;
   for (int g = 0; g < 2; ++g) {
     const int nb0 = a.nbr[e * 6 + 0 + g], nb1 = a.nbr[e * 6 + 2 + g], nb2 = a.nbr[e * 6 + 4 + g];
@@ -453,11 +455,11 @@ __device__ __forceinline__ void FacePhase(const ResidualArgs &a, const int e, co
         if (pt == 0) atomicAdd(a.status + 1, 1);
         for (int n = 0; n < 5; ++n) {
           const int o = (d * 5 + n) * M2 + pt;
-          P1[o] = P1[15 * M2 + o] = P1[30 * M2 + o] = P2[o] = 0.0;
+          P1[o] = P1[15 * M2 + o] = P1[30 * M2 + o] = P2[o] = T(0.0);
         }
         continue;
       }
-      const double lenScale = fmin(sc[d], a.elem_scalars[(size_t)nb * 15 + d]);
+      const T lenScale = Fmin(T(sc[d]), T(a.elem_scalars[(size_t)nb * 15 + d]));
       const double *fmOwn = a.face_metric + ((size_t)e * 6 + 2 * d + g) * 13 * M2;
       const double *fmNb = a.face_metric + ((size_t)nb * 6 + 2 * d + 1 - g) * 13 * M2;
       GroupFacePoint<K, M>(a, g, d, pt, TR, fmOwn, fmNb, lenScale, P1, P2);
@@ -471,27 +473,27 @@ __device__ __forceinline__ void FacePhase(const ResidualArgs &a, const int e, co
     Contract<NT, SLOT, K, M, kLegT, 0, 30, M, K, 1, M, K, false>(Q1 + 15 * K * M, RFN);
     Contract<NT, SLOT, K, M, kLegT, 0, 15, M, K, 1, M, K, false>(Q2, RS);
     __syncthreads();
-    const double *fv = s_fv + g * K, *dfv = s_fv + (2 + g) * K;
+    const T *fv = s_fv + g * K, *dfv = s_fv + (2 + g) * K;
     for (int idx = threadIdx.x; idx < 5 * KD; idx += NT) {
       const int v = idx / KD, r = idx - v * KD;
       const int k = r / K2, r2 = r - k * K2, j = r2 / K, i = r2 - j * K;
-      double acc = s_R[idx];
+      T acc = s_R[idx];
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
         const int n = d == 0 ? i : (d == 1 ? j : k);
         const int sf = d == 0 ? k * K + j : (d == 1 ? k * K + i : j * K + i);
         const int o = (d * 5 + v) * K2 + sf;
-        const double aF = fv[n], aD = dfv[n];
-        const double tFlux = RFN[o], tN = RFN[15 * K2 + o], tFast = RF[o], tSlow = RS[o];
+        const T aF = fv[n], aD = dfv[n];
+        const T tFlux = RFN[o], tN = RFN[15 * K2 + o], tFast = RF[o], tSlow = RS[o];
         // Reference order: normal flux, then the r, s, t symmetrizing fluxes.
         const int pFast = FastParam(d);
-        double c = g == 0 ? acc : 0.0;
-        c = fma(aF, tFlux, c);
+        T c = g == 0 ? acc : T(0.0);
+        c = Fma(aF, tFlux, c);
 #pragma unroll
         for (int p = 0; p < 3; ++p) {
-          if (p == d) c = fma(aD, tN, c);
-          else if (p == pFast) c = fma(aF, tFast, c);
-          else c = fma(aF, tSlow, c);
+          if (p == d) c = Fma(aD, tN, c);
+          else if (p == pFast) c = Fma(aF, tFast, c);
+          else c = Fma(aF, tSlow, c);
         }
         acc = g == 0 ? c : acc + c;
       }
@@ -508,49 +510,49 @@ __device__ __forceinline__ void FacePhase(const ResidualArgs &a, const int e, co
 // 100 iterations (the cap raises a status flag instead of aborting).
 // r is s_R (overwritten); the solution is returned in x.
 // ---------------------------------------------------------------------------
-template <int NT, int K, int M>
-__device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, const double *s_sol,
-                                          double *s_R, const double *s_cgp, const double *s_jw,
-                                          double *work, double *s_red, double *&xOut) {
+template <int NT, int K, int M, typename T>
+__device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, const T *s_sol,
+                                          T *s_R, const T *s_cgp, const T *s_jw,
+                                          T *work, T *s_red, T *&xOut) {
   constexpr int SLOT = Slot<K, M>::value;
-  using P = Plan<K, M>;
+  using P = Plan<K, M, T>;
   constexpr int KD = P::KD, MD = P::MD;
-  double *z = work, *p = z + 5 * KD, *Ap = p + 5 * KD, *x = Ap + 5 * KD;
-  double *pInt = x + 5 * KD, *tK = pInt + 5 * MD, *tJ = tK + P::TK;
-  double *dvdu = s_red + 32;  // 15 preconditioner entries
-  double *r = s_R;
+  T *z = work, *p = z + 5 * KD, *Ap = p + 5 * KD, *x = Ap + 5 * KD;
+  T *pInt = x + 5 * KD, *tK = pInt + 5 * MD, *tJ = tK + P::TK;
+  T *dvdu = s_red + 32;  // 15 preconditioner entries
+  T *r = s_R;
   xOut = x;
-  const double volElem = a.elem_scalars[(size_t)e * 15 + 5];
-  const double JacInv = 8.0 / volElem;
+  const T volElem = a.elem_scalars[(size_t)e * 15 + 5];
+  const T JacInv = T(8.0) / volElem;
 
-  double m = 0.0;
+  T m = T(0.0);
   for (int i = threadIdx.x; i < 5 * KD; i += NT) {
-    m = fmax(m, fabs(r[i]));
-    x[i] = 0.0;
+    m = Fmax(m, Fabs(r[i]));
+    x[i] = T(0.0);
   }
-  const double rInitMax = BlockMax<NT>(m, s_red);
-  if (!(rInitMax * JacInv > 1.e-10)) return;
+  const T rInitMax = BlockMax<NT>(m, s_red);
+  if (!(rInitMax * JacInv > T(1.e-10))) return;
 
   // Entropy variables at the element centre and dV/dU there (src/CG_MassMatrix.cpp:313-361).
   if (threadIdx.x < 5) {
-    double V = 0.0;
-    for (int l = 0; l < KD; ++l) V += c_ops[SLOT].center[l] * s_sol[threadIdx.x * KD + l];
+    T V = T(0.0);
+    for (int l = 0; l < KD; ++l) V += CenterBasis<SLOT, T>(l) * s_sol[threadIdx.x * KD + l];
     dvdu[threadIdx.x + 16] = V;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    const double gm1 = kGam - 1.0, ov1mg = 1.0 / (1.0 - kGam), govgm1 = kGam / gm1;
-    const double V0 = dvdu[16], V1 = dvdu[17], V2 = dvdu[18], V3 = dvdu[19], V4 = dvdu[20];
-    const double V4Inv = 1.0 / V4;
-    const double u = -V4Inv * V1, v = -V4Inv * V2, w = -V4Inv * V3;
-    const double eKin = 0.5 * (u * u + v * v + w * w);
-    const double sEnt = kGam - gm1 * (V0 - V4 * eKin);
-    const double tmp = -V4 * exp(sEnt);
-    const double rho = pow(tmp, ov1mg);
-    const double pr = -rho * V4Inv;
-    const double pInv = 1.0 / pr;
-    const double abv1 = gm1 * rho * pInv * pInv;
-    const double abv2 = eKin * abv1;
+    const T gm1 = T(kGam) - T(1.0), ov1mg = T(1.0) / (T(1.0) - T(kGam)), govgm1 = T(kGam) / gm1;
+    const T V0 = dvdu[16], V1 = dvdu[17], V2 = dvdu[18], V3 = dvdu[19], V4 = dvdu[20];
+    const T V4Inv = T(1.0) / V4;
+    const T u = -V4Inv * V1, v = -V4Inv * V2, w = -V4Inv * V3;
+    const T eKin = T(0.5) * (u * u + v * v + w * w);
+    const T sEnt = T(kGam) - gm1 * (V0 - V4 * eKin);
+    const T tmp = -V4 * exp(sEnt);
+    const T rho = pow(tmp, ov1mg);
+    const T pr = -rho * V4Inv;
+    const T pInv = T(1.0) / pr;
+    const T abv1 = gm1 * rho * pInv * pInv;
+    const T abv2 = eKin * abv1;
     dvdu[0] = JacInv * (govgm1 / rho + abv2 * eKin);
     dvdu[1] = -JacInv * u * abv2;
     dvdu[2] = -JacInv * v * abv2;
@@ -568,12 +570,12 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
     dvdu[14] = JacInv * abv1;
   }
   __syncthreads();
-  double D[15];
+  T D[15];
 #pragma unroll
   for (int q = 0; q < 15; ++q) D[q] = dvdu[q];
   auto precond = [&](void) {
     for (int l = threadIdx.x; l < KD; l += NT) {
-      const double r0 = r[l], r1 = r[KD + l], r2 = r[2 * KD + l], r3 = r[3 * KD + l],
+      const T r0 = r[l], r1 = r[KD + l], r2 = r[2 * KD + l], r3 = r[3 * KD + l],
                    r4 = r[4 * KD + l];
       z[l] = D[0] * r0 + D[1] * r1 + D[2] * r2 + D[3] * r3 + D[4] * r4;
       z[KD + l] = D[1] * r0 + D[5] * r1 + D[6] * r2 + D[7] * r3 + D[8] * r4;
@@ -584,12 +586,12 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
   };
   precond();
   __syncthreads();
-  double part = 0.0;
+  T part = T(0.0);
   for (int i = threadIdx.x; i < 5 * KD; i += NT) {
     p[i] = z[i];
-    part = fma(r[i], z[i], part);
+    part = Fma(r[i], z[i], part);
   }
-  double dotrz = BlockSum<NT>(part, s_red);
+  T dotrz = BlockSum<NT>(part, s_red);
 
   int iter = 0;
   for (;; ++iter) {
@@ -605,13 +607,13 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
     Contract<NT, SLOT, K, M, kLeg, 0, 5, K, M, M, K, M, false>(tJ, pInt);
     __syncthreads();
     for (int l = threadIdx.x; l < MD; l += NT) {
-      const double iw = s_jw[l];
-      const double p0 = iw * pInt[l], p1 = iw * pInt[MD + l], p2 = iw * pInt[2 * MD + l],
+      const T iw = s_jw[l];
+      const T p0 = iw * pInt[l], p1 = iw * pInt[MD + l], p2 = iw * pInt[2 * MD + l],
                    p3 = iw * pInt[3 * MD + l], p4 = iw * pInt[4 * MD + l];
-      const double rho = s_cgp[l], u = s_cgp[MD + l], v = s_cgp[2 * MD + l],
+      const T rho = s_cgp[l], u = s_cgp[MD + l], v = s_cgp[2 * MD + l],
                    w = s_cgp[3 * MD + l], pr = s_cgp[4 * MD + l], rE = s_cgp[5 * MD + l];
-      const double ru = rho * u, rv = rho * v, rw = rho * w, rH = rE + pr;
-      const double d0 = rho, d1 = ru, d2 = rv, d3 = rw, d4 = rE, d5 = ru * u + pr, d6 = ru * v,
+      const T ru = rho * u, rv = rho * v, rw = rho * w, rH = rE + pr;
+      const T d0 = rho, d1 = ru, d2 = rv, d3 = rw, d4 = rE, d5 = ru * u + pr, d6 = ru * v,
                    d7 = ru * w, d8 = rH * u, d9 = rv * v + pr, d10 = rv * w, d11 = rH * v,
                    d12 = rw * w + pr, d13 = rH * w, d14 = s_cgp[6 * MD + l];
       pInt[l] = d0 * p0 + d1 * p1 + d2 * p2 + d3 * p3 + d4 * p4;
@@ -627,22 +629,22 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
     __syncthreads();
     Contract<NT, SLOT, K, M, kLegT, 0, 5, M, K, K, M, K, false>(tK, Ap);
     __syncthreads();
-    part = 0.0;
-    for (int i = threadIdx.x; i < 5 * KD; i += NT) part = fma(p[i], Ap[i], part);
-    const double alpha = dotrz / BlockSum<NT>(part, s_red);
+    part = T(0.0);
+    for (int i = threadIdx.x; i < 5 * KD; i += NT) part = Fma(p[i], Ap[i], part);
+    const T alpha = dotrz / BlockSum<NT>(part, s_red);
     // Each thread owns whole DOFs: update x and r, precondition, and form the
     // partial sums of the three reductions that close the iteration.
-    double zAp = 0.0, rzNew = 0.0, rMax = 0.0;
+    T zAp = T(0.0), rzNew = T(0.0), rMax = T(0.0);
     for (int l = threadIdx.x; l < KD; l += NT) {
-      double rr[5];
+      T rr[5];
 #pragma unroll
       for (int q = 0; q < 5; ++q) {
-        x[q * KD + l] = fma(alpha, p[q * KD + l], x[q * KD + l]);
-        rr[q] = fma(-alpha, Ap[q * KD + l], r[q * KD + l]);
+        x[q * KD + l] = Fma(alpha, p[q * KD + l], x[q * KD + l]);
+        rr[q] = Fma(-alpha, Ap[q * KD + l], r[q * KD + l]);
         r[q * KD + l] = rr[q];
-        rMax = fmax(rMax, fabs(rr[q]));
+        rMax = Fmax(rMax, Fabs(rr[q]));
       }
-      const double zz[5] = {
+      const T zz[5] = {
           D[0] * rr[0] + D[1] * rr[1] + D[2] * rr[2] + D[3] * rr[3] + D[4] * rr[4],
           D[1] * rr[0] + D[5] * rr[1] + D[6] * rr[2] + D[7] * rr[3] + D[8] * rr[4],
           D[2] * rr[0] + D[6] * rr[1] + D[9] * rr[2] + D[10] * rr[3] + D[11] * rr[4],
@@ -651,13 +653,13 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
 #pragma unroll
       for (int q = 0; q < 5; ++q) {
         z[q * KD + l] = zz[q];
-        zAp = fma(zz[q], Ap[q * KD + l], zAp);
-        rzNew = fma(rr[q], zz[q], rzNew);
+        zAp = Fma(zz[q], Ap[q * KD + l], zAp);
+        rzNew = Fma(rr[q], zz[q], rzNew);
       }
     }
     BlockReduce3<NT>(zAp, rzNew, rMax, s_red);
-    if (rMax < 1.e-10 * rInitMax) break;
-    const double beta = -alpha * zAp / dotrz;
+    if (rMax < T(a.cg_tol) * rInitMax) break;
+    const T beta = -alpha * zAp / dotrz;
     dotrz = rzNew;
     for (int i = threadIdx.x; i < 5 * KD; i += NT) p[i] = beta * p[i] + z[i];
     __syncthreads();
@@ -671,34 +673,35 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
 // ---------------------------------------------------------------------------
 // The fused kernel.
 // ---------------------------------------------------------------------------
-template <int K, int M, int NT>
-__global__ void __launch_bounds__(NT, Plan<K, M>::MIN_BLOCKS) ResidualKernel(const ResidualArgs a) {
-  using P = Plan<K, M>;
+template <int K, int M, int NT, typename T>
+__global__ void __launch_bounds__(NT, Plan<K, M, T>::MIN_BLOCKS) ResidualKernel(const ResidualArgs a) {
+  using P = Plan<K, M, T>;
   constexpr int KD = P::KD, MD = P::MD;
-  extern __shared__ double smem[];
-  double *s_sol = smem, *s_R = s_sol + 5 * KD, *s_cgp = s_R + 5 * KD, *s_jw = s_cgp + 8 * MD;
-  double *s_red = s_jw + MD, *s_fv = s_red + 64, *work = s_fv + 4 * kKMax;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *smem = reinterpret_cast<T *>(smem_raw);
+  T *s_sol = smem, *s_R = s_sol + 5 * KD, *s_cgp = s_R + 5 * KD, *s_jw = s_cgp + 8 * MD;
+  T *s_red = s_jw + MD, *s_fv = s_red + 64, *work = s_fv + 4 * kKMax;
   const int e = blockIdx.x;
   if (e >= a.n_elem) return;
   const double *src = a.sol + (size_t)e * 5 * KD;
-  for (int i = threadIdx.x; i < 5 * KD; i += NT) s_sol[i] = src[i];
+  for (int i = threadIdx.x; i < 5 * KD; i += NT) s_sol[i] = T(src[i]);
   if (threadIdx.x < 2 * K) {
-    s_fv[threadIdx.x] = c_ops[Slot<K, M>::value].face[threadIdx.x];
-    s_fv[2 * K + threadIdx.x] = c_ops[Slot<K, M>::value].dface[threadIdx.x];
+    s_fv[threadIdx.x] = FaceVal<Slot<K, M>::value, T>(threadIdx.x);
+    s_fv[2 * K + threadIdx.x] = FaceDer<Slot<K, M>::value, T>(threadIdx.x);
   }
   __syncthreads();
   VolumePhase<NT, K, M>(a, e, s_sol, s_R, s_cgp, s_jw, work, s_red);
   FacePhase<NT, K, M>(a, e, s_sol, s_R, s_fv, work);
   if (a.res_raw) {
     double *dst = a.res_raw + (size_t)e * 5 * KD;
-    for (int i = threadIdx.x; i < 5 * KD; i += NT) dst[i] = s_R[i];
+    for (int i = threadIdx.x; i < 5 * KD; i += NT) dst[i] = double(s_R[i]);
   }
   __syncthreads();
-  double *x;
+  T *x;
   MassSolve<NT, K, M>(a, e, s_sol, s_R, s_cgp, s_jw, work, s_red, x);
   __syncthreads();
   double *dst = a.res + (size_t)e * 5 * KD;
-  for (int i = threadIdx.x; i < 5 * KD; i += NT) dst[i] = x[i];
+  for (int i = threadIdx.x; i < 5 * KD; i += NT) dst[i] = double(x[i]);
 }
 
 }  // namespace vcpg

@@ -19,6 +19,8 @@
 
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 namespace vcpg {
 
 constexpr int kKMax = 7;   // up to polynomial degree 6
@@ -32,6 +34,13 @@ struct OpTable {
   double w[kMMax];                  // 1-D Gauss weights
   double legdof[kKMax * kKMax];     // legdof[k * K + i]: basis k at nodal DOF i
   double center[kKMax * kKMax * kKMax];
+  // FP32 copies for the mixed-precision form.
+  float legf[kKMax * kMMax];
+  float dlegf[kKMax * kMMax];
+  float facef[2 * kKMax];
+  float dfacef[2 * kKMax];
+  float wf[kMMax];
+  float centerf[kKMax * kKMax * kKMax];
 };
 
 // Supported (K, M) pairs and their constant-memory slot.
@@ -56,20 +65,50 @@ enum OpSel {
   kLegDof = 4  // K -> K: out[i] = sum_k legdof[k][i] in[k]   (modal -> nodal)
 };
 
-template <int SLOT, int K, int M, int OP>
-__device__ __forceinline__ double Coef(const int c, const int o) {
-  if (OP == kLeg) return c_ops[SLOT].leg[c * M + o];
-  if (OP == kDLeg) return c_ops[SLOT].dleg[c * M + o];
-  if (OP == kLegT) return c_ops[SLOT].leg[o * M + c];
-  if (OP == kLegDof) return c_ops[SLOT].legdof[c * K + o];
-  return c_ops[SLOT].dleg[o * M + c];
+template <int SLOT, int K, int M, int OP, typename T = double>
+__device__ __forceinline__ T Coef(const int c, const int o) {
+  if constexpr (std::is_same<T, float>::value) {
+    if (OP == kLeg) return c_ops[SLOT].legf[c * M + o];
+    if (OP == kDLeg) return c_ops[SLOT].dlegf[c * M + o];
+    if (OP == kLegT) return c_ops[SLOT].legf[o * M + c];
+    return c_ops[SLOT].dlegf[o * M + c];
+  } else {
+    if (OP == kLeg) return c_ops[SLOT].leg[c * M + o];
+    if (OP == kDLeg) return c_ops[SLOT].dleg[c * M + o];
+    if (OP == kLegT) return c_ops[SLOT].leg[o * M + c];
+    if (OP == kLegDof) return c_ops[SLOT].legdof[c * K + o];
+    return c_ops[SLOT].dleg[o * M + c];
+  }
+}
+
+// Face basis values (side 0: r = -1, side 1: r = +1), 1-D weights and the centre
+// basis in the compute precision.
+template <int SLOT, typename T>
+__device__ __forceinline__ T FaceVal(const int i) {
+  if constexpr (std::is_same<T, float>::value) return c_ops[SLOT].facef[i];
+  else return c_ops[SLOT].face[i];
+}
+template <int SLOT, typename T>
+__device__ __forceinline__ T FaceDer(const int i) {
+  if constexpr (std::is_same<T, float>::value) return c_ops[SLOT].dfacef[i];
+  else return c_ops[SLOT].dface[i];
+}
+template <int SLOT, typename T>
+__device__ __forceinline__ T Weight1D(const int i) {
+  if constexpr (std::is_same<T, float>::value) return c_ops[SLOT].wf[i];
+  else return c_ops[SLOT].w[i];
+}
+template <int SLOT, typename T>
+__device__ __forceinline__ T CenterBasis(const int i) {
+  if constexpr (std::is_same<T, float>::value) return c_ops[SLOT].centerf[i];
+  else return c_ops[SLOT].center[i];
 }
 
 // Apply a 1-D operator along axis AX of in[NV][D2][D1][D0] (D_AX == NIN) and
 // write (ACC: add) out[NV][D2'][D1'][D0'] where D_AX' == NOUT.
 template <int NT, int SLOT, int K, int M, int OP, int AX, int NV, int D0, int D1, int D2,
-          int NIN, int NOUT, bool ACC>
-__device__ __forceinline__ void Contract(const double *__restrict__ in, double *__restrict__ out) {
+          int NIN, int NOUT, bool ACC, typename T = double>
+__device__ __forceinline__ void Contract(const T *__restrict__ in, T *__restrict__ out) {
   constexpr int O0 = AX == 0 ? NOUT : D0;
   constexpr int O1 = AX == 1 ? NOUT : D1;
   constexpr int O2 = AX == 2 ? NOUT : D2;
@@ -95,72 +134,19 @@ __device__ __forceinline__ void Contract(const double *__restrict__ in, double *
       ib = v * D2 * D1 * D0 + b * D0 + a;
       ob = v * O2 * O1 * O0 + b * O0 + a;
     }
-    double x[NIN];
+    T x[NIN];
 #pragma unroll
     for (int c = 0; c < NIN; ++c) x[c] = in[ib + c * IS];
 #pragma unroll
     for (int o = 0; o < NOUT; ++o) {
-      double acc = 0.0;
+      T acc = T(0);
 #pragma unroll
-      for (int c = 0; c < NIN; ++c) acc = fma(Coef<SLOT, K, M, OP>(c, o), x[c], acc);
+      for (int c = 0; c < NIN; ++c) acc = fma(Coef<SLOT, K, M, OP, T>(c, o), x[c], acc);
       if (ACC)
         out[ob + o * OS] += acc;
       else
         out[ob + o * OS] = acc;
     }
-  }
-}
-
-// Face-normal evaluation of volume DOF data b[NV][K][K][K] (from shared or
-// global memory) on the face DIR (0: i, 1: j, 2: k) at side SIDE (0 min, 1 max):
-//   val[v][s][f] = sum_n face[SIDE][n] b(n, s, f),  der[...] with dface.
-// Output face layout [NV][K][K] with (slow, fast) = (k, j) for i-faces and
-// (k, i) / (j, i) for j- / k-faces.
-template <int NT, int SLOT, int K, int DIR, int NV, bool GLOBAL_SRC>
-__device__ __forceinline__ void FaceNormal(const double *__restrict__ b, const int side,
-                                           double *__restrict__ val, double *__restrict__ der) {
-  constexpr int NL = NV * K * K;
-  constexpr int NS = DIR == 0 ? 1 : (DIR == 1 ? K : K * K);  // stride of the normal axis
-  for (int line = threadIdx.x; line < NL; line += NT) {
-    const int v = line / (K * K);
-    const int r = line - v * K * K;
-    const int s = r / K;
-    const int f = r - s * K;
-    int base;
-    if (DIR == 0) base = v * K * K * K + s * K * K + f * K;  // (k, j), i normal
-    else if (DIR == 1) base = v * K * K * K + s * K * K + f;  // (k, i), j normal
-    else base = v * K * K * K + s * K + f;                    // (j, i), k normal
-    double a = 0.0, d = 0.0;
-#pragma unroll
-    for (int n = 0; n < K; ++n) {
-      const double x = GLOBAL_SRC ? __ldg(b + base + n * NS) : b[base + n * NS];
-      a = fma(c_ops[SLOT].face[side * K + n], x, a);
-      d = fma(c_ops[SLOT].dface[side * K + n], x, d);
-    }
-    val[line] = a;
-    der[line] = d;
-  }
-}
-
-// Last stage of the face-residual templates: res[v][k][j][i] +=
-// face[SIDE][n] * t[v][s][f] with n the face-normal index (DFACE: derivative).
-template <int NT, int SLOT, int K, int DIR, int NV, bool DFACE>
-__device__ __forceinline__ void FaceExpand(const double *__restrict__ t, const int side,
-                                           double *__restrict__ res) {
-  constexpr int N = NV * K * K * K;
-  for (int idx = threadIdx.x; idx < N; idx += NT) {
-    const int v = idx / (K * K * K);
-    const int r = idx - v * K * K * K;
-    const int k = r / (K * K);
-    const int r2 = r - k * K * K;
-    const int j = r2 / K;
-    const int i = r2 - j * K;
-    int n, s, f;
-    if (DIR == 0) { n = i; s = k; f = j; }
-    else if (DIR == 1) { n = j; s = k; f = i; }
-    else { n = k; s = j; f = i; }
-    const double a = DFACE ? c_ops[SLOT].dface[side * K + n] : c_ops[SLOT].face[side * K + n];
-    res[idx] = fma(a, t[(v * K + s) * K + f], res[idx]);
   }
 }
 

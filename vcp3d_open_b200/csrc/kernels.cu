@@ -106,19 +106,25 @@ __global__ void LsrkStageKernel(double *sol, double *du, const double *res, cons
 // ---------------------------------------------------------------------------
 // Launchers.
 // ---------------------------------------------------------------------------
-template <int K, int M>
-static cudaError_t LaunchResidualKM(const ResidualArgs &a, cudaStream_t st) {
-  constexpr int NT = Plan<K, M>::NT;
-  const size_t bytes = Plan<K, M>::BYTES;
+template <int K, int M, typename T>
+static cudaError_t LaunchResidualKMT(const ResidualArgs &a, cudaStream_t st) {
+  constexpr int NT = Plan<K, M, T>::NT;
+  const size_t bytes = Plan<K, M, T>::BYTES;
   static bool configured = false;
   if (!configured) {
-    cudaError_t err = cudaFuncSetAttribute(ResidualKernel<K, M, NT>,
+    cudaError_t err = cudaFuncSetAttribute(ResidualKernel<K, M, NT, T>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (err != cudaSuccess) return err;
     configured = true;
   }
-  ResidualKernel<K, M, NT><<<a.n_elem, NT, bytes, st>>>(a);
+  ResidualKernel<K, M, NT, T><<<a.n_elem, NT, bytes, st>>>(a);
   return cudaGetLastError();
+}
+
+// FP64 form or the mixed form (FP32 compute, FP64 inputs and outputs).
+template <int K, int M>
+static cudaError_t LaunchResidualKM(const ResidualArgs &a, cudaStream_t st) {
+  return a.mixed ? LaunchResidualKMT<K, M, float>(a, st) : LaunchResidualKMT<K, M, double>(a, st);
 }
 
 template <int K, int M>

@@ -200,10 +200,16 @@ class Solver:
         return int(self.lib.vcpg_launch_count(self.h))
 
 
-def create(case: CaseData, metric_compat: bool = True) -> Solver:
-    """Set-up + handle + initial state for a generated case."""
-    params = make_params(case, metric_compat=metric_compat)
-    disc = setup_discretization(case, params)
+def create(case: CaseData, metric_compat: bool = True, precision: int = capi.FP64,
+           disc: Optional[Discretization] = None) -> Solver:
+    """Set-up + handle + initial state for a generated case.
+
+    precision: capi.FP64 (the reference's arithmetic) or capi.MIXED (residual in
+    FP32, state and time integration in FP64). A Discretization of the same case
+    may be passed to share the host-side set-up between handles."""
+    params = make_params(case, metric_compat=metric_compat, precision=precision)
+    if disc is None:
+        disc = setup_discretization(case, params)
     s = Solver(params, disc)
     s.set_state(nodal_to_modal(case, params))
     return s

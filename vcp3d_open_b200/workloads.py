@@ -1,0 +1,34 @@
+"""Named synthetic workloads of the benchmark, the precision report and the tests.
+
+Every workload is a seeded, generated case (vcp3d_open_b200.cases): there is no
+grid or restart file to download. The Taylor-Green cases use Re 1600 and
+Mach 0.1 on the periodic box [0, 2pi]^3 with a +-1% random node perturbation
+(curvilinear elements, so the full metric terms are exercised).
+"""
+from __future__ import annotations
+
+from .cases import CaseSpec
+
+TWO_PI = 6.283185307179586
+
+_TGV = dict(kind="tgv", hi=(TWO_PI,) * 3, mach=0.1, reynolds=1600.0, grid_map="random",
+            grid_amp=0.01, seed=1)
+
+WORKLOADS = {
+    # Headline: 32^3 elements of degree 3, 2,097,152 DOFs.
+    "tgv32_p3_lsrk4": dict(_TGV, n_elem=(32, 32, 32), p=3),
+    # Isentropic vortex, 8^3 elements of degree 3 (the reference's own test case shape).
+    "vortex8_p3_lsrk4": dict(kind="vortex", n_elem=(8, 8, 8), p=3),
+    # Degree 4 on 48^3 elements (13.8M DOFs): the mixed-precision configuration's size.
+    "tgv48_p4_lsrk4": dict(_TGV, n_elem=(48, 48, 48), p=4),
+    # Profiling size: state + metrics ~200 MB (above the 126 MB L2), 8000 elements.
+    "tgv20_p3_lsrk4": dict(_TGV, n_elem=(20, 20, 20), p=3),
+    # Degree 4 on 16^3 elements: the mixed-versus-FP64 test case (fits a test's time).
+    "tgv16_p4_lsrk4": dict(_TGV, n_elem=(16, 16, 16), p=4),
+}
+
+
+def make_spec(name: str) -> CaseSpec:
+    if name not in WORKLOADS:
+        raise KeyError(f"unknown workload {name!r}; known: {sorted(WORKLOADS)}")
+    return CaseSpec(name=name, **WORKLOADS[name])
