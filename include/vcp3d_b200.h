@@ -190,6 +190,62 @@ int vcpg_time_step_noalloc(const vcpg_params *params, const vcpg_operators *ops,
                            const double *d_sol, const double *d_elem_scalars, double *d_dt,
                            void *stream);
 
+/* ------------------------------------------------------------------------- */
+/* Open boundaries: characteristic (PC-NSCBC) boundary conditions, sponge     */
+/* layers and the characteristic matching layer.                              */
+/* ------------------------------------------------------------------------- */
+
+/* Boundary condition of one block face (face numbering as above). */
+enum vcpg_bc {
+  VCPG_BC_NONE = 0,                 /* interior / periodic: the face has neighbours     */
+  VCPG_BC_OUTFLOW_NSCBC = 1,        /* "BCOutflowNSCBC": prescribed static pressure,
+                                       BCOutflowCharacteristicSubfaceClass
+                                       (src/BoundaryState.cpp:1300-1568)              */
+  VCPG_BC_INFLOW_STATIC_NSCBC = 2   /* "BCInflowStaticNSCBC": prescribed density and
+                                       velocity, BCInflowStaticCharacteristicSubfaceClass
+                                       (src/BoundaryState.cpp:1579-1847)              */
+};
+
+/* The reference's "NSCBC tuning parameters", "Prescribed boundary data" and
+ * "Sponge layer information" blocks (src/InputParamClass.cpp:406-431, 1196-1330).
+ * Dimensional prescribed values are non-dimensionalised with the handle's
+ * reference conditions, as ConvertPrescribedData does (src/SubfaceClasses.cpp). */
+typedef struct vcpg_open_boundary {
+  int32_t bc[6];                  /* enum vcpg_bc per block face                       */
+  double p_out[6];                /* outflow: static pressure (Pa)                     */
+  double inflow[6][4];            /* static inflow: density, velocity x, y, z          */
+  double outlet_len;              /* "Outlet characteristic length"                    */
+  double outlet_sigma;            /* "Outlet normal relaxation (sigma)"                */
+  double outlet_beta_l;           /* "Outlet coupled transverse relaxation (beta_l)";
+                                     negative: use the boundary-averaged Mach number   */
+  double outlet_beta_t;           /* "Outlet uncoupled transverse relaxation (beta_t)" */
+  int32_t outlet_one_minus_beta;  /* "Outlet use one minus beta transverse relaxation" */
+  int32_t inlet_incoming;         /* "Inlet use outgoing wave amplitude"               */
+  double inlet_len;               /* "Inlet characteristic length"                     */
+  double inlet_sigma;             /* "Inlet normal relaxation (sigma)"                 */
+  int32_t sponge_elems[6];        /* sponge-layer thickness in elements per block face */
+  double sponge_sigma[6];         /* damping constant per block face                   */
+  double sponge_alpha[6];         /* damping exponent per block face                   */
+  int32_t cml;                    /* "Characteristic matching layer" in sponge elements */
+  double sponge_state[5];         /* damping (averaged) state: density, velocity x, y,
+                                     z, pressure, dimensional                          */
+} vcpg_open_boundary;
+
+/* Configures open boundaries on a handle whose geometry has boundary faces
+ * (neighbors == -1 on the faces listed in bc). geom must be the same host
+ * arrays given to vcpg_create; grid_nodes ([n_elem][3][(p_grid+1)^3], nodes at
+ * the dof_location positions as in vcpg_setup_geometry) are needed when any
+ * sponge_elems is non-zero and may be NULL otherwise. Every later residual
+ * first averages the projected Mach number over each characteristic boundary
+ * (SolverClass::AverageDataNSCBC, src/SolverClass.cpp:2492-2581) and builds the
+ * boundary states and fluxes in FP64 (also in the mixed form). Characteristic
+ * faces must be aligned with a parametric direction
+ * (IdentifyBoundaryIndices, src/BoundaryState.cpp:829-928), otherwise
+ * VCPG_E_INVALID. Call once, after vcpg_create and before the first residual. */
+int vcpg_set_open_boundary(vcpg_handle *h, const vcpg_open_boundary *ob,
+                           const vcpg_geometry *geom, int32_t p_grid, int32_t dof_location,
+                           const double *grid_nodes);
+
 #ifdef __cplusplus
 }
 #endif

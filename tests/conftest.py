@@ -21,7 +21,13 @@ def pytest_configure(config):
 
 
 def golden_files():
+    """Fixtures of periodic blocks."""
     return sorted(glob.glob(os.path.join(GOLDEN, "case_*.npz")))
+
+
+def open_golden_files():
+    """Fixtures of blocks with characteristic boundaries, sponge and matching layers."""
+    return sorted(glob.glob(os.path.join(GOLDEN, "open_*.npz")))
 
 
 def load_golden(path):

@@ -4,7 +4,8 @@ oracle/Makefile) on small generated cases.
 
     make -C oracle && python tests/golden/make_golden.py
 
-Each fixture case_<name>.npz holds, for one case:
+Each fixture case_<name>.npz (periodic blocks) or open_<name>.npz (blocks with
+characteristic boundaries, sponge and matching layers) holds, for one case:
   spec_json       the CaseSpec (JSON) that regenerates grid and initial state
   sol0            initial modal entropy-variable state [nE][5][K^3] (reference's
                   own restart-file conversion)
@@ -55,18 +56,50 @@ GOLDEN_SPECS = {
 }
 
 
+_OPEN = dict(kind="pulse", mach=0.3, grid_map="random", grid_amp=0.01, pulse_amp=1.0e-2,
+             pulse_width=0.5)
+
+OPEN_SPECS = {
+    # Static inflow (i-min), outflow on i-max and both j faces with sponge layers and
+    # the matching layer, k periodic: the config-3 boundary set on a reduced block.
+    # The pulses of the open cases sit next to a boundary so that the boundary
+    # terms carry a large part of the residual.
+    "pulse_p3_6x4x2_sponge_cml": cases.CaseSpec(
+        name="pulse_p3_6x4x2_sponge_cml", n_elem=(6, 4, 2), p=3, hi=(6.0, 4.0, 2.0),
+        center=(5.2, 0.8, 1.0), seed=4,
+        bc=("inflow_static_nscbc", "outflow_nscbc", "outflow_nscbc", "outflow_nscbc",
+            "periodic", "periodic"), sponge=(0, 2, 1, 1, 0, 0), cml=True, **_OPEN),
+    # Degree 4, Roe flux, inflow / outflow in i only, inlet keeping the outgoing
+    # acoustic amplitudes; j and k periodic; no sponge.
+    "pulse_p4_4x3x2_roe": cases.CaseSpec(
+        name="pulse_p4_4x3x2_roe", n_elem=(4, 3, 2), p=4, hi=(4.0, 3.0, 2.0),
+        center=(0.6, 1.5, 1.0), riemann="Roe", seed=5, inlet_incoming=True,
+        bc=("inflow_static_nscbc", "outflow_nscbc", "periodic", "periodic", "periodic",
+            "periodic"), **_OPEN),
+    # Outflow on the k faces, Mach-averaged transverse relaxation (beta < 0) without
+    # the (1 - beta) form, sponge only on k-max, flow along z.
+    "pulse_p3_3x3x4_kfaces": cases.CaseSpec(
+        name="pulse_p3_3x3x4_kfaces", n_elem=(3, 3, 4), p=3, hi=(3.0, 3.0, 4.0),
+        center=(1.5, 1.5, 0.7), vel_dir=(0.0, 0.0, 1.0), seed=6, outlet_beta_l=-1.0,
+        outlet_beta_t=-1.0, outlet_one_minus_beta=False,
+        bc=("periodic", "periodic", "periodic", "periodic", "inflow_static_nscbc",
+            "outflow_nscbc"), sponge=(0, 0, 0, 0, 0, 1), **_OPEN),
+}
+
+
 def spec_to_json(spec: cases.CaseSpec) -> str:
     return json.dumps(dataclasses.asdict(spec))
 
 
 def spec_from_json(text: str) -> cases.CaseSpec:
     d = json.loads(text)
-    for k in ("n_elem", "lo", "hi", "vel_dir", "center"):
-        d[k] = tuple(d[k])
+    for k in ("n_elem", "lo", "hi", "vel_dir", "center", "bc", "sponge"):
+        if k in d:
+            d[k] = tuple(d[k])
     return cases.CaseSpec(**d)
 
 
-def make(name: str, spec: cases.CaseSpec, out_dir: str) -> str:
+def make(name: str, spec: cases.CaseSpec, out_dir: str, prefix: str = "case") -> str:
     K = spec.p + 1
     KD = K ** 3
     case = cases.build_case(spec)
@@ -86,7 +119,7 @@ def make(name: str, spec: cases.CaseSpec, out_dir: str) -> str:
     sums = [np.abs(d["volMetric"][:, :10, :MD]).sum()] + \
            [np.abs(d[f][:, :13, :M2]).sum() for f in faces] + \
            [np.abs(d["elemScalars"]).sum()]
-    path = os.path.join(out_dir, f"case_{name}.npz")
+    path = os.path.join(out_dir, f"{prefix}_{name}.npz")
     np.savez_compressed(
         path, spec_json=np.array(spec_to_json(spec)), sol0=d["sol"][:, :, :KD],
         res_raw=r["resRaw"][:, :, :KD], res=r["res"][:, :, :KD], monitor=r["monitor"],
@@ -101,8 +134,13 @@ def make(name: str, spec: cases.CaseSpec, out_dir: str) -> str:
 def main():
     if not records.have_reference_build():
         raise SystemExit("build the oracle first: make -C oracle")
+    only = set(sys.argv[1:])
     for name, spec in GOLDEN_SPECS.items():
-        print(make(name, spec, HERE))
+        if not only or name in only:
+            print(make(name, spec, HERE))
+    for name, spec in OPEN_SPECS.items():
+        if not only or name in only:
+            print(make(name, spec, HERE, prefix="open"))
 
 
 if __name__ == "__main__":

@@ -10,7 +10,7 @@ import re
 import numpy as np
 import pytest
 
-from conftest import ROOT, golden_files, load_golden, rel_l2
+from conftest import ROOT, golden_files, load_golden, open_golden_files, rel_l2
 from vcp3d_open_b200 import capi, cases, solver
 
 
@@ -49,7 +49,7 @@ def test_create_rejects_bad_arguments_without_touching_the_device():
     assert lib.vcpg_step(None, 0, 1, -1.0, None) == 8
 
 
-@pytest.mark.parametrize("path", golden_files(), ids=os.path.basename)
+@pytest.mark.parametrize("path", golden_files() + open_golden_files(), ids=os.path.basename)
 def test_setup_matches_reference_metrics(path):
     g = load_golden(path)
     spec = g["spec"]

@@ -18,6 +18,7 @@ ERRORS = {1: "VCPG_E_CUDA", 2: "VCPG_E_CG_NOCONV", 3: "VCPG_E_NEG_A2", 4: "VCPG_
 ROE, ISMAIL_ROE = 0, 1
 FP64, MIXED = 0, 1
 SSPRK3, LSRK4 = 0, 1
+BC_NONE, BC_OUTFLOW_NSCBC, BC_INFLOW_STATIC_NSCBC = 0, 1, 2
 
 # Every symbol include/vcp3d_b200.h declares.
 EXPORTED = [
@@ -25,7 +26,7 @@ EXPORTED = [
     "vcpg_nodal_conservative_to_modal", "vcpg_set_state", "vcpg_get_state",
     "vcpg_get_residual", "vcpg_residual", "vcpg_get_raw_residual", "vcpg_time_step",
     "vcpg_step", "vcpg_sync", "vcpg_stream", "vcpg_launch_count", "vcpg_stats",
-    "vcpg_time_step_noalloc",
+    "vcpg_time_step_noalloc", "vcpg_set_open_boundary",
 ]
 
 
@@ -46,6 +47,18 @@ class Operators(C.Structure):
 class Geometry(C.Structure):
     _fields_ = [("vol_metric", C.POINTER(C.c_double)), ("face_metric", C.POINTER(C.c_double)),
                 ("elem_scalars", C.POINTER(C.c_double)), ("neighbors", C.POINTER(C.c_int32))]
+
+
+class OpenBoundary(C.Structure):
+    """vcpg_open_boundary: characteristic BCs, sponge layers, matching layer."""
+    _fields_ = [("bc", C.c_int32 * 6), ("p_out", C.c_double * 6),
+                ("inflow", (C.c_double * 4) * 6), ("outlet_len", C.c_double),
+                ("outlet_sigma", C.c_double), ("outlet_beta_l", C.c_double),
+                ("outlet_beta_t", C.c_double), ("outlet_one_minus_beta", C.c_int32),
+                ("inlet_incoming", C.c_int32), ("inlet_len", C.c_double),
+                ("inlet_sigma", C.c_double), ("sponge_elems", C.c_int32 * 6),
+                ("sponge_sigma", C.c_double * 6), ("sponge_alpha", C.c_double * 6),
+                ("cml", C.c_int32), ("sponge_state", C.c_double * 5)]
 
 
 class VcpgError(RuntimeError):
@@ -88,6 +101,8 @@ def load() -> C.CDLL:
     lib.vcpg_stats.argtypes = [hp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     lib.vcpg_time_step_noalloc.argtypes = [C.POINTER(Params), C.POINTER(Operators), C.c_void_p,
                                            C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.vcpg_set_open_boundary.argtypes = [hp, C.POINTER(OpenBoundary), C.POINTER(Geometry),
+                                           C.c_int32, C.c_int32, dp]
     _lib = lib
     return lib
 

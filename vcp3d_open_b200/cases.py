@@ -32,6 +32,9 @@ import numpy as np
 
 GAMMA = 1.4
 R_GAS = 287.058
+# Boundary-condition names of the subface table (src/InputParamClass.cpp:1441-1580).
+BC_NAMES = {"periodic": "Periodic1to1Trans", "outflow_nscbc": "BCOutflowNSCBC",
+            "inflow_static_nscbc": "BCInflowStaticNSCBC"}
 MU_DIM = 1.716e-5
 SU2_MAGIC = 535532
 NAME_LEN = 33
@@ -117,6 +120,26 @@ class CaseSpec:
     # Pressure pulse amplitude (relative) and width.
     pulse_amp: float = 1.0e-3
     pulse_width: float = 0.5
+    # Block-face boundary conditions (iMin, iMax, jMin, jMax, kMin, kMax): "periodic",
+    # "outflow_nscbc" (BCOutflowNSCBC, prescribed static pressure) or
+    # "inflow_static_nscbc" (BCInflowStaticNSCBC, prescribed density and velocity).
+    bc: Tuple[str, ...] = ("periodic",) * 6
+    p_inf: float = 101325.0          # free-stream static pressure of open cases (Pa)
+    # NSCBC tuning parameters (src/InputParamClass.cpp:406-424).
+    outlet_len: float = 1.0
+    outlet_sigma: float = 0.25
+    outlet_beta_l: float = 0.5
+    outlet_beta_t: float = 0.5
+    outlet_one_minus_beta: bool = True
+    inlet_len: float = 1.0
+    inlet_sigma: float = 1.0
+    inlet_incoming: bool = False
+    # Sponge layers: elements per block face, damping constant and exponent; the
+    # characteristic matching layer acts in every sponge element.
+    sponge: Tuple[int, ...] = (0,) * 6
+    sponge_sigma: float = 20.0
+    sponge_alpha: float = 2.0
+    cml: bool = False
 
     def __post_init__(self):
         if self.p_grid is None:
@@ -124,6 +147,25 @@ class CaseSpec:
         if self.n_poly_int is None:
             self.n_poly_int = 3 * self.p
         self.n_elem = tuple(int(v) for v in self.n_elem)
+        self.bc = tuple(str(b) for b in self.bc)
+        self.sponge = tuple(int(v) for v in self.sponge)
+        for d in range(3):
+            a, b = self.bc[2 * d], self.bc[2 * d + 1]
+            if (a == "periodic") != (b == "periodic"):
+                raise ValueError("a direction is periodic on both faces or on neither")
+        for b in self.bc:
+            if b not in BC_NAMES:
+                raise ValueError(f"unknown boundary condition {b!r}")
+        if self.cml and not any(self.sponge):
+            raise ValueError("the matching layer needs sponge layers")
+
+    @property
+    def is_open(self) -> bool:
+        return any(b != "periodic" for b in self.bc) or any(self.sponge)
+
+    @property
+    def periodic(self) -> Tuple[int, int, int]:
+        return tuple(int(self.bc[2 * d] == "periodic") for d in range(3))
 
     @property
     def n_dofs_1d(self) -> int:
@@ -157,13 +199,21 @@ class RefConditions:
 
 
 def reference_conditions(spec: CaseSpec) -> RefConditions:
+    """With a prescribed outflow pressure and inflow density (open cases) those are
+    the reference pressure and density and the Reynolds number is not used, as in
+    the reference; otherwise the far-field branch."""
     v_inf = spec.mach * math.sqrt(GAMMA * R_GAS * spec.t_inf)
-    rho_ref = spec.reynolds * MU_DIM / (spec.reynolds_length * v_inf)
-    p_ref = rho_ref * R_GAS * spec.t_inf
-    u_ref = math.sqrt(p_ref / rho_ref)
     d = np.asarray(spec.vel_dir, dtype=float)
     d = d / math.sqrt(float(d @ d))
-    return RefConditions(p_ref, rho_ref, u_ref, MU_DIM * u_ref / p_ref, v_inf, tuple(d))
+    if "outflow_nscbc" in spec.bc and "inflow_static_nscbc" in spec.bc:
+        p_ref = spec.p_inf
+        rho_ref = spec.p_inf / (R_GAS * spec.t_inf)
+    else:
+        rho_ref = spec.reynolds * MU_DIM / (spec.reynolds_length * v_inf)
+        p_ref = rho_ref * R_GAS * spec.t_inf
+    u_ref = math.sqrt(p_ref / rho_ref)
+    return RefConditions(p_ref, rho_ref, u_ref, MU_DIM * u_ref / p_ref, v_inf,
+                         tuple(float(c) for c in d))
 
 
 # ---------------------------------------------------------------------------
@@ -259,12 +309,13 @@ def primitive_state(spec: CaseSpec, xyz: np.ndarray, ref: RefConditions):
         rho = p / (R_GAS * spec.t_inf)
         return rho, u, v, w, p
     if spec.kind == "pulse":
-        # Gaussian pressure pulse p = p_inf (1 + a exp(-r^2/(2 w^2))), isentropic density.
+        # Gaussian pressure pulse p = p_inf (1 + a exp(-r^2/(2 w^2))) on the free
+        # stream, density unchanged (the reference's "Pressure pulse" fluctuation,
+        # src/ElementClass.cpp:600-663).
         r2 = sum((c - spec.center[d]) ** 2 for d, c in enumerate((x, y, z)))
-        p = p_inf * (1.0 + spec.pulse_amp * np.exp(-r2 / (2.0 * spec.pulse_width ** 2)))
-        rho = rho_inf * (p / p_inf) ** (1.0 / GAMMA)
+        p = p_inf * (1.0 + spec.pulse_amp * np.exp(-r2 * (0.5 / (spec.pulse_width ** 2))))
         ones = np.ones_like(x)
-        return rho, u_inf[0] * ones, u_inf[1] * ones, u_inf[2] * ones, p
+        return rho_inf * ones, u_inf[0] * ones, u_inf[1] * ones, u_inf[2] * ones, p
     raise ValueError(f"unknown case kind {spec.kind!r}")
 
 
@@ -318,14 +369,20 @@ def read_plot3d(path: str) -> np.ndarray:
     return arr.reshape(3, kl, jl, il).copy()
 
 
-def write_su2_restart(path: str, dof_xyz: np.ndarray, cons: np.ndarray) -> None:
-    """SU2 restart: per element, per DOF: x y z rho rhou rhov rhow rhoE (doubles).
+def write_su2_restart(path: str, dof_xyz: np.ndarray, cons: np.ndarray,
+                      extra: Optional[np.ndarray] = None, extra_names=()) -> None:
+    """SU2 restart: per element, per DOF: x y z rho rhou rhov rhow rhoE (doubles),
+    followed by the `extra` variables (shape (nElem, nExtra, nDOFs)) if given.
 
     dof_xyz has shape (nElem, 3, nDOFs); cons has shape (nElem, 5, nDOFs).
     """
     n_elem, _, n_dofs = dof_xyz.shape
     names = ["x", "y", "z", "Density", "Momentum_x", "Momentum_y", "Momentum_z", "Energy"]
-    body = np.concatenate([dof_xyz, cons], axis=1).transpose(0, 2, 1)  # elem, dof, var
+    cols = [dof_xyz, cons]
+    if extra is not None:
+        names += list(extra_names)
+        cols.append(extra)
+    body = np.concatenate(cols, axis=1).transpose(0, 2, 1)  # elem, dof, var
     with open(path, "wb") as f:
         f.write(struct.pack("<5i", SU2_MAGIC, len(names), n_elem * n_dofs, 1, 8))
         for nm in names:
@@ -348,7 +405,9 @@ def read_su2_restart(path: str, n_elem: int, n_dofs: int):
     return body[:, :3].copy(), body[:, 3:8].copy()
 
 
-def _periodic_subfaces(spec: CaseSpec) -> str:
+def _subfaces(spec: CaseSpec) -> str:
+    """Subface table: one subface per block face, periodic (1-to-1 with a
+    translation) or a physical boundary condition over the whole face."""
     nI, nJ, nK = spec.n_elem
     L = [spec.hi[d] - spec.lo[d] for d in range(3)]
     I, J, K = nI + 1, nJ + 1, nK + 1
@@ -363,14 +422,68 @@ def _periodic_subfaces(spec: CaseSpec) -> str:
     out = []
     for face, (own, donor, t) in enumerate(rows, start=1):
         out.append(f"    {face}    1")
-        out.append(f"        Periodic1to1Trans  {own}   {donor}   1 2 3   "
-                   f"{t[0]!r} {t[1]!r} {t[2]!r}")
+        bc = spec.bc[face - 1]
+        if bc == "periodic":
+            out.append(f"        Periodic1to1Trans  {own}   {donor}   1 2 3   "
+                       f"{t[0]!r} {t[1]!r} {t[2]!r}")
+        else:
+            out.append(f"        {BC_NAMES[bc]}  {own}")
     return "\n".join(out)
+
+
+def _open_blocks(spec: CaseSpec, ref: "RefConditions") -> Tuple[str, str, str]:
+    """(parameter lines, sponge block, prescribed-data block) of an open case."""
+    if not spec.is_open:
+        return "", "", ""
+    yn = lambda v: "yes" if v else "no"
+    params = f"""Outlet characteristic length: {spec.outlet_len!r}
+Outlet normal relaxation (sigma): {spec.outlet_sigma!r}
+Outlet use one minus beta transverse relaxation: {yn(spec.outlet_one_minus_beta)}
+Outlet use local (element) averaged Mach number: no
+Outlet coupled   transverse relaxation (beta_l): {spec.outlet_beta_l!r}
+Outlet uncoupled transverse relaxation (beta_t): {spec.outlet_beta_t!r}
+Inlet characteristic length: {spec.inlet_len!r}
+Inlet normal relaxation (sigma): {spec.inlet_sigma!r}
+Inlet use outgoing wave amplitude: {yn(spec.inlet_incoming)}
+"""
+    sponge = ""
+    if any(spec.sponge):
+        params += f"""Sponge layer: yes
+Characteristic matching layer: {yn(spec.cml)}
+Averaged solution file name: averaged.dat
+"""
+        rows = "\n".join(f"    {f + 1}    {spec.sponge[f]}    {spec.sponge_sigma!r}    "
+                         f"{spec.sponge_alpha!r}" for f in range(6))
+        sponge = f"""
+Sponge layer information
+#Face nBufferElem DampingConstant DampingExponent
+{rows}
+"""
+    p_out, rho_in, vel_in = prescribed_values(spec, ref)
+    lines = []
+    for f, bc in enumerate(spec.bc):
+        if bc == "outflow_nscbc":
+            lines.append(f"    {f + 1}    1    1    Pressure")
+            lines.append(f"        {p_out!r}")
+        elif bc == "inflow_static_nscbc":
+            lines.append(f"    {f + 1}    1    1    Density VelocityX VelocityY VelocityZ")
+            lines.append(f"        {rho_in!r} {vel_in[0]!r} {vel_in[1]!r} {vel_in[2]!r}")
+    presc = ""
+    if lines:
+        presc = "\nPrescribed boundary data\n" + "\n".join(lines) + "\n"
+    return params, sponge, presc
+
+
+def prescribed_values(spec: CaseSpec, ref: "RefConditions"):
+    """Outflow pressure, inflow density and velocity (dimensional): the free stream."""
+    vel = tuple(float(ref.v_inf * c) for c in ref.vel_dir)
+    return float(ref.p_ref), float(ref.rho_ref), vel
 
 
 def param_cfg_text(spec: CaseSpec, grid_file="grid.xyz", restart_file="restart.dat",
                    restart=True) -> str:
     d = spec.vel_dir
+    open_params, sponge, presc = _open_blocks(spec, reference_conditions(spec))
     return f"""# Generated case {spec.name} ({spec.kind})
 Polynomial degree grid: {spec.p_grid}
 Polynomial degree solution: {spec.p}
@@ -403,10 +516,10 @@ Number of synchronization time steps: 1
 Synchronization time step: 1.0
 CFL number: {spec.cfl!r}
 Compute average solution: no
-
+{open_params}{sponge}
 Subface information
-{_periodic_subfaces(spec)}
-"""
+{_subfaces(spec)}
+{presc}"""
 
 
 @dataclasses.dataclass
@@ -435,7 +548,27 @@ def write_case(case: CaseData, directory: str) -> str:
         os.makedirs(os.path.join(directory, sub), exist_ok=True)
     write_plot3d(os.path.join(directory, "grid.xyz"), case.grid)
     write_su2_restart(os.path.join(directory, "restart.dat"), case.dof_xyz, case.cons)
+    if any(case.spec.sponge):
+        write_averaged_solution(os.path.join(directory, "averaged.dat"), case)
     cfg = os.path.join(directory, "param.cfg")
     with open(cfg, "w") as f:
         f.write(param_cfg_text(case.spec))
     return cfg
+
+
+def write_averaged_solution(path: str, case: CaseData) -> None:
+    """The averaged-solution file that supplies the sponge-layer damping state
+    (SolverClass::ReadAveragedSolutionSpongeLayer, src/SpongeLayer.cpp:667-843):
+    an SU2 restart with the solution, the averaged primitive variables
+    (density, velocity, pressure), six averaged velocity products and the
+    averaged eddy viscosity. The averaged state written here is the free stream."""
+    ref = case.ref
+    n_elem, _, n_dofs = case.dof_xyz.shape
+    vel = [ref.v_inf * c for c in ref.vel_dir]
+    avg = np.zeros((n_elem, 12, n_dofs))
+    avg[:, 0] = ref.rho_ref
+    avg[:, 1], avg[:, 2], avg[:, 3] = vel
+    avg[:, 4] = ref.p_ref
+    names = ["Density_avg", "VelocityX_avg", "VelocityY_avg", "VelocityZ_avg", "Pressure_avg",
+             "R_uu", "R_vv", "R_ww", "R_uv", "R_uw", "R_vw", "EddyVisc_avg"]
+    write_su2_restart(path, case.dof_xyz, case.cons, avg, names)

@@ -10,9 +10,11 @@
 #include <vector>
 
 #include "../../include/vcp3d_b200.h"
+#include "dg_boundary.cuh"
 #include "dg_residual.cuh"
 #include "host_setup.h"
 #include "kernels.h"
+#include "open_boundary.h"
 
 
 using namespace vcpg;
@@ -35,6 +37,16 @@ struct vcpg_handle {
   int graph_launches[2] = {0, 0};
   int64_t launches = 0;
   bool res_valid = false;  // d_res holds the residual of d_sol
+  // Open boundaries (vcpg_set_open_boundary): characteristic boundary faces and sponges.
+  bool open = false;
+  int nB = 0;
+  int *d_bface = nullptr;
+  double *d_bpresc = nullptr, *d_pc = nullptr, *d_dlq = nullptr;
+  double *d_btrace = nullptr, *d_bmach = nullptr, *d_bflux = nullptr;
+  int *d_sponge = nullptr;
+  double *d_dampfn = nullptr, *d_dampst = nullptr, *d_cml = nullptr;
+  int cml_on = 0;
+  BlockFaceCfg cfg[6] = {};
   std::string err;
 };
 
@@ -83,6 +95,13 @@ ResidualArgs MakeResidualArgs(vcpg_handle *h, double *rawOut, unsigned long long
   // tolerance FP32 can reach (1e-5 relative), the FP64 form at the reference's 1e-10.
   a.mixed = h->prm.precision == VCPG_MIXED ? 1 : 0;
   a.cg_tol = a.mixed ? 1.e-5 : 1.e-10;
+  a.open = h->open ? 1 : 0;
+  a.bflux = h->d_bflux;
+  a.sponge_idx = h->d_sponge;
+  a.damp_fn = h->d_dampfn;
+  a.damp_state = h->d_dampst;
+  a.cml = h->d_cml;
+  a.cml_on = h->cml_on;
   return a;
 }
 
@@ -116,6 +135,44 @@ int CheckStatus(vcpg_handle *h) {
   return VCPG_OK;
 }
 
+BoundaryArgs MakeBoundaryArgs(vcpg_handle *h) {
+  BoundaryArgs b{};
+  b.sol = h->d_sol;
+  b.face_metric = h->d_face;
+  b.elem_scalars = h->d_sc;
+  b.bface = h->d_bface;
+  b.bpresc = h->d_bpresc;
+  b.pc = h->d_pc;
+  b.dlq = h->d_dlq;
+  b.btrace = h->d_btrace;
+  b.bmach = h->d_bmach;
+  b.bflux = h->d_bflux;
+  b.nB = h->nB;
+  b.mu = h->prm.mu;
+  b.tau_num = (double)((h->prm.n_poly + 1) * (h->prm.n_poly + 1)) * h->prm.rel_penalty;
+  b.theta_sym = h->prm.theta_sym;
+  b.riemann = h->prm.riemann;
+  b.metric_compat = h->prm.metric_index_compat;
+  for (int f = 0; f < 6; ++f) b.cfg[f] = h->cfg[f];
+  return b;
+}
+
+// One residual evaluation: the characteristic boundary kernels (when the block
+// has characteristic faces) and the fused residual kernel. Returns the launches.
+int EnqueueResidual(vcpg_handle *h, const ResidualArgs &a, int *launches) {
+  int n = 0;
+  if (h->open && h->nB > 0) {
+    VCPG_CUDA(h, LaunchBoundary(h->K, h->M, MakeBoundaryArgs(h), h->stream));
+    n += 2;
+  }
+  VCPG_CUDA(h, LaunchResidual(h->K, h->M, a, h->stream));
+  n += 1;
+  if (launches) *launches = n;
+  return VCPG_OK;
+}
+
+int ResidualLaunches(const vcpg_handle *h) { return (h->open && h->nB > 0) ? 3 : 1; }
+
 int EnqueueStep(vcpg_handle *h, int scheme) {
   const size_t n = (size_t)h->nE * 5 * h->KD;
   TimeStepArgs t = MakeTimeStepArgs(h);
@@ -130,13 +187,15 @@ int EnqueueStep(vcpg_handle *h, int scheme) {
     for (int s = 0; s < 3; ++s) {
       VCPG_CUDA(h, LaunchSspStage(h->d_sol, h->d_solOld, h->d_res, h->d_dt, alphaRK[s], betaRK[s],
                                   s == 0, n, h->stream));
-      VCPG_CUDA(h, LaunchResidual(h->K, h->M, a, h->stream));
+      int rc = EnqueueResidual(h, a, nullptr);
+      if (rc) return rc;
     }
   } else {
     for (int s = 0; s < 5; ++s) {
       VCPG_CUDA(h, LaunchLsrkStage(h->d_sol, h->d_solOld, h->d_res, h->d_dt, kLsA[s], kLsB[s], n,
                                    h->stream));
-      VCPG_CUDA(h, LaunchResidual(h->K, h->M, a, h->stream));
+      int rc = EnqueueResidual(h, a, nullptr);
+      if (rc) return rc;
     }
   }
   return VCPG_OK;
@@ -156,7 +215,9 @@ int vcpg_destroy(vcpg_handle *h) {
   }
   void *bufs[] = {h->d_sol, h->d_solOld, h->d_res, h->d_resRaw, h->d_vol, h->d_face, h->d_sc,
                   h->d_nbr, h->d_dtbits, h->d_mach2, h->d_dt, h->d_fixed, h->d_hist,
-                  h->d_status, h->d_counter, h->d_cgstats};
+                  h->d_status, h->d_counter, h->d_cgstats, h->d_bface, h->d_bpresc, h->d_pc,
+                  h->d_dlq, h->d_btrace, h->d_bmach, h->d_bflux, h->d_sponge, h->d_dampfn,
+                  h->d_dampst, h->d_cml};
   for (void *p : bufs)
     if (p) cudaFree(p);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -304,9 +365,11 @@ int vcpg_residual(vcpg_handle *h, double *monitoring, int32_t keep_raw) {
   if (monitoring) VCPG_CUDA(h, cudaMemsetAsync(h->d_mach2, 0, 8, h->stream));
   ResidualArgs a = MakeResidualArgs(h, keep_raw ? h->d_resRaw : nullptr,
                                     monitoring ? h->d_mach2 : nullptr);
-  VCPG_CUDA(h, LaunchResidual(h->K, h->M, a, h->stream));
-  h->launches += 1;
-  int rc = CheckStatus(h);
+  int nl = 0;
+  int rc = EnqueueResidual(h, a, &nl);
+  if (rc) return rc;
+  h->launches += nl;
+  rc = CheckStatus(h);
   h->res_valid = rc == VCPG_OK;
   if (monitoring) {
     unsigned long long bits = 0;
@@ -355,8 +418,10 @@ int vcpg_step(vcpg_handle *h, int32_t scheme, int32_t n_steps, double fixed_dt,
   if (!h->res_valid) {
     // The first stage uses the residual of the current state: evaluate it once
     // after a new state was set (later steps reuse the last stage's residual).
-    VCPG_CUDA(h, LaunchResidual(h->K, h->M, MakeResidualArgs(h, nullptr, nullptr), h->stream));
-    h->launches += 1;
+    int nl = 0;
+    int rc0 = EnqueueResidual(h, MakeResidualArgs(h, nullptr, nullptr), &nl);
+    if (rc0) return rc0;
+    h->launches += nl;
   }
   const double fx = fixed_dt > 0.0 ? fixed_dt : -1.0;
   VCPG_CUDA(h, cudaMemcpyAsync(h->d_fixed, &fx, 8, cudaMemcpyHostToDevice, h->stream));
@@ -370,7 +435,7 @@ int vcpg_step(vcpg_handle *h, int32_t scheme, int32_t n_steps, double fixed_dt,
     if (e != cudaSuccess) return CudaFail(h, e, "cudaStreamEndCapture");
     h->graph[scheme] = g;
     VCPG_CUDA(h, cudaGraphInstantiate(&h->exec[scheme], g, 0));
-    h->graph_launches[scheme] = 2 + (scheme == VCPG_SSPRK3 ? 3 : 5) * 2;
+    h->graph_launches[scheme] = 2 + (scheme == VCPG_SSPRK3 ? 3 : 5) * (1 + ResidualLaunches(h));
   }
   for (int s = 0; s < n_steps; ++s) VCPG_CUDA(h, cudaGraphLaunch(h->exec[scheme], h->stream));
   h->launches += (int64_t)n_steps * h->graph_launches[scheme];
@@ -398,6 +463,55 @@ int vcpg_stats(vcpg_handle *h, int64_t *cg_iterations, int64_t *element_solves) 
   VCPG_CUDA(h, cudaStreamSynchronize(h->stream));
   if (cg_iterations) *cg_iterations = (int64_t)st[0];
   if (element_solves) *element_solves = (int64_t)st[1];
+  return VCPG_OK;
+}
+
+int vcpg_set_open_boundary(vcpg_handle *h, const vcpg_open_boundary *ob,
+                           const vcpg_geometry *geom, int32_t p_grid, int32_t dof_location,
+                           const double *grid_nodes) {
+  if (!h || !ob || !geom) return VCPG_E_INVALID;
+  if (h->open) return Fail(h, VCPG_E_INVALID, "open boundaries are already configured");
+  OpenBoundaryHost ob_host;
+  std::string err;
+  int rc = BuildOpenBoundary(h->prm, *ob, *geom, p_grid, dof_location, grid_nodes, ob_host, err);
+  if (rc != VCPG_OK) return Fail(h, rc, err);
+  const int M2 = h->M2, MD = h->MD;
+  auto upload = [&](void **dst, const void *src, size_t bytes) -> int {
+    if (bytes == 0) return VCPG_OK;
+    cudaError_t e = cudaMalloc(dst, bytes);
+    if (e != cudaSuccess) return Fail(h, VCPG_E_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    if (src) {
+      e = cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) return CudaFail(h, e, "cudaMemcpy open boundary");
+    }
+    return VCPG_OK;
+  };
+  const size_t nB = (size_t)ob_host.nB, nS = (size_t)ob_host.nS;
+  if ((rc = upload((void **)&h->d_bface, ob_host.bface.data(), sizeof(int) * ob_host.bface.size())) ||
+      (rc = upload((void **)&h->d_bpresc, ob_host.bpresc.data(), sizeof(double) * ob_host.bpresc.size())) ||
+      (rc = upload((void **)&h->d_pc, ob_host.pc.data(), sizeof(double) * ob_host.pc.size())) ||
+      (rc = upload((void **)&h->d_dlq, ob_host.dlq.data(), sizeof(double) * ob_host.dlq.size())) ||
+      (rc = upload((void **)&h->d_btrace, nullptr, sizeof(double) * nB * 4 * 5 * M2)) ||
+      (rc = upload((void **)&h->d_bmach, nullptr, sizeof(double) * nB)) ||
+      (rc = upload((void **)&h->d_bflux, nullptr, sizeof(double) * nB * 4 * 5 * M2)) ||
+      (rc = upload((void **)&h->d_sponge, ob_host.spongeIdx.data(), sizeof(int) * ob_host.spongeIdx.size())) ||
+      (rc = upload((void **)&h->d_dampfn, ob_host.dampFn.data(), sizeof(double) * nS * 3 * MD)) ||
+      (rc = upload((void **)&h->d_dampst, ob_host.dampState.data(), sizeof(double) * nS * 5 * MD)) ||
+      (rc = upload((void **)&h->d_cml, ob_host.cml.data(), sizeof(double) * nS * 6)))
+    return rc;
+  // Boundary faces are coded in the neighbour table as -2 - (boundary-face index).
+  VCPG_CUDA(h, cudaMemcpy(h->d_nbr, ob_host.nbrCode.data(), sizeof(int32_t) * ob_host.nbrCode.size(),
+                          cudaMemcpyHostToDevice));
+  h->nB = ob_host.nB;
+  h->cml_on = ob_host.cmlOn;
+  for (int f = 0; f < 6; ++f) h->cfg[f] = ob_host.cfg[f];
+  h->open = true;
+  h->res_valid = false;
+  // Captured steps hold the previous launch sequence.
+  for (int s = 0; s < 2; ++s) {
+    if (h->exec[s]) { cudaGraphExecDestroy(h->exec[s]); h->exec[s] = nullptr; }
+    if (h->graph[s]) { cudaGraphDestroy(h->graph[s]); h->graph[s] = nullptr; }
+  }
   return VCPG_OK;
 }
 

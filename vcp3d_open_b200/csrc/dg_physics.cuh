@@ -212,14 +212,15 @@ __device__ __forceinline__ void RoeFlux(const T *VL, const T *VR, const T nx,
 // PenAndSymFluxesSymmVar (src/FluxesFace.cpp:1152-1284).
 //   VL, VR      left/right entropy variables
 //   gx, gy, gz  averaged Cartesian gradients of the entropy variables
-//   nnx..nnz    unit normal times factNorm; wf, area: face weight and area
+//   nnx..nnz    unit normal times factNorm (-1 when the own element is on the
+//               right of a boundary face); wf, area: face weight and area
 //   tau         penalty parameter (p+1)^2 C_pen / lenScale
 // Subtracts the viscous flux from f, adds the penalty terms, and returns the
 // Cartesian symmetrizing fluxes in sx, sy, sz (component 0 is zero).
 template <typename T>
 __device__ __forceinline__ void ViscousPenaltySymFlux(
     const T *VL, const T *VR, const T *gx, const T *gy, const T *gz,
-    const T nnx, const T nny, const T nnz, const T factNorm, const T wf,
+    const T nnx, const T nny, const T nnz, const T wf,
     const T area, const T mu, const T tau, const T thetaSym, T *f,
     T *sx, T *sy, T *sz) {
   const T gm1 = T(kGam) - T(1.0), ovgm1 = T(1.0) / gm1, ov1mg = -ovgm1;
@@ -244,9 +245,10 @@ __device__ __forceinline__ void ViscousPenaltySymFlux(
   const T dV4 = VL[4] - VR[4];
   const T pOvRho = -V4Inv;
 
-  // Viscous normal flux (src/FluxesFace.cpp:1565-1614).
+  // Viscous normal flux (src/FluxesFace.cpp:1565-1614): the reference scales the
+  // metric normal by factNorm * w * area; nnx already carries factNorm.
   {
-    const T Area = factNorm * wf * area;
+    const T Area = wf * area;
     const T nx = Area * nnx, ny = Area * nny, nz = Area * nnz;
     const T lamDivVel = T(kLamOverMu) * (dudx + dvdy + dwdz);
     const T muTot = mu + T(0.0);

@@ -39,6 +39,15 @@ struct ResidualArgs {
   unsigned long long *cg_stats;  // [0] CG iterations, [1] element solves (cumulative)
   double cg_tol;               // relative CG stopping tolerance (1e-10 in the FP64 form)
   int mixed;                   // 1: FP32 compute (contractions, fluxes, mass solve)
+  // Open boundaries (null / 0 for a block without them). Boundary faces carry
+  // nbr = -2 - b, b indexing bflux; nbr = -1 is a physical face without a BC.
+  int open;                    // 1: launch the variant with boundary faces and sponges
+  const double *bflux;         // [nB][4][5][M^2] boundary-face fluxes (dg_boundary.cuh)
+  const int *sponge_idx;       // [nE] sponge-layer index or -1
+  const double *damp_fn;       // [nS][3][M^3] damping function per direction
+  const double *damp_state;    // [nS][5][M^3] conservative damping state
+  const double *cml;           // [nS][6] 1/sigma per direction, layer orientation
+  int cml_on;                  // characteristic matching layer in sponge elements
 };
 
 // Arguments of the CFL time-step kernel (kernels.cu).
@@ -103,12 +112,12 @@ __device__ __forceinline__ void BlockReduce3(T &a, T &b, T &c, T *red) {
 }
 
 // Shared-memory plan (doubles) of the fused kernel for a (K, M) pair.
-template <int K, int M, typename T = double> struct Plan {
+template <int K, int M, typename T = double, bool OPEN = false> struct Plan {
   static constexpr int KD = K * K * K, MD = M * M * M, M2 = M * M;
   static constexpr int TK = 5 * K * K * M;      // first-stage buffer
   static constexpr int TJ = 5 * K * M * M;      // second-stage buffer
-  // Volume phase: tK, tJ, Var, dX, dY, dZ.
-  static constexpr int VOL = TK + TJ + 20 * MD;
+  // Volume phase: tK, tJ, Var, dX, dY, dZ (+ the matching-layer source when OPEN).
+  static constexpr int VOL = TK + TJ + 20 * MD + (OPEN ? 5 * MD : 0);
   // Face phase: per face-side trace (value + 3 derivatives) 20*M2, two sides,
   // three faces at a time, plus normal-evaluation and stage buffers.
   // Face phase: BN/BND 60 K^2, three fast-axis buffers 90 K M, traces 120 M^2.
@@ -129,20 +138,113 @@ template <int K, int M, typename T = double> struct Plan {
 
 
 // ---------------------------------------------------------------------------
+// Characteristic matching layer source of one integration point
+// (src/ElementClass.cpp:3885-4108): the incoming-wave LODI amplitudes of each
+// direction, weighted by -J w sigma_d / sigma_max, written to bufC[5][M^3].
+// V: entropy variables; gx, gy, gz: their Cartesian gradients.
+// ---------------------------------------------------------------------------
+template <int M, typename T>
+__device__ __forceinline__ void MatchingLayerSource(const ResidualArgs &a, const int sp,
+                                                    const int l, const T *V, const T *gx,
+                                                    const T *gy, const T *gz, const T rho,
+                                                    const T u, const T v, const T w, const T p,
+                                                    const T ek, const T rE, const T weight,
+                                                    T *bufC) {
+  constexpr int MD = M * M * M;
+  const double *fn = a.damp_fn + (size_t)sp * 3 * MD;
+  const double *cm = a.cml + (size_t)sp * 6;
+  const T gm1 = T(kGam) - T(1.0), ovgm1 = T(1.0) / gm1;
+  const T wx = weight * T(cm[0]) * LdT<T>(fn + l);
+  const T wy = weight * T(cm[1]) * LdT<T>(fn + MD + l);
+  const T wz = weight * T(cm[2]) * LdT<T>(fn + 2 * MD + l);
+  const T nx = T(cm[3]), ny = T(cm[4]), nz = T(cm[5]);
+  const T V4Inv = T(1.0) / V[4];
+  const T H = rE / rho - V4Inv;
+  const T a2 = -T(kGam) * V4Inv;
+  const T c = Sqrt(a2);
+  const T rhoa = rho * c, ovra = T(1.0) / rhoa, ova2 = T(1.0) / a2, rova = rho / c;
+  const T rhou = rho * u, rhov = rho * v, rhow = rho * w;
+  // Jacobian entropy -> primitive (rows rho, u, v, w, p).
+  const T J11 = rho, J12 = rhou, J13 = rhov, J14 = rhow, J15 = rE;
+  const T J22 = -V4Inv, J25 = -V4Inv * u, J33 = -V4Inv, J35 = -V4Inv * v;
+  const T J44 = -V4Inv, J45 = -V4Inv * w;
+  const T J51 = p, J52 = p * u, J53 = p * v, J54 = p * w, J55 = p * H;
+  T dq[3][5];
+  const T *g[3] = {gx, gy, gz};
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const T *x = g[q];
+    dq[q][0] = J11 * x[0] + J12 * x[1] + J13 * x[2] + J14 * x[3] + J15 * x[4];
+    dq[q][1] = J22 * x[1] + J25 * x[4];
+    dq[q][2] = J33 * x[2] + J35 * x[4];
+    dq[q][3] = J44 * x[3] + J45 * x[4];
+    dq[q][4] = J51 * x[0] + J52 * x[1] + J53 * x[2] + J54 * x[3] + J55 * x[4];
+  }
+  // Eigenvalues with the outgoing ones removed.
+  const T vel[3] = {u, v, w}, dir[3] = {nx, ny, nz};
+  T l1[3], l2[3], l3[3];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    l1[q] = vel[q] - c; l2[q] = vel[q]; l3[q] = vel[q] + c;
+    if (dir[q] * l1[q] > T(0.0)) l1[q] = T(0.0);
+    if (dir[q] * l2[q] > T(0.0)) l2[q] = T(0.0);
+    if (dir[q] * l3[q] > T(0.0)) l3[q] = T(0.0);
+  }
+  // Wave amplitudes and P = S L per direction.
+  const T Lx1 = T(0.5) * l1[0] * (ovra * dq[0][4] - dq[0][1]);
+  const T Lx2 = l2[0] * (dq[0][0] - ova2 * dq[0][4]);
+  const T Lx3 = l2[0] * (dq[0][3]);
+  const T Lx4 = l2[0] * (-dq[0][2]);
+  const T Lx5 = T(0.5) * l3[0] * (ovra * dq[0][4] + dq[0][1]);
+  const T Ly1 = T(0.5) * l1[1] * (ovra * dq[1][4] - dq[1][2]);
+  const T Ly2 = l2[1] * (-dq[1][3]);
+  const T Ly3 = l2[1] * (dq[1][0] - ova2 * dq[1][4]);
+  const T Ly4 = l2[1] * (dq[1][1]);
+  const T Ly5 = T(0.5) * l3[1] * (ovra * dq[1][4] + dq[1][2]);
+  const T Lz1 = T(0.5) * l1[2] * (ovra * dq[2][4] - dq[2][3]);
+  const T Lz2 = l2[2] * (dq[2][2]);
+  const T Lz3 = l2[2] * (-dq[2][1]);
+  const T Lz4 = l2[2] * (dq[2][0] - ova2 * dq[2][4]);
+  const T Lz5 = T(0.5) * l3[2] * (ovra * dq[2][4] + dq[2][3]);
+  const T Lx51 = Lx5 + Lx1, Ly51 = Ly5 + Ly1, Lz51 = Lz5 + Lz1;
+  const T P[3][5] = {{rova * (Lx51) + Lx2, (Lx5 - Lx1), -Lx4, Lx3, rhoa * (Lx51)},
+                     {rova * (Ly51) + Ly3, Ly4, (Ly5 - Ly1), -Ly2, rhoa * (Ly51)},
+                     {rova * (Lz51) + Lz4, -Lz3, Lz2, (Lz5 - Lz1), rhoa * (Lz51)}};
+  const T wd[3] = {wx, wy, wz};
+  T out[5];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const T *P_ = P[q];
+    const T t0 = wd[q] * (P_[0]);
+    const T t1 = wd[q] * (u * P_[0] + rho * P_[1]);
+    const T t2 = wd[q] * (v * P_[0] + rho * P_[2]);
+    const T t3 = wd[q] * (w * P_[0] + rho * P_[3]);
+    const T t4 = wd[q] * (ek * P_[0] + rhou * P_[1] + rhov * P_[2] + rhow * P_[3] + ovgm1 * P_[4]);
+    if (q == 0) { out[0] = t0; out[1] = t1; out[2] = t2; out[3] = t3; out[4] = t4; }
+    else { out[0] += t0; out[1] += t1; out[2] += t2; out[3] += t3; out[4] += t4; }
+  }
+#pragma unroll
+  for (int n = 0; n < 5; ++n) bufC[n * MD + l] = out[n];
+}
+
+// ---------------------------------------------------------------------------
 // Volume phase: solution and gradients at the integration points
 // (TPSAGV), pointwise fluxes, and the three transposed contractions (TPAVR)
 // into s_R. Also stores the CG point data (rho, u, v, w, p, rhoE, dUdV(4,4))
 // and J*w.  Follows ElementClass::VolumeResidual, src/ElementClass.cpp:3809-4443.
 // ---------------------------------------------------------------------------
-template <int NT, int K, int M, typename T>
+template <int NT, int K, int M, typename T, bool OPEN>
 __device__ __forceinline__ void VolumePhase(const ResidualArgs &a, const int e,
                                             const T *s_sol, T *s_R, T *s_cgp,
                                             T *s_jw, T *work, T *s_red) {
   constexpr int SLOT = Slot<K, M>::value;
-  using P = Plan<K, M, T>;
+  using P = Plan<K, M, T, OPEN>;
   constexpr int MD = P::MD, KD = P::KD, M2 = P::M2;
   T *tK = work, *tJ = work + P::TK, *Var = tJ + P::TJ;
   T *dX = Var + 5 * MD, *dY = dX + 5 * MD, *dZ = dY + 5 * MD;
+  T *bufC = dZ + 5 * MD;  // matching-layer source (OPEN only)
+  const int sp = OPEN ? a.sponge_idx[e] : -1;
+  const bool cmlHere = OPEN && sp >= 0 && a.cml_on;
 
   // TPSAGV (include/TensorProductSolAndGradVolume.hpp:5-249): k, then j, then i.
   Contract<NT, SLOT, K, M, kLeg, 2, 5, K, K, K, K, M, false>(s_sol, tK);
@@ -207,6 +309,11 @@ __device__ __forceinline__ void VolumePhase(const ResidualArgs &a, const int e,
     s_cgp[5 * MD + l] = rE;
     s_cgp[6 * MD + l] = rE * rH / rho + p * eKin;  // dUdV(4,4)
     mach2 = Fmax(mach2, rho * (u * u + v * v + w * w) / (T(kGam) * p));
+    if (OPEN && cmlHere)
+      MatchingLayerSource<M>(a, sp, l, V, gx, gy, gz, rho, u, v, w, p, eKin, rE,
+                             -LdT<T>(vm + l) * Weight1D<SLOT, T>(i) * Weight1D<SLOT, T>(j) *
+                                 Weight1D<SLOT, T>(k),
+                             bufC);
 
     // Inviscid + viscous fluxes times -J w and the metric (src/ElementClass.cpp:4320-4416).
     const T Wl = Weight1D<SLOT, T>(i) * Weight1D<SLOT, T>(j) * Weight1D<SLOT, T>(k);
@@ -250,6 +357,15 @@ __device__ __forceinline__ void VolumePhase(const ResidualArgs &a, const int e,
   }
   __syncthreads();
 
+  // The matching-layer source initialises the residual (src/ElementClass.cpp:3885-4117).
+  if (OPEN && cmlHere) {
+    Contract<NT, SLOT, K, M, kLegT, 2, 5, M, M, M, M, K, false>(bufC, tJ);
+    __syncthreads();
+    Contract<NT, SLOT, K, M, kLegT, 1, 5, M, M, K, M, K, false>(tJ, tK);
+    __syncthreads();
+    Contract<NT, SLOT, K, M, kLegT, 0, 5, M, K, K, M, K, true>(tK, s_R);
+    __syncthreads();
+  }
   // TPAVR for the three flux directions (src/ElementClass.cpp:4425-4443).
   Contract<NT, SLOT, K, M, kLegT, 2, 5, M, M, M, M, K, false>(dX, tJ);
   __syncthreads();
@@ -269,6 +385,27 @@ __device__ __forceinline__ void VolumePhase(const ResidualArgs &a, const int e,
   __syncthreads();
   Contract<NT, SLOT, K, M, kLegT, 0, 5, M, K, K, M, K, true>(tK, s_R);
   __syncthreads();
+  // Sponge-layer damping J w sum_d sigma_d (U - U_damp) (src/ElementClass.cpp:4450-4489).
+  if (OPEN && sp >= 0) {
+    const double *fn = a.damp_fn + (size_t)sp * 3 * MD;
+    const double *ds = a.damp_state + (size_t)sp * 5 * MD;
+    for (int l = threadIdx.x; l < MD; l += NT) {
+      const T sigma = s_jw[l] * (LdT<T>(fn + l) + LdT<T>(fn + MD + l) + LdT<T>(fn + 2 * MD + l));
+      const T rho = s_cgp[0 * MD + l];
+      dX[0 * MD + l] = sigma * (rho - LdT<T>(ds + 0 * MD + l));
+      dX[1 * MD + l] = sigma * (rho * s_cgp[1 * MD + l] - LdT<T>(ds + 1 * MD + l));
+      dX[2 * MD + l] = sigma * (rho * s_cgp[2 * MD + l] - LdT<T>(ds + 2 * MD + l));
+      dX[3 * MD + l] = sigma * (rho * s_cgp[3 * MD + l] - LdT<T>(ds + 3 * MD + l));
+      dX[4 * MD + l] = sigma * (s_cgp[5 * MD + l] - LdT<T>(ds + 4 * MD + l));
+    }
+    __syncthreads();
+    Contract<NT, SLOT, K, M, kLegT, 2, 5, M, M, M, M, K, false>(dX, tJ);
+    __syncthreads();
+    Contract<NT, SLOT, K, M, kLegT, 1, 5, M, M, K, M, K, false>(tJ, tK);
+    __syncthreads();
+    Contract<NT, SLOT, K, M, kLegT, 0, 5, M, K, K, M, K, true>(tK, s_R);
+    __syncthreads();
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -398,7 +535,7 @@ __device__ __forceinline__ void GroupFacePoint(const ResidualArgs &a, const int 
   else
     RoeFlux(VL, VR, nx, ny, nz, T(0.5) * wf * area, flux);
   T sx[5], sy[5], sz[5];
-  ViscousPenaltySymFlux(VL, VR, gx, gy, gz, nx, ny, nz, T(1.0), wf, area, T(a.mu),
+  ViscousPenaltySymFlux(VL, VR, gx, gy, gz, nx, ny, nz, wf, area, T(a.mu),
                         T(a.tau_num) / lenScale, T(a.theta_sym), flux, sx, sy, sz);
   const double *fm = g == 0 ? fmR : fmL;  // the own side's metric
   const int pFast = FastParam(d);
@@ -419,7 +556,7 @@ __device__ __forceinline__ void GroupFacePoint(const ResidualArgs &a, const int 
   }
 }
 
-template <int NT, int K, int M, typename T>
+template <int NT, int K, int M, typename T, bool OPEN>
 __device__ __forceinline__ void FacePhase(const ResidualArgs &a, const int e, const T *s_sol,
                                           T *s_R, const T *s_fv, T *work) {
   constexpr int SLOT = Slot<K, M>::value;
@@ -450,8 +587,21 @@ __device__ __forceinline__ void FacePhase(const ResidualArgs &a, const int e, co
     for (int idx = threadIdx.x; idx < 3 * M2; idx += NT) {
       const int d = idx / M2, pt = idx - d * M2;
       const int nb = d == 0 ? nb0 : (d == 1 ? nb1 : nb2);
+      if (OPEN && nb <= -2) {
+        // Characteristic boundary face: fluxes from BoundaryFluxKernel (FP64).
+        const double *bf = a.bflux + (size_t)(-2 - nb) * 4 * 5 * M2;
+#pragma unroll
+        for (int n = 0; n < 5; ++n) {
+          const int o = (d * 5 + n) * M2 + pt;
+          P1[o] = T(bf[(0 * 5 + n) * M2 + pt]);
+          P1[15 * M2 + o] = T(bf[(1 * 5 + n) * M2 + pt]);
+          P1[30 * M2 + o] = T(bf[(2 * 5 + n) * M2 + pt]);
+          P2[o] = T(bf[(3 * 5 + n) * M2 + pt]);
+        }
+        continue;
+      }
       if (nb < 0) {
-        // Physical boundary faces are not part of this interior-face path.
+        // A physical boundary face without a boundary condition.
         if (pt == 0) atomicAdd(a.status + 1, 1);
         for (int n = 0; n < 5; ++n) {
           const int o = (d * 5 + n) * M2 + pt;
@@ -673,9 +823,9 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
 // ---------------------------------------------------------------------------
 // The fused kernel.
 // ---------------------------------------------------------------------------
-template <int K, int M, int NT, typename T>
-__global__ void __launch_bounds__(NT, Plan<K, M, T>::MIN_BLOCKS) ResidualKernel(const ResidualArgs a) {
-  using P = Plan<K, M, T>;
+template <int K, int M, int NT, typename T, bool OPEN>
+__global__ void __launch_bounds__(NT, (Plan<K, M, T, OPEN>::MIN_BLOCKS)) ResidualKernel(const ResidualArgs a) {
+  using P = Plan<K, M, T, OPEN>;
   constexpr int KD = P::KD, MD = P::MD;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *smem = reinterpret_cast<T *>(smem_raw);
@@ -690,8 +840,8 @@ __global__ void __launch_bounds__(NT, Plan<K, M, T>::MIN_BLOCKS) ResidualKernel(
     s_fv[2 * K + threadIdx.x] = FaceDer<Slot<K, M>::value, T>(threadIdx.x);
   }
   __syncthreads();
-  VolumePhase<NT, K, M>(a, e, s_sol, s_R, s_cgp, s_jw, work, s_red);
-  FacePhase<NT, K, M>(a, e, s_sol, s_R, s_fv, work);
+  VolumePhase<NT, K, M, T, OPEN>(a, e, s_sol, s_R, s_cgp, s_jw, work, s_red);
+  FacePhase<NT, K, M, T, OPEN>(a, e, s_sol, s_R, s_fv, work);
   if (a.res_raw) {
     double *dst = a.res_raw + (size_t)e * 5 * KD;
     for (int i = threadIdx.x; i < 5 * KD; i += NT) dst[i] = double(s_R[i]);

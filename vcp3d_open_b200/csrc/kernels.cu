@@ -1,6 +1,7 @@
 // Kernel instantiations and launchers for every supported (K, M) pair:
 // the fused residual kernel, the CFL time-step kernel and the Runge-Kutta
 // stage updates.
+#include "dg_boundary.cuh"
 #include "dg_residual.cuh"
 #include "kernels.h"
 
@@ -106,25 +107,40 @@ __global__ void LsrkStageKernel(double *sol, double *du, const double *res, cons
 // ---------------------------------------------------------------------------
 // Launchers.
 // ---------------------------------------------------------------------------
-template <int K, int M, typename T>
+template <int K, int M, typename T, bool OPEN>
 static cudaError_t LaunchResidualKMT(const ResidualArgs &a, cudaStream_t st) {
-  constexpr int NT = Plan<K, M, T>::NT;
-  const size_t bytes = Plan<K, M, T>::BYTES;
+  using P = Plan<K, M, T, OPEN>;
+  constexpr int NT = P::NT;
+  const size_t bytes = P::BYTES;
   static bool configured = false;
   if (!configured) {
-    cudaError_t err = cudaFuncSetAttribute(ResidualKernel<K, M, NT, T>,
+    cudaError_t err = cudaFuncSetAttribute(ResidualKernel<K, M, NT, T, OPEN>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (err != cudaSuccess) return err;
     configured = true;
   }
-  ResidualKernel<K, M, NT, T><<<a.n_elem, NT, bytes, st>>>(a);
+  ResidualKernel<K, M, NT, T, OPEN><<<a.n_elem, NT, bytes, st>>>(a);
   return cudaGetLastError();
 }
 
-// FP64 form or the mixed form (FP32 compute, FP64 inputs and outputs).
+// FP64 form or the mixed form (FP32 compute, FP64 inputs and outputs), each
+// with or without open boundaries and sponge layers.
 template <int K, int M>
 static cudaError_t LaunchResidualKM(const ResidualArgs &a, cudaStream_t st) {
-  return a.mixed ? LaunchResidualKMT<K, M, float>(a, st) : LaunchResidualKMT<K, M, double>(a, st);
+  if (a.open)
+    return a.mixed ? LaunchResidualKMT<K, M, float, true>(a, st)
+                   : LaunchResidualKMT<K, M, double, true>(a, st);
+  return a.mixed ? LaunchResidualKMT<K, M, float, false>(a, st)
+                 : LaunchResidualKMT<K, M, double, false>(a, st);
+}
+
+// The two characteristic-boundary kernels (dg_boundary.cuh).
+template <int K, int M>
+static cudaError_t LaunchBoundaryKM(const BoundaryArgs &a, cudaStream_t st) {
+  constexpr int NT = M * M > 64 ? 128 : 64;
+  BoundaryTraceKernel<K, M, NT><<<a.nB, NT, 0, st>>>(a);
+  BoundaryFluxKernel<K, M, NT><<<a.nB, NT, 0, st>>>(a);
+  return cudaGetLastError();
 }
 
 template <int K, int M>
@@ -168,6 +184,16 @@ cudaError_t LaunchResidual(int K, int M, const ResidualArgs &a, cudaStream_t st)
   if (K == 4 && M == 5) return LaunchResidualKM<4, 5>(a, st);
   if (K == 5 && M == 7) return LaunchResidualKM<5, 7>(a, st);
   if (K == 6 && M == 8) return LaunchResidualKM<6, 8>(a, st);
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t LaunchBoundary(int K, int M, const BoundaryArgs &a, cudaStream_t st) {
+  if (a.nB <= 0) return cudaSuccess;
+  if (K == 2 && M == 3) return LaunchBoundaryKM<2, 3>(a, st);
+  if (K == 3 && M == 4) return LaunchBoundaryKM<3, 4>(a, st);
+  if (K == 4 && M == 5) return LaunchBoundaryKM<4, 5>(a, st);
+  if (K == 5 && M == 7) return LaunchBoundaryKM<5, 7>(a, st);
+  if (K == 6 && M == 8) return LaunchBoundaryKM<6, 8>(a, st);
   return cudaErrorInvalidValue;
 }
 

@@ -10,6 +10,7 @@ namespace vcpg {
 
 struct ResidualArgs;
 struct TimeStepArgs;
+struct BoundaryArgs;
 
 bool Supported(int K, int M);
 int SlotOf(int K, int M);
@@ -17,6 +18,8 @@ size_t ResidualSmemBytes(int K, int M);
 cudaError_t UploadOpTable(int slot, const OpTable &t);
 
 cudaError_t LaunchResidual(int K, int M, const ResidualArgs &a, cudaStream_t st);
+// Boundary traces + Mach weights, then the boundary states and fluxes (2 launches).
+cudaError_t LaunchBoundary(int K, int M, const BoundaryArgs &a, cudaStream_t st);
 cudaError_t LaunchTimeStep(int K, int M, const TimeStepArgs &a, cudaStream_t st);
 cudaError_t LaunchFinalizeDt(unsigned long long *dt_bits, const double *fixed_dt, double *d_dt,
                              double *hist, int hist_cap, int *counter, cudaStream_t st);

@@ -1,0 +1,305 @@
+// Host-side set-up of open boundaries: the characteristic boundary-face list and
+// its configuration, the polynomial-correction (PC) operators, the boundary
+// areas, and the sponge-layer / characteristic-matching-layer data.
+//
+// Reference routines whose results this reproduces:
+//   PC matrix, Lagrange operators   StandardElementClass::AssemblePolynomialCorrectionOperators
+//                                   and ValuesLagrangeBasis1D (src/StandardElementClass.cpp:181-394)
+//   boundary indices                BCStandardCharacteristicSubfaceClass::IdentifyBoundaryIndices
+//                                   (src/BoundaryState.cpp:829-928)
+//   NSCBC parameters                ConfigureParamNSCBC (src/SubfaceClasses.cpp:1349-1436)
+//   prescribed data                 ConvertPrescribedData (src/SubfaceClasses.cpp:1304-1318, 1473-1495)
+//   boundary areas                  ElementClass::ComputeSurfaceAreaBoundary (src/ElementClass.cpp:303-330)
+//   sponge layer                    SolverClass::InitSpongeLayer / SetUpSpongeLayer[IJK]M(IN|AX),
+//                                   ElementClass::ConfigureSpongeLayer / InitializeDampingState
+//                                   (src/SpongeLayer.cpp:13-665, 844-1000)
+#include "open_boundary.h"
+
+#include <cmath>
+#include <cstring>
+#include <stdexcept>
+
+#include "host_setup.h"
+
+namespace vcpg {
+namespace {
+
+constexpr double kGamma = 1.4;
+constexpr double kEpsThreshold = 1.e-10;  // include/VCP3D_CurviLinear.hpp:137
+
+// Lagrange basis on `nodes` at `pts`: val[j * nP + i] = L_j(pts[i]) and its
+// derivative, through the Legendre Vandermonde matrices as in
+// StandardElementClass::LagrangianBasisFunctions (src/StandardElementClass.cpp:498-600).
+void Lagrange(const std::vector<double> &nodes, const std::vector<double> &pts,
+              std::vector<double> &val, std::vector<double> &der) {
+  const int n = (int)nodes.size(), nP = (int)pts.size();
+  std::vector<double> V(n * n);
+  for (int i = 0; i < n; ++i)
+    for (int k = 0; k < n; ++k) V[i * n + k] = host::NormJacobi(k, 0, 0, nodes[i]);
+  host::Invert(n, V);  // (V^-1)(k, j) at [k * n + j]
+  val.assign((size_t)n * nP, 0.0);
+  der.assign((size_t)n * nP, 0.0);
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < nP; ++i)
+      for (int k = 0; k < n; ++k) {
+        val[j * nP + i] += host::NormJacobi(k, 0, 0, pts[i]) * V[k * n + j];
+        der[j * nP + i] += host::GradNormJacobi(k, 0, 0, pts[i]) * V[k * n + j];
+      }
+}
+
+// Coordinates of the integration points of one element from its grid nodes
+// gridNodes[3][Kg^3] with the grid Lagrange basis lag[Kg][M]: out[3][M^3].
+void IntegrationPointCoordinates(const double *gridNodes, int Kg, int M,
+                                 const std::vector<double> &lag, double *out) {
+  const int KG3 = Kg * Kg * Kg, MD = M * M * M;
+  for (int x = 0; x < 3; ++x) {
+    const double *g = gridNodes + x * KG3;
+    for (int k = 0; k < M; ++k)
+      for (int j = 0; j < M; ++j)
+        for (int i = 0; i < M; ++i) {
+          double acc = 0.0;
+          for (int c = 0; c < Kg; ++c)
+            for (int b = 0; b < Kg; ++b)
+              for (int a = 0; a < Kg; ++a)
+                acc += lag[a * M + i] * lag[b * M + j] * lag[c * M + k] *
+                       g[(c * Kg + b) * Kg + a];
+          out[x * MD + (k * M + j) * M + i] = acc;
+        }
+  }
+}
+
+// Parametric axis of the face normal and the transverse axes, from the face
+// metric at point 0: the normal is the axis whose metric gradient is parallel
+// to the unit normal (cosine within 1e-10 of one).
+bool IdentifyBoundaryIndices(const double *fm, int M2, int grad[3]) {
+  const double nx = fm[0 * M2], ny = fm[1 * M2], nz = fm[2 * M2];
+  int found = -1;
+  for (int i = 0; i < 3; ++i) {
+    const double gx = fm[(4 + 3 * i) * M2], gy = fm[(5 + 3 * i) * M2], gz = fm[(6 + 3 * i) * M2];
+    const double len = std::sqrt(gx * gx + gy * gy + gz * gz);
+    const double cosT = (nx * gx + ny * gy + nz * gz) / len;
+    if (std::fabs(cosT - 1.0) < kEpsThreshold) {
+      if (found >= 0) return false;
+      found = i;
+    }
+  }
+  if (found < 0) return false;
+  grad[0] = found;
+  grad[1] = found == 0 ? 1 : 0;
+  grad[2] = found == 2 ? 1 : 2;
+  return true;
+}
+
+}  // namespace
+
+int BuildOpenBoundary(const vcpg_params &prm, const vcpg_open_boundary &ob,
+                      const vcpg_geometry &geom, int pGrid, int dofLocation,
+                      const double *gridNodes, OpenBoundaryHost &out, std::string &err) {
+  try {
+    const int K = prm.n_poly + 1, M = prm.n_int_1d, M2 = M * M, MD = M * M * M;
+    const int nI = prm.n_elem[0], nJ = prm.n_elem[1], nK = prm.n_elem[2];
+    const int64_t nE = (int64_t)nI * nJ * nK;
+    if (!geom.face_metric || !geom.neighbors) { err = "geometry arrays missing"; return VCPG_E_INVALID; }
+    for (int f = 0; f < 6; ++f)
+      if (ob.bc[f] < VCPG_BC_NONE || ob.bc[f] > VCPG_BC_INFLOW_STATIC_NSCBC) {
+        err = "unknown boundary condition on face " + std::to_string(f);
+        return VCPG_E_INVALID;
+      }
+
+    // 1-D operators: Lagrange basis of the solution DOFs at the Gauss points, its
+    // derivative at the DOFs, and the Lagrange derivative on the Gauss points.
+    std::vector<double> rInt, wInt, rDof;
+    host::GaussLegendre(M, rInt, wInt);
+    host::DofLocations(K, dofLocation, rDof);
+    std::vector<double> lqv, lqd, ldv, ldd, qqv, qqd;
+    Lagrange(rDof, rInt, lqv, lqd);   // lqv[j * M + i] = L_j(q_i)
+    Lagrange(rDof, rDof, ldv, ldd);   // ldd[j * K + i] = L_j'(r_i)
+    Lagrange(rInt, rInt, qqv, qqd);   // qqd[k * M + i] = l_k'(q_i)
+    const double c0 = -ldd[0];        // -L_0'(r_0)
+    out.dlq.assign(M * M, 0.0);
+    for (int i = 0; i < M; ++i)
+      for (int k = 0; k < M; ++k) out.dlq[i * M + k] = qqd[k * M + i];
+
+    // PC matrix A = L2D (dL2D^T dL2D)^-1 dL2D^T with dL2D = c0 L2D, where L2D maps
+    // the K^2 face DOFs to the M^2 face integration points.
+    const int K2 = K * K;
+    std::vector<double> L2D((size_t)M2 * K2), dL2D((size_t)M2 * K2);
+    for (int i1 = 0; i1 < M; ++i1)
+      for (int i2 = 0; i2 < M; ++i2)
+        for (int j1 = 0; j1 < K; ++j1)
+          for (int j2 = 0; j2 < K; ++j2) {
+            const double v = lqv[j1 * M + i1] * lqv[j2 * M + i2];
+            L2D[(size_t)(i1 * M + i2) * K2 + j1 * K + j2] = v;
+            dL2D[(size_t)(i1 * M + i2) * K2 + j1 * K + j2] = v * c0;
+          }
+    std::vector<double> LS((size_t)K2 * K2, 0.0);
+    for (int i = 0; i < K2; ++i)
+      for (int j = 0; j < K2; ++j)
+        for (int k = 0; k < M2; ++k) LS[i * K2 + j] += dL2D[(size_t)k * K2 + i] * dL2D[(size_t)k * K2 + j];
+    host::Invert(K2, LS);
+    std::vector<double> PCt((size_t)K2 * M2, 0.0);
+    for (int i = 0; i < K2; ++i)
+      for (int j = 0; j < M2; ++j) {
+        double t = 0.0;
+        for (int k = 0; k < K2; ++k) t += LS[i * K2 + k] * dL2D[(size_t)j * K2 + k];
+        PCt[(size_t)i * M2 + j] = t;
+      }
+    out.pc.assign((size_t)M2 * M2, 0.0);
+    for (int i = 0; i < M2; ++i)
+      for (int j = 0; j < M2; ++j) {
+        double t = 0.0;
+        for (int k = 0; k < K2; ++k) t += L2D[(size_t)i * K2 + k] * PCt[(size_t)k * M2 + j];
+        out.pc[(size_t)i * M2 + j] = t;
+      }
+
+    // Boundary faces, per block face in element order (the order of the
+    // reference's boundary sums), and their configuration.
+    out.nbrCode.assign(geom.neighbors, geom.neighbors + nE * 6);
+    out.bface.clear();
+    out.bpresc.clear();
+    out.nB = 0;
+    for (int f = 0; f < 6; ++f) {
+      BlockFaceCfg &c = out.cfg[f];
+      c = BlockFaceCfg{};
+      c.type = ob.bc[f];
+      c.first = out.nB;
+      const double factNorm = (f % 2 == 0) ? -1.0 : 1.0;
+      c.dell = factNorm * c0;
+      c.iPhi = factNorm > 0.0 ? 0 : 4;
+      if (c.type == VCPG_BC_OUTFLOW_NSCBC) {
+        c.sigma = ob.outlet_sigma; c.len = ob.outlet_len;
+        c.betaL = ob.outlet_beta_l; c.betaT = ob.outlet_beta_t;
+        c.oneMinusBeta = ob.outlet_one_minus_beta ? 1 : 0;
+      } else if (c.type == VCPG_BC_INFLOW_STATIC_NSCBC) {
+        c.sigma = ob.inlet_sigma; c.len = ob.inlet_len;
+        c.incoming = ob.inlet_incoming ? 1 : 0;
+      }
+      if (c.type != VCPG_BC_NONE && !(c.len > 0.0)) {
+        err = "characteristic length must be positive on face " + std::to_string(f);
+        return VCPG_E_INVALID;
+      }
+      for (int64_t e = 0; e < nE; ++e) {
+        if (geom.neighbors[e * 6 + f] >= 0) continue;
+        if (c.type == VCPG_BC_NONE) continue;  // stays -1: flagged by the residual kernel
+        const double *fm = geom.face_metric + ((size_t)e * 6 + f) * 13 * M2;
+        int grad[3];
+        if (!IdentifyBoundaryIndices(fm, M2, grad)) {
+          err = "could not identify the boundary indices of element " + std::to_string(e) +
+                " face " + std::to_string(f) + " (characteristic faces must be aligned with "
+                "a parametric direction)";
+          return VCPG_E_INVALID;
+        }
+        const int b = out.nB++;
+        int row[kBfStride] = {(int)e, f, c.type, grad[0], grad[1], grad[2], 0, 0};
+        out.bface.insert(out.bface.end(), row, row + kBfStride);
+        double pres[4] = {0.0, 0.0, 0.0, 0.0};
+        if (c.type == VCPG_BC_OUTFLOW_NSCBC) {
+          pres[0] = ob.p_out[f] / prm.p_ref;
+        } else {
+          pres[0] = ob.inflow[f][0] / prm.rho_ref;
+          pres[1] = ob.inflow[f][1] / prm.u_ref;
+          pres[2] = ob.inflow[f][2] / prm.u_ref;
+          pres[3] = ob.inflow[f][3] / prm.u_ref;
+        }
+        out.bpresc.insert(out.bpresc.end(), pres, pres + 4);
+        out.nbrCode[e * 6 + f] = -2 - b;
+        for (int l = 0; l < M2; ++l) c.area += wInt[l % M] * wInt[l / M] * fm[3 * M2 + l];
+      }
+      c.count = out.nB - c.first;
+    }
+
+    // Sponge layers and the characteristic matching layer.
+    const int *nb = ob.sponge_elems;
+    bool anySponge = false;
+    for (int f = 0; f < 6; ++f) {
+      if (nb[f] < 0) { err = "negative sponge-layer thickness"; return VCPG_E_INVALID; }
+      anySponge = anySponge || nb[f] > 0;
+    }
+    out.spongeIdx.assign(nE, -1);
+    out.nS = 0;
+    out.dampFn.clear(); out.dampState.clear(); out.cml.clear();
+    out.cmlOn = ob.cml ? 1 : 0;
+    if (ob.cml && !anySponge) { err = "the matching layer acts in sponge elements: no sponge given"; return VCPG_E_INVALID; }
+    if (anySponge) {
+      if (!gridNodes || pGrid < 1) { err = "sponge layers need the grid nodes"; return VCPG_E_INVALID; }
+      const int Kg = pGrid + 1, KG3 = Kg * Kg * Kg;
+      std::vector<double> rGrid, lgv, lgd;
+      host::DofLocations(Kg, dofLocation, rGrid);
+      Lagrange(rGrid, rInt, lgv, lgd);
+      const int n[3] = {nI, nJ, nK};
+      // Layer membership per element and direction: bit 2 d = min side, 2 d + 1 = max side.
+      std::vector<int> flags(nE, 0);
+      for (int k = 0; k < nK; ++k)
+        for (int j = 0; j < nJ; ++j)
+          for (int i = 0; i < nI; ++i) {
+            const int idx[3] = {i, j, k};
+            int fl = 0;
+            for (int d = 0; d < 3; ++d) {
+              if (idx[d] < nb[2 * d]) fl |= 1 << (2 * d);
+              if (idx[d] >= n[d] - nb[2 * d + 1]) fl |= 1 << (2 * d + 1);
+              if (((fl >> (2 * d)) & 3) == 3) {
+                err = "sponge layers of opposite faces overlap";
+                return VCPG_E_INVALID;
+              }
+            }
+            flags[((int64_t)k * nJ + j) * nI + i] = fl;
+          }
+      // Extent of each layer: coordinate of the element's first DOF and of the
+      // last DOF along the layer direction (grid corners).
+      double lo[6], hi[6];
+      for (int f = 0; f < 6; ++f) { lo[f] = 1.e+30; hi[f] = -1.e+30; }
+      for (int64_t e = 0; e < nE; ++e)
+        for (int f = 0; f < 6; ++f) {
+          if (!((flags[e] >> f) & 1)) continue;
+          const int d = f / 2;
+          const int last = d == 0 ? Kg - 1 : (d == 1 ? (Kg - 1) * Kg : (Kg - 1) * Kg * Kg);
+          const double *g = gridNodes + e * 3 * KG3 + d * KG3;
+          lo[f] = std::min(lo[f], g[0]);
+          hi[f] = std::max(hi[f], g[last]);
+        }
+      std::vector<double> xyz(3 * MD);
+      const double gm1 = kGamma - 1.0;
+      const double *st = ob.sponge_state;
+      const double rhoS = st[0] / prm.rho_ref, uS = st[1] / prm.u_ref, vS = st[2] / prm.u_ref,
+                   wS = st[3] / prm.u_ref, pS = st[4] / prm.p_ref;
+      const double cons[5] = {rhoS, rhoS * uS, rhoS * vS, rhoS * wS,
+                              pS / gm1 + 0.5 * rhoS * (uS * uS + vS * vS + wS * wS)};
+      for (int64_t e = 0; e < nE; ++e) {
+        if (!flags[e]) continue;
+        const int s = out.nS++;
+        out.spongeIdx[e] = s;
+        IntegrationPointCoordinates(gridNodes + e * 3 * KG3, Kg, M, lgv, xyz.data());
+        double cm[6] = {0.0, 0.0, 0.0, 1.0, 1.0, 1.0};
+        for (int d = 0; d < 3; ++d) {
+          const bool mn = (flags[e] >> (2 * d)) & 1, mx = (flags[e] >> (2 * d + 1)) & 1;
+          if (mn) cm[3 + d] = -1.0;
+          for (int l = 0; l < MD; ++l) {
+            double val = 0.0;
+            if (mn || mx) {
+              const int f = mn ? 2 * d : 2 * d + 1;
+              const double ss = ob.sponge_sigma[f], aa = ob.sponge_alpha[f];
+              const double x0 = mn ? hi[f] : lo[f];
+              const double x = xyz[d * MD + l];
+              if (mn ? x > x0 : x < x0) { err = "inconsistent sponge layer location"; return VCPG_E_INVALID; }
+              val = ss * std::pow(std::fabs(x - x0) / (hi[f] - lo[f]), aa);
+            }
+            out.dampFn.push_back(val);
+          }
+          if (mn || mx) {
+            const double ss = ob.sponge_sigma[mn ? 2 * d : 2 * d + 1];
+            cm[d] = ob.cml ? (std::fabs(ss) < 1.0e-4 ? 1.0 : 1.0 / ss) : 0.0;
+          }
+        }
+        for (int v = 0; v < 5; ++v)
+          for (int l = 0; l < MD; ++l) out.dampState.push_back(cons[v]);
+        out.cml.insert(out.cml.end(), cm, cm + 6);
+      }
+    }
+    return VCPG_OK;
+  } catch (const std::exception &ex) {
+    err = ex.what();
+    return VCPG_E_INVALID;
+  }
+}
+
+}  // namespace vcpg

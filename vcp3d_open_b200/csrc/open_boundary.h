@@ -1,0 +1,59 @@
+// Open-boundary set-up shared by the host builder (open_boundary.cpp) and the
+// device kernels (dg_boundary.cuh): characteristic boundary faces, the
+// polynomial-correction operators and the sponge / matching-layer data.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/vcp3d_b200.h"
+
+namespace vcpg {
+
+// Per block face (0 iMin .. 5 kMax) settings of a characteristic boundary.
+struct BlockFaceCfg {
+  int type;            // enum vcpg_bc
+  int first, count;    // range of this block face's entries in the boundary-face list
+  int iPhi;            // index of the incoming acoustic wave amplitude (0 or 4)
+  int oneMinusBeta;    // outlet: transverse terms weighted by (1 - beta)
+  int incoming;        // inlet: keep the outgoing acoustic amplitudes of the interior
+  double dell;         // factNorm * (-dL_0(r_0)): Lagrange derivative at the boundary DOF
+  double area;         // sum of w * area over the block face (SolverClass::InitNSCBC)
+  double sigma, len;   // normal relaxation coefficient and characteristic length
+  double betaL, betaT; // outlet transverse relaxation coefficients
+};
+
+// Entries of one boundary face in the boundary-face list (ints).
+enum BFaceField {
+  kBfElem = 0,   // element index
+  kBfFace = 1,   // block face / element face 0..5 (2 d + side)
+  kBfType = 2,   // enum vcpg_bc
+  kBfGrad = 3,   // 3 entries: parametric axis of the normal, first and second transverse
+  kBfStride = 8
+};
+
+struct OpenBoundaryHost {
+  int nB = 0;                       // boundary faces with a characteristic BC
+  std::vector<int> bface;           // [nB][kBfStride]
+  std::vector<double> bpresc;       // [nB][4] non-dimensional prescribed data
+  std::vector<double> pc;           // [M^2][M^2] polynomial-correction matrix
+  std::vector<double> dlq;          // [M][M]: dlq[i * M + k] = dL_k(q_i), Lagrange basis
+                                    // on the Gauss points
+  BlockFaceCfg cfg[6] = {};
+  std::vector<int32_t> nbrCode;     // [nE][6] neighbour table with boundary faces coded
+                                    // as -2 - (index in the boundary-face list)
+  int nS = 0;                       // sponge elements
+  std::vector<int32_t> spongeIdx;   // [nE] sponge index or -1
+  std::vector<double> dampFn;       // [nS][3][M^3] damping function per direction
+  std::vector<double> dampState;    // [nS][5][M^3] conservative damping state
+  std::vector<double> cml;          // [nS][6]: 1/sigma per direction, layer orientation
+  int cmlOn = 0;
+};
+
+// Builds the open-boundary data of a block. Returns a vcpg status and sets err.
+int BuildOpenBoundary(const vcpg_params &prm, const vcpg_open_boundary &ob,
+                      const vcpg_geometry &geom, int pGrid, int dofLocation,
+                      const double *gridNodes, OpenBoundaryHost &out, std::string &err);
+
+}  // namespace vcpg

@@ -64,8 +64,11 @@ def make_params(case: CaseData, metric_compat: bool = True,
 
 
 def setup_discretization(case: CaseData, params: capi.Params,
-                         periodic=(1, 1, 1)) -> Discretization:
-    """Operators and metric terms from the case grid (host C++ in the library)."""
+                         periodic=None) -> Discretization:
+    """Operators and metric terms from the case grid (host C++ in the library).
+    periodic defaults to the case's periodic directions."""
+    if periodic is None:
+        periodic = case.spec.periodic
     lib = capi.load()
     s = case.spec
     K, M, nE = s.p + 1, params.n_int_1d, s.n_elements
@@ -100,6 +103,32 @@ def nodal_to_modal(case: CaseData, params: capi.Params) -> np.ndarray:
     return out
 
 
+def open_boundary(case: CaseData) -> capi.OpenBoundary:
+    """vcpg_open_boundary of a case: its boundary conditions with the free stream
+    as prescribed data, NSCBC tuning parameters, sponge layers and matching layer."""
+    from .cases import prescribed_values
+    s, ref = case.spec, case.ref
+    ob = capi.OpenBoundary()
+    codes = {"periodic": capi.BC_NONE, "outflow_nscbc": capi.BC_OUTFLOW_NSCBC,
+             "inflow_static_nscbc": capi.BC_INFLOW_STATIC_NSCBC}
+    p_out, rho_in, vel_in = prescribed_values(s, ref)
+    for f, bc in enumerate(s.bc):
+        ob.bc[f] = codes[bc]
+        ob.p_out[f] = p_out
+        ob.inflow[f][0], ob.inflow[f][1], ob.inflow[f][2], ob.inflow[f][3] = (rho_in, *vel_in)
+        ob.sponge_elems[f] = s.sponge[f]
+        ob.sponge_sigma[f] = s.sponge_sigma
+        ob.sponge_alpha[f] = s.sponge_alpha
+    ob.outlet_len, ob.outlet_sigma = s.outlet_len, s.outlet_sigma
+    ob.outlet_beta_l, ob.outlet_beta_t = s.outlet_beta_l, s.outlet_beta_t
+    ob.outlet_one_minus_beta = 1 if s.outlet_one_minus_beta else 0
+    ob.inlet_len, ob.inlet_sigma = s.inlet_len, s.inlet_sigma
+    ob.inlet_incoming = 1 if s.inlet_incoming else 0
+    ob.cml = 1 if s.cml else 0
+    ob.sponge_state[:] = [rho_in, vel_in[0], vel_in[1], vel_in[2], p_out]
+    return ob
+
+
 class Solver:
     """One GPU-resident case. All work runs in the CUDA library."""
 
@@ -125,6 +154,17 @@ class Solver:
             raise capi.VcpgError(rc, msg)
         K = params.n_poly + 1
         self.shape = (disc.n_elements, 5, K ** 3)
+
+    def set_open_boundary(self, case: CaseData):
+        """Characteristic boundaries, sponge and matching layers of an open case."""
+        ob = open_boundary(case)
+        self._keep_ob = (ob, np.ascontiguousarray(case.elem_nodes, dtype=np.float64))
+        geom = capi.Geometry(capi.ptr(self._keep[7]), capi.ptr(self._keep[8]),
+                             capi.ptr(self._keep[9]), capi.ptr(self._keep[10]))
+        self._check(self.lib.vcpg_set_open_boundary(self.h, C.byref(ob), C.byref(geom),
+                                                     case.spec.p_grid, 1,
+                                                     capi.ptr(self._keep_ob[1])),
+                    "set_open_boundary")
 
     def _check(self, rc: int, what: str):
         if rc != capi.VCPG_OK:
@@ -211,5 +251,7 @@ def create(case: CaseData, metric_compat: bool = True, precision: int = capi.FP6
     if disc is None:
         disc = setup_discretization(case, params)
     s = Solver(params, disc)
+    if case.spec.is_open:
+        s.set_open_boundary(case)
     s.set_state(nodal_to_modal(case, params))
     return s
