@@ -246,6 +246,81 @@ int vcpg_set_open_boundary(vcpg_handle *h, const vcpg_open_boundary *ob,
                            const vcpg_geometry *geom, int32_t p_grid, int32_t dof_location,
                            const double *grid_nodes);
 
+/* ------------------------------------------------------------------------- */
+/* Served ensemble: many cases resident on one GPU, batched by degree.        */
+/* ------------------------------------------------------------------------- */
+/* This has no counterpart in the reference solver, which runs one case per
+ * process. An ensemble keeps every admitted case's state and geometry resident
+ * in per-degree buckets: pre-allocated arenas of elements, boundary faces and
+ * sponge elements. One time step of a bucket advances all of its running cases
+ * together -- one launch of each fused kernel over the bucket's elements,
+ * captured once as a CUDA graph -- each case with its own CFL time step and
+ * parameters. Buckets run on their own streams, so different degrees overlap
+ * on the device. Cases join (vcpg_ensemble_submit) and leave
+ * (vcpg_ensemble_retire) between steps: continuous batching. A case's result
+ * does not depend on the other cases in the mix (every element reads only its
+ * own case's data). Not thread-safe: one host thread drives an ensemble. */
+
+typedef struct vcpg_ensemble vcpg_ensemble;
+
+typedef struct vcpg_ensemble_config {
+  int32_t precision;            /* enum vcpg_precision, all cases                     */
+  int32_t scheme;               /* enum vcpg_scheme, all cases                        */
+  int32_t riemann;              /* enum vcpg_riemann, all cases                       */
+  int32_t metric_index_compat;  /* as in vcpg_params, all cases                       */
+  double theta_sym;             /* as in vcpg_params, all cases                       */
+  double rel_penalty;           /* as in vcpg_params, all cases                       */
+  int64_t bucket_elems[8];      /* element capacity of the bucket of degree p (index
+                                   p, 1..6); 0 = no bucket for that degree            */
+  int64_t bucket_bfaces[8];     /* characteristic boundary faces per bucket           */
+  int64_t bucket_sponge[8];     /* sponge elements per bucket                         */
+  int32_t max_cases;            /* case slots per bucket                              */
+} vcpg_ensemble_config;
+
+/* Allocates every bucket's arenas on the current device (the admission budget). */
+int vcpg_ensemble_create(const vcpg_ensemble_config *cfg, vcpg_ensemble **out);
+int vcpg_ensemble_destroy(vcpg_ensemble *ens);
+const char *vcpg_ensemble_last_error(const vcpg_ensemble *ens);
+
+/* Device bytes one case occupies in its bucket (its admission footprint). */
+int64_t vcpg_ensemble_footprint(int32_t n_poly, int32_t n_int_1d, int64_t n_elem,
+                                int64_t n_bfaces, int64_t n_sponge);
+
+/* Admits a case to run n_steps time steps: the inputs of vcpg_create (params
+ * must match the ensemble's shared settings and the bucket's degree), its
+ * modal state (as vcpg_set_state) and, when ob is non-NULL, its open
+ * boundaries (as vcpg_set_open_boundary). Returns VCPG_E_ADMISSION, with
+ * nothing changed, when the bucket has no contiguous room for the case's
+ * elements, boundary faces or sponge elements, or no free case slot; the
+ * caller keeps the request and submits it again after cases retire. The
+ * uploads are ordered on the bucket's stream before its next step; the case
+ * first evaluates its residual inside that step and then steps with the rest. */
+int vcpg_ensemble_submit(vcpg_ensemble *ens, const vcpg_params *params,
+                         const vcpg_operators *ops, const vcpg_geometry *geom,
+                         const double *modal_state, int32_t n_steps,
+                         const vcpg_open_boundary *ob, int32_t p_grid, int32_t dof_location,
+                         const double *grid_nodes, int64_t *case_id);
+
+/* Enqueues one time step of every bucket with resident cases; does not wait. */
+int vcpg_ensemble_step(vcpg_ensemble *ens);
+
+/* Non-blocking: ids of cases that have completed their steps since the last
+ * poll (at most max_ids), from the most recent step whose state copy has
+ * arrived. */
+int vcpg_ensemble_poll(vcpg_ensemble *ens, int64_t *done_ids, int32_t max_ids,
+                       int32_t *n_done);
+
+/* Copies a completed case's modal state ([n_elem][5][K^3]) and simulated time
+ * to the host and frees its slots for new cases. */
+int vcpg_ensemble_retire(vcpg_ensemble *ens, int64_t case_id, double *modal_state,
+                         double *sim_time);
+
+/* Waits for all enqueued work; reports device-side errors (CG cap, a^2 < 0). */
+int vcpg_ensemble_sync(vcpg_ensemble *ens);
+
+/* Resident (pending or running) cases and this library's launches so far. */
+int vcpg_ensemble_stats(vcpg_ensemble *ens, int32_t *resident, int64_t *launches);
+
 #ifdef __cplusplus
 }
 #endif

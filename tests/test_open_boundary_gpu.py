@@ -9,12 +9,14 @@ and characteristic k faces with Mach-averaged transverse relaxation.
 from __future__ import annotations
 
 import os
+import tempfile
 
 import numpy as np
 import pytest
 
 from conftest import load_golden, open_golden_files, rel_l2
-from vcp3d_open_b200 import capi, cases, solver
+from oracle import records
+from vcp3d_open_b200 import capi, cases, solver, workloads
 
 pytestmark = pytest.mark.gpu
 
@@ -108,5 +110,28 @@ def test_boundary_face_without_condition_is_reported(gpu_available):
         with pytest.raises(capi.VcpgError) as ei:
             s.residual()
         assert ei.value.code == 8
+    finally:
+        s.close()
+
+
+@pytest.mark.skipif(not records.have_reference_build(), reason="oracle/_ref not built")
+def test_config3_pulse_full_size_matches_reference_build(gpu_available):
+    """The open-boundary configuration at full size (40x20x20 elements, p4, NSCBC
+    inflow/outflow, sponge and matching layers): 2 LSRK4 steps vs the reference
+    build run on the same files."""
+    spec = workloads.make_spec("pulse40_p4_lsrk4")
+    case = cases.build_case(spec)
+    s = solver.create(case)
+    try:
+        hist = s.step(2, capi.LSRK4)
+        with tempfile.TemporaryDirectory() as tmp:
+            cfg = cases.write_case(case, tmp)
+            out = os.path.join(tmp, "run.bin")
+            records.run_reference(cfg, "run", out, "--steps", "2", "--scheme", "lsrk4",
+                                  threads=os.cpu_count() or 1)
+            r = records.read_records(out)
+        K3 = (spec.p + 1) ** 3
+        assert rel_l2(s.get_state(), r["sol"][:, :, :K3]) < TOL_STATE
+        np.testing.assert_allclose(hist, r["dtHist"], rtol=TOL_DT)
     finally:
         s.close()

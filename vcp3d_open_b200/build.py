@@ -16,6 +16,7 @@ ROOT = os.path.dirname(PKG)
 BUILD = os.path.join(ROOT, "_build")
 LIB = os.path.join(PKG, "libvcp3d_b200.so")
 SOURCES = ["kernels.cu", "capi.cu", "capi_setup.cpp", "host_setup.cpp", "open_boundary.cpp",
+           "ensemble.cu",
            "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",

@@ -26,7 +26,10 @@ EXPORTED = [
     "vcpg_nodal_conservative_to_modal", "vcpg_set_state", "vcpg_get_state",
     "vcpg_get_residual", "vcpg_residual", "vcpg_get_raw_residual", "vcpg_time_step",
     "vcpg_step", "vcpg_sync", "vcpg_stream", "vcpg_launch_count", "vcpg_stats",
-    "vcpg_time_step_noalloc", "vcpg_set_open_boundary",
+    "vcpg_time_step_noalloc", "vcpg_set_open_boundary", "vcpg_ensemble_create",
+    "vcpg_ensemble_destroy", "vcpg_ensemble_last_error", "vcpg_ensemble_footprint",
+    "vcpg_ensemble_submit", "vcpg_ensemble_step", "vcpg_ensemble_poll", "vcpg_ensemble_retire",
+    "vcpg_ensemble_sync", "vcpg_ensemble_stats",
 ]
 
 
@@ -59,6 +62,15 @@ class OpenBoundary(C.Structure):
                 ("inlet_sigma", C.c_double), ("sponge_elems", C.c_int32 * 6),
                 ("sponge_sigma", C.c_double * 6), ("sponge_alpha", C.c_double * 6),
                 ("cml", C.c_int32), ("sponge_state", C.c_double * 5)]
+
+
+class EnsembleConfig(C.Structure):
+    """vcpg_ensemble_config: shared settings and per-degree bucket capacities."""
+    _fields_ = [("precision", C.c_int32), ("scheme", C.c_int32), ("riemann", C.c_int32),
+                ("metric_index_compat", C.c_int32), ("theta_sym", C.c_double),
+                ("rel_penalty", C.c_double), ("bucket_elems", C.c_int64 * 8),
+                ("bucket_bfaces", C.c_int64 * 8), ("bucket_sponge", C.c_int64 * 8),
+                ("max_cases", C.c_int32)]
 
 
 class VcpgError(RuntimeError):
@@ -103,6 +115,21 @@ def load() -> C.CDLL:
                                            C.c_void_p, C.c_void_p, C.c_void_p]
     lib.vcpg_set_open_boundary.argtypes = [hp, C.POINTER(OpenBoundary), C.POINTER(Geometry),
                                            C.c_int32, C.c_int32, dp]
+    lib.vcpg_ensemble_create.argtypes = [C.POINTER(EnsembleConfig), C.POINTER(C.c_void_p)]
+    lib.vcpg_ensemble_destroy.argtypes = [hp]
+    lib.vcpg_ensemble_last_error.argtypes = [hp]
+    lib.vcpg_ensemble_last_error.restype = C.c_char_p
+    lib.vcpg_ensemble_footprint.argtypes = [C.c_int32, C.c_int32, C.c_int64, C.c_int64, C.c_int64]
+    lib.vcpg_ensemble_footprint.restype = C.c_int64
+    lib.vcpg_ensemble_submit.argtypes = [hp, C.POINTER(Params), C.POINTER(Operators),
+                                         C.POINTER(Geometry), dp, C.c_int32,
+                                         C.POINTER(OpenBoundary), C.c_int32, C.c_int32, dp,
+                                         C.POINTER(C.c_int64)]
+    lib.vcpg_ensemble_step.argtypes = [hp]
+    lib.vcpg_ensemble_poll.argtypes = [hp, C.POINTER(C.c_int64), C.c_int32, C.POINTER(C.c_int32)]
+    lib.vcpg_ensemble_retire.argtypes = [hp, C.c_int64, dp, dp]
+    lib.vcpg_ensemble_sync.argtypes = [hp]
+    lib.vcpg_ensemble_stats.argtypes = [hp, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
     _lib = lib
     return lib
 

@@ -43,6 +43,7 @@ struct vcpg_handle {
   int *d_bface = nullptr;
   double *d_bpresc = nullptr, *d_pc = nullptr, *d_dlq = nullptr;
   double *d_btrace = nullptr, *d_bmach = nullptr, *d_bflux = nullptr;
+  BlockFaceCfg *d_cfg = nullptr;
   int *d_sponge = nullptr;
   double *d_dampfn = nullptr, *d_dampst = nullptr, *d_cml = nullptr;
   int cml_on = 0;
@@ -153,7 +154,7 @@ BoundaryArgs MakeBoundaryArgs(vcpg_handle *h) {
   b.theta_sym = h->prm.theta_sym;
   b.riemann = h->prm.riemann;
   b.metric_compat = h->prm.metric_index_compat;
-  for (int f = 0; f < 6; ++f) b.cfg[f] = h->cfg[f];
+  b.cfgs = h->d_cfg;
   return b;
 }
 
@@ -186,14 +187,14 @@ int EnqueueStep(vcpg_handle *h, int scheme) {
     const double betaRK[] = {1.0, 1.0 / 4.0, 2.0 / 3.0};
     for (int s = 0; s < 3; ++s) {
       VCPG_CUDA(h, LaunchSspStage(h->d_sol, h->d_solOld, h->d_res, h->d_dt, alphaRK[s], betaRK[s],
-                                  s == 0, n, h->stream));
+                                  s == 0, n, h->stream, CaseView{}, 5 * h->KD));
       int rc = EnqueueResidual(h, a, nullptr);
       if (rc) return rc;
     }
   } else {
     for (int s = 0; s < 5; ++s) {
       VCPG_CUDA(h, LaunchLsrkStage(h->d_sol, h->d_solOld, h->d_res, h->d_dt, kLsA[s], kLsB[s], n,
-                                   h->stream));
+                                   h->stream, CaseView{}, 5 * h->KD));
       int rc = EnqueueResidual(h, a, nullptr);
       if (rc) return rc;
     }
@@ -217,7 +218,7 @@ int vcpg_destroy(vcpg_handle *h) {
                   h->d_nbr, h->d_dtbits, h->d_mach2, h->d_dt, h->d_fixed, h->d_hist,
                   h->d_status, h->d_counter, h->d_cgstats, h->d_bface, h->d_bpresc, h->d_pc,
                   h->d_dlq, h->d_btrace, h->d_bmach, h->d_bflux, h->d_sponge, h->d_dampfn,
-                  h->d_dampst, h->d_cml};
+                  h->d_dampst, h->d_cml, h->d_cfg};
   for (void *p : bufs)
     if (p) cudaFree(p);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -257,26 +258,10 @@ int vcpg_create(const vcpg_params *params, const vcpg_operators *ops, const vcpg
   const int K = h->K, M = h->M;
   // Operator table into the (K, M) constant slot.
   OpTable t;
-  std::memset(&t, 0, sizeof(t));
-  for (int k = 0; k < K; ++k)
-    for (int m = 0; m < M; ++m) {
-      t.leg[k * M + m] = ops->leg_int[k * M + m];
-      t.dleg[k * M + m] = ops->dleg_int[k * M + m];
-    }
-  for (int i = 0; i < 2 * K; ++i) {
-    t.face[i] = ops->leg_face[i];
-    t.dface[i] = ops->dleg_face[i];
-  }
-  for (int m = 0; m < M; ++m) t.w[m] = ops->w_int[m];
-  for (int i = 0; i < K * K; ++i) t.legdof[i] = ops->leg_dofs[i];
-  for (int i = 0; i < h->KD; ++i) t.center[i] = ops->basis_center[i];
-  // FP32 copies, rounded once from the FP64 operators, for the mixed form.
-  for (int i = 0; i < K * M; ++i) { t.legf[i] = (float)t.leg[i]; t.dlegf[i] = (float)t.dleg[i]; }
-  for (int i = 0; i < 2 * K; ++i) { t.facef[i] = (float)t.face[i]; t.dfacef[i] = (float)t.dface[i]; }
-  for (int m = 0; m < M; ++m) t.wf[m] = (float)t.w[m];
-  for (int i = 0; i < h->KD; ++i) t.centerf[i] = (float)t.center[i];
+  FillOpTable(ops, K, M, &t);
   VCPG_CUDA(h, UploadOpTable(SlotOf(K, M), t));
 
+  VCPG_CUDA(h, ConfigureResidual(K, M));
   VCPG_CUDA(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
   const size_t nState = (size_t)h->nE * 5 * h->KD;
   auto alloc = [&](void **p, size_t bytes) -> int {
@@ -497,7 +482,8 @@ int vcpg_set_open_boundary(vcpg_handle *h, const vcpg_open_boundary *ob,
       (rc = upload((void **)&h->d_sponge, ob_host.spongeIdx.data(), sizeof(int) * ob_host.spongeIdx.size())) ||
       (rc = upload((void **)&h->d_dampfn, ob_host.dampFn.data(), sizeof(double) * nS * 3 * MD)) ||
       (rc = upload((void **)&h->d_dampst, ob_host.dampState.data(), sizeof(double) * nS * 5 * MD)) ||
-      (rc = upload((void **)&h->d_cml, ob_host.cml.data(), sizeof(double) * nS * 6)))
+      (rc = upload((void **)&h->d_cml, ob_host.cml.data(), sizeof(double) * nS * 6)) ||
+      (rc = upload((void **)&h->d_cfg, ob_host.cfg, sizeof(BlockFaceCfg) * 6)))
     return rc;
   // Boundary faces are coded in the neighbour table as -2 - (boundary-face index).
   VCPG_CUDA(h, cudaMemcpy(h->d_nbr, ob_host.nbrCode.data(), sizeof(int32_t) * ob_host.nbrCode.size(),

@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include "dg_physics.cuh"
+#include "dg_residual.cuh"
 #include "dg_tensor.cuh"
 #include "open_boundary.h"
 
@@ -41,8 +42,20 @@ struct BoundaryArgs {
   int nB;
   double mu, tau_num, theta_sym;
   int riemann, metric_compat;
-  BlockFaceCfg cfg[6];
+  const BlockFaceCfg *cfgs;    // [nCases][6] per case and block face
+  // Several cases per launch (null case_state: one case): the case slot is entry
+  // kBfCase of the boundary-face row; only faces of cases in state `require` run.
+  const int *case_state;
+  const double *case_par;      // [nCases][kCasePar]
+  int require;
 };
+
+// True when boundary face row bf belongs to a case this launch processes.
+__device__ __forceinline__ bool BoundaryFaceActive(const BoundaryArgs &a, const int *bf) {
+  if (!a.case_state) return true;
+  const int c = bf[kBfCase];
+  return c >= 0 && a.case_state[c] == a.require;
+}
 
 __device__ __forceinline__ int BFastParam(const int d) { return d == 0 ? 1 : 0; }
 
@@ -56,6 +69,7 @@ __global__ void __launch_bounds__(NT) BoundaryTraceKernel(const BoundaryArgs a) 
   const int b = blockIdx.x;
   if (b >= a.nB) return;
   const int *bf = a.bface + b * kBfStride;
+  if (!BoundaryFaceActive(a, bf)) return;
   const int e = bf[kBfElem], f = bf[kBfFace], d = f / 2, side = f % 2;
   const double *src = a.sol + (size_t)e * 5 * KD;
   for (int i = threadIdx.x; i < 5 * KD; i += NT) s_sol[i] = src[i];
@@ -125,9 +139,12 @@ __global__ void __launch_bounds__(NT) BoundaryFluxKernel(const BoundaryArgs a) {
   const int b = blockIdx.x;
   if (b >= a.nB) return;
   const int *bf = a.bface + b * kBfStride;
+  if (!BoundaryFaceActive(a, bf)) return;
   const int e = bf[kBfElem], f = bf[kBfFace], type = bf[kBfType], d = f / 2;
   const int ig[3] = {bf[kBfGrad], bf[kBfGrad + 1], bf[kBfGrad + 2]};
-  const BlockFaceCfg &c = a.cfg[f];
+  const int cs = a.case_state ? bf[kBfCase] : 0;
+  const BlockFaceCfg c = a.cfgs[cs * 6 + f];
+  const double mu = a.case_state ? a.case_par[cs * kCasePar + kParMu] : a.mu;
   const double factNorm = (f % 2 == 0) ? -1.0 : 1.0;
   const double *fm = a.face_metric + ((size_t)e * 6 + f) * 13 * M2;
   const double *tr = a.btrace + (size_t)b * 4 * 5 * M2;
@@ -352,7 +369,7 @@ __global__ void __launch_bounds__(NT) BoundaryFluxKernel(const BoundaryArgs a) {
       IsmailRoeFlux(VL, VR, nx, ny, nz, wf * area, flux);
     else
       RoeFlux(VL, VR, nx, ny, nz, 0.5 * wf * area, flux);
-    ViscousPenaltySymFlux(VL, VR, gx, gy, gz, nx, ny, nz, wf, area, a.mu,
+    ViscousPenaltySymFlux(VL, VR, gx, gy, gz, nx, ny, nz, wf, area, mu,
                           a.tau_num / lenScale, a.theta_sym, flux, sx, sy, sz);
     double *out = a.bflux + (size_t)b * 4 * 5 * M2;
     const int pFast = BFastParam(d), pSlow = 3 - d - pFast;

@@ -20,6 +20,21 @@
 
 namespace vcpg {
 
+// States of a case in a bucket that holds several cases (csrc/ensemble.cu).
+enum CaseState { kCaseFree = 0, kCasePending = 1, kCaseRunning = 2, kCaseDone = 3 };
+// Per-case parameters, [nCases][kCasePar].
+enum CasePar { kParMu = 0, kParPRef = 1, kParURef = 2, kParRhoRef = 3, kParCfl = 4, kCasePar = 8 };
+
+// Per-case view of a bucket holding several cases of one (K, M) pair; a null
+// elem_case means a single case (case 0) whose parameters are the scalars of
+// the launch arguments.
+struct CaseView {
+  const int *elem_case;  // [nE] case slot of each element, -1 = unused element
+  const int *state;      // [nCases] enum CaseState
+  const double *par;     // [nCases][kCasePar]
+  int require;           // the state a residual or boundary launch processes
+};
+
 struct ResidualArgs {
   const double *sol;           // [nE][5][K^3]
   double *res;                 // [nE][5][K^3] residual after the mass-matrix solve
@@ -48,6 +63,7 @@ struct ResidualArgs {
   const double *damp_state;    // [nS][5][M^3] conservative damping state
   const double *cml;           // [nS][6] 1/sigma per direction, layer orientation
   int cml_on;                  // characteristic matching layer in sponge elements
+  CaseView cases;              // several cases per launch (null elem_case: one case)
 };
 
 // Arguments of the CFL time-step kernel (kernels.cu).
@@ -57,8 +73,9 @@ struct TimeStepArgs {
   int n_elem;
   int n_poly;
   double cfl, mu, p_ref, u_ref, rho_ref;
-  unsigned long long *dt_bits;
+  unsigned long long *dt_bits;  // per case: bits of the minimum over its elements
   int *status;  // [2]: negative a^2 seen
+  CaseView cases;  // several cases: per-case parameters and time steps
 };
 
 template <int NT, typename T>
@@ -234,7 +251,7 @@ __device__ __forceinline__ void MatchingLayerSource(const ResidualArgs &a, const
 // and J*w.  Follows ElementClass::VolumeResidual, src/ElementClass.cpp:3809-4443.
 // ---------------------------------------------------------------------------
 template <int NT, int K, int M, typename T, bool OPEN>
-__device__ __forceinline__ void VolumePhase(const ResidualArgs &a, const int e,
+__device__ __forceinline__ void VolumePhase(const ResidualArgs &a, const int e, const double mu,
                                             const T *s_sol, T *s_R, T *s_cgp,
                                             T *s_jw, T *work, T *s_red) {
   constexpr int SLOT = Slot<K, M>::value;
@@ -321,8 +338,8 @@ __device__ __forceinline__ void VolumePhase(const ResidualArgs &a, const int e,
     s_jw[l] = Wl * Jl;
     const T weight = -Jl * Wl;
     const T ru = rho * u, rv = rho * v, rw = rho * w;
-    const T muTot = a.mu + T(0.0);
-    const T factHeatFluxTot = a.mu * T(kFactHFLam) + T(0.0) * T(kFactHFTurb);
+    const T muTot = T(mu) + T(0.0);
+    const T factHeatFluxTot = T(mu) * T(kFactHFLam) + T(0.0) * T(kFactHFTurb);
     const T divVelTerm = T(kLamOverMu) * (dudx + dvdy + dwdz);
     const T tauxx = muTot * (T(2.0) * dudx + divVelTerm);
     const T tauyy = muTot * (T(2.0) * dvdy + divVelTerm);
@@ -499,8 +516,8 @@ __device__ __forceinline__ void TraceCartesianGrad(const T *TR, const int t, con
 // the own side's sign), 2 face-normal symmetrizing flux; P2[d][v][M2] the
 // slow-axis symmetrizing flux.
 template <int K, int M, typename T>
-__device__ __forceinline__ void GroupFacePoint(const ResidualArgs &a, const int g, const int d,
-                                               const int pt, const T *TR,
+__device__ __forceinline__ void GroupFacePoint(const ResidualArgs &a, const double mu, const int g,
+                                               const int d, const int pt, const T *TR,
                                                const double *fmOwn, const double *fmNb,
                                                const T lenScale, T *P1, T *P2) {
   constexpr int SLOT = Slot<K, M>::value;
@@ -535,7 +552,7 @@ __device__ __forceinline__ void GroupFacePoint(const ResidualArgs &a, const int 
   else
     RoeFlux(VL, VR, nx, ny, nz, T(0.5) * wf * area, flux);
   T sx[5], sy[5], sz[5];
-  ViscousPenaltySymFlux(VL, VR, gx, gy, gz, nx, ny, nz, wf, area, T(a.mu),
+  ViscousPenaltySymFlux(VL, VR, gx, gy, gz, nx, ny, nz, wf, area, T(mu),
                         T(a.tau_num) / lenScale, T(a.theta_sym), flux, sx, sy, sz);
   const double *fm = g == 0 ? fmR : fmL;  // the own side's metric
   const int pFast = FastParam(d);
@@ -557,8 +574,8 @@ __device__ __forceinline__ void GroupFacePoint(const ResidualArgs &a, const int 
 }
 
 template <int NT, int K, int M, typename T, bool OPEN>
-__device__ __forceinline__ void FacePhase(const ResidualArgs &a, const int e, const T *s_sol,
-                                          T *s_R, const T *s_fv, T *work) {
+__device__ __forceinline__ void FacePhase(const ResidualArgs &a, const int e, const double mu,
+                                          const T *s_sol, T *s_R, const T *s_fv, T *work) {
   constexpr int SLOT = Slot<K, M>::value;
   constexpr int KD = K * K * K, M2 = M * M, K2 = K * K;
   static_assert(2 * M <= 3 * K && K <= 2 * M, "face-phase buffer aliasing");
@@ -612,7 +629,7 @@ __device__ __forceinline__ void FacePhase(const ResidualArgs &a, const int e, co
       const T lenScale = Fmin(T(sc[d]), T(a.elem_scalars[(size_t)nb * 15 + d]));
       const double *fmOwn = a.face_metric + ((size_t)e * 6 + 2 * d + g) * 13 * M2;
       const double *fmNb = a.face_metric + ((size_t)nb * 6 + 2 * d + 1 - g) * 13 * M2;
-      GroupFacePoint<K, M>(a, g, d, pt, TR, fmOwn, fmNb, lenScale, P1, P2);
+      GroupFacePoint<K, M>(a, mu, g, d, pt, TR, fmOwn, fmNb, lenScale, P1, P2);
     }
     __syncthreads();
     // Distribution (TPR[IJK]F): slow axis, fast axis, then the face-normal expansion.
@@ -833,6 +850,13 @@ __global__ void __launch_bounds__(NT, (Plan<K, M, T, OPEN>::MIN_BLOCKS)) Residua
   T *s_red = s_jw + MD, *s_fv = s_red + 64, *work = s_fv + 4 * kKMax;
   const int e = blockIdx.x;
   if (e >= a.n_elem) return;
+  // Several cases per launch: skip unused elements and cases in another state.
+  double mu = a.mu;
+  if (a.cases.elem_case) {
+    const int cs = a.cases.elem_case[e];
+    if (cs < 0 || a.cases.state[cs] != a.cases.require) return;
+    mu = a.cases.par[cs * kCasePar + kParMu];
+  }
   const double *src = a.sol + (size_t)e * 5 * KD;
   for (int i = threadIdx.x; i < 5 * KD; i += NT) s_sol[i] = T(src[i]);
   if (threadIdx.x < 2 * K) {
@@ -840,8 +864,8 @@ __global__ void __launch_bounds__(NT, (Plan<K, M, T, OPEN>::MIN_BLOCKS)) Residua
     s_fv[2 * K + threadIdx.x] = FaceDer<Slot<K, M>::value, T>(threadIdx.x);
   }
   __syncthreads();
-  VolumePhase<NT, K, M, T, OPEN>(a, e, s_sol, s_R, s_cgp, s_jw, work, s_red);
-  FacePhase<NT, K, M, T, OPEN>(a, e, s_sol, s_R, s_fv, work);
+  VolumePhase<NT, K, M, T, OPEN>(a, e, mu, s_sol, s_R, s_cgp, s_jw, work, s_red);
+  FacePhase<NT, K, M, T, OPEN>(a, e, mu, s_sol, s_R, s_fv, work);
   if (a.res_raw) {
     double *dst = a.res_raw + (size_t)e * 5 * KD;
     for (int i = threadIdx.x; i < 5 * KD; i += NT) dst[i] = double(s_R[i]);

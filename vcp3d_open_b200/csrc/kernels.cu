@@ -1,6 +1,8 @@
 // Kernel instantiations and launchers for every supported (K, M) pair:
 // the fused residual kernel, the CFL time-step kernel and the Runge-Kutta
 // stage updates.
+#include <cstring>
+
 #include "dg_boundary.cuh"
 #include "dg_residual.cuh"
 #include "kernels.h"
@@ -21,6 +23,18 @@ __global__ void __launch_bounds__(NT) TimeStepKernel(const TimeStepArgs a) {
   __shared__ double s_sol[5 * KD], s_t1[5 * KD], s_t2[5 * KD], s_red[64];
   const int e = blockIdx.x;
   if (e >= a.n_elem) return;
+  // Several cases per launch: per-case parameters, pending and running cases only.
+  int cs = 0;
+  double cfl = a.cfl, mu = a.mu, pRef = a.p_ref, uRef = a.u_ref, rhoRef = a.rho_ref;
+  if (a.cases.elem_case) {
+    cs = a.cases.elem_case[e];
+    if (cs < 0) return;
+    const int st = a.cases.state[cs];
+    if (st != kCasePending && st != kCaseRunning) return;
+    const double *pc = a.cases.par + cs * kCasePar;
+    mu = pc[kParMu]; pRef = pc[kParPRef]; uRef = pc[kParURef]; rhoRef = pc[kParRhoRef];
+    cfl = pc[kParCfl];
+  }
   const double *src = a.sol + (size_t)e * 5 * KD;
   for (int i = threadIdx.x; i < 5 * KD; i += NT) s_sol[i] = src[i];
   __syncthreads();
@@ -31,7 +45,7 @@ __global__ void __launch_bounds__(NT) TimeStepKernel(const TimeStepArgs a) {
   Contract<NT, SLOT, K, M, kLegDof, 0, 5, K, K, K, K, K, false>(s_t2, s_t1);
   __syncthreads();
   const double *sc = a.elem_scalars + (size_t)e * 15;
-  const double muDim = a.mu * a.p_ref / a.u_ref;
+  const double muDim = mu * pRef / uRef;
   const double dliInv = 1.0 / sc[0], dljInv = 1.0 / sc[1], dlkInv = 1.0 / sc[2];
   const double dli2Inv = dliInv * dliInv, dlj2Inv = dljInv * dljInv, dlk2Inv = dlkInv * dlkInv;
   const double dLen2Inv = dli2Inv + dlj2Inv + dlk2Inv;
@@ -41,7 +55,7 @@ __global__ void __launch_bounds__(NT) TimeStepKernel(const TimeStepArgs a) {
     double rho, u, v, w, p, eKin;
     EntropyToPrim(s_t1[l], s_t1[KD + l], s_t1[2 * KD + l], s_t1[3 * KD + l], s_t1[4 * KD + l],
                   rho, u, v, w, p, eKin);
-    rho *= a.rho_ref; u *= a.u_ref; v *= a.u_ref; w *= a.u_ref; p *= a.p_ref;
+    rho *= rhoRef; u *= uRef; v *= uRef; w *= uRef; p *= pRef;
     const double rhoInv = 1.0 / rho;
     const double a2 = kGam * p * rhoInv;
     const double velI = u * sc[6] + v * sc[7] + w * sc[8];
@@ -63,8 +77,8 @@ __global__ void __launch_bounds__(NT) TimeStepKernel(const TimeStepArgs a) {
     const double f1[] = {2.0, 6.0, 12.0, 20.0, 28.0, 38.0, 50.0, 64.0, 80.0, 98.0};
     const double f2[] = {6.0, 36.0, 150.0, 420.0, 980.0, 1975.0, 3575.0, 7000.0, 14000.0, 28000.0};
     const double dtInv = f1[a.n_poly] * radInvMax + f2[a.n_poly] * radVisMax;
-    const double dtElem = a.cfl * a.u_ref / dtInv;
-    atomicMin(a.dt_bits, (unsigned long long)__double_as_longlong(dtElem));
+    const double dtElem = cfl * uRef / dtInv;
+    atomicMin(a.dt_bits + cs, (unsigned long long)__double_as_longlong(dtElem));
   }
 }
 
@@ -80,12 +94,49 @@ __global__ void FinalizeDtKernel(unsigned long long *dt_bits, const double *fixe
   *dt_bits = (unsigned long long)__double_as_longlong(1.e+10);
 }
 
+// Case of state entry i for several cases per launch (elem_case non-null):
+// -1 unless the case is running. One case: 0.
+__device__ __forceinline__ int StageCase(const CaseView &cv, const size_t i, const int elemSize) {
+  if (!cv.elem_case) return 0;
+  const int c = cv.elem_case[i / (size_t)elemSize];
+  return (c >= 0 && cv.state[c] == kCaseRunning) ? c : -1;
+}
+
+// Per-case start of a time step in a bucket holding several cases: a pending
+// case (its residual was evaluated earlier in this step) starts running; a
+// running case that has taken its target steps is done (time step 0, skipped
+// by every later kernel); otherwise its reduced CFL step is taken and counted.
+__global__ void EnsembleFinalizeKernel(int n_cases, int *state, const int *target, int *done,
+                                       unsigned long long *dt_bits, double *dt,
+                                       double *sim_time) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n_cases) return;
+  int st = state[c];
+  if (st == kCasePending) st = kCaseRunning;
+  if (st == kCaseRunning) {
+    if (done[c] >= target[c]) {
+      st = kCaseDone;
+      dt[c] = 0.0;
+    } else {
+      const double d = __longlong_as_double((long long)dt_bits[c]);
+      dt[c] = d;
+      sim_time[c] += d;
+      done[c] += 1;
+    }
+  }
+  state[c] = st;
+  dt_bits[c] = (unsigned long long)__double_as_longlong(1.e+10);
+}
+
 // SSP-RK3 stage (src/SolverClass.cpp:2368-2396); stage 0 also stores solOld.
 __global__ void SspStageKernel(double *sol, double *solOld, const double *res, const double *d_dt,
-                               double alpha, double beta, int copyOld, size_t n) {
+                               double alpha, double beta, int copyOld, size_t n,
+                               const CaseView cv, int elemSize) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const double betaDt = beta * (*d_dt);
+  const int c = StageCase(cv, i, elemSize);
+  if (c < 0) return;
+  const double betaDt = beta * d_dt[c];
   const double oneMinAlpha = 1.0 - alpha;
   const double s = sol[i];
   double so;
@@ -95,10 +146,12 @@ __global__ void SspStageKernel(double *sol, double *solOld, const double *res, c
 
 // Low-storage RK stage: dU = a dU - dt R; U += b dU (a == 0 starts a new step).
 __global__ void LsrkStageKernel(double *sol, double *du, const double *res, const double *d_dt,
-                                double ca, double cb, size_t n) {
+                                double ca, double cb, size_t n, const CaseView cv, int elemSize) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const double dt = *d_dt;
+  const int c = StageCase(cv, i, elemSize);
+  if (c < 0) return;
+  const double dt = d_dt[c];
   const double d = (ca == 0.0) ? -dt * res[i] : ca * du[i] - dt * res[i];
   du[i] = d;
   sol[i] = sol[i] + cb * d;
@@ -107,19 +160,35 @@ __global__ void LsrkStageKernel(double *sol, double *du, const double *res, cons
 // ---------------------------------------------------------------------------
 // Launchers.
 // ---------------------------------------------------------------------------
+// Dynamic shared-memory limit of one residual-kernel variant, set once (outside
+// any stream capture: ConfigureResidual runs before the first captured step).
+template <int K, int M, typename T, bool OPEN>
+static cudaError_t ConfigureKMT() {
+  using P = Plan<K, M, T, OPEN>;
+  static bool configured = false;
+  if (configured) return cudaSuccess;
+  cudaError_t err = cudaFuncSetAttribute(ResidualKernel<K, M, P::NT, T, OPEN>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)P::BYTES);
+  if (err == cudaSuccess) configured = true;
+  return err;
+}
+
+template <int K, int M>
+static cudaError_t ConfigureKM() {
+  cudaError_t e = ConfigureKMT<K, M, double, false>();
+  if (e == cudaSuccess) e = ConfigureKMT<K, M, float, false>();
+  if (e == cudaSuccess) e = ConfigureKMT<K, M, double, true>();
+  if (e == cudaSuccess) e = ConfigureKMT<K, M, float, true>();
+  return e;
+}
+
 template <int K, int M, typename T, bool OPEN>
 static cudaError_t LaunchResidualKMT(const ResidualArgs &a, cudaStream_t st) {
   using P = Plan<K, M, T, OPEN>;
-  constexpr int NT = P::NT;
-  const size_t bytes = P::BYTES;
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t err = cudaFuncSetAttribute(ResidualKernel<K, M, NT, T, OPEN>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    if (err != cudaSuccess) return err;
-    configured = true;
-  }
-  ResidualKernel<K, M, NT, T, OPEN><<<a.n_elem, NT, bytes, st>>>(a);
+  cudaError_t err = ConfigureKMT<K, M, T, OPEN>();
+  if (err != cudaSuccess) return err;
+  ResidualKernel<K, M, P::NT, T, OPEN><<<a.n_elem, P::NT, P::BYTES, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -187,6 +256,15 @@ cudaError_t LaunchResidual(int K, int M, const ResidualArgs &a, cudaStream_t st)
   return cudaErrorInvalidValue;
 }
 
+cudaError_t ConfigureResidual(int K, int M) {
+  if (K == 2 && M == 3) return ConfigureKM<2, 3>();
+  if (K == 3 && M == 4) return ConfigureKM<3, 4>();
+  if (K == 4 && M == 5) return ConfigureKM<4, 5>();
+  if (K == 5 && M == 7) return ConfigureKM<5, 7>();
+  if (K == 6 && M == 8) return ConfigureKM<6, 8>();
+  return cudaErrorInvalidValue;
+}
+
 cudaError_t LaunchBoundary(int K, int M, const BoundaryArgs &a, cudaStream_t st) {
   if (a.nB <= 0) return cudaSuccess;
   if (K == 2 && M == 3) return LaunchBoundaryKM<2, 3>(a, st);
@@ -213,19 +291,52 @@ cudaError_t LaunchFinalizeDt(unsigned long long *dt_bits, const double *fixed_dt
   return cudaGetLastError();
 }
 
+cudaError_t LaunchEnsembleFinalize(int n_cases, int *state, const int *target, int *done,
+                                   unsigned long long *dt_bits, double *dt, double *sim_time,
+                                   cudaStream_t st) {
+  if (n_cases <= 0) return cudaSuccess;
+  EnsembleFinalizeKernel<<<(n_cases + 127) / 128, 128, 0, st>>>(n_cases, state, target, done,
+                                                                dt_bits, dt, sim_time);
+  return cudaGetLastError();
+}
+
 cudaError_t LaunchSspStage(double *sol, double *solOld, const double *res, const double *d_dt,
-                           double alpha, double beta, int copyOld, size_t n, cudaStream_t st) {
+                           double alpha, double beta, int copyOld, size_t n, cudaStream_t st,
+                           const CaseView &cv, int elemSize) {
   const int nt = 256;
   SspStageKernel<<<(unsigned)((n + nt - 1) / nt), nt, 0, st>>>(sol, solOld, res, d_dt, alpha,
-                                                               beta, copyOld, n);
+                                                               beta, copyOld, n, cv, elemSize);
   return cudaGetLastError();
 }
 
 cudaError_t LaunchLsrkStage(double *sol, double *du, const double *res, const double *d_dt,
-                            double ca, double cb, size_t n, cudaStream_t st) {
+                            double ca, double cb, size_t n, cudaStream_t st, const CaseView &cv,
+                            int elemSize) {
   const int nt = 256;
-  LsrkStageKernel<<<(unsigned)((n + nt - 1) / nt), nt, 0, st>>>(sol, du, res, d_dt, ca, cb, n);
+  LsrkStageKernel<<<(unsigned)((n + nt - 1) / nt), nt, 0, st>>>(sol, du, res, d_dt, ca, cb, n,
+                                                                cv, elemSize);
   return cudaGetLastError();
+}
+
+void FillOpTable(const vcpg_operators *ops, int K, int M, OpTable *t) {
+  std::memset(t, 0, sizeof(*t));
+  for (int k = 0; k < K; ++k)
+    for (int m = 0; m < M; ++m) {
+      t->leg[k * M + m] = ops->leg_int[k * M + m];
+      t->dleg[k * M + m] = ops->dleg_int[k * M + m];
+    }
+  for (int i = 0; i < 2 * K; ++i) {
+    t->face[i] = ops->leg_face[i];
+    t->dface[i] = ops->dleg_face[i];
+  }
+  for (int m = 0; m < M; ++m) t->w[m] = ops->w_int[m];
+  for (int i = 0; i < K * K; ++i) t->legdof[i] = ops->leg_dofs[i];
+  for (int i = 0; i < K * K * K; ++i) t->center[i] = ops->basis_center[i];
+  // FP32 copies, rounded once from the FP64 operators, for the mixed form.
+  for (int i = 0; i < K * M; ++i) { t->legf[i] = (float)t->leg[i]; t->dlegf[i] = (float)t->dleg[i]; }
+  for (int i = 0; i < 2 * K; ++i) { t->facef[i] = (float)t->face[i]; t->dfacef[i] = (float)t->dface[i]; }
+  for (int m = 0; m < M; ++m) t->wf[m] = (float)t->w[m];
+  for (int i = 0; i < K * K * K; ++i) t->centerf[i] = (float)t->center[i];
 }
 
 cudaError_t UploadOpTable(int slot, const OpTable &t) {

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <cstddef>
 
+#include "../../include/vcp3d_b200.h"
 #include "dg_tensor.cuh"
 
 namespace vcpg {
@@ -11,21 +12,34 @@ namespace vcpg {
 struct ResidualArgs;
 struct TimeStepArgs;
 struct BoundaryArgs;
+struct CaseView;
 
 bool Supported(int K, int M);
 int SlotOf(int K, int M);
 size_t ResidualSmemBytes(int K, int M);
+// Operator table of a (K, M) pair from the C-ABI operators (FP64 and FP32 copies).
+void FillOpTable(const vcpg_operators *ops, int K, int M, OpTable *t);
 cudaError_t UploadOpTable(int slot, const OpTable &t);
+// Per-case step bookkeeping of a bucket holding several cases (csrc/ensemble.cu).
+cudaError_t LaunchEnsembleFinalize(int n_cases, int *state, const int *target, int *done,
+                                   unsigned long long *dt_bits, double *dt, double *sim_time,
+                                   cudaStream_t st);
 
 cudaError_t LaunchResidual(int K, int M, const ResidualArgs &a, cudaStream_t st);
+// Sets the shared-memory limits of all residual-kernel variants of a (K, M) pair;
+// call before capturing launches into a CUDA graph.
+cudaError_t ConfigureResidual(int K, int M);
 // Boundary traces + Mach weights, then the boundary states and fluxes (2 launches).
 cudaError_t LaunchBoundary(int K, int M, const BoundaryArgs &a, cudaStream_t st);
 cudaError_t LaunchTimeStep(int K, int M, const TimeStepArgs &a, cudaStream_t st);
 cudaError_t LaunchFinalizeDt(unsigned long long *dt_bits, const double *fixed_dt, double *d_dt,
                              double *hist, int hist_cap, int *counter, cudaStream_t st);
+// Stage updates; d_dt holds one time step per case (one entry for a single case).
 cudaError_t LaunchSspStage(double *sol, double *solOld, const double *res, const double *d_dt,
-                           double alpha, double beta, int copyOld, size_t n, cudaStream_t st);
+                           double alpha, double beta, int copyOld, size_t n, cudaStream_t st,
+                           const CaseView &cv, int elemSize);
 cudaError_t LaunchLsrkStage(double *sol, double *du, const double *res, const double *d_dt,
-                            double ca, double cb, size_t n, cudaStream_t st);
+                            double ca, double cb, size_t n, cudaStream_t st, const CaseView &cv,
+                            int elemSize);
 
 }  // namespace vcpg

@@ -30,6 +30,7 @@ enum BFaceField {
   kBfFace = 1,   // block face / element face 0..5 (2 d + side)
   kBfType = 2,   // enum vcpg_bc
   kBfGrad = 3,   // 3 entries: parametric axis of the normal, first and second transverse
+  kBfCase = 6,   // case slot when a launch holds several cases (0 for one case)
   kBfStride = 8
 };
 

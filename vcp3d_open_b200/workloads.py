@@ -25,6 +25,18 @@ WORKLOADS = {
     "tgv20_p3_lsrk4": dict(_TGV, n_elem=(20, 20, 20), p=3),
     # Degree 4 on 16^3 elements: the mixed-versus-FP64 test case (fits a test's time).
     "tgv16_p4_lsrk4": dict(_TGV, n_elem=(16, 16, 16), p=4),
+    # Acoustic pulse with open boundaries: [0,20]x[0,10]x[0,10], 40x20x20 elements of
+    # degree 4 (2,000,000 DOFs), pressure pulse 1e-3 of width 0.5 at (10, 5, 5) in a
+    # Mach 0.3 stream along x; static-inflow PC-NSCBC on i-min, outflow PC-NSCBC
+    # (sigma 0.25, L 1, beta_l = beta_t = 0.5, (1 - beta) form, boundary-averaged
+    # Mach) on i-max and both j faces, sponge layers of 4 (i-max) and 3 (j faces)
+    # elements with the matching layer, k periodic.
+    "pulse40_p4_lsrk4": dict(kind="pulse", n_elem=(40, 20, 20), p=4, hi=(20.0, 10.0, 10.0),
+                             mach=0.3, grid_map="none", center=(10.0, 5.0, 5.0),
+                             pulse_amp=1.0e-3, pulse_width=0.5,
+                             bc=("inflow_static_nscbc", "outflow_nscbc", "outflow_nscbc",
+                                 "outflow_nscbc", "periodic", "periodic"),
+                             sponge=(0, 4, 3, 3, 0, 0), cml=True),
 }
 
 
