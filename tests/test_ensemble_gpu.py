@@ -124,3 +124,39 @@ def test_request_loop_small_stream(gpu_available):
     assert rep["latency_p99_s"] >= rep["latency_p50_s"] > 0.0
     for state, t in rep["results"].values():
         assert np.all(np.isfinite(state)) and t > 0.0
+
+
+def test_slot_reuse_keeps_results(gpu_available):
+    """Fewer case slots than cases: slots are reused while other cases keep
+    stepping; every result stays bit-identical to the case run alone."""
+    specs = _specs()
+    prepared = [serving.prepare(s, capi.FP64) for s in specs]
+    caps = _caps(specs)
+    alone = []
+    for pc in prepared:
+        ens = serving.Ensemble(caps, precision=capi.FP64, max_cases=2)
+        cid = ens.submit(pc, STEPS)
+        alone.append(_run_to_completion(ens, [cid])[cid])
+        ens.close()
+    ens = serving.Ensemble(caps, precision=capi.FP64, max_cases=2)
+    queue = list(range(len(prepared)))
+    owner, results = {}, {}
+    for _ in range(10000):
+        rest = []
+        for k in queue:
+            cid = ens.submit(prepared[k], STEPS)
+            if cid is None:
+                rest.append(k)
+            else:
+                owner[cid] = k
+        queue = rest
+        ens.step()
+        for cid in ens.poll():
+            results[owner[cid]] = ens.retire(cid)
+        if len(results) == len(prepared):
+            break
+    ens.sync()
+    ens.close()
+    assert len(results) == len(prepared)
+    for k in range(len(prepared)):
+        np.testing.assert_array_equal(results[k][0], alone[k][0], err_msg=specs[k].name)

@@ -265,12 +265,13 @@ def element_nodes(grid: np.ndarray, n_elem: Sequence[int], p: int) -> np.ndarray
     """
     nI, nJ, nK = n_elem
     n1 = p + 1
-    out = np.empty((nK, nJ, nI, 3, n1, n1, n1))
-    for k in range(nK):
-        for j in range(nJ):
-            for i in range(nI):
-                out[k, j, i] = grid[:, k * p:k * p + n1, j * p:j * p + n1, i * p:i * p + n1]
-    return out.reshape(nI * nJ * nK, 3, n1 ** 3)
+    g = np.ascontiguousarray(grid)
+    s3, sk, sj, si = g.strides
+    # View [k, j, i, x, c, b, a] of the overlapping element blocks (stride p nodes).
+    view = np.lib.stride_tricks.as_strided(
+        g, shape=(nK, nJ, nI, 3, n1, n1, n1),
+        strides=(p * sk, p * sj, p * si, s3, sk, sj, si), writeable=False)
+    return np.ascontiguousarray(view).reshape(nI * nJ * nK, 3, n1 ** 3)
 
 
 # ---------------------------------------------------------------------------

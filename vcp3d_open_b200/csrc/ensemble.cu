@@ -101,6 +101,9 @@ struct HostCase {
   int deg = 0, slot = -1;
   int64_t eFirst = 0, nE = 0, bFirst = 0, nB = 0, sFirst = 0, nS = 0;
   bool reported = false;
+  // Recorded on the bucket stream after the slot became pending: until it has
+  // completed, the slot's device state may still be its previous occupant's.
+  cudaEvent_t admitted = nullptr;
 };
 
 struct Bucket {
@@ -413,6 +416,8 @@ const char *vcpg_ensemble_last_error(const vcpg_ensemble *ens) {
 
 int vcpg_ensemble_destroy(vcpg_ensemble *ens) {
   if (!ens) return VCPG_OK;
+  for (auto &kv : ens->cases)
+    if (kv.second.admitted) cudaEventDestroy(kv.second.admitted);
   for (Bucket &b : ens->b)
     if (b.deg >= 0) FreeBucket(b);
   if (ens->upload) cudaStreamDestroy(ens->upload);
@@ -467,19 +472,29 @@ int vcpg_ensemble_submit(vcpg_ensemble *ens, const vcpg_params *params,
   if (nE <= 0) return Fail(e, VCPG_E_INVALID, "invalid element count");
   const int KD = b.KD, MD = b.MD, M2 = b.M2;
 
-  // Open boundaries of this case (host set-up), with local indices.
-  OpenBoundaryHost obh;
+  // Sizes first (cheap), so that a refused case costs no set-up work.
+  int64_t nB = 0, nS = 0;
   if (ob) {
-    std::string err;
-    int rc = BuildOpenBoundary(*params, *ob, *geom, p_grid, dof_location, grid_nodes, obh, err);
-    if (rc) return Fail(e, rc, err);
+    for (int64_t e2 = 0; e2 < nE; ++e2)
+      for (int f = 0; f < 6; ++f)
+        if (geom->neighbors[e2 * 6 + f] < 0 && ob->bc[f] != VCPG_BC_NONE) ++nB;
+    const int n3[3] = {params->n_elem[0], params->n_elem[1], params->n_elem[2]};
+    for (int k = 0; k < n3[2]; ++k)
+      for (int j = 0; j < n3[1]; ++j)
+        for (int i = 0; i < n3[0]; ++i) {
+          const int idx[3] = {i, j, k};
+          bool in = false;
+          for (int d = 0; d < 3; ++d)
+            in = in || idx[d] < ob->sponge_elems[2 * d] ||
+                 idx[d] >= n3[d] - ob->sponge_elems[2 * d + 1];
+          if (in) ++nS;
+        }
   } else {
     for (int64_t i = 0; i < nE * 6; ++i)
       if (geom->neighbors[i] < 0)
         return Fail(e, VCPG_E_INVALID, "the case has boundary faces but no boundary conditions");
   }
-  const int64_t nB = obh.nB, nS = obh.nS;
-  if ((nB > 0 && b.capB == 0) || (nS > 0 && b.capS == 0) || (nS > 0 && !b.capS))
+  if ((nB > 0 && b.capB == 0) || (nS > 0 && b.capS == 0))
     return Fail(e, VCPG_E_ADMISSION, "the bucket has no boundary-face or sponge arena");
 
   // Admission: a free slot and contiguous ranges in the three arenas.
@@ -503,6 +518,18 @@ int vcpg_ensemble_submit(vcpg_ensemble *ens, const vcpg_params *params,
     b.bfaces.Free(bFirst, nB);
     b.sponge.Free(sFirst, nS);
   };
+
+  // Open boundaries of this case (host set-up), with local indices.
+  OpenBoundaryHost obh;
+  if (ob) {
+    std::string err;
+    int rc = BuildOpenBoundary(*params, *ob, *geom, p_grid, dof_location, grid_nodes, obh, err);
+    if (rc) { rollback(); return Fail(e, rc, err); }
+    if (obh.nB != nB || obh.nS != nS) {
+      rollback();
+      return Fail(e, VCPG_E_INVALID, "boundary-face or sponge count mismatch");
+    }
+  }
 
   // Bucket-wide operators on first use.
   if (!b.opsReady) {
@@ -583,12 +610,20 @@ int vcpg_ensemble_submit(vcpg_ensemble *ens, const vcpg_params *params,
   if (ce == cudaSuccess)
     ce = cudaMemcpyAsync(b.state + slot, &pending, 4, cudaMemcpyHostToDevice, b.stream);
   if (ev) cudaEventDestroy(ev);
-  if (ce != cudaSuccess) { rollback(); return Fail(e, VCPG_E_CUDA, cudaGetErrorString(ce)); }
+  cudaEvent_t admitted = nullptr;
+  if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&admitted, cudaEventDisableTiming);
+  if (ce == cudaSuccess) ce = cudaEventRecord(admitted, b.stream);
+  if (ce != cudaSuccess) {
+    if (admitted) cudaEventDestroy(admitted);
+    rollback();
+    return Fail(e, VCPG_E_CUDA, cudaGetErrorString(ce));
+  }
 
   const int64_t id = e->nextId++;
   HostCase hc;
   hc.deg = deg; hc.slot = slot;
   hc.eFirst = eFirst; hc.nE = nE; hc.bFirst = bFirst; hc.nB = nB; hc.sFirst = sFirst; hc.nS = nS;
+  hc.admitted = admitted;
   e->cases[id] = hc;
   b.slotCase[slot] = id;
   b.resident += 1;
@@ -639,6 +674,7 @@ int vcpg_ensemble_poll(vcpg_ensemble *ens, int64_t *done_ids, int32_t max_ids, i
       if (id < 0 || e->hostState[s] != kCaseDone) continue;
       HostCase &hc = e->cases[id];
       if (hc.reported) continue;
+      if (cudaEventQuery(hc.admitted) != cudaSuccess) continue;  // stale state word
       hc.reported = true;
       done_ids[(*n_done)++] = id;
     }
@@ -654,6 +690,8 @@ int vcpg_ensemble_retire(vcpg_ensemble *ens, int64_t case_id, double *modal_stat
   if (it == e->cases.end()) return Fail(e, VCPG_E_INVALID, "unknown case id");
   HostCase hc = it->second;
   Bucket &b = e->b[hc.deg];
+  if (cudaEventQuery(hc.admitted) != cudaSuccess)
+    return Fail(e, VCPG_E_INVALID, "the case has not completed its steps");
   int st = 0;
   ENS_CUDA(e, cudaMemcpyAsync(&st, b.state + hc.slot, 4, cudaMemcpyDeviceToHost, e->copy));
   ENS_CUDA(e, cudaStreamSynchronize(e->copy));
@@ -680,6 +718,7 @@ int vcpg_ensemble_retire(vcpg_ensemble *ens, int64_t case_id, double *modal_stat
   b.sponge.Free(hc.sFirst, hc.nS);
   b.slotCase[hc.slot] = -1;
   b.resident -= 1;
+  cudaEventDestroy(hc.admitted);
   e->cases.erase(it);
   return VCPG_OK;
 }

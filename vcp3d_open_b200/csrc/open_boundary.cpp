@@ -48,21 +48,33 @@ void Lagrange(const std::vector<double> &nodes, const std::vector<double> &pts,
 }
 
 // Coordinates of the integration points of one element from its grid nodes
-// gridNodes[3][Kg^3] with the grid Lagrange basis lag[Kg][M]: out[3][M^3].
+// gridNodes[3][Kg^3] with the grid Lagrange basis lag[Kg][M]: out[3][M^3],
+// contracted one axis at a time (k, then j, then i).
 void IntegrationPointCoordinates(const double *gridNodes, int Kg, int M,
                                  const std::vector<double> &lag, double *out) {
   const int KG3 = Kg * Kg * Kg, MD = M * M * M;
+  std::vector<double> t1((size_t)M * Kg * Kg), t2((size_t)M * M * Kg);
   for (int x = 0; x < 3; ++x) {
-    const double *g = gridNodes + x * KG3;
+    const double *g = gridNodes + x * KG3;  // [c][b][a]
+    for (int k = 0; k < M; ++k)
+      for (int b = 0; b < Kg; ++b)
+        for (int a = 0; a < Kg; ++a) {
+          double acc = 0.0;
+          for (int c = 0; c < Kg; ++c) acc += lag[c * M + k] * g[(c * Kg + b) * Kg + a];
+          t1[((size_t)k * Kg + b) * Kg + a] = acc;
+        }
+    for (int k = 0; k < M; ++k)
+      for (int j = 0; j < M; ++j)
+        for (int a = 0; a < Kg; ++a) {
+          double acc = 0.0;
+          for (int b = 0; b < Kg; ++b) acc += lag[b * M + j] * t1[((size_t)k * Kg + b) * Kg + a];
+          t2[((size_t)k * M + j) * Kg + a] = acc;
+        }
     for (int k = 0; k < M; ++k)
       for (int j = 0; j < M; ++j)
         for (int i = 0; i < M; ++i) {
           double acc = 0.0;
-          for (int c = 0; c < Kg; ++c)
-            for (int b = 0; b < Kg; ++b)
-              for (int a = 0; a < Kg; ++a)
-                acc += lag[a * M + i] * lag[b * M + j] * lag[c * M + k] *
-                       g[(c * Kg + b) * Kg + a];
+          for (int a = 0; a < Kg; ++a) acc += lag[a * M + i] * t2[((size_t)k * M + j) * Kg + a];
           out[x * MD + (k * M + j) * M + i] = acc;
         }
   }

@@ -151,6 +151,7 @@ class Ensemble:
             cfg.bucket_elems[p], cfg.bucket_bfaces[p], cfg.bucket_sponge[p] = ne, nb, ns
         cfg.max_cases = max_cases
         self.cfg = cfg
+        self.max_cases = max_cases
         self.precision, self.scheme = precision, scheme
         h = C.c_void_p()
         rc = self.lib.vcpg_ensemble_create(C.byref(cfg), C.byref(h))
@@ -267,7 +268,7 @@ def plan_capacities(requests: List[Request], budget_bytes: int) -> Dict[int, tup
 
 
 def serve(requests: List[Request], ens: Ensemble, prepare_workers: int = 8,
-          keep_results: bool = False) -> dict:
+          keep_results: bool = False, progress_every: float = 0.0) -> dict:
     """Continuous batching: admit arrived requests whenever their bucket has room,
     step every bucket with resident cases, retire finished cases."""
     t0 = time.perf_counter()
@@ -279,8 +280,16 @@ def serve(requests: List[Request], ens: Ensemble, prepare_workers: int = 8,
     admitted_at, finished_at, results = {}, {}, {}
     dof_updates = 0
     steps = 0
+    next_report = progress_every
+    slots = collections.Counter()       # resident cases per degree bucket
+    max_slots = getattr(ens, "max_cases", None)
     while upcoming or waiting or running:
         now = time.perf_counter() - t0
+        if progress_every and now >= next_report:
+            next_report += progress_every
+            print(f"[serve] t={now:.1f}s finished={len(finished_at)} running={len(running)} "
+                  f"waiting={len(waiting)} upcoming={len(upcoming)} steps={steps}",
+                  file=sys.stderr, flush=True)
         while upcoming and upcoming[0].arrival <= now:
             r = upcoming.popleft()
             future_of[r.rid] = pool.submit(prepare, r.spec, ens.precision)
@@ -290,13 +299,14 @@ def serve(requests: List[Request], ens: Ensemble, prepare_workers: int = 8,
         still = []
         for r in waiting:
             fut = future_of[r.rid]
-            if not fut.done():
+            if not fut.done() or (max_slots and slots[r.spec.p] >= max_slots):
                 still.append(r)
                 continue
             cid = ens.submit(fut.result(), r.steps)
             if cid is None:
                 still.append(r)
                 continue
+            slots[r.spec.p] += 1
             running[cid] = r
             admitted_at[r.rid] = time.perf_counter() - t0
             del future_of[r.rid]
@@ -310,6 +320,7 @@ def serve(requests: List[Request], ens: Ensemble, prepare_workers: int = 8,
             time.sleep(0.001)
         for cid in ens.poll():
             r = running.pop(cid)
+            slots[r.spec.p] -= 1
             state, sim_time = ens.retire(cid)
             finished_at[r.rid] = time.perf_counter() - t0
             dof_updates += r.spec.n_dofs * r.steps
@@ -342,14 +353,18 @@ def main(argv=None) -> int:
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--budget-gb", type=float, default=100.0)
     ap.add_argument("--workers", type=int, default=16)
+    ap.add_argument("--max-cases", type=int, default=8,
+                    help="case slots per degree bucket: the cases stepped together")
+    ap.add_argument("--progress", type=float, default=0.0, help="seconds between progress lines")
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
     reqs = request_stream(a.cases, a.seed, steps=a.steps)
     caps = plan_capacities(reqs, int(a.budget_gb * 1e9))
     prec = capi.MIXED if a.precision == "mixed" else capi.FP64
-    ens = Ensemble(caps, precision=prec)
-    rep = serve(reqs, ens, prepare_workers=a.workers)
+    ens = Ensemble(caps, precision=prec, max_cases=a.max_cases)
+    rep = serve(reqs, ens, prepare_workers=a.workers, progress_every=a.progress)
     rep.update({"precision": a.precision, "steps_per_case": a.steps, "seed": a.seed,
+                "max_cases_per_bucket": a.max_cases,
                 "capacities": {str(k): list(v) for k, v in caps.items()}})
     ens.close()
     line = json.dumps(rep)
