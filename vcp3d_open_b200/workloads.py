@@ -37,6 +37,14 @@ WORKLOADS = {
                              bc=("inflow_static_nscbc", "outflow_nscbc", "outflow_nscbc",
                                  "outflow_nscbc", "periodic", "periodic"),
                              sponge=(0, 4, 3, 3, 0, 0), cml=True),
+    # Profiling size of the open-boundary configuration: 24x12x12 elements of degree 4
+    # on [0,12]x[0,6]x[0,6] (state + metrics ~260 MB, above the 126 MB L2).
+    "pulse24_p4_lsrk4": dict(kind="pulse", n_elem=(24, 12, 12), p=4, hi=(12.0, 6.0, 6.0),
+                             mach=0.3, grid_map="none", center=(6.0, 3.0, 3.0),
+                             pulse_amp=1.0e-3, pulse_width=0.5,
+                             bc=("inflow_static_nscbc", "outflow_nscbc", "outflow_nscbc",
+                                 "outflow_nscbc", "periodic", "periodic"),
+                             sponge=(0, 3, 2, 2, 0, 0), cml=True),
 }
 
 
