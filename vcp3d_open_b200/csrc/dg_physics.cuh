@@ -21,8 +21,6 @@ __device__ __forceinline__ double Exp(double x) { return exp(x); }
 __device__ __forceinline__ float Exp(float x) { return expf(x); }
 __device__ __forceinline__ double Log(double x) { return log(x); }
 __device__ __forceinline__ float Log(float x) { return logf(x); }
-__device__ __forceinline__ double Pow(double x, double y) { return pow(x, y); }
-__device__ __forceinline__ float Pow(float x, float y) { return powf(x, y); }
 __device__ __forceinline__ double Sqrt(double x) { return sqrt(x); }
 __device__ __forceinline__ float Sqrt(float x) { return sqrtf(x); }
 __device__ __forceinline__ double Fabs(double x) { return fabs(x); }
@@ -52,8 +50,9 @@ __device__ __forceinline__ void EntropyToPrim(const T V0, const T V1, const T V2
   w = -V4Inv * V3;
   eKin = T(0.5) * (u * u + v * v + w * w);
   const T s = T(kGam) - gm1 * (V0 - V4 * eKin);
-  const T tmp = -V4 * Exp(s);
-  rho = Pow(tmp, ov1mg);
+  // rho = (-V4 exp(s))^(-1/(gam-1)) (the reference's POW(-V4*EXP(s), ov1mg)),
+  // evaluated as exp(ov1mg (log(-V4) + s)): one exponential and one logarithm.
+  rho = Exp(ov1mg * (Log(-V4) + s));
   p = -rho * V4Inv;
 }
 
@@ -70,8 +69,8 @@ __device__ __forceinline__ void FaceStatePrim(const T *V, T &rho, T &u, T &v,
   w = -V4Inv * V[3];
   vTot2 = u * u + v * v + w * w;
   const T s = T(kGam) - gm1 * (V[0] - T(0.5) * V[4] * vTot2);
-  const T tmp = -V[4] * Exp(s);
-  rho = Pow(tmp, ov1mg);
+  // rho = (-V4 exp(s))^(-1/(gam-1)), as in EntropyToPrim.
+  rho = Exp(ov1mg * (Log(-V[4]) + s));
   p = -V4Inv * rho;
 }
 

@@ -128,6 +128,13 @@ __device__ __forceinline__ void BlockReduce3(T &a, T &b, T &c, T *red) {
   }
 }
 
+// Upper bound of the CTAs per SM that __launch_bounds__ asks the register
+// allocator for in the FP64 form (a higher value caps the registers per thread
+// lower: 4 CTAs of 128 threads allow 128).
+#ifndef VCPG_FP64_MAX_MIN_BLOCKS
+#define VCPG_FP64_MAX_MIN_BLOCKS 4
+#endif
+
 // Shared-memory plan (doubles) of the fused kernel for a (K, M) pair.
 template <int K, int M, typename T = double, bool OPEN = false> struct Plan {
   static constexpr int KD = K * K * K, MD = M * M * M, M2 = M * M;
@@ -138,19 +145,27 @@ template <int K, int M, typename T = double, bool OPEN = false> struct Plan {
   // Face phase: per face-side trace (value + 3 derivatives) 20*M2, two sides,
   // three faces at a time, plus normal-evaluation and stage buffers.
   // Face phase: BN/BND 60 K^2, three fast-axis buffers 90 K M, traces 120 M^2.
-  static constexpr int FACE = 60 * K * K + 90 * K * M + 120 * M2;
+  static constexpr int FACE = 90 * K * M + 120 * M2;
   // CG phase: z, p, Ap, x, pInt and the contraction buffers.
   static constexpr int CG = 20 * KD + 5 * MD + TK + TJ;
   static constexpr int WORK = VOL > FACE ? (VOL > CG ? VOL : CG) : (FACE > CG ? FACE : CG);
-  // Persistent: sol, R, CG point data (8 per point), J*w, reduction scratch,
+  // Persistent: sol, R, CG point data (rho, u, v, w, p per point), J*w, reduction scratch,
   // face vectors (basis and derivative at r = -1, +1).
-  static constexpr int PERSIST = 10 * KD + 9 * MD + 64 + 4 * kKMax;
+  static constexpr int PERSIST = 10 * KD + 6 * MD + 64 + 4 * kKMax;
   static constexpr int TOTAL = PERSIST + WORK;
   static constexpr size_t BYTES = sizeof(T) * (size_t)TOTAL;
   // Threads per CTA and the CTAs per SM that the shared memory allows (227 KB).
-  static constexpr int NT = K >= 5 ? 256 : 128;
-  static constexpr int MIN_BLOCKS =
-      (int)(227 * 1024 / BYTES) < 1 ? 1 : ((int)(227 * 1024 / BYTES) > 4 ? 4 : (int)(227 * 1024 / BYTES));
+  // Threads per CTA and CTAs per SM (through __launch_bounds__ they bound the
+  // registers per thread). FP64: 128 threads cover the widest contraction stage
+  // of degrees <= 4 in one or two passes; two CTAs of 128 threads are used
+  // whenever two fit the 227 KB of shared memory (up to 255 registers per thread
+  // then), else one CTA of 256 threads. FP32: 256 threads from degree 4 up, as
+  // many CTAs as the shared memory allows (at most 4).
+  static constexpr int FIT = (int)(227 * 1024 / BYTES);
+  static constexpr bool FP64 = sizeof(T) == 8;
+  static constexpr int NT = FP64 ? ((K <= 4 || FIT >= 2) ? 128 : 256) : (K >= 5 ? 256 : 128);
+  static constexpr int CAP = FP64 ? VCPG_FP64_MAX_MIN_BLOCKS : 4;
+  static constexpr int MIN_BLOCKS = FIT < 1 ? 1 : (FIT > CAP ? CAP : FIT);
 };
 
 
@@ -247,7 +262,7 @@ __device__ __forceinline__ void MatchingLayerSource(const ResidualArgs &a, const
 // ---------------------------------------------------------------------------
 // Volume phase: solution and gradients at the integration points
 // (TPSAGV), pointwise fluxes, and the three transposed contractions (TPAVR)
-// into s_R. Also stores the CG point data (rho, u, v, w, p, rhoE, dUdV(4,4))
+// into s_R. Also stores the CG point data (rho, u, v, w, p)
 // and J*w.  Follows ElementClass::VolumeResidual, src/ElementClass.cpp:3809-4443.
 // ---------------------------------------------------------------------------
 template <int NT, int K, int M, typename T, bool OPEN>
@@ -323,8 +338,6 @@ __device__ __forceinline__ void VolumePhase(const ResidualArgs &a, const int e, 
     s_cgp[2 * MD + l] = v;
     s_cgp[3 * MD + l] = w;
     s_cgp[4 * MD + l] = p;
-    s_cgp[5 * MD + l] = rE;
-    s_cgp[6 * MD + l] = rE * rH / rho + p * eKin;  // dUdV(4,4)
     mach2 = Fmax(mach2, rho * (u * u + v * v + w * w) / (T(kGam) * p));
     if (OPEN && cmlHere)
       MatchingLayerSource<M>(a, sp, l, V, gx, gy, gz, rho, u, v, w, p, eKin, rE,
@@ -413,7 +426,10 @@ __device__ __forceinline__ void VolumePhase(const ResidualArgs &a, const int e, 
       dX[1 * MD + l] = sigma * (rho * s_cgp[1 * MD + l] - LdT<T>(ds + 1 * MD + l));
       dX[2 * MD + l] = sigma * (rho * s_cgp[2 * MD + l] - LdT<T>(ds + 2 * MD + l));
       dX[3 * MD + l] = sigma * (rho * s_cgp[3 * MD + l] - LdT<T>(ds + 3 * MD + l));
-      dX[4 * MD + l] = sigma * (s_cgp[5 * MD + l] - LdT<T>(ds + 4 * MD + l));
+      const T u = s_cgp[1 * MD + l], v = s_cgp[2 * MD + l], w = s_cgp[3 * MD + l];
+      const T rE = -s_cgp[4 * MD + l] * (-T(1.0) / (T(kGam) - T(1.0))) +
+                   rho * (T(0.5) * (u * u + v * v + w * w));
+      dX[4 * MD + l] = sigma * (rE - LdT<T>(ds + 4 * MD + l));
     }
     __syncthreads();
     Contract<NT, SLOT, K, M, kLegT, 2, 5, M, M, M, M, K, false>(dX, tJ);
@@ -578,13 +594,18 @@ __device__ __forceinline__ void FacePhase(const ResidualArgs &a, const int e, co
                                           const T *s_sol, T *s_R, const T *s_fv, T *work) {
   constexpr int SLOT = Slot<K, M>::value;
   constexpr int KD = K * K * K, M2 = M * M, K2 = K * K;
-  static_assert(2 * M <= 3 * K && K <= 2 * M, "face-phase buffer aliasing");
-  T *BN = work, *BND = BN + 30 * K2;        // 60 K^2
-  T *T1a = BND + 30 * K2, *T1b = T1a + 30 * K * M, *T1c = T1b + 30 * K * M;  // 90 K M
-  T *TR = T1c + 30 * K * M;                 // 120 M^2
+  // Buffer reuse within a group (each stage's inputs are dead when it writes):
+  //   T1 [90 K M]: fast-axis stage, then the distribution inputs P (60 M^2), then
+  //                the fast-axis distribution results RF/RFN/RS (60 K^2);
+  //   BN [60 K^2] then TR [120 M^2] at the same place: face-normal stage, traces,
+  //                then the slow-axis distribution results Q (60 K M).
+  static_assert(2 * M <= 3 * K && K <= M, "face-phase buffer aliasing");
+  T *T1a = work, *T1b = T1a + 30 * K * M, *T1c = T1b + 30 * K * M;  // 90 K M
+  T *BN = T1c + 30 * K * M, *BND = BN + 30 * K2;  // 60 K^2
+  T *TR = BN;                               // 120 M^2 (BN is dead when TR is written)
   T *P1 = T1a, *P2 = T1a + 45 * M2;         // distribution inputs (in T1)
   T *Q1 = TR, *Q2 = TR + 45 * K * M;        // after the slow-axis contraction (in TR)
-  T *RF = BN, *RFN = RF + 15 * K2, *RS = RFN + 30 * K2;  // after the fast axis (in BN)
+  T *RF = T1a, *RFN = RF + 15 * K2, *RS = RFN + 30 * K2;  // after the fast axis (in T1)
   const double *sc = a.elem_scalars + (size_t)e * 15;
   for (int g = 0; g < 2; ++g) {
     const int nb0 = a.nbr[e * 6 + 0 + g], nb1 = a.nbr[e * 6 + 2 + g], nb2 = a.nbr[e * 6 + 4 + g];
@@ -778,11 +799,14 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
       const T p0 = iw * pInt[l], p1 = iw * pInt[MD + l], p2 = iw * pInt[2 * MD + l],
                    p3 = iw * pInt[3 * MD + l], p4 = iw * pInt[4 * MD + l];
       const T rho = s_cgp[l], u = s_cgp[MD + l], v = s_cgp[2 * MD + l],
-                   w = s_cgp[3 * MD + l], pr = s_cgp[4 * MD + l], rE = s_cgp[5 * MD + l];
+                   w = s_cgp[3 * MD + l], pr = s_cgp[4 * MD + l];
+      // rho E and dU/dV(4,4) from the primitive variables, as in the volume phase.
+      const T eKin = T(0.5) * (u * u + v * v + w * w);
+      const T rE = -pr * (-T(1.0) / (T(kGam) - T(1.0))) + rho * eKin;
       const T ru = rho * u, rv = rho * v, rw = rho * w, rH = rE + pr;
       const T d0 = rho, d1 = ru, d2 = rv, d3 = rw, d4 = rE, d5 = ru * u + pr, d6 = ru * v,
                    d7 = ru * w, d8 = rH * u, d9 = rv * v + pr, d10 = rv * w, d11 = rH * v,
-                   d12 = rw * w + pr, d13 = rH * w, d14 = s_cgp[6 * MD + l];
+                   d12 = rw * w + pr, d13 = rH * w, d14 = rE * rH / rho + pr * eKin;
       pInt[l] = d0 * p0 + d1 * p1 + d2 * p2 + d3 * p3 + d4 * p4;
       pInt[MD + l] = d1 * p0 + d5 * p1 + d6 * p2 + d7 * p3 + d8 * p4;
       pInt[2 * MD + l] = d2 * p0 + d6 * p1 + d9 * p2 + d10 * p3 + d11 * p4;
@@ -846,7 +870,7 @@ __global__ void __launch_bounds__(NT, (Plan<K, M, T, OPEN>::MIN_BLOCKS)) Residua
   constexpr int KD = P::KD, MD = P::MD;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *smem = reinterpret_cast<T *>(smem_raw);
-  T *s_sol = smem, *s_R = s_sol + 5 * KD, *s_cgp = s_R + 5 * KD, *s_jw = s_cgp + 8 * MD;
+  T *s_sol = smem, *s_R = s_sol + 5 * KD, *s_cgp = s_R + 5 * KD, *s_jw = s_cgp + 5 * MD;
   T *s_red = s_jw + MD, *s_fv = s_red + 64, *work = s_fv + 4 * kKMax;
   const int e = blockIdx.x;
   if (e >= a.n_elem) return;
