@@ -64,19 +64,20 @@ def test_open_boundary_steps_match_reference(gpu_available, path):
 
 
 def test_open_boundary_launches_and_graph(gpu_available):
-    """Every residual of an open block is three launches: boundary traces and Mach
-    weights, boundary states and fluxes, and the fused residual kernel."""
+    """Every residual of an open block is four launches: boundary traces and Mach
+    weights, boundary states and fluxes, interior face fluxes, and the fused
+    residual kernel."""
     g = load_golden(open_golden_files()[0])
     s = _solver(g["spec"])
     try:
         s.set_state(g["sol0"])
         n0 = s.launch_count
         s.residual()
-        assert s.launch_count - n0 == 3
+        assert s.launch_count - n0 == 4
         n0 = s.launch_count
         s.step(2, capi.LSRK4)
-        # dt + finalize + 5 x (stage update + 3 residual launches) per step.
-        assert s.launch_count - n0 == 2 * (2 + 5 * 4)
+        # dt + finalize + 5 x (stage update + 4 residual launches) per step.
+        assert s.launch_count - n0 == 2 * (2 + 5 * 5)
     finally:
         s.close()
 

@@ -158,8 +158,8 @@ def test_launch_count_and_graph_reuse(gpu_available):
         n0 = s.launch_count
         s.step(2, capi.SSPRK3)
         s.step(2, capi.SSPRK3)
-        # dt + finalize + 3 x (stage update + residual) per step.
-        assert s.launch_count - n0 == 4 * 8
+        # dt + finalize + 3 x (stage update + face fluxes + residual) per step.
+        assert s.launch_count - n0 == 4 * 11
     finally:
         s.close()
 
@@ -176,7 +176,7 @@ def test_step_after_set_state_evaluates_the_residual_first(gpu_available):
         s.set_state(g["sol0"])
         n0 = s.launch_count
         s.step(2, capi.LSRK4)
-        assert s.launch_count - n0 == 1 + 2 * 12
+        assert s.launch_count - n0 == 2 + 2 * 17
         np.testing.assert_array_equal(s.get_state(), want)
     finally:
         s.close()

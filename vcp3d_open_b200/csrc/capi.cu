@@ -44,6 +44,7 @@ struct vcpg_handle {
   double *d_bpresc = nullptr, *d_pc = nullptr, *d_dlq = nullptr;
   double *d_btrace = nullptr, *d_bmach = nullptr, *d_bflux = nullptr;
   BlockFaceCfg *d_cfg = nullptr;
+  void *d_fflux = nullptr;  // fluxes of every element's Min faces (FaceFluxKernel)
   int *d_sponge = nullptr;
   double *d_dampfn = nullptr, *d_dampst = nullptr, *d_cml = nullptr;
   int cml_on = 0;
@@ -103,6 +104,7 @@ ResidualArgs MakeResidualArgs(vcpg_handle *h, double *rawOut, unsigned long long
   a.damp_state = h->d_dampst;
   a.cml = h->d_cml;
   a.cml_on = h->cml_on;
+  a.face_flux = h->d_fflux;
   return a;
 }
 
@@ -167,12 +169,12 @@ int EnqueueResidual(vcpg_handle *h, const ResidualArgs &a, int *launches) {
     n += 2;
   }
   VCPG_CUDA(h, LaunchResidual(h->K, h->M, a, h->stream));
-  n += 1;
+  n += 2;
   if (launches) *launches = n;
   return VCPG_OK;
 }
 
-int ResidualLaunches(const vcpg_handle *h) { return (h->open && h->nB > 0) ? 3 : 1; }
+int ResidualLaunches(const vcpg_handle *h) { return (h->open && h->nB > 0) ? 4 : 2; }
 
 int EnqueueStep(vcpg_handle *h, int scheme) {
   const size_t n = (size_t)h->nE * 5 * h->KD;
@@ -218,7 +220,7 @@ int vcpg_destroy(vcpg_handle *h) {
                   h->d_nbr, h->d_dtbits, h->d_mach2, h->d_dt, h->d_fixed, h->d_hist,
                   h->d_status, h->d_counter, h->d_cgstats, h->d_bface, h->d_bpresc, h->d_pc,
                   h->d_dlq, h->d_btrace, h->d_bmach, h->d_bflux, h->d_sponge, h->d_dampfn,
-                  h->d_dampst, h->d_cml, h->d_cfg};
+                  h->d_dampst, h->d_cml, h->d_cfg, h->d_fflux};
   for (void *p : bufs)
     if (p) cudaFree(p);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -273,6 +275,7 @@ int vcpg_create(const vcpg_params *params, const vcpg_operators *ops, const vcpg
   if ((rc = alloc((void **)&h->d_sol, nState * 8))) return rc;
   if ((rc = alloc((void **)&h->d_solOld, nState * 8))) return rc;
   if ((rc = alloc((void **)&h->d_res, nState * 8))) return rc;
+  if ((rc = alloc((void **)&h->d_fflux, (size_t)h->nE * FaceFluxBytesPerElement(K, M)))) return rc;
   if ((rc = alloc((void **)&h->d_vol, (size_t)h->nE * 10 * h->MD * 8))) return rc;
   if ((rc = alloc((void **)&h->d_face, (size_t)h->nE * 6 * 13 * h->M2 * 8))) return rc;
   if ((rc = alloc((void **)&h->d_sc, (size_t)h->nE * 15 * 8))) return rc;

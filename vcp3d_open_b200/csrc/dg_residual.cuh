@@ -64,6 +64,9 @@ struct ResidualArgs {
   const double *cml;           // [nS][6] 1/sigma per direction, layer orientation
   int cml_on;                  // characteristic matching layer in sponge elements
   CaseView cases;              // several cases per launch (null elem_case: one case)
+  // [nE][3][20][M^2] fluxes of every element's Min faces in the compute precision
+  // (FaceFluxKernel writes them, the residual kernel reads them).
+  void *face_flux;
 };
 
 // Arguments of the CFL time-step kernel (kernels.cu).
@@ -145,7 +148,9 @@ template <int K, int M, typename T = double, bool OPEN = false> struct Plan {
   // Face phase: per face-side trace (value + 3 derivatives) 20*M2, two sides,
   // three faces at a time, plus normal-evaluation and stage buffers.
   // Face phase: BN/BND 60 K^2, three fast-axis buffers 90 K M, traces 120 M^2.
-  static constexpr int FACE = 90 * K * M + 120 * M2;
+  // Face phase: distribution inputs (60 M^2) and the slow-axis results (60 K M);
+  // the traces and fluxes are computed by FaceFluxKernel.
+  static constexpr int FACE = 60 * M2 + 60 * K * M;
   // CG phase: z, p, Ap, x, pInt and the contraction buffers.
   static constexpr int CG = 20 * KD + 5 * MD + TK + TJ;
   static constexpr int WORK = VOL > FACE ? (VOL > CG ? VOL : CG) : (FACE > CG ? FACE : CG);
@@ -160,11 +165,11 @@ template <int K, int M, typename T = double, bool OPEN = false> struct Plan {
   // of degrees <= 4 in one or two passes; two CTAs of 128 threads are used
   // whenever two fit the 227 KB of shared memory (up to 255 registers per thread
   // then), else one CTA of 256 threads. FP32: 256 threads from degree 4 up, as
-  // many CTAs as the shared memory allows (at most 4).
+  // many CTAs as the shared memory allows (at most 3 of 256 or 4 of 128 threads).
   static constexpr int FIT = (int)(227 * 1024 / BYTES);
   static constexpr bool FP64 = sizeof(T) == 8;
   static constexpr int NT = FP64 ? ((K <= 4 || FIT >= 2) ? 128 : 256) : (K >= 5 ? 256 : 128);
-  static constexpr int CAP = FP64 ? VCPG_FP64_MAX_MIN_BLOCKS : 4;
+  static constexpr int CAP = FP64 ? VCPG_FP64_MAX_MIN_BLOCKS : (NT == 256 ? 3 : 4);
   static constexpr int MIN_BLOCKS = FIT < 1 ? 1 : (FIT > CAP ? CAP : FIT);
 };
 
@@ -526,22 +531,19 @@ __device__ __forceinline__ void TraceCartesianGrad(const T *TR, const int t, con
   }
 }
 
-// Fluxes of one interior face point (FluxesInternalFace, src/FluxesFace.cpp:220-343),
-// seen from the own side. Writes the own-side distribution inputs by role:
-// P1[role][d][v][M2] with role 0 fast-axis symmetrizing flux, 1 normal flux (with
-// the own side's sign), 2 face-normal symmetrizing flux; P2[d][v][M2] the
-// slow-axis symmetrizing flux.
+// Fluxes of one interior face point (FluxesInternalFace, src/FluxesFace.cpp:220-343)
+// from the traces TR of the face's two sides: tL / tR are the trace slots of the
+// lower (left) and upper (right) element, fmL / fmR their face metrics; the
+// normal is the left element's. Writes the normal flux and the Cartesian
+// symmetrizing fluxes (component 0 of those is zero) to out[20][M^2]:
+// 0-4 flux, 5-9 x, 10-14 y, 15-19 z.
 template <int K, int M, typename T>
-__device__ __forceinline__ void GroupFacePoint(const ResidualArgs &a, const double mu, const int g,
-                                               const int d, const int pt, const T *TR,
-                                               const double *fmOwn, const double *fmNb,
-                                               const T lenScale, T *P1, T *P2) {
+__device__ __forceinline__ void FacePointFlux(const ResidualArgs &a, const double mu, const int d,
+                                              const int pt, const T *TR, const int tL,
+                                              const int tR, const double *fmL,
+                                              const double *fmR, const T lenScale, T *out) {
   constexpr int SLOT = Slot<K, M>::value;
   constexpr int M2 = M * M;
-  const int tOwn = 2 * d, tNb = 2 * d + 1;
-  // g == 0: own Min face, the neighbour is the left state; g == 1: own Max face.
-  const int tL = g == 0 ? tNb : tOwn, tR = g == 0 ? tOwn : tNb;
-  const double *fmL = g == 0 ? fmNb : fmOwn, *fmR = g == 0 ? fmOwn : fmNb;
   T VL[5], VR[5], gxL[5], gyL[5], gzL[5], gxR[5], gyR[5], gzR[5];
 #pragma unroll
   for (int n = 0; n < 5; ++n) {
@@ -570,58 +572,99 @@ __device__ __forceinline__ void GroupFacePoint(const ResidualArgs &a, const doub
   T sx[5], sy[5], sz[5];
   ViscousPenaltySymFlux(VL, VR, gx, gy, gz, nx, ny, nz, wf, area, T(mu),
                         T(a.tau_num) / lenScale, T(a.theta_sym), flux, sx, sy, sz);
-  const double *fm = g == 0 ? fmR : fmL;  // the own side's metric
+#pragma unroll
+  for (int n = 0; n < 5; ++n) {
+    out[n * M2 + pt] = flux[n];
+    out[(5 + n) * M2 + pt] = sx[n];
+    out[(10 + n) * M2 + pt] = sy[n];
+    out[(15 + n) * M2 + pt] = sz[n];
+  }
+}
+
+// Distribution inputs of one face point for the own element from the face's
+// fluxes F[20][M^2] (FacePointFlux layout): P1[role][d][v][M2] with role 0 the
+// fast-axis symmetrizing flux, 1 the normal flux with the own side's sign (the
+// own element is the right state of its Min faces), 2 the face-normal
+// symmetrizing flux; P2[d][v][M2] the slow-axis symmetrizing flux. The
+// symmetrizing fluxes are turned parametric with the own side's metric fm.
+template <int K, int M, typename T>
+__device__ __forceinline__ void FaceRoles(const ResidualArgs &a, const int g, const int d,
+                                          const int pt, const T *F, const double *fm, T *P1,
+                                          T *P2) {
+  constexpr int M2 = M * M;
   const int pFast = FastParam(d);
 #pragma unroll
   for (int n = 0; n < 5; ++n) {
     const int mi = a.metric_compat ? n : pt;
+    const T flux = F[n * M2 + pt], sx = F[(5 + n) * M2 + pt], sy = F[(10 + n) * M2 + pt],
+            sz = F[(15 + n) * M2 + pt];
     T sym[3];
 #pragma unroll
     for (int p = 0; p < 3; ++p)
-      sym[p] = sx[n] * LdT<T>(fm + (4 + 3 * p) * M2 + mi) +
-               sy[n] * LdT<T>(fm + (5 + 3 * p) * M2 + mi) +
-               sz[n] * LdT<T>(fm + (6 + 3 * p) * M2 + mi);
+      sym[p] = sx * LdT<T>(fm + (4 + 3 * p) * M2 + mi) + sy * LdT<T>(fm + (5 + 3 * p) * M2 + mi) +
+               sz * LdT<T>(fm + (6 + 3 * p) * M2 + mi);
     const int o = (d * 5 + n) * M2 + pt;
-    P1[1 * 15 * M2 + o] = g == 0 ? -flux[n] : flux[n];
+    P1[1 * 15 * M2 + o] = g == 0 ? -flux : flux;
     P1[2 * 15 * M2 + o] = sym[d];
     P1[0 * 15 * M2 + o] = sym[pFast];
     P2[o] = sym[3 - d - pFast];
   }
 }
 
-template <int NT, int K, int M, typename T, bool OPEN>
-__device__ __forceinline__ void FacePhase(const ResidualArgs &a, const int e, const double mu,
-                                          const T *s_sol, T *s_R, const T *s_fv, T *work) {
+// Face fluxes of an element's three Min faces (each interior face is computed
+// once, by its upper element): the traces of both sides (TPSAG[IJK]) and the
+// pointwise fluxes, into face_flux[e][d][20][M^2]. Boundary faces are skipped
+// (their fluxes come from the boundary kernels).
+template <int NT, int K, int M, typename T>
+__device__ __forceinline__ void MinFaceFluxes(const ResidualArgs &a, const int e, const double mu,
+                                              const T *s_sol, const T *s_fv, T *work) {
   constexpr int SLOT = Slot<K, M>::value;
-  constexpr int KD = K * K * K, M2 = M * M, K2 = K * K;
-  // Buffer reuse within a group (each stage's inputs are dead when it writes):
-  //   T1 [90 K M]: fast-axis stage, then the distribution inputs P (60 M^2), then
-  //                the fast-axis distribution results RF/RFN/RS (60 K^2);
-  //   BN [60 K^2] then TR [120 M^2] at the same place: face-normal stage, traces,
-  //                then the slow-axis distribution results Q (60 K M).
-  static_assert(2 * M <= 3 * K && K <= M, "face-phase buffer aliasing");
+  constexpr int M2 = M * M, K2 = K * K;
+  static_assert(K <= M, "face-flux buffer aliasing");
   T *T1a = work, *T1b = T1a + 30 * K * M, *T1c = T1b + 30 * K * M;  // 90 K M
   T *BN = T1c + 30 * K * M, *BND = BN + 30 * K2;  // 60 K^2
   T *TR = BN;                               // 120 M^2 (BN is dead when TR is written)
-  T *P1 = T1a, *P2 = T1a + 45 * M2;         // distribution inputs (in T1)
-  T *Q1 = TR, *Q2 = TR + 45 * K * M;        // after the slow-axis contraction (in TR)
-  T *RF = T1a, *RFN = RF + 15 * K2, *RS = RFN + 30 * K2;  // after the fast axis (in T1)
+  const int nb0 = a.nbr[e * 6 + 0], nb1 = a.nbr[e * 6 + 2], nb2 = a.nbr[e * 6 + 4];
+  FaceNormalBatch<NT, SLOT, K>(s_sol, a.sol, nb0, nb1, nb2, 0, s_fv, BN, BND);
+  __syncthreads();
+  Contract<NT, SLOT, K, M, kLeg, 0, 30, K, K, 1, K, M, false>(BN, T1a);
+  Contract<NT, SLOT, K, M, kDLeg, 0, 30, K, K, 1, K, M, false>(BN, T1b);
+  Contract<NT, SLOT, K, M, kLeg, 0, 30, K, K, 1, K, M, false>(BND, T1c);
+  __syncthreads();
+  Contract<NT, SLOT, K, M, kLeg, 1, 30, M, K, 1, K, M, false>(T1a, TR);
+  Contract<NT, SLOT, K, M, kDLeg, 1, 30, M, K, 1, K, M, false>(T1a, TR + 3 * 30 * M2);
+  Contract<NT, SLOT, K, M, kLeg, 1, 30, M, K, 1, K, M, false>(T1b, TR + 2 * 30 * M2);
+  Contract<NT, SLOT, K, M, kLeg, 1, 30, M, K, 1, K, M, false>(T1c, TR + 1 * 30 * M2);
+  __syncthreads();
   const double *sc = a.elem_scalars + (size_t)e * 15;
+  T *out = reinterpret_cast<T *>(a.face_flux) + (size_t)e * 3 * 20 * M2;
+  for (int idx = threadIdx.x; idx < 3 * M2; idx += NT) {
+    const int d = idx / M2, pt = idx - d * M2;
+    const int nb = d == 0 ? nb0 : (d == 1 ? nb1 : nb2);
+    if (nb < 0) continue;
+    const T lenScale = Fmin(T(sc[d]), T(a.elem_scalars[(size_t)nb * 15 + d]));
+    const double *fmOwn = a.face_metric + ((size_t)e * 6 + 2 * d) * 13 * M2;
+    const double *fmNb = a.face_metric + ((size_t)nb * 6 + 2 * d + 1) * 13 * M2;
+    // The lower element (the neighbour, trace slot 2d+1) is the left state.
+    FacePointFlux<K, M>(a, mu, d, pt, TR, 2 * d + 1, 2 * d, fmNb, fmOwn, lenScale,
+                        out + d * 20 * M2);
+  }
+}
+
+template <int NT, int K, int M, typename T, bool OPEN>
+__device__ __forceinline__ void FacePhase(const ResidualArgs &a, const int e, T *s_R,
+                                          const T *s_fv, T *work) {
+  constexpr int SLOT = Slot<K, M>::value;
+  constexpr int KD = K * K * K, M2 = M * M, K2 = K * K;
+  // P [60 M^2], then the fast-axis results RF/RFN/RS (60 K^2) in its place;
+  // Q [60 K M] after the slow axis.
+  static_assert(K <= M, "face-phase buffer aliasing");
+  T *P1 = work, *P2 = P1 + 45 * M2;
+  T *Q1 = P1 + 60 * M2, *Q2 = Q1 + 45 * K * M;
+  T *RF = work, *RFN = RF + 15 * K2, *RS = RFN + 30 * K2;
+  const T *faceFlux = reinterpret_cast<const T *>(a.face_flux);
   for (int g = 0; g < 2; ++g) {
     const int nb0 = a.nbr[e * 6 + 0 + g], nb1 = a.nbr[e * 6 + 2 + g], nb2 = a.nbr[e * 6 + 4 + g];
-    // Traces of the six sides (TPSAG[IJK]): normal, fast axis, slow axis.
-    FaceNormalBatch<NT, SLOT, K>(s_sol, a.sol, nb0, nb1, nb2, g, s_fv, BN, BND);
-    __syncthreads();
-    Contract<NT, SLOT, K, M, kLeg, 0, 30, K, K, 1, K, M, false>(BN, T1a);
-    Contract<NT, SLOT, K, M, kDLeg, 0, 30, K, K, 1, K, M, false>(BN, T1b);
-    Contract<NT, SLOT, K, M, kLeg, 0, 30, K, K, 1, K, M, false>(BND, T1c);
-    __syncthreads();
-    Contract<NT, SLOT, K, M, kLeg, 1, 30, M, K, 1, K, M, false>(T1a, TR);
-    Contract<NT, SLOT, K, M, kDLeg, 1, 30, M, K, 1, K, M, false>(T1a, TR + 3 * 30 * M2);
-    Contract<NT, SLOT, K, M, kLeg, 1, 30, M, K, 1, K, M, false>(T1b, TR + 2 * 30 * M2);
-    Contract<NT, SLOT, K, M, kLeg, 1, 30, M, K, 1, K, M, false>(T1c, TR + 1 * 30 * M2);
-    __syncthreads();
-    // Pointwise fluxes of the three faces.
     for (int idx = threadIdx.x; idx < 3 * M2; idx += NT) {
       const int d = idx / M2, pt = idx - d * M2;
       const int nb = d == 0 ? nb0 : (d == 1 ? nb1 : nb2);
@@ -647,10 +690,12 @@ __device__ __forceinline__ void FacePhase(const ResidualArgs &a, const int e, co
         }
         continue;
       }
-      const T lenScale = Fmin(T(sc[d]), T(a.elem_scalars[(size_t)nb * 15 + d]));
+      // The face's fluxes were computed by its upper element: this element for
+      // its Min faces, the neighbour for this element's Max faces.
+      const int upper = g == 0 ? e : nb;
+      const T *F = faceFlux + ((size_t)upper * 3 + d) * 20 * M2;
       const double *fmOwn = a.face_metric + ((size_t)e * 6 + 2 * d + g) * 13 * M2;
-      const double *fmNb = a.face_metric + ((size_t)nb * 6 + 2 * d + 1 - g) * 13 * M2;
-      GroupFacePoint<K, M>(a, mu, g, d, pt, TR, fmOwn, fmNb, lenScale, P1, P2);
+      FaceRoles<K, M>(a, g, d, pt, F, fmOwn, P1, P2);
     }
     __syncthreads();
     // Distribution (TPR[IJK]F): slow axis, fast axis, then the face-normal expansion.
@@ -889,7 +934,7 @@ __global__ void __launch_bounds__(NT, (Plan<K, M, T, OPEN>::MIN_BLOCKS)) Residua
   }
   __syncthreads();
   VolumePhase<NT, K, M, T, OPEN>(a, e, mu, s_sol, s_R, s_cgp, s_jw, work, s_red);
-  FacePhase<NT, K, M, T, OPEN>(a, e, mu, s_sol, s_R, s_fv, work);
+  FacePhase<NT, K, M, T, OPEN>(a, e, s_R, s_fv, work);
   if (a.res_raw) {
     double *dst = a.res_raw + (size_t)e * 5 * KD;
     for (int i = threadIdx.x; i < 5 * KD; i += NT) dst[i] = double(s_R[i]);
@@ -900,6 +945,42 @@ __global__ void __launch_bounds__(NT, (Plan<K, M, T, OPEN>::MIN_BLOCKS)) Residua
   __syncthreads();
   double *dst = a.res + (size_t)e * 5 * KD;
   for (int i = threadIdx.x; i < 5 * KD; i += NT) dst[i] = double(x[i]);
+}
+
+// Shared memory (in T) and launch shape of the face-flux kernel.
+template <int K, int M, typename T = double> struct FluxPlan {
+  static constexpr int KD = K * K * K, M2 = M * M;
+  static constexpr int TOTAL = 5 * KD + 4 * kKMax + 90 * K * M + 120 * M2;
+  static constexpr size_t BYTES = sizeof(T) * (size_t)TOTAL;
+  static constexpr int NT = 128;
+  static constexpr int FIT = (int)(227 * 1024 / BYTES);
+  static constexpr int MIN_BLOCKS = FIT < 1 ? 1 : (FIT > 3 ? 3 : FIT);
+};
+
+// The fluxes of every interior face, computed once by the face's upper element
+// (its Min faces), before the residual kernel distributes them to both sides.
+template <int K, int M, int NT, typename T>
+__global__ void __launch_bounds__(NT, (FluxPlan<K, M, T>::MIN_BLOCKS)) FaceFluxKernel(const ResidualArgs a) {
+  constexpr int KD = K * K * K;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *smem = reinterpret_cast<T *>(smem_raw);
+  T *s_sol = smem, *s_fv = s_sol + 5 * KD, *work = s_fv + 4 * kKMax;
+  const int e = blockIdx.x;
+  if (e >= a.n_elem) return;
+  double mu = a.mu;
+  if (a.cases.elem_case) {
+    const int cs = a.cases.elem_case[e];
+    if (cs < 0 || a.cases.state[cs] != a.cases.require) return;
+    mu = a.cases.par[cs * kCasePar + kParMu];
+  }
+  const double *src = a.sol + (size_t)e * 5 * KD;
+  for (int i = threadIdx.x; i < 5 * KD; i += NT) s_sol[i] = T(src[i]);
+  if (threadIdx.x < 2 * K) {
+    s_fv[threadIdx.x] = FaceVal<Slot<K, M>::value, T>(threadIdx.x);
+    s_fv[2 * K + threadIdx.x] = FaceDer<Slot<K, M>::value, T>(threadIdx.x);
+  }
+  __syncthreads();
+  MinFaceFluxes<NT, K, M, T>(a, e, mu, s_sol, s_fv, work);
 }
 
 }  // namespace vcpg

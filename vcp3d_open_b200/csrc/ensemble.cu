@@ -115,6 +115,7 @@ struct Bucket {
   double *sol = nullptr, *solOld = nullptr, *res = nullptr, *vol = nullptr, *face = nullptr,
          *sc = nullptr;
   int *nbr = nullptr, *elemCase = nullptr, *spongeIdx = nullptr;
+  void *fflux = nullptr;  // Min-face fluxes (FaceFluxKernel)
   // Boundary-face and sponge arenas.
   int *bface = nullptr;
   double *bpresc = nullptr, *btrace = nullptr, *bmach = nullptr, *bflux = nullptr;
@@ -173,7 +174,7 @@ int IntegrationPoints(int deg) {
 
 int64_t ElementBytes(int K, int M) {
   const int64_t KD = (int64_t)K * K * K, MD = (int64_t)M * M * M, M2 = (int64_t)M * M;
-  return 8 * (3 * 5 * KD + 10 * MD + 6 * 13 * M2 + 15) + 4 * (6 + 2);
+  return 8 * (3 * 5 * KD + 10 * MD + 6 * 13 * M2 + 15 + 3 * 20 * M2) + 4 * (6 + 2);
 }
 
 int64_t BFaceBytes(int M) { return 8 * (4 + 2 * 4 * 5 * (int64_t)M * M + 1) + 4 * kBfStride; }
@@ -189,7 +190,7 @@ void FreeBucket(Bucket &b) {
     if (ev) cudaEventDestroy(ev);
   if (b.exec) cudaGraphExecDestroy(b.exec);
   if (b.graph) cudaGraphDestroy(b.graph);
-  void *bufs[] = {b.sol, b.solOld, b.res, b.vol, b.face, b.sc, b.nbr, b.elemCase, b.spongeIdx,
+  void *bufs[] = {b.fflux, b.sol, b.solOld, b.res, b.vol, b.face, b.sc, b.nbr, b.elemCase, b.spongeIdx,
                   b.bface, b.bpresc, b.btrace, b.bmach, b.bflux, b.pc, b.dlq, b.dampFn,
                   b.dampSt, b.cml, b.state, b.target, b.done, b.status, b.par, b.dt,
                   b.simTime, b.dtBits, b.cgStats, b.cfgs};
@@ -226,6 +227,7 @@ int AllocBucket(vcpg_ensemble *e, Bucket &b, int deg, int64_t capE, int64_t capB
   int rc;
   if ((rc = alloc((void **)&b.sol, 8 * nState)) || (rc = alloc((void **)&b.solOld, 8 * nState)) ||
       (rc = alloc((void **)&b.res, 8 * nState)) ||
+      (rc = alloc((void **)&b.fflux, E * FaceFluxBytesPerElement(b.K, b.M))) ||
       (rc = alloc((void **)&b.vol, 8 * E * 10 * b.MD)) ||
       (rc = alloc((void **)&b.face, 8 * E * 6 * 13 * b.M2)) ||
       (rc = alloc((void **)&b.sc, 8 * E * 15)) || (rc = alloc((void **)&b.nbr, 4 * E * 6)) ||
@@ -291,6 +293,7 @@ ResidualArgs BucketResidualArgs(const vcpg_ensemble *e, const Bucket &b, int req
   a.cml = b.cml;
   a.cml_on = b.capS > 0 ? 1 : 0;
   a.cases = CaseView{b.elemCase, b.state, b.par, require};
+  a.face_flux = b.fflux;
   return a;
 }
 
@@ -325,7 +328,7 @@ int EnqueueBucketResidual(vcpg_ensemble *e, Bucket &b, int require, int *launche
     *launches += 2;
   }
   ENS_CUDA(e, LaunchResidual(b.K, b.M, BucketResidualArgs(e, b, require), b.stream));
-  *launches += 1;
+  *launches += 2;
   return VCPG_OK;
 }
 

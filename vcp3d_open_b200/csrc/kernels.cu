@@ -174,20 +174,38 @@ static cudaError_t ConfigureKMT() {
   return err;
 }
 
+template <int K, int M, typename T>
+static cudaError_t ConfigureFluxKMT() {
+  using P = FluxPlan<K, M, T>;
+  static bool configured = false;
+  if (configured) return cudaSuccess;
+  cudaError_t err = cudaFuncSetAttribute(FaceFluxKernel<K, M, P::NT, T>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)P::BYTES);
+  if (err == cudaSuccess) configured = true;
+  return err;
+}
+
 template <int K, int M>
 static cudaError_t ConfigureKM() {
-  cudaError_t e = ConfigureKMT<K, M, double, false>();
+  cudaError_t e = ConfigureFluxKMT<K, M, double>();
+  if (e == cudaSuccess) e = ConfigureFluxKMT<K, M, float>();
+  if (e == cudaSuccess) e = ConfigureKMT<K, M, double, false>();
   if (e == cudaSuccess) e = ConfigureKMT<K, M, float, false>();
   if (e == cudaSuccess) e = ConfigureKMT<K, M, double, true>();
   if (e == cudaSuccess) e = ConfigureKMT<K, M, float, true>();
   return e;
 }
 
+// One residual: the face fluxes, then the fused volume / distribution / mass-solve kernel.
 template <int K, int M, typename T, bool OPEN>
 static cudaError_t LaunchResidualKMT(const ResidualArgs &a, cudaStream_t st) {
   using P = Plan<K, M, T, OPEN>;
+  using PF = FluxPlan<K, M, T>;
   cudaError_t err = ConfigureKMT<K, M, T, OPEN>();
+  if (err == cudaSuccess) err = ConfigureFluxKMT<K, M, T>();
   if (err != cudaSuccess) return err;
+  FaceFluxKernel<K, M, PF::NT, T><<<a.n_elem, PF::NT, PF::BYTES, st>>>(a);
   ResidualKernel<K, M, P::NT, T, OPEN><<<a.n_elem, P::NT, P::BYTES, st>>>(a);
   return cudaGetLastError();
 }
@@ -244,6 +262,11 @@ size_t ResidualSmemBytes(int K, int M) {
   if (K == 6 && M == 8) return Plan<6, 8>::BYTES;
   if (K == 7 && M == 10) return Plan<7, 10>::BYTES;
   return 0;
+}
+
+size_t FaceFluxBytesPerElement(int K, int M) {
+  (void)K;
+  return sizeof(double) * 3 * 20 * (size_t)M * M;
 }
 
 cudaError_t LaunchResidual(int K, int M, const ResidualArgs &a, cudaStream_t st) {

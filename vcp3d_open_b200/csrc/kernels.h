@@ -17,6 +17,8 @@ struct CaseView;
 bool Supported(int K, int M);
 int SlotOf(int K, int M);
 size_t ResidualSmemBytes(int K, int M);
+// Device bytes per element of the face-flux buffer (ResidualArgs::face_flux).
+size_t FaceFluxBytesPerElement(int K, int M);
 // Operator table of a (K, M) pair from the C-ABI operators (FP64 and FP32 copies).
 void FillOpTable(const vcpg_operators *ops, int K, int M, OpTable *t);
 cudaError_t UploadOpTable(int slot, const OpTable &t);
@@ -25,6 +27,7 @@ cudaError_t LaunchEnsembleFinalize(int n_cases, int *state, const int *target, i
                                    unsigned long long *dt_bits, double *dt, double *sim_time,
                                    cudaStream_t st);
 
+// One residual = FaceFluxKernel + ResidualKernel (2 launches).
 cudaError_t LaunchResidual(int K, int M, const ResidualArgs &a, cudaStream_t st);
 // Sets the shared-memory limits of all residual-kernel variants of a (K, M) pair;
 // call before capturing launches into a CUDA graph.
