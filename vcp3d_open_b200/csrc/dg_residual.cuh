@@ -952,9 +952,15 @@ template <int K, int M, typename T = double> struct FluxPlan {
   static constexpr int KD = K * K * K, M2 = M * M;
   static constexpr int TOTAL = 5 * KD + 4 * kKMax + 90 * K * M + 120 * M2;
   static constexpr size_t BYTES = sizeof(T) * (size_t)TOTAL;
-  static constexpr int NT = 128;
+  // Launch shape measured best on B200 over 96..192 threads and 2..4 CTAs per SM:
+  // 128 threads and up to 4 CTAs (<= 128 registers) for degree <= 3; from degree
+  // 4 on, 160 threads (the 3 M^2 face points of a group in one pass) with up to
+  // 2 CTAs (FP64) or 3 CTAs (FP32).
+  static constexpr bool FP64 = sizeof(T) == 8;
+  static constexpr int NT = K <= 4 ? 128 : 160;
+  static constexpr int CAP = K <= 4 ? 4 : (FP64 ? 2 : 3);
   static constexpr int FIT = (int)(227 * 1024 / BYTES);
-  static constexpr int MIN_BLOCKS = FIT < 1 ? 1 : (FIT > 3 ? 3 : FIT);
+  static constexpr int MIN_BLOCKS = FIT < 1 ? 1 : (FIT > CAP ? CAP : FIT);
 };
 
 // The fluxes of every interior face, computed once by the face's upper element
