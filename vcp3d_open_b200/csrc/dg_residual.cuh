@@ -109,7 +109,23 @@ __device__ __forceinline__ T BlockMax(T v, T *red) {
   return s;
 }
 
-// Block-wide (sum a, sum b, max c) with one pair of barriers; red needs 3*NT/32.
+// Single-barrier block reductions for loops that alternate two scratch areas:
+// the caller guarantees that no thread still reads `red` from its previous use
+// (a barrier lies between that read and this call).
+template <int NT, typename T>
+__device__ __forceinline__ T BlockSum1(T v, T *red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  T s = T(0.0);
+#pragma unroll
+  for (int i = 0; i < NT / 32; ++i) s += red[i];
+  return s;
+}
+
+// Block-wide (sum a, sum b, max c) with one barrier, under the same condition
+// as BlockSum1; red needs 3*NT/32.
 template <int NT, typename T>
 __device__ __forceinline__ void BlockReduce3(T &a, T &b, T &c, T *red) {
 #pragma unroll
@@ -119,7 +135,6 @@ __device__ __forceinline__ void BlockReduce3(T &a, T &b, T &c, T *red) {
     c = Fmax(c, __shfl_xor_sync(0xffffffffu, c, o));
   }
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  __syncthreads();
   if (lane == 0) { red[w] = a; red[NT / 32 + w] = b; red[2 * (NT / 32) + w] = c; }
   __syncthreads();
   a = T(0.0); b = T(0.0); c = red[2 * (NT / 32)];
@@ -145,12 +160,10 @@ template <int K, int M, typename T = double, bool OPEN = false> struct Plan {
   static constexpr int TJ = 5 * K * M * M;      // second-stage buffer
   // Volume phase: tK, tJ, Var, dX, dY, dZ (+ the matching-layer source when OPEN).
   static constexpr int VOL = TK + TJ + 20 * MD + (OPEN ? 5 * MD : 0);
-  // Face phase: per face-side trace (value + 3 derivatives) 20*M2, two sides,
-  // three faces at a time, plus normal-evaluation and stage buffers.
-  // Face phase: BN/BND 60 K^2, three fast-axis buffers 90 K M, traces 120 M^2.
-  // Face phase: distribution inputs (60 M^2) and the slow-axis results (60 K M);
-  // the traces and fluxes are computed by FaceFluxKernel.
-  static constexpr int FACE = 60 * M2 + 60 * K * M;
+  // Face phase: the distribution inputs of the six faces (120 M^2) and their
+  // slow-axis results (120 K M); the traces and fluxes are computed by
+  // FaceFluxKernel.
+  static constexpr int FACE = 120 * M2 + 120 * K * M;
   // CG phase: z, p, Ap, x, pInt and the contraction buffers.
   static constexpr int CG = 20 * KD + 5 * MD + TK + TJ;
   static constexpr int WORK = VOL > FACE ? (VOL > CG ? VOL : CG) : (FACE > CG ? FACE : CG);
@@ -581,16 +594,28 @@ __device__ __forceinline__ void FacePointFlux(const ResidualArgs &a, const doubl
   }
 }
 
-// Distribution inputs of one face point for the own element from the face's
-// fluxes F[20][M^2] (FacePointFlux layout): P1[role][d][v][M2] with role 0 the
-// fast-axis symmetrizing flux, 1 the normal flux with the own side's sign (the
-// own element is the right state of its Min faces), 2 the face-normal
-// symmetrizing flux; P2[d][v][M2] the slow-axis symmetrizing flux. The
-// symmetrizing fluxes are turned parametric with the own side's metric fm.
+// Distribution inputs of the six faces (TPR[IJK]F), both sides g = 0 (Min
+// faces) and g = 1 (Max faces), grouped by the operators they take; within a
+// group [g][d][v][B] (B = M^2 face points, later K^2 after both axes):
+//   set 0 (PA, 30 blocks)   fast-axis symmetrizing flux: slow Leg^T, fast DLeg^T
+//   set 1 (PB, 30 blocks)   normal flux:                 slow Leg^T, fast Leg^T
+//   set 2 (PB, 30 blocks)   face-normal symmetrizing flux (expanded with the
+//                           derivative of the face basis)
+//   set 3 (PC, 30 blocks)   slow-axis symmetrizing flux: slow DLeg^T, fast Leg^T
+// Sets 0-2 are contiguous, so one slow-axis contraction covers them.
+template <int B>
+__device__ __forceinline__ int RoleIndex(const int set, const int g, const int d, const int v,
+                                         const int pt) {
+  return ((set * 2 + g) * 15 + d * 5 + v) * B + pt;
+}
+
+// The roles of the fluxes F[20][M^2] (FacePointFlux layout) of one face point
+// for side g of the element: the normal flux with the own side's sign (the own
+// element is the right state of its Min faces) and the symmetrizing fluxes
+// turned parametric with the own side's metric fm.
 template <int K, int M, typename T>
 __device__ __forceinline__ void FaceRoles(const ResidualArgs &a, const int g, const int d,
-                                          const int pt, const T *F, const double *fm, T *P1,
-                                          T *P2) {
+                                          const int pt, const T *F, const double *fm, T *P) {
   constexpr int M2 = M * M;
   const int pFast = FastParam(d);
 #pragma unroll
@@ -603,11 +628,10 @@ __device__ __forceinline__ void FaceRoles(const ResidualArgs &a, const int g, co
     for (int p = 0; p < 3; ++p)
       sym[p] = sx * LdT<T>(fm + (4 + 3 * p) * M2 + mi) + sy * LdT<T>(fm + (5 + 3 * p) * M2 + mi) +
                sz * LdT<T>(fm + (6 + 3 * p) * M2 + mi);
-    const int o = (d * 5 + n) * M2 + pt;
-    P1[1 * 15 * M2 + o] = g == 0 ? -flux : flux;
-    P1[2 * 15 * M2 + o] = sym[d];
-    P1[0 * 15 * M2 + o] = sym[pFast];
-    P2[o] = sym[3 - d - pFast];
+    P[RoleIndex<M2>(0, g, d, n, pt)] = sym[pFast];
+    P[RoleIndex<M2>(1, g, d, n, pt)] = g == 0 ? -flux : flux;
+    P[RoleIndex<M2>(2, g, d, n, pt)] = sym[d];
+    P[RoleIndex<M2>(3, g, d, n, pt)] = sym[3 - d - pFast];
   }
 }
 
@@ -656,69 +680,65 @@ __device__ __forceinline__ void FacePhase(const ResidualArgs &a, const int e, T 
                                           const T *s_fv, T *work) {
   constexpr int SLOT = Slot<K, M>::value;
   constexpr int KD = K * K * K, M2 = M * M, K2 = K * K;
-  // P [60 M^2], then the fast-axis results RF/RFN/RS (60 K^2) in its place;
-  // Q [60 K M] after the slow axis.
+  // P [120 M^2] (RoleIndex order), Q [120 K M] after the slow axis, R [120 K^2]
+  // after the fast axis in P's place.
   static_assert(K <= M, "face-phase buffer aliasing");
-  T *P1 = work, *P2 = P1 + 45 * M2;
-  T *Q1 = P1 + 60 * M2, *Q2 = Q1 + 45 * K * M;
-  T *RF = work, *RFN = RF + 15 * K2, *RS = RFN + 30 * K2;
+  T *P = work, *Q = work + 120 * M2, *R = work;
   const T *faceFlux = reinterpret_cast<const T *>(a.face_flux);
-  for (int g = 0; g < 2; ++g) {
-    const int nb0 = a.nbr[e * 6 + 0 + g], nb1 = a.nbr[e * 6 + 2 + g], nb2 = a.nbr[e * 6 + 4 + g];
-    for (int idx = threadIdx.x; idx < 3 * M2; idx += NT) {
-      const int d = idx / M2, pt = idx - d * M2;
-      const int nb = d == 0 ? nb0 : (d == 1 ? nb1 : nb2);
-      if (OPEN && nb <= -2) {
-        // Characteristic boundary face: fluxes from BoundaryFluxKernel (FP64).
-        const double *bf = a.bflux + (size_t)(-2 - nb) * 4 * 5 * M2;
+  for (int idx = threadIdx.x; idx < 6 * M2; idx += NT) {
+    const int f = idx / M2, pt = idx - f * M2;
+    const int g = f / 3, d = f - 3 * g;
+    const int nb = a.nbr[e * 6 + 2 * d + g];
+    if (OPEN && nb <= -2) {
+      // Characteristic boundary face: fluxes from BoundaryFluxKernel (FP64),
+      // roles [0] fast-axis sym, [1] flux, [2] normal sym, [3] slow-axis sym.
+      const double *bf = a.bflux + (size_t)(-2 - nb) * 4 * 5 * M2;
 #pragma unroll
-        for (int n = 0; n < 5; ++n) {
-          const int o = (d * 5 + n) * M2 + pt;
-          P1[o] = T(bf[(0 * 5 + n) * M2 + pt]);
-          P1[15 * M2 + o] = T(bf[(1 * 5 + n) * M2 + pt]);
-          P1[30 * M2 + o] = T(bf[(2 * 5 + n) * M2 + pt]);
-          P2[o] = T(bf[(3 * 5 + n) * M2 + pt]);
-        }
-        continue;
-      }
-      if (nb < 0) {
-        // A physical boundary face without a boundary condition.
-        if (pt == 0) atomicAdd(a.status + 1, 1);
-        for (int n = 0; n < 5; ++n) {
-          const int o = (d * 5 + n) * M2 + pt;
-          P1[o] = P1[15 * M2 + o] = P1[30 * M2 + o] = P2[o] = T(0.0);
-        }
-        continue;
-      }
-      // The face's fluxes were computed by its upper element: this element for
-      // its Min faces, the neighbour for this element's Max faces.
-      const int upper = g == 0 ? e : nb;
-      const T *F = faceFlux + ((size_t)upper * 3 + d) * 20 * M2;
-      const double *fmOwn = a.face_metric + ((size_t)e * 6 + 2 * d + g) * 13 * M2;
-      FaceRoles<K, M>(a, g, d, pt, F, fmOwn, P1, P2);
+      for (int n = 0; n < 5; ++n)
+#pragma unroll
+        for (int set = 0; set < 4; ++set)
+          P[RoleIndex<M2>(set, g, d, n, pt)] = T(bf[(set * 5 + n) * M2 + pt]);
+      continue;
     }
-    __syncthreads();
-    // Distribution (TPR[IJK]F): slow axis, fast axis, then the face-normal expansion.
-    Contract<NT, SLOT, K, M, kLegT, 1, 45, M, M, 1, M, K, false>(P1, Q1);
-    Contract<NT, SLOT, K, M, kDLegT, 1, 15, M, M, 1, M, K, false>(P2, Q2);
-    __syncthreads();
-    Contract<NT, SLOT, K, M, kDLegT, 0, 15, M, K, 1, M, K, false>(Q1, RF);
-    Contract<NT, SLOT, K, M, kLegT, 0, 30, M, K, 1, M, K, false>(Q1 + 15 * K * M, RFN);
-    Contract<NT, SLOT, K, M, kLegT, 0, 15, M, K, 1, M, K, false>(Q2, RS);
-    __syncthreads();
-    const T *fv = s_fv + g * K, *dfv = s_fv + (2 + g) * K;
-    for (int idx = threadIdx.x; idx < 5 * KD; idx += NT) {
-      const int v = idx / KD, r = idx - v * KD;
-      const int k = r / K2, r2 = r - k * K2, j = r2 / K, i = r2 - j * K;
-      T acc = s_R[idx];
+    if (nb < 0) {
+      // A physical boundary face without a boundary condition.
+      if (pt == 0) atomicAdd(a.status + 1, 1);
+      for (int n = 0; n < 5; ++n)
+        for (int set = 0; set < 4; ++set) P[RoleIndex<M2>(set, g, d, n, pt)] = T(0.0);
+      continue;
+    }
+    // The face's fluxes were computed by its upper element: this element for
+    // its Min faces, the neighbour for this element's Max faces.
+    const int upper = g == 0 ? e : nb;
+    const T *F = faceFlux + ((size_t)upper * 3 + d) * 20 * M2;
+    const double *fmOwn = a.face_metric + ((size_t)e * 6 + 2 * d + g) * 13 * M2;
+    FaceRoles<K, M>(a, g, d, pt, F, fmOwn, P);
+  }
+  __syncthreads();
+  // Slow axis, fast axis, then the face-normal expansion.
+  Contract<NT, SLOT, K, M, kLegT, 1, 90, M, M, 1, M, K, false>(P, Q);
+  Contract<NT, SLOT, K, M, kDLegT, 1, 30, M, M, 1, M, K, false>(P + 90 * M2, Q + 90 * K * M);
+  __syncthreads();
+  Contract<NT, SLOT, K, M, kDLegT, 0, 30, M, K, 1, M, K, false>(Q, R);
+  Contract<NT, SLOT, K, M, kLegT, 0, 90, M, K, 1, M, K, false>(Q + 30 * K * M, R + 30 * K2);
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < 5 * KD; idx += NT) {
+    const int v = idx / KD, r = idx - v * KD;
+    const int k = r / K2, r2 = r - k * K2, j = r2 / K, i = r2 - j * K;
+    T acc = s_R[idx];
+    // Reference order: the own Min faces (i, j, k) accumulate onto the volume
+    // term; each Max face's contribution is summed from zero and added.
+#pragma unroll
+    for (int g = 0; g < 2; ++g) {
+      const T *fv = s_fv + g * K, *dfv = s_fv + (2 + g) * K;
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
         const int n = d == 0 ? i : (d == 1 ? j : k);
         const int sf = d == 0 ? k * K + j : (d == 1 ? k * K + i : j * K + i);
-        const int o = (d * 5 + v) * K2 + sf;
         const T aF = fv[n], aD = dfv[n];
-        const T tFlux = RFN[o], tN = RFN[15 * K2 + o], tFast = RF[o], tSlow = RS[o];
-        // Reference order: normal flux, then the r, s, t symmetrizing fluxes.
+        const T tFast = R[RoleIndex<K2>(0, g, d, v, sf)], tFlux = R[RoleIndex<K2>(1, g, d, v, sf)],
+                tN = R[RoleIndex<K2>(2, g, d, v, sf)], tSlow = R[RoleIndex<K2>(3, g, d, v, sf)];
+        // Normal flux, then the r, s, t symmetrizing fluxes.
         const int pFast = FastParam(d);
         T c = g == 0 ? acc : T(0.0);
         c = Fma(aF, tFlux, c);
@@ -730,10 +750,82 @@ __device__ __forceinline__ void FacePhase(const ResidualArgs &a, const int e, T 
         }
         acc = g == 0 ? c : acc + c;
       }
-      s_R[idx] = acc;
     }
-    __syncthreads();
+    s_R[idx] = acc;
   }
+  __syncthreads();
+}
+
+// The first and the last transform of the mass-matrix operator, with the work
+// that shares their loads: p = beta p + z before the forward k transform (from
+// the second iteration on), and the partial sum of p . Ap after the backward
+// i transform. Lines, summation order and coefficients are those of
+// Contract<..., AX = 2, ...> and Contract<..., AX = 0, ...>.
+template <int NT, int SLOT, int K, int M, typename T>
+__device__ __forceinline__ void KForwardUpdate(T *__restrict__ p, const T *__restrict__ z,
+                                               const T beta, const bool update,
+                                               T *__restrict__ out) {
+  constexpr int K2 = K * K, NLINES = 5 * K2;
+  for (int line = threadIdx.x; line < NLINES; line += NT) {
+    const int v = line / K2, r = line - v * K2;
+    const int ib = v * K2 * K + r, ob = v * K2 * M + r;
+    T xv[K];
+#pragma unroll
+    for (int c = 0; c < K; ++c) xv[c] = p[ib + c * K2];
+    if (update) {
+#pragma unroll
+      for (int c = 0; c < K; ++c) {
+        xv[c] = Fma(beta, xv[c], z[ib + c * K2]);
+        p[ib + c * K2] = xv[c];
+      }
+    }
+#pragma unroll
+    for (int o = 0; o < M; ++o) {
+      T acc = T(0);
+#pragma unroll
+      for (int c = 0; c < K; ++c) acc = fma(Coef<SLOT, K, M, kLeg, T>(c, o), xv[c], acc);
+      out[ob + o * K2] = acc;
+    }
+  }
+}
+
+template <int NT, int SLOT, int K, int M, typename T>
+__device__ __forceinline__ T IBackwardDot(const T *__restrict__ in, const T *__restrict__ p,
+                                          T *__restrict__ Ap) {
+  constexpr int NLINES = 5 * K * K;
+  T part = T(0);
+  for (int line = threadIdx.x; line < NLINES; line += NT) {
+    T xv[M];
+#pragma unroll
+    for (int c = 0; c < M; ++c) xv[c] = in[line * M + c];
+#pragma unroll
+    for (int o = 0; o < K; ++o) {
+      T acc = T(0);
+#pragma unroll
+      for (int c = 0; c < M; ++c) acc = fma(Coef<SLOT, K, M, kLegT, T>(c, o), xv[c], acc);
+      Ap[line * K + o] = acc;
+      part = Fma(p[line * K + o], acc, part);
+    }
+  }
+  return part;
+}
+
+// w J dU/dV at one integration point from the stored point data (rho, u, v, w, p)
+// (src/CG_MassMatrix.cpp:408-443 with dU/dV as in the volume phase): d[0..14] the
+// symmetric 5x5 matrix by rows of its upper triangle, d[15] = w J.
+template <int MD, typename T>
+__device__ __forceinline__ void PointOperator(const T *s_cgp, const T *s_jw, const int l, T d[16]) {
+  const T rho = s_cgp[l], u = s_cgp[MD + l], v = s_cgp[2 * MD + l], w = s_cgp[3 * MD + l],
+          pr = s_cgp[4 * MD + l];
+  const T eKin = T(0.5) * (u * u + v * v + w * w);
+  const T rE = -pr * (-T(1.0) / (T(kGam) - T(1.0))) + rho * eKin;
+  const T ru = rho * u, rv = rho * v, rw = rho * w, rH = rE + pr;
+  d[0] = rho; d[1] = ru; d[2] = rv; d[3] = rw; d[4] = rE;
+  d[5] = ru * u + pr; d[6] = ru * v; d[7] = ru * w; d[8] = rH * u;
+  d[9] = rv * v + pr; d[10] = rv * w; d[11] = rH * v;
+  d[12] = rw * w + pr; d[13] = rH * w;
+  d[14] = rE * rH / rho + pr * eKin;
+  d[15] = s_jw[l];
 }
 
 // ---------------------------------------------------------------------------
@@ -742,6 +834,14 @@ __device__ __forceinline__ void FacePhase(const ResidualArgs &a, const int e, T 
 // dV/dU * 8/vol preconditioner, stop at ||r||_inf < 1e-10 ||r0||_inf, at most
 // 100 iterations (the cap raises a status flag instead of aborting).
 // r is s_R (overwritten); the solution is returned in x.
+//
+// One iteration is seven barrier-separated steps: k, j transforms to the
+// integration points (the first with the search-direction update), the
+// i transform fused with the point operator (one thread per point, its
+// w J dU/dV kept in registers where the register budget allows),
+// k, j, i transforms back (the last with the partial sums of p . Ap), and the
+// update of x, r and z with the three sums that close the iteration. The two
+// reductions use one barrier each and alternate their scratch areas.
 // ---------------------------------------------------------------------------
 template <int NT, int K, int M, typename T>
 __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, const T *s_sol,
@@ -749,10 +849,15 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
                                           T *work, T *s_red, T *&xOut) {
   constexpr int SLOT = Slot<K, M>::value;
   using P = Plan<K, M, T>;
-  constexpr int KD = P::KD, MD = P::MD;
+  constexpr int KD = P::KD, MD = P::MD, M2 = M * M;
+  constexpr int PP = (MD + NT - 1) / NT;   // integration points per thread
+  // Point operators held in registers: one point per thread, or two when the
+  // launch bounds leave at least 168 registers per thread.
+  constexpr bool kRegD = PP == 1 || (PP == 2 && 65536 / (NT * P::MIN_BLOCKS) >= 168);
   T *z = work, *p = z + 5 * KD, *Ap = p + 5 * KD, *x = Ap + 5 * KD;
   T *pInt = x + 5 * KD, *tK = pInt + 5 * MD, *tJ = tK + P::TK;
   T *dvdu = s_red + 32;  // 15 preconditioner entries
+  T *redA = s_red, *redB = s_red + 32;
   T *r = s_R;
   xOut = x;
   const T volElem = a.elem_scalars[(size_t)e * 15 + 5];
@@ -806,18 +911,27 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
   T D[15];
 #pragma unroll
   for (int q = 0; q < 15; ++q) D[q] = dvdu[q];
-  auto precond = [&](void) {
-    for (int l = threadIdx.x; l < KD; l += NT) {
-      const T r0 = r[l], r1 = r[KD + l], r2 = r[2 * KD + l], r3 = r[3 * KD + l],
-                   r4 = r[4 * KD + l];
-      z[l] = D[0] * r0 + D[1] * r1 + D[2] * r2 + D[3] * r3 + D[4] * r4;
-      z[KD + l] = D[1] * r0 + D[5] * r1 + D[6] * r2 + D[7] * r3 + D[8] * r4;
-      z[2 * KD + l] = D[2] * r0 + D[6] * r1 + D[9] * r2 + D[10] * r3 + D[11] * r4;
-      z[3 * KD + l] = D[3] * r0 + D[7] * r1 + D[10] * r2 + D[12] * r3 + D[13] * r4;
-      z[4 * KD + l] = D[4] * r0 + D[8] * r1 + D[11] * r2 + D[13] * r3 + D[14] * r4;
+  // The i-direction basis values and the point operators of this thread's points.
+  T lc[PP][K];
+  T dd[kRegD ? PP : 1][16];
+#pragma unroll
+  for (int n = 0; n < PP; ++n) {
+    const int l = threadIdx.x + n * NT;
+    if (l < MD) {
+#pragma unroll
+      for (int c = 0; c < K; ++c) lc[n][c] = Coef<SLOT, K, M, kLeg, T>(c, l % M);
+      if constexpr (kRegD) PointOperator<MD>(s_cgp, s_jw, l, dd[n]);
     }
-  };
-  precond();
+  }
+  for (int l = threadIdx.x; l < KD; l += NT) {
+    const T r0 = r[l], r1 = r[KD + l], r2 = r[2 * KD + l], r3 = r[3 * KD + l],
+            r4 = r[4 * KD + l];
+    z[l] = D[0] * r0 + D[1] * r1 + D[2] * r2 + D[3] * r3 + D[4] * r4;
+    z[KD + l] = D[1] * r0 + D[5] * r1 + D[6] * r2 + D[7] * r3 + D[8] * r4;
+    z[2 * KD + l] = D[2] * r0 + D[6] * r1 + D[9] * r2 + D[10] * r3 + D[11] * r4;
+    z[3 * KD + l] = D[3] * r0 + D[7] * r1 + D[10] * r2 + D[12] * r3 + D[13] * r4;
+    z[4 * KD + l] = D[4] * r0 + D[8] * r1 + D[11] * r2 + D[13] * r3 + D[14] * r4;
+  }
   __syncthreads();
   T part = T(0.0);
   for (int i = threadIdx.x; i < 5 * KD; i += NT) {
@@ -827,47 +941,52 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
   T dotrz = BlockSum<NT>(part, s_red);
 
   int iter = 0;
+  T beta = T(0.0);
   for (;; ++iter) {
     if (iter == 100) {
       if (threadIdx.x == 0) atomicAdd(a.status, 1);
       break;
     }
     // Ap = Leg^T3 (w J dU/dV (Leg3 p)) (src/CG_MassMatrix.cpp:408-443).
-    Contract<NT, SLOT, K, M, kLeg, 2, 5, K, K, K, K, M, false>(p, tK);
+    KForwardUpdate<NT, SLOT, K, M, T>(p, z, beta, iter > 0, tK);
     __syncthreads();
     Contract<NT, SLOT, K, M, kLeg, 1, 5, K, K, M, K, M, false>(tK, tJ);
     __syncthreads();
-    Contract<NT, SLOT, K, M, kLeg, 0, 5, K, M, M, K, M, false>(tJ, pInt);
-    __syncthreads();
-    for (int l = threadIdx.x; l < MD; l += NT) {
-      const T iw = s_jw[l];
-      const T p0 = iw * pInt[l], p1 = iw * pInt[MD + l], p2 = iw * pInt[2 * MD + l],
-                   p3 = iw * pInt[3 * MD + l], p4 = iw * pInt[4 * MD + l];
-      const T rho = s_cgp[l], u = s_cgp[MD + l], v = s_cgp[2 * MD + l],
-                   w = s_cgp[3 * MD + l], pr = s_cgp[4 * MD + l];
-      // rho E and dU/dV(4,4) from the primitive variables, as in the volume phase.
-      const T eKin = T(0.5) * (u * u + v * v + w * w);
-      const T rE = -pr * (-T(1.0) / (T(kGam) - T(1.0))) + rho * eKin;
-      const T ru = rho * u, rv = rho * v, rw = rho * w, rH = rE + pr;
-      const T d0 = rho, d1 = ru, d2 = rv, d3 = rw, d4 = rE, d5 = ru * u + pr, d6 = ru * v,
-                   d7 = ru * w, d8 = rH * u, d9 = rv * v + pr, d10 = rv * w, d11 = rH * v,
-                   d12 = rw * w + pr, d13 = rH * w, d14 = rE * rH / rho + pr * eKin;
-      pInt[l] = d0 * p0 + d1 * p1 + d2 * p2 + d3 * p3 + d4 * p4;
-      pInt[MD + l] = d1 * p0 + d5 * p1 + d6 * p2 + d7 * p3 + d8 * p4;
-      pInt[2 * MD + l] = d2 * p0 + d6 * p1 + d9 * p2 + d10 * p3 + d11 * p4;
-      pInt[3 * MD + l] = d3 * p0 + d7 * p1 + d10 * p2 + d12 * p3 + d13 * p4;
-      pInt[4 * MD + l] = d4 * p0 + d8 * p1 + d11 * p2 + d13 * p3 + d14 * p4;
+#pragma unroll
+    for (int n = 0; n < PP; ++n) {
+      const int l = threadIdx.x + n * NT;
+      if (l < MD) {
+        const T *src = tJ + (l / M) * K;   // tJ[v][mk][mj][0..K-1] of this point's line
+        T q[5];
+#pragma unroll
+        for (int vv = 0; vv < 5; ++vv) {
+          T acc = T(0);
+#pragma unroll
+          for (int c = 0; c < K; ++c) acc = fma(lc[n][c], src[vv * M2 * K + c], acc);
+          q[vv] = acc;
+        }
+        T dl[16];
+        if constexpr (kRegD) {
+#pragma unroll
+          for (int i = 0; i < 16; ++i) dl[i] = dd[n][i];
+        } else {
+          PointOperator<MD>(s_cgp, s_jw, l, dl);
+        }
+        const T iw = dl[15];
+        const T p0 = iw * q[0], p1 = iw * q[1], p2 = iw * q[2], p3 = iw * q[3], p4 = iw * q[4];
+        pInt[l] = dl[0] * p0 + dl[1] * p1 + dl[2] * p2 + dl[3] * p3 + dl[4] * p4;
+        pInt[MD + l] = dl[1] * p0 + dl[5] * p1 + dl[6] * p2 + dl[7] * p3 + dl[8] * p4;
+        pInt[2 * MD + l] = dl[2] * p0 + dl[6] * p1 + dl[9] * p2 + dl[10] * p3 + dl[11] * p4;
+        pInt[3 * MD + l] = dl[3] * p0 + dl[7] * p1 + dl[10] * p2 + dl[12] * p3 + dl[13] * p4;
+        pInt[4 * MD + l] = dl[4] * p0 + dl[8] * p1 + dl[11] * p2 + dl[13] * p3 + dl[14] * p4;
+      }
     }
     __syncthreads();
     Contract<NT, SLOT, K, M, kLegT, 2, 5, M, M, M, M, K, false>(pInt, tJ);
     __syncthreads();
     Contract<NT, SLOT, K, M, kLegT, 1, 5, M, M, K, M, K, false>(tJ, tK);
     __syncthreads();
-    Contract<NT, SLOT, K, M, kLegT, 0, 5, M, K, K, M, K, false>(tK, Ap);
-    __syncthreads();
-    part = T(0.0);
-    for (int i = threadIdx.x; i < 5 * KD; i += NT) part = Fma(p[i], Ap[i], part);
-    const T alpha = dotrz / BlockSum<NT>(part, s_red);
+    const T alpha = dotrz / BlockSum1<NT>(IBackwardDot<NT, SLOT, K, M, T>(tK, p, Ap), redA);
     // Each thread owns whole DOFs: update x and r, precondition, and form the
     // partial sums of the three reductions that close the iteration.
     T zAp = T(0.0), rzNew = T(0.0), rMax = T(0.0);
@@ -893,12 +1012,10 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
         rzNew = Fma(rr[q], zz[q], rzNew);
       }
     }
-    BlockReduce3<NT>(zAp, rzNew, rMax, s_red);
+    BlockReduce3<NT>(zAp, rzNew, rMax, redB);
     if (rMax < T(a.cg_tol) * rInitMax) break;
-    const T beta = -alpha * zAp / dotrz;
+    beta = -alpha * zAp / dotrz;
     dotrz = rzNew;
-    for (int i = threadIdx.x; i < 5 * KD; i += NT) p[i] = beta * p[i] + z[i];
-    __syncthreads();
   }
   if (threadIdx.x == 0 && a.cg_stats) {
     atomicAdd(a.cg_stats, (unsigned long long)(iter + 1));
