@@ -15,6 +15,8 @@
 // the Max-face contributions each summed from zero and added (i, j, k).
 #pragma once
 
+#include <type_traits>
+
 #include "dg_physics.cuh"
 #include "dg_tensor.cuh"
 
@@ -158,15 +160,29 @@ template <int K, int M, typename T = double, bool OPEN = false> struct Plan {
   static constexpr int KD = K * K * K, MD = M * M * M, M2 = M * M;
   static constexpr int TK = 5 * K * K * M;      // first-stage buffer
   static constexpr int TJ = 5 * K * M * M;      // second-stage buffer
-  // Volume phase: tK, tJ, Var, dX, dY, dZ (+ the matching-layer source when OPEN).
-  static constexpr int VOL = TK + TJ + 20 * MD + (OPEN ? 5 * MD : 0);
   // Face phase: the distribution inputs of the six faces (120 M^2) and their
   // slow-axis results (120 K M); the traces and fluxes are computed by
   // FaceFluxKernel.
   static constexpr int FACE = 120 * M2 + 120 * K * M;
-  // CG phase: z, p, Ap, x, pInt and the contraction buffers.
-  static constexpr int CG = 20 * KD + 5 * MD + TK + TJ;
-  static constexpr int WORK = VOL > FACE ? (VOL > CG ? VOL : CG) : (FACE > CG ? FACE : CG);
+  // CG phase: z, p, Ap, x, pInt and the contraction buffers (padded layouts).
+  using CL = CgLayout<K, M, (int)sizeof(T)>;
+  static constexpr int CG_TK = 5 * (CL::A::SV > CL::E::SV ? CL::A::SV : CL::E::SV);
+  static constexpr int CG_TJ = 5 * (CL::B::SV > CL::D::SV ? CL::B::SV : CL::D::SV);
+  static constexpr int CG = 20 * CL::P::SV + 5 * CL::C::SV + CG_TK + CG_TJ;
+  // Volume phase: tK, tJ, Var, dX, dY, dZ (+ the matching-layer source when
+  // OPEN). tK and tJ take the CG's padded layouts where that does not enlarge
+  // the shared memory of the kernel.
+  static constexpr int VOL_DENSE = TK + TJ + 20 * MD + (OPEN ? 5 * MD : 0);
+  static constexpr int VOL_PAD = CG_TK + CG_TJ + 20 * MD + (OPEN ? 5 * MD : 0);
+  static constexpr int OTHER = FACE > CG ? FACE : CG;
+  static constexpr bool PADVOL = VOL_PAD <= (VOL_DENSE > OTHER ? VOL_DENSE : OTHER);
+  static constexpr int VOL = PADVOL ? VOL_PAD : VOL_DENSE;
+  static constexpr int VTK = PADVOL ? CG_TK : TK, VTJ = PADVOL ? CG_TJ : TJ;
+  using VA = std::conditional_t<PADVOL, typename CL::A, Dense<K, K, M>>;
+  using VB = std::conditional_t<PADVOL, typename CL::B, Dense<K, M, M>>;
+  using VD = std::conditional_t<PADVOL, typename CL::D, Dense<M, M, K>>;
+  using VE = std::conditional_t<PADVOL, typename CL::E, Dense<M, K, K>>;
+  static constexpr int WORK = VOL > OTHER ? VOL : OTHER;
   // Persistent: sol, R, CG point data (rho, u, v, w, p per point), J*w, reduction scratch,
   // face vectors (basis and derivative at r = -1, +1).
   static constexpr int PERSIST = 10 * KD + 6 * MD + 64 + 4 * kKMax;
@@ -290,29 +306,29 @@ __device__ __forceinline__ void VolumePhase(const ResidualArgs &a, const int e, 
   constexpr int SLOT = Slot<K, M>::value;
   using P = Plan<K, M, T, OPEN>;
   constexpr int MD = P::MD, KD = P::KD, M2 = P::M2;
-  T *tK = work, *tJ = work + P::TK, *Var = tJ + P::TJ;
+  T *tK = work, *tJ = work + P::VTK, *Var = tJ + P::VTJ;
   T *dX = Var + 5 * MD, *dY = dX + 5 * MD, *dZ = dY + 5 * MD;
   T *bufC = dZ + 5 * MD;  // matching-layer source (OPEN only)
   const int sp = OPEN ? a.sponge_idx[e] : -1;
   const bool cmlHere = OPEN && sp >= 0 && a.cml_on;
 
   // TPSAGV (include/TensorProductSolAndGradVolume.hpp:5-249): k, then j, then i.
-  Contract<NT, SLOT, K, M, kLeg, 2, 5, K, K, K, K, M, false>(s_sol, tK);
+  ContractL<NT, SLOT, K, M, kLeg, 2, 5, K, K, K, K, M, false, T, Dense<K, K, K>, typename P::VA>(s_sol, tK);
   __syncthreads();
-  Contract<NT, SLOT, K, M, kLeg, 1, 5, K, K, M, K, M, false>(tK, tJ);
+  ContractL<NT, SLOT, K, M, kLeg, 1, 5, K, K, M, K, M, false, T, typename P::VA, typename P::VB>(tK, tJ);
   __syncthreads();
-  Contract<NT, SLOT, K, M, kLeg, 0, 5, K, M, M, K, M, false>(tJ, Var);
-  Contract<NT, SLOT, K, M, kDLeg, 0, 5, K, M, M, K, M, false>(tJ, dX);
+  ContractL<NT, SLOT, K, M, kLeg, 0, 5, K, M, M, K, M, false, T, typename P::VB, Dense<M, M, M>>(tJ, Var);
+  ContractL<NT, SLOT, K, M, kDLeg, 0, 5, K, M, M, K, M, false, T, typename P::VB, Dense<M, M, M>>(tJ, dX);
   __syncthreads();
-  Contract<NT, SLOT, K, M, kDLeg, 1, 5, K, K, M, K, M, false>(tK, tJ);
+  ContractL<NT, SLOT, K, M, kDLeg, 1, 5, K, K, M, K, M, false, T, typename P::VA, typename P::VB>(tK, tJ);
   __syncthreads();
-  Contract<NT, SLOT, K, M, kLeg, 0, 5, K, M, M, K, M, false>(tJ, dY);
+  ContractL<NT, SLOT, K, M, kLeg, 0, 5, K, M, M, K, M, false, T, typename P::VB, Dense<M, M, M>>(tJ, dY);
   __syncthreads();
-  Contract<NT, SLOT, K, M, kDLeg, 2, 5, K, K, K, K, M, false>(s_sol, tK);
+  ContractL<NT, SLOT, K, M, kDLeg, 2, 5, K, K, K, K, M, false, T, Dense<K, K, K>, typename P::VA>(s_sol, tK);
   __syncthreads();
-  Contract<NT, SLOT, K, M, kLeg, 1, 5, K, K, M, K, M, false>(tK, tJ);
+  ContractL<NT, SLOT, K, M, kLeg, 1, 5, K, K, M, K, M, false, T, typename P::VA, typename P::VB>(tK, tJ);
   __syncthreads();
-  Contract<NT, SLOT, K, M, kLeg, 0, 5, K, M, M, K, M, false>(tJ, dZ);
+  ContractL<NT, SLOT, K, M, kLeg, 0, 5, K, M, M, K, M, false, T, typename P::VB, Dense<M, M, M>>(tJ, dZ);
   for (int i = threadIdx.x; i < 5 * KD; i += NT) s_R[i] = T(0.0);
   __syncthreads();
 
@@ -407,31 +423,31 @@ __device__ __forceinline__ void VolumePhase(const ResidualArgs &a, const int e, 
 
   // The matching-layer source initialises the residual (src/ElementClass.cpp:3885-4117).
   if (OPEN && cmlHere) {
-    Contract<NT, SLOT, K, M, kLegT, 2, 5, M, M, M, M, K, false>(bufC, tJ);
+    ContractL<NT, SLOT, K, M, kLegT, 2, 5, M, M, M, M, K, false, T, Dense<M, M, M>, typename P::VD>(bufC, tJ);
     __syncthreads();
-    Contract<NT, SLOT, K, M, kLegT, 1, 5, M, M, K, M, K, false>(tJ, tK);
+    ContractL<NT, SLOT, K, M, kLegT, 1, 5, M, M, K, M, K, false, T, typename P::VD, typename P::VE>(tJ, tK);
     __syncthreads();
-    Contract<NT, SLOT, K, M, kLegT, 0, 5, M, K, K, M, K, true>(tK, s_R);
+    ContractL<NT, SLOT, K, M, kLegT, 0, 5, M, K, K, M, K, true, T, typename P::VE, Dense<K, K, K>>(tK, s_R);
     __syncthreads();
   }
   // TPAVR for the three flux directions (src/ElementClass.cpp:4425-4443).
-  Contract<NT, SLOT, K, M, kLegT, 2, 5, M, M, M, M, K, false>(dX, tJ);
+  ContractL<NT, SLOT, K, M, kLegT, 2, 5, M, M, M, M, K, false, T, Dense<M, M, M>, typename P::VD>(dX, tJ);
   __syncthreads();
-  Contract<NT, SLOT, K, M, kLegT, 1, 5, M, M, K, M, K, false>(tJ, tK);
+  ContractL<NT, SLOT, K, M, kLegT, 1, 5, M, M, K, M, K, false, T, typename P::VD, typename P::VE>(tJ, tK);
   __syncthreads();
-  Contract<NT, SLOT, K, M, kDLegT, 0, 5, M, K, K, M, K, true>(tK, s_R);
+  ContractL<NT, SLOT, K, M, kDLegT, 0, 5, M, K, K, M, K, true, T, typename P::VE, Dense<K, K, K>>(tK, s_R);
   __syncthreads();
-  Contract<NT, SLOT, K, M, kLegT, 2, 5, M, M, M, M, K, false>(dY, tJ);
+  ContractL<NT, SLOT, K, M, kLegT, 2, 5, M, M, M, M, K, false, T, Dense<M, M, M>, typename P::VD>(dY, tJ);
   __syncthreads();
-  Contract<NT, SLOT, K, M, kDLegT, 1, 5, M, M, K, M, K, false>(tJ, tK);
+  ContractL<NT, SLOT, K, M, kDLegT, 1, 5, M, M, K, M, K, false, T, typename P::VD, typename P::VE>(tJ, tK);
   __syncthreads();
-  Contract<NT, SLOT, K, M, kLegT, 0, 5, M, K, K, M, K, true>(tK, s_R);
+  ContractL<NT, SLOT, K, M, kLegT, 0, 5, M, K, K, M, K, true, T, typename P::VE, Dense<K, K, K>>(tK, s_R);
   __syncthreads();
-  Contract<NT, SLOT, K, M, kDLegT, 2, 5, M, M, M, M, K, false>(dZ, tJ);
+  ContractL<NT, SLOT, K, M, kDLegT, 2, 5, M, M, M, M, K, false, T, Dense<M, M, M>, typename P::VD>(dZ, tJ);
   __syncthreads();
-  Contract<NT, SLOT, K, M, kLegT, 1, 5, M, M, K, M, K, false>(tJ, tK);
+  ContractL<NT, SLOT, K, M, kLegT, 1, 5, M, M, K, M, K, false, T, typename P::VD, typename P::VE>(tJ, tK);
   __syncthreads();
-  Contract<NT, SLOT, K, M, kLegT, 0, 5, M, K, K, M, K, true>(tK, s_R);
+  ContractL<NT, SLOT, K, M, kLegT, 0, 5, M, K, K, M, K, true, T, typename P::VE, Dense<K, K, K>>(tK, s_R);
   __syncthreads();
   // Sponge-layer damping J w sum_d sigma_d (U - U_damp) (src/ElementClass.cpp:4450-4489).
   if (OPEN && sp >= 0) {
@@ -450,11 +466,11 @@ __device__ __forceinline__ void VolumePhase(const ResidualArgs &a, const int e, 
       dX[4 * MD + l] = sigma * (rE - LdT<T>(ds + 4 * MD + l));
     }
     __syncthreads();
-    Contract<NT, SLOT, K, M, kLegT, 2, 5, M, M, M, M, K, false>(dX, tJ);
+    ContractL<NT, SLOT, K, M, kLegT, 2, 5, M, M, M, M, K, false, T, Dense<M, M, M>, typename P::VD>(dX, tJ);
     __syncthreads();
-    Contract<NT, SLOT, K, M, kLegT, 1, 5, M, M, K, M, K, false>(tJ, tK);
+    ContractL<NT, SLOT, K, M, kLegT, 1, 5, M, M, K, M, K, false, T, typename P::VD, typename P::VE>(tJ, tK);
     __syncthreads();
-    Contract<NT, SLOT, K, M, kLegT, 0, 5, M, K, K, M, K, true>(tK, s_R);
+    ContractL<NT, SLOT, K, M, kLegT, 0, 5, M, K, K, M, K, true, T, typename P::VE, Dense<K, K, K>>(tK, s_R);
     __syncthreads();
   }
 }
@@ -760,23 +776,25 @@ __device__ __forceinline__ void FacePhase(const ResidualArgs &a, const int e, T 
 // that shares their loads: p = beta p + z before the forward k transform (from
 // the second iteration on), and the partial sum of p . Ap after the backward
 // i transform. Lines, summation order and coefficients are those of
-// Contract<..., AX = 2, ...> and Contract<..., AX = 0, ...>.
-template <int NT, int SLOT, int K, int M, typename T>
+// ContractL<..., AX = 2, ...> and ContractL<..., AX = 0, ...>; LP is the layout
+// of the DOF vectors, LO / LI of the transformed arrays.
+template <int NT, int SLOT, int K, int M, typename T, typename LP, typename LO>
 __device__ __forceinline__ void KForwardUpdate(T *__restrict__ p, const T *__restrict__ z,
                                                const T beta, const bool update,
                                                T *__restrict__ out) {
   constexpr int K2 = K * K, NLINES = 5 * K2;
   for (int line = threadIdx.x; line < NLINES; line += NT) {
     const int v = line / K2, r = line - v * K2;
-    const int ib = v * K2 * K + r, ob = v * K2 * M + r;
+    const int j = r / K, i = r - j * K;
+    const int ib = v * LP::SV + j * LP::S1 + i, ob = v * LO::SV + j * LO::S1 + i;
     T xv[K];
 #pragma unroll
-    for (int c = 0; c < K; ++c) xv[c] = p[ib + c * K2];
+    for (int c = 0; c < K; ++c) xv[c] = p[ib + c * LP::S2];
     if (update) {
 #pragma unroll
       for (int c = 0; c < K; ++c) {
-        xv[c] = Fma(beta, xv[c], z[ib + c * K2]);
-        p[ib + c * K2] = xv[c];
+        xv[c] = Fma(beta, xv[c], z[ib + c * LP::S2]);
+        p[ib + c * LP::S2] = xv[c];
       }
     }
 #pragma unroll
@@ -784,27 +802,31 @@ __device__ __forceinline__ void KForwardUpdate(T *__restrict__ p, const T *__res
       T acc = T(0);
 #pragma unroll
       for (int c = 0; c < K; ++c) acc = fma(Coef<SLOT, K, M, kLeg, T>(c, o), xv[c], acc);
-      out[ob + o * K2] = acc;
+      out[ob + o * LO::S2] = acc;
     }
   }
 }
 
-template <int NT, int SLOT, int K, int M, typename T>
+template <int NT, int SLOT, int K, int M, typename T, typename LI, typename LP>
 __device__ __forceinline__ T IBackwardDot(const T *__restrict__ in, const T *__restrict__ p,
                                           T *__restrict__ Ap) {
-  constexpr int NLINES = 5 * K * K;
+  constexpr int K2 = K * K, NLINES = 5 * K2;
   T part = T(0);
   for (int line = threadIdx.x; line < NLINES; line += NT) {
+    const int v = line / K2, r = line - v * K2;
+    const int kk = r / K, kj = r - kk * K;
+    const int ib = v * LI::SV + kk * LI::S2 + kj * LI::S1;
+    const int ob = v * LP::SV + kk * LP::S2 + kj * LP::S1;
     T xv[M];
 #pragma unroll
-    for (int c = 0; c < M; ++c) xv[c] = in[line * M + c];
+    for (int c = 0; c < M; ++c) xv[c] = in[ib + c];
 #pragma unroll
     for (int o = 0; o < K; ++o) {
       T acc = T(0);
 #pragma unroll
       for (int c = 0; c < M; ++c) acc = fma(Coef<SLOT, K, M, kLegT, T>(c, o), xv[c], acc);
-      Ap[line * K + o] = acc;
-      part = Fma(p[line * K + o], acc, part);
+      Ap[ob + o] = acc;
+      part = Fma(p[ob + o], acc, part);
     }
   }
   return part;
@@ -833,7 +855,7 @@ __device__ __forceinline__ void PointOperator(const T *s_cgp, const T *s_jw, con
 // (src/CG_MassMatrix.cpp:250-504): flexible PCG with the element-centre
 // dV/dU * 8/vol preconditioner, stop at ||r||_inf < 1e-10 ||r0||_inf, at most
 // 100 iterations (the cap raises a status flag instead of aborting).
-// r is s_R (overwritten); the solution is returned in x.
+// r is s_R (dense, overwritten); the solution is written to dst (global, dense).
 //
 // One iteration is seven barrier-separated steps: k, j transforms to the
 // integration points (the first with the search-direction update), the
@@ -841,35 +863,45 @@ __device__ __forceinline__ void PointOperator(const T *s_cgp, const T *s_jw, con
 // w J dU/dV kept in registers where the register budget allows),
 // k, j, i transforms back (the last with the partial sums of p . Ap), and the
 // update of x, r and z with the three sums that close the iteration. The two
-// reductions use one barrier each and alternate their scratch areas.
+// reductions use one barrier each and alternate their scratch areas. The CG
+// arrays use the padded layouts of CgLayout.
 // ---------------------------------------------------------------------------
 template <int NT, int K, int M, typename T>
 __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, const T *s_sol,
                                           T *s_R, const T *s_cgp, const T *s_jw,
-                                          T *work, T *s_red, T *&xOut) {
+                                          T *work, T *s_red, double *dst) {
   constexpr int SLOT = Slot<K, M>::value;
   using P = Plan<K, M, T>;
-  constexpr int KD = P::KD, MD = P::MD, M2 = M * M;
+  using L = typename P::CL;
+  using LP = typename L::P;
+  using LB = typename L::B;
+  using LC = typename L::C;
+  constexpr int KD = P::KD, MD = P::MD, M2 = M * M, K2 = K * K;
   constexpr int PP = (MD + NT - 1) / NT;   // integration points per thread
   // Point operators held in registers: one point per thread, or two when the
   // launch bounds leave at least 168 registers per thread.
   constexpr bool kRegD = PP == 1 || (PP == 2 && 65536 / (NT * P::MIN_BLOCKS) >= 168);
-  T *z = work, *p = z + 5 * KD, *Ap = p + 5 * KD, *x = Ap + 5 * KD;
-  T *pInt = x + 5 * KD, *tK = pInt + 5 * MD, *tJ = tK + P::TK;
+  T *z = work, *p = z + 5 * LP::SV, *Ap = p + 5 * LP::SV, *x = Ap + 5 * LP::SV;
+  T *pInt = x + 5 * LP::SV, *tK = pInt + 5 * LC::SV, *tJ = tK + P::CG_TK;
   T *dvdu = s_red + 32;  // 15 preconditioner entries
   T *redA = s_red, *redB = s_red + 32;
   T *r = s_R;
-  xOut = x;
   const T volElem = a.elem_scalars[(size_t)e * 15 + 5];
   const T JacInv = T(8.0) / volElem;
+  // Padded offset of DOF l = (k K + j) K + i.
+  auto off = [](const int l) { return (l / K2) * LP::S2 + ((l / K) % K) * LP::S1 + l % K; };
 
   T m = T(0.0);
-  for (int i = threadIdx.x; i < 5 * KD; i += NT) {
-    m = Fmax(m, Fabs(r[i]));
-    x[i] = T(0.0);
+  for (int i = threadIdx.x; i < 5 * KD; i += NT) m = Fmax(m, Fabs(r[i]));
+  for (int l = threadIdx.x; l < KD; l += NT) {
+#pragma unroll
+    for (int q = 0; q < 5; ++q) x[q * LP::SV + off(l)] = T(0.0);
   }
   const T rInitMax = BlockMax<NT>(m, s_red);
-  if (!(rInitMax * JacInv > T(1.e-10))) return;
+  if (!(rInitMax * JacInv > T(1.e-10))) {
+    for (int i = threadIdx.x; i < 5 * KD; i += NT) dst[i] = 0.0;
+    return;
+  }
 
   // Entropy variables at the element centre and dV/dU there (src/CG_MassMatrix.cpp:313-361).
   if (threadIdx.x < 5) {
@@ -923,20 +955,23 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
       if constexpr (kRegD) PointOperator<MD>(s_cgp, s_jw, l, dd[n]);
     }
   }
+  T part = T(0.0);
   for (int l = threadIdx.x; l < KD; l += NT) {
     const T r0 = r[l], r1 = r[KD + l], r2 = r[2 * KD + l], r3 = r[3 * KD + l],
             r4 = r[4 * KD + l];
-    z[l] = D[0] * r0 + D[1] * r1 + D[2] * r2 + D[3] * r3 + D[4] * r4;
-    z[KD + l] = D[1] * r0 + D[5] * r1 + D[6] * r2 + D[7] * r3 + D[8] * r4;
-    z[2 * KD + l] = D[2] * r0 + D[6] * r1 + D[9] * r2 + D[10] * r3 + D[11] * r4;
-    z[3 * KD + l] = D[3] * r0 + D[7] * r1 + D[10] * r2 + D[12] * r3 + D[13] * r4;
-    z[4 * KD + l] = D[4] * r0 + D[8] * r1 + D[11] * r2 + D[13] * r3 + D[14] * r4;
-  }
-  __syncthreads();
-  T part = T(0.0);
-  for (int i = threadIdx.x; i < 5 * KD; i += NT) {
-    p[i] = z[i];
-    part = Fma(r[i], z[i], part);
+    const T zz[5] = {D[0] * r0 + D[1] * r1 + D[2] * r2 + D[3] * r3 + D[4] * r4,
+                     D[1] * r0 + D[5] * r1 + D[6] * r2 + D[7] * r3 + D[8] * r4,
+                     D[2] * r0 + D[6] * r1 + D[9] * r2 + D[10] * r3 + D[11] * r4,
+                     D[3] * r0 + D[7] * r1 + D[10] * r2 + D[12] * r3 + D[13] * r4,
+                     D[4] * r0 + D[8] * r1 + D[11] * r2 + D[13] * r3 + D[14] * r4};
+    const T rr[5] = {r0, r1, r2, r3, r4};
+    const int o = off(l);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      z[q * LP::SV + o] = zz[q];
+      p[q * LP::SV + o] = zz[q];
+      part = Fma(rr[q], zz[q], part);
+    }
   }
   T dotrz = BlockSum<NT>(part, s_red);
 
@@ -948,21 +983,22 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
       break;
     }
     // Ap = Leg^T3 (w J dU/dV (Leg3 p)) (src/CG_MassMatrix.cpp:408-443).
-    KForwardUpdate<NT, SLOT, K, M, T>(p, z, beta, iter > 0, tK);
+    KForwardUpdate<NT, SLOT, K, M, T, LP, typename L::A>(p, z, beta, iter > 0, tK);
     __syncthreads();
-    Contract<NT, SLOT, K, M, kLeg, 1, 5, K, K, M, K, M, false>(tK, tJ);
+    ContractL<NT, SLOT, K, M, kLeg, 1, 5, K, K, M, K, M, false, T, typename L::A, LB>(tK, tJ);
     __syncthreads();
 #pragma unroll
     for (int n = 0; n < PP; ++n) {
       const int l = threadIdx.x + n * NT;
       if (l < MD) {
-        const T *src = tJ + (l / M) * K;   // tJ[v][mk][mj][0..K-1] of this point's line
+        const int mk = l / M2, mj = (l / M) % M, mi = l % M;
+        const T *src = tJ + mk * LB::S2 + mj * LB::S1;  // tJ[v][mk][mj][0..K-1]
         T q[5];
 #pragma unroll
         for (int vv = 0; vv < 5; ++vv) {
           T acc = T(0);
 #pragma unroll
-          for (int c = 0; c < K; ++c) acc = fma(lc[n][c], src[vv * M2 * K + c], acc);
+          for (int c = 0; c < K; ++c) acc = fma(lc[n][c], src[vv * LB::SV + c], acc);
           q[vv] = acc;
         }
         T dl[16];
@@ -974,28 +1010,33 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
         }
         const T iw = dl[15];
         const T p0 = iw * q[0], p1 = iw * q[1], p2 = iw * q[2], p3 = iw * q[3], p4 = iw * q[4];
-        pInt[l] = dl[0] * p0 + dl[1] * p1 + dl[2] * p2 + dl[3] * p3 + dl[4] * p4;
-        pInt[MD + l] = dl[1] * p0 + dl[5] * p1 + dl[6] * p2 + dl[7] * p3 + dl[8] * p4;
-        pInt[2 * MD + l] = dl[2] * p0 + dl[6] * p1 + dl[9] * p2 + dl[10] * p3 + dl[11] * p4;
-        pInt[3 * MD + l] = dl[3] * p0 + dl[7] * p1 + dl[10] * p2 + dl[12] * p3 + dl[13] * p4;
-        pInt[4 * MD + l] = dl[4] * p0 + dl[8] * p1 + dl[11] * p2 + dl[13] * p3 + dl[14] * p4;
+        T *dstp = pInt + mk * LC::S2 + mj * LC::S1 + mi;
+        dstp[0] = dl[0] * p0 + dl[1] * p1 + dl[2] * p2 + dl[3] * p3 + dl[4] * p4;
+        dstp[LC::SV] = dl[1] * p0 + dl[5] * p1 + dl[6] * p2 + dl[7] * p3 + dl[8] * p4;
+        dstp[2 * LC::SV] = dl[2] * p0 + dl[6] * p1 + dl[9] * p2 + dl[10] * p3 + dl[11] * p4;
+        dstp[3 * LC::SV] = dl[3] * p0 + dl[7] * p1 + dl[10] * p2 + dl[12] * p3 + dl[13] * p4;
+        dstp[4 * LC::SV] = dl[4] * p0 + dl[8] * p1 + dl[11] * p2 + dl[13] * p3 + dl[14] * p4;
       }
     }
     __syncthreads();
-    Contract<NT, SLOT, K, M, kLegT, 2, 5, M, M, M, M, K, false>(pInt, tJ);
+    ContractL<NT, SLOT, K, M, kLegT, 2, 5, M, M, M, M, K, false, T, LC, typename L::D>(pInt, tJ);
     __syncthreads();
-    Contract<NT, SLOT, K, M, kLegT, 1, 5, M, M, K, M, K, false>(tJ, tK);
+    ContractL<NT, SLOT, K, M, kLegT, 1, 5, M, M, K, M, K, false, T, typename L::D,
+              typename L::E>(tJ, tK);
     __syncthreads();
-    const T alpha = dotrz / BlockSum1<NT>(IBackwardDot<NT, SLOT, K, M, T>(tK, p, Ap), redA);
+    const T alpha =
+        dotrz / BlockSum1<NT>(IBackwardDot<NT, SLOT, K, M, T, typename L::E, LP>(tK, p, Ap), redA);
     // Each thread owns whole DOFs: update x and r, precondition, and form the
     // partial sums of the three reductions that close the iteration.
     T zAp = T(0.0), rzNew = T(0.0), rMax = T(0.0);
     for (int l = threadIdx.x; l < KD; l += NT) {
-      T rr[5];
+      const int o = off(l);
+      T rr[5], ap[5];
 #pragma unroll
       for (int q = 0; q < 5; ++q) {
-        x[q * KD + l] = Fma(alpha, p[q * KD + l], x[q * KD + l]);
-        rr[q] = Fma(-alpha, Ap[q * KD + l], r[q * KD + l]);
+        ap[q] = Ap[q * LP::SV + o];
+        x[q * LP::SV + o] = Fma(alpha, p[q * LP::SV + o], x[q * LP::SV + o]);
+        rr[q] = Fma(-alpha, ap[q], r[q * KD + l]);
         r[q * KD + l] = rr[q];
         rMax = Fmax(rMax, Fabs(rr[q]));
       }
@@ -1007,8 +1048,8 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
           D[4] * rr[0] + D[8] * rr[1] + D[11] * rr[2] + D[13] * rr[3] + D[14] * rr[4]};
 #pragma unroll
       for (int q = 0; q < 5; ++q) {
-        z[q * KD + l] = zz[q];
-        zAp = Fma(zz[q], Ap[q * KD + l], zAp);
+        z[q * LP::SV + o] = zz[q];
+        zAp = Fma(zz[q], ap[q], zAp);
         rzNew = Fma(rr[q], zz[q], rzNew);
       }
     }
@@ -1020,6 +1061,12 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
   if (threadIdx.x == 0 && a.cg_stats) {
     atomicAdd(a.cg_stats, (unsigned long long)(iter + 1));
     atomicAdd(a.cg_stats + 1, 1ull);
+  }
+  // Every thread reads back the entries it wrote itself in the last update.
+  for (int l = threadIdx.x; l < KD; l += NT) {
+    const int o = off(l);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) dst[q * KD + l] = double(x[q * LP::SV + o]);
   }
 }
 
@@ -1057,11 +1104,7 @@ __global__ void __launch_bounds__(NT, (Plan<K, M, T, OPEN>::MIN_BLOCKS)) Residua
     for (int i = threadIdx.x; i < 5 * KD; i += NT) dst[i] = double(s_R[i]);
   }
   __syncthreads();
-  T *x;
-  MassSolve<NT, K, M>(a, e, s_sol, s_R, s_cgp, s_jw, work, s_red, x);
-  __syncthreads();
-  double *dst = a.res + (size_t)e * 5 * KD;
-  for (int i = threadIdx.x; i < 5 * KD; i += NT) dst[i] = double(x[i]);
+  MassSolve<NT, K, M>(a, e, s_sol, s_R, s_cgp, s_jw, work, s_red, a.res + (size_t)e * 5 * KD);
 }
 
 // Shared memory (in T) and launch shape of the face-flux kernel.

@@ -104,20 +104,25 @@ __device__ __forceinline__ T CenterBasis(const int i) {
   else return c_ops[SLOT].center[i];
 }
 
-// Apply a 1-D operator along axis AX of in[NV][D2][D1][D0] (D_AX == NIN) and
-// write (ACC: add) out[NV][D2'][D1'][D0'] where D_AX' == NOUT.
+// Strides (in elements) of an array [NV][D2][D1][D0] with unit stride along D0:
+// S1 along D1, S2 along D2, SV between variables. Padded strides keep the
+// lines that one warp touches on distinct shared-memory banks.
+template <int S1_, int S2_, int SV_> struct Lay {
+  static constexpr int S1 = S1_, S2 = S2_, SV = SV_;
+};
+template <int D0, int D1, int D2> using Dense = Lay<D0, D0 * D1, D0 * D1 * D2>;
+
+// Apply a 1-D operator along axis AX of in[NV][D2][D1][D0] (layout LI, D_AX ==
+// NIN) and write (ACC: add) out[NV][D2'][D1'][D0'] (layout LO) where D_AX' == NOUT.
 template <int NT, int SLOT, int K, int M, int OP, int AX, int NV, int D0, int D1, int D2,
-          int NIN, int NOUT, bool ACC, typename T = double>
-__device__ __forceinline__ void Contract(const T *__restrict__ in, T *__restrict__ out) {
-  constexpr int O0 = AX == 0 ? NOUT : D0;
-  constexpr int O1 = AX == 1 ? NOUT : D1;
-  constexpr int O2 = AX == 2 ? NOUT : D2;
+          int NIN, int NOUT, bool ACC, typename T, typename LI, typename LO>
+__device__ __forceinline__ void ContractL(const T *__restrict__ in, T *__restrict__ out) {
   // Non-contracted extents, the faster one first.
   constexpr int A = AX == 0 ? D1 : D0;
   constexpr int B = AX == 2 ? D1 : D2;
   constexpr int NLINES = NV * A * B;
-  constexpr int IS = AX == 0 ? 1 : (AX == 1 ? D0 : D0 * D1);
-  constexpr int OS = AX == 0 ? 1 : (AX == 1 ? O0 : O0 * O1);
+  constexpr int IS = AX == 0 ? 1 : (AX == 1 ? LI::S1 : LI::S2);
+  constexpr int OS = AX == 0 ? 1 : (AX == 1 ? LO::S1 : LO::S2);
   for (int line = threadIdx.x; line < NLINES; line += NT) {
     const int v = line / (A * B);
     const int r = line - v * (A * B);
@@ -125,14 +130,14 @@ __device__ __forceinline__ void Contract(const T *__restrict__ in, T *__restrict
     const int a = r - b * A;
     int ib, ob;
     if (AX == 0) {
-      ib = ((v * D2 + b) * D1 + a) * D0;
-      ob = ((v * O2 + b) * O1 + a) * O0;
+      ib = v * LI::SV + b * LI::S2 + a * LI::S1;
+      ob = v * LO::SV + b * LO::S2 + a * LO::S1;
     } else if (AX == 1) {
-      ib = (v * D2 + b) * D1 * D0 + a;
-      ob = (v * O2 + b) * O1 * O0 + a;
+      ib = v * LI::SV + b * LI::S2 + a;
+      ob = v * LO::SV + b * LO::S2 + a;
     } else {
-      ib = v * D2 * D1 * D0 + b * D0 + a;
-      ob = v * O2 * O1 * O0 + b * O0 + a;
+      ib = v * LI::SV + b * LI::S1 + a;
+      ob = v * LO::SV + b * LO::S1 + a;
     }
     T x[NIN];
 #pragma unroll
@@ -149,5 +154,63 @@ __device__ __forceinline__ void Contract(const T *__restrict__ in, T *__restrict
     }
   }
 }
+
+// Dense layouts on both sides.
+template <int NT, int SLOT, int K, int M, int OP, int AX, int NV, int D0, int D1, int D2,
+          int NIN, int NOUT, bool ACC, typename T = double>
+__device__ __forceinline__ void Contract(const T *__restrict__ in, T *__restrict__ out) {
+  constexpr int O0 = AX == 0 ? NOUT : D0;
+  constexpr int O1 = AX == 1 ? NOUT : D1;
+  constexpr int O2 = AX == 2 ? NOUT : D2;
+  ContractL<NT, SLOT, K, M, OP, AX, NV, D0, D1, D2, NIN, NOUT, ACC, T, Dense<D0, D1, D2>,
+            Dense<O0, O1, O2>>(in, out);
+}
+
+// Padded shared-memory layouts of the mass-matrix CG arrays, chosen per (K, M)
+// and element size by minimising the shared-memory wavefronts of one iteration
+// in a bank model (16 eight-byte or 32 four-byte banks; the warps' lines as the
+// CG steps assign them at the launch's threads per CTA):
+//   P  DOF vectors z, p, Ap, x      [5][K][K][K]
+//   A  k-transformed                [5][M][K][K]   (forward)
+//   B  k,j-transformed              [5][M][M][K]   (forward)
+//   C  integration points           [5][M][M][M]
+//   D  k-transformed back           [5][K][M][M]
+//   E  k,j-transformed back         [5][K][K][M]
+template <int K, int M, int ES> struct CgLayout {
+  using P = Dense<K, K, K>;
+  using A = Dense<K, K, M>;
+  using B = Dense<K, M, M>;
+  using C = Dense<M, M, M>;
+  using D = Dense<M, M, K>;
+  using E = Dense<M, K, K>;
+};
+#define VCPG_CG_LAYOUT(K_, M_, ES_, P_, A_, B_, C_, D_, E_)                                \
+  template <> struct CgLayout<K_, M_, ES_> {                                              \
+    using P = Lay<P_>; using A = Lay<A_>; using B = Lay<B_>;                              \
+    using C = Lay<C_>; using D = Lay<D_>; using E = Lay<E_>;                              \
+  };
+#define VCPG_L(a, b, c) a, b, c
+VCPG_CG_LAYOUT(2, 3, 8, VCPG_L(2, 5, 10), VCPG_L(2, 5, 18), VCPG_L(3, 9, 27), VCPG_L(3, 11, 41),
+               VCPG_L(3, 13, 26), VCPG_L(3, 8, 19))
+VCPG_CG_LAYOUT(3, 4, 8, VCPG_L(3, 9, 27), VCPG_L(3, 10, 41), VCPG_L(4, 19, 76), VCPG_L(4, 16, 64),
+               VCPG_L(4, 18, 54), VCPG_L(7, 21, 63))
+VCPG_CG_LAYOUT(4, 5, 8, VCPG_L(4, 17, 68), VCPG_L(4, 18, 90), VCPG_L(5, 28, 140),
+               VCPG_L(5, 26, 137), VCPG_L(5, 26, 105), VCPG_L(8, 37, 148))
+VCPG_CG_LAYOUT(5, 7, 8, VCPG_L(5, 25, 125), VCPG_L(6, 37, 259), VCPG_L(5, 37, 259),
+               VCPG_L(7, 49, 343), VCPG_L(7, 55, 275), VCPG_L(10, 55, 275))
+VCPG_CG_LAYOUT(6, 8, 8, VCPG_L(6, 36, 217), VCPG_L(6, 38, 308), VCPG_L(6, 54, 432),
+               VCPG_L(8, 64, 512), VCPG_L(8, 72, 432), VCPG_L(9, 56, 336))
+VCPG_CG_LAYOUT(2, 3, 4, VCPG_L(2, 5, 12), VCPG_L(2, 6, 18), VCPG_L(2, 6, 18), VCPG_L(3, 11, 41),
+               VCPG_L(3, 17, 41), VCPG_L(4, 15, 35))
+VCPG_CG_LAYOUT(3, 4, 4, VCPG_L(3, 11, 41), VCPG_L(3, 9, 43), VCPG_L(6, 29, 116),
+               VCPG_L(4, 16, 64), VCPG_L(4, 20, 60), VCPG_L(5, 20, 60))
+VCPG_CG_LAYOUT(4, 5, 4, VCPG_L(4, 16, 65), VCPG_L(4, 20, 100), VCPG_L(4, 20, 100),
+               VCPG_L(5, 25, 125), VCPG_L(6, 37, 148), VCPG_L(8, 37, 148))
+VCPG_CG_LAYOUT(5, 7, 4, VCPG_L(5, 25, 125), VCPG_L(5, 26, 185), VCPG_L(5, 37, 259),
+               VCPG_L(7, 49, 343), VCPG_L(7, 53, 273), VCPG_L(9, 45, 225))
+VCPG_CG_LAYOUT(6, 8, 4, VCPG_L(6, 36, 217), VCPG_L(6, 38, 304), VCPG_L(8, 70, 560),
+               VCPG_L(8, 64, 512), VCPG_L(8, 72, 432), VCPG_L(9, 56, 336))
+#undef VCPG_L
+#undef VCPG_CG_LAYOUT
 
 }  // namespace vcpg
