@@ -152,6 +152,17 @@ int vcpg_time_step(vcpg_handle *h, double *dt);
 int vcpg_step(vcpg_handle *h, int32_t scheme, int32_t n_steps, double fixed_dt,
               double *dt_history);
 
+/* One synchronization time step (SolverClass::ExecuteTimeSynchronizationStep,
+ * src/SolverClass.cpp:2177-2422): SSP-RK3 steps with the CFL step of the
+ * current state until the non-dimensional time dt_sync (the reference's
+ * "Synchronization time step" times u_ref) is reached; the step that would pass
+ * 0.99 dt_sync is shortened to end on dt_sync exactly. Reads one time step back
+ * to the host per RK step. n_steps (optional) receives the number of RK steps;
+ * monitoring (optional) the 8 monitoring values of the final state, at the cost
+ * of one more residual. More than max_steps RK steps is an error. */
+int vcpg_synchronization_step(vcpg_handle *h, double dt_sync, int32_t max_steps,
+                              int32_t *n_steps, double *monitoring);
+
 /* Synchronises the handle's stream and reports the first device-side error
  * (CG cap, negative a^2) recorded since the last call. */
 int vcpg_sync(vcpg_handle *h);

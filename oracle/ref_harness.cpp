@@ -11,6 +11,7 @@
 //   vcp3d_ref <param.cfg> residual <out.bin> [--state <in.bin>]
 //   vcp3d_ref <param.cfg> run      <out.bin> --scheme ssprk3|lsrk4 --steps N
 //                                  [--dt DT] [--state <in.bin>] [--time]
+//   vcp3d_ref <param.cfg> sync     <out.bin> --steps N
 //
 // The residual command replicates the loop structure of SolverClass::Residual
 // (src/SolverClass.cpp:3381-3795) so that the residual can be captured both
@@ -20,7 +21,9 @@
 // without the synchronisation-time clip, and calls the reference's own
 // SolverClass::Residual for every stage. The low-storage RK4 scheme has no
 // counterpart in the reference; it drives the same Residual with the
-// Carpenter-Kennedy (1994) five-stage 2N-storage coefficients.
+// Carpenter-Kennedy (1994) five-stage 2N-storage coefficients. The sync command
+// calls the reference's own ExecuteTimeSynchronizationStep N times after the
+// initial residual, as the reference main program does.
 
 #include <fstream>
 #include <iostream>
@@ -365,7 +368,7 @@ void ResidualWithCapture(SolverClass &s, Writer &w) {
 
 int main(int argc, char **argv) {
   if (argc < 4) {
-    std::fprintf(stderr, "usage: %s <param.cfg> dump|residual|run <out.bin> [options]\n", argv[0]);
+    std::fprintf(stderr, "usage: %s <param.cfg> dump|residual|run|sync <out.bin> [options]\n", argv[0]);
     return 2;
   }
   std::string cfg = argv[1], cmd = argv[2], out = argv[3];
@@ -477,6 +480,21 @@ int main(int argc, char **argv) {
     w.rec("res", {nE, 5, nDOFsPad}, Gather(solver, &ElementClass::mRes, 5, nDOFsPad).data());
     w.rec("dtHist", {(int64_t)dtHist.size()}, dtHist.data());
     w.rec("monitor", {8}, mon);
+    w.rec("seconds", {1}, &secs);
+  } else if (cmd == "sync") {
+    // The reference main program's loop (src/VCP3D_CurviLinear.cpp:88-116):
+    // the residual of the initial state, then --steps calls of the reference's
+    // own ExecuteTimeSynchronizationStep.
+    su2double mon[8];
+    DoResidual(solver, mon, true);
+    auto t0 = std::chrono::steady_clock::now();
+    for (int step = 0; step < steps; ++step) solver.ExecuteTimeSynchronizationStep(mon);
+    auto t1 = std::chrono::steady_clock::now();
+    const double secs = std::chrono::duration<double>(t1 - t0).count();
+    const double nrk = (double)solver.mCurrentTimeStep;
+    w.rec("sol", {nE, 5, nDOFsPad}, Gather(solver, &ElementClass::mSol, 5, nDOFsPad).data());
+    w.rec("monitor", {8}, mon);
+    w.rec("rkSteps", {1}, &nrk);
     w.rec("seconds", {1}, &secs);
   } else {
     std::fprintf(stderr, "unknown command %s\n", cmd.c_str());

@@ -30,6 +30,21 @@ def open_golden_files():
     return sorted(glob.glob(os.path.join(GOLDEN, "open_*.npz")))
 
 
+def sync_golden_files():
+    """Fixtures of synchronisation steps run from a parameter file."""
+    return sorted(glob.glob(os.path.join(GOLDEN, "sync_*.npz")))
+
+
+def write_sync_case(g, directory):
+    """The files of a sync fixture: grid, restart and averaged solution from the
+    generator, the parameter file from the fixture. Returns the file's path."""
+    from vcp3d_open_b200 import cases
+    cfg = cases.write_case(cases.build_case(g["spec"]), directory)
+    with open(cfg, "w") as f:
+        f.write(str(g["param_text"]))
+    return cfg
+
+
 def load_golden(path):
     g = dict(np.load(path))
     g["spec"] = spec_from_json(str(g["spec_json"]))

@@ -16,6 +16,13 @@ characteristic boundaries, sponge and matching layers) holds, for one case:
   ls_sol, ls_dt   state and time steps after N_STEPS low-storage RK4 steps
   metric_sums     per-array checksums of the reference's metric terms
   vol_metric_e0, face_metric_e0  metric terms of element 0 (unpadded)
+
+Each sync_<name>.npz holds a case run through the reference main program's
+loop of synchronisation steps from its parameter file (param_text, with the
+grid and restart / averaged-solution files that write_case generates from
+spec_json): sol0 (initial modal state after the fluctuations), refcond,
+sync_sol (state after n_sync synchronisation steps), monitor and rk_steps
+(Runge-Kutta steps taken).
 """
 from __future__ import annotations
 
@@ -87,6 +94,63 @@ OPEN_SPECS = {
 }
 
 
+# Synchronisation steps through the reference main program's loop
+# (ExecuteTimeSynchronizationStep): (spec, parameter-file overrides, steps).
+# The vortex restarts from the generated restart file; the open case starts
+# from the free stream that the prescribed boundary data define, with the
+# pressure-pulse fluctuation of the parameter file.
+SYNC_SPECS = {
+    "vortex_p3_4x4x4": (GOLDEN_SPECS["vortex_p3_4x4x4"],
+                        {"Synchronization time step": "1.0e-4"}, 3),
+    "pulse_p3_6x4x2_sponge_cml": (OPEN_SPECS["pulse_p3_6x4x2_sponge_cml"],
+                                  {"Synchronization time step": "5.0e-5", "Restart": "no",
+                                   "Fluctuations to add to initial solution": "Pressure pulse",
+                                   "Pressure pulse center": "5.2 0.8 1.0",
+                                   "Pressure pulse strength": "1.0e-2",
+                                   "Pressure pulse width": "0.5"}, 2),
+}
+
+
+def sync_param_text(spec: cases.CaseSpec, overrides: dict, steps: int) -> str:
+    """The generated parameter file with the synchronisation settings applied:
+    existing keyword lines are replaced, new ones appended before the subfaces."""
+    lines = cases.param_cfg_text(spec).split("\n")
+    ov = dict(overrides)
+    ov["Number of synchronization time steps"] = str(steps)
+    out = []
+    for ln in lines:
+        key = ln.split(":", 1)[0].strip() if ":" in ln else None
+        if key in ov:
+            out.append(f"{key}: {ov.pop(key)}")
+            continue
+        if ln.strip() == "Subface information":
+            out.extend(f"{k}: {v}" for k, v in ov.items())
+            ov = {}
+        out.append(ln)
+    return "\n".join(out)
+
+
+def make_sync(name: str, spec: cases.CaseSpec, overrides: dict, steps: int, out_dir: str) -> str:
+    K = spec.p + 1
+    KD = K ** 3
+    case = cases.build_case(spec)
+    text = sync_param_text(spec, overrides, steps)
+    with tempfile.TemporaryDirectory() as tmp:
+        cfg = cases.write_case(case, tmp)
+        with open(cfg, "w") as f:
+            f.write(text)
+        f_dump, f_sync = os.path.join(tmp, "dump.bin"), os.path.join(tmp, "sync.bin")
+        records.run_reference(cfg, "dump", f_dump)
+        records.run_reference(cfg, "sync", f_sync, "--steps", str(steps))
+        d, r = records.read_records(f_dump), records.read_records(f_sync)
+    path = os.path.join(out_dir, f"sync_{name}.npz")
+    np.savez_compressed(
+        path, spec_json=np.array(spec_to_json(spec)), param_text=np.array(text),
+        sol0=d["sol"][:, :, :KD], refcond=d["refcond"], sync_sol=r["sol"][:, :, :KD],
+        monitor=r["monitor"], rk_steps=r["rkSteps"], n_sync=np.array(steps))
+    return path
+
+
 def spec_to_json(spec: cases.CaseSpec) -> str:
     return json.dumps(dataclasses.asdict(spec))
 
@@ -141,6 +205,9 @@ def main():
     for name, spec in OPEN_SPECS.items():
         if not only or name in only:
             print(make(name, spec, HERE, prefix="open"))
+    for name, (spec, overrides, steps) in SYNC_SPECS.items():
+        if not only or f"sync_{name}" in only:
+            print(make_sync(name, spec, overrides, steps, HERE))
 
 
 if __name__ == "__main__":

@@ -25,7 +25,7 @@ EXPORTED = [
     "vcpg_create", "vcpg_destroy", "vcpg_last_error", "vcpg_setup_geometry",
     "vcpg_nodal_conservative_to_modal", "vcpg_set_state", "vcpg_get_state",
     "vcpg_get_residual", "vcpg_residual", "vcpg_get_raw_residual", "vcpg_time_step",
-    "vcpg_step", "vcpg_sync", "vcpg_stream", "vcpg_launch_count", "vcpg_stats",
+    "vcpg_step", "vcpg_synchronization_step", "vcpg_sync", "vcpg_stream", "vcpg_launch_count", "vcpg_stats",
     "vcpg_time_step_noalloc", "vcpg_set_open_boundary", "vcpg_ensemble_create",
     "vcpg_ensemble_destroy", "vcpg_ensemble_last_error", "vcpg_ensemble_footprint",
     "vcpg_ensemble_submit", "vcpg_ensemble_step", "vcpg_ensemble_poll", "vcpg_ensemble_retire",
@@ -105,6 +105,8 @@ def load() -> C.CDLL:
     lib.vcpg_residual.argtypes = [hp, dp, C.c_int32]
     lib.vcpg_time_step.argtypes = [hp, dp]
     lib.vcpg_step.argtypes = [hp, C.c_int32, C.c_int32, C.c_double, dp]
+    lib.vcpg_synchronization_step.argtypes = [hp, C.c_double, C.c_int32,
+                                              C.POINTER(C.c_int32), dp]
     lib.vcpg_sync.argtypes = [hp]
     lib.vcpg_stream.argtypes = [hp]
     lib.vcpg_stream.restype = C.c_void_p

@@ -137,9 +137,15 @@ class CaseSpec:
     # Sponge layers: elements per block face, damping constant and exponent; the
     # characteristic matching layer acts in every sponge element.
     sponge: Tuple[int, ...] = (0,) * 6
-    sponge_sigma: float = 20.0
-    sponge_alpha: float = 2.0
+    sponge_sigma: float = 20.0           # one value, or one per block face
+    sponge_alpha: float = 2.0            # one value, or one per block face
     cml: bool = False
+    # Prescribed data of the characteristic boundaries (dimensional), per block
+    # face: outflow pressure and inflow (rho, u, v, w); None: the free stream.
+    prescribed_p: Optional[Tuple[float, ...]] = None
+    prescribed_inflow: Optional[Tuple[Tuple[float, float, float, float], ...]] = None
+    # Sponge-layer target state (rho, u, v, w, p, dimensional); None: the free stream.
+    sponge_state: Optional[Tuple[float, ...]] = None
 
     def __post_init__(self):
         if self.p_grid is None:

@@ -435,6 +435,39 @@ int vcpg_step(vcpg_handle *h, int32_t scheme, int32_t n_steps, double fixed_dt,
   return rc;
 }
 
+int vcpg_synchronization_step(vcpg_handle *h, double dt_sync, int32_t max_steps,
+                              int32_t *n_steps, double *monitoring) {
+  if (!h || !(dt_sync > 0.0) || max_steps < 1) return VCPG_E_INVALID;
+  // SolverClass::ExecuteTimeSynchronizationStep (src/SolverClass.cpp:2177-2422):
+  // SSP-RK3 steps with the CFL step of the current state; the step that would
+  // reach 0.99 of the synchronisation time is shortened to end on it exactly.
+  double elapsed = 0.0;
+  int32_t taken = 0;
+  bool reached = false;
+  while (!reached) {
+    if (taken == max_steps) {
+      if (n_steps) *n_steps = taken;
+      return Fail(h, VCPG_E_INVALID, "synchronization time not reached within max_steps");
+    }
+    double dt = 0.0;
+    int rc = vcpg_time_step(h, &dt);
+    if (rc) return rc;
+    if (elapsed + dt >= 0.99 * dt_sync) {
+      dt = dt_sync - elapsed;
+      reached = true;
+    }
+    elapsed += dt;
+    rc = vcpg_step(h, VCPG_SSPRK3, 1, dt, nullptr);
+    if (rc) return rc;
+    ++taken;
+  }
+  if (n_steps) *n_steps = taken;
+  // The reference fills the monitoring data in the last stage's residual, the
+  // residual of the new state: evaluate it once more with monitoring.
+  if (monitoring) return vcpg_residual(h, monitoring, 0);
+  return VCPG_OK;
+}
+
 int vcpg_sync(vcpg_handle *h) {
   if (!h) return VCPG_E_INVALID;
   return CheckStatus(h);

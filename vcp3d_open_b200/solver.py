@@ -112,20 +112,23 @@ def open_boundary(case: CaseData) -> capi.OpenBoundary:
     codes = {"periodic": capi.BC_NONE, "outflow_nscbc": capi.BC_OUTFLOW_NSCBC,
              "inflow_static_nscbc": capi.BC_INFLOW_STATIC_NSCBC}
     p_out, rho_in, vel_in = prescribed_values(s, ref)
+    per_face = lambda v, f: v[f] if isinstance(v, (tuple, list)) else v
     for f, bc in enumerate(s.bc):
         ob.bc[f] = codes[bc]
-        ob.p_out[f] = p_out
-        ob.inflow[f][0], ob.inflow[f][1], ob.inflow[f][2], ob.inflow[f][3] = (rho_in, *vel_in)
+        ob.p_out[f] = s.prescribed_p[f] if s.prescribed_p else p_out
+        inflow = s.prescribed_inflow[f] if s.prescribed_inflow else (rho_in, *vel_in)
+        ob.inflow[f][0], ob.inflow[f][1], ob.inflow[f][2], ob.inflow[f][3] = inflow
         ob.sponge_elems[f] = s.sponge[f]
-        ob.sponge_sigma[f] = s.sponge_sigma
-        ob.sponge_alpha[f] = s.sponge_alpha
+        ob.sponge_sigma[f] = per_face(s.sponge_sigma, f)
+        ob.sponge_alpha[f] = per_face(s.sponge_alpha, f)
     ob.outlet_len, ob.outlet_sigma = s.outlet_len, s.outlet_sigma
     ob.outlet_beta_l, ob.outlet_beta_t = s.outlet_beta_l, s.outlet_beta_t
     ob.outlet_one_minus_beta = 1 if s.outlet_one_minus_beta else 0
     ob.inlet_len, ob.inlet_sigma = s.inlet_len, s.inlet_sigma
     ob.inlet_incoming = 1 if s.inlet_incoming else 0
     ob.cml = 1 if s.cml else 0
-    ob.sponge_state[:] = [rho_in, vel_in[0], vel_in[1], vel_in[2], p_out]
+    ob.sponge_state[:] = (list(s.sponge_state) if s.sponge_state else
+                          [rho_in, vel_in[0], vel_in[1], vel_in[2], p_out])
     return ob
 
 
@@ -221,6 +224,18 @@ class Solver:
         hist = np.zeros(max(n_steps, 1))
         self._check(self.lib.vcpg_step(self.h, scheme, n_steps, fixed_dt, capi.ptr(hist)), "step")
         return hist[:n_steps]
+
+    def synchronization_step(self, dt_sync: float, max_steps: int = 1000000,
+                             monitoring: bool = False):
+        """SolverClass::ExecuteTimeSynchronizationStep: SSP-RK3 CFL steps that end
+        exactly on the non-dimensional synchronisation time dt_sync. Returns the
+        number of RK steps and, with monitoring, the 8 monitoring values."""
+        n = C.c_int32(0)
+        mon = np.zeros(8)
+        self._check(self.lib.vcpg_synchronization_step(
+            self.h, float(dt_sync), int(max_steps), C.byref(n),
+            capi.ptr(mon) if monitoring else None), "synchronization step")
+        return (int(n.value), mon) if monitoring else int(n.value)
 
     def sync(self):
         self._check(self.lib.vcpg_sync(self.h), "sync")
