@@ -212,9 +212,13 @@ enum vcpg_bc {
   VCPG_BC_OUTFLOW_NSCBC = 1,        /* "BCOutflowNSCBC": prescribed static pressure,
                                        BCOutflowCharacteristicSubfaceClass
                                        (src/BoundaryState.cpp:1300-1568)              */
-  VCPG_BC_INFLOW_STATIC_NSCBC = 2   /* "BCInflowStaticNSCBC": prescribed density and
+  VCPG_BC_INFLOW_STATIC_NSCBC = 2,  /* "BCInflowStaticNSCBC": prescribed density and
                                        velocity, BCInflowStaticCharacteristicSubfaceClass
                                        (src/BoundaryState.cpp:1579-1847)              */
+  VCPG_BC_INFLOW_TOTAL_NSCBC = 3    /* "BCInflowTotalNSCBC": prescribed total pressure,
+                                       total temperature and velocity direction,
+                                       BCInflowTotalCharacteristicSubfaceClass
+                                       (src/BoundaryState.cpp:1848-2238)              */
 };
 
 /* The reference's "NSCBC tuning parameters", "Prescribed boundary data" and
@@ -240,6 +244,8 @@ typedef struct vcpg_open_boundary {
   int32_t cml;                    /* "Characteristic matching layer" in sponge elements */
   double sponge_state[5];         /* damping (averaged) state: density, velocity x, y,
                                      z, pressure, dimensional                          */
+  double inflow_total[6][5];      /* total inflow: total pressure (Pa), total
+                                     temperature (K), velocity direction x, y, z      */
 } vcpg_open_boundary;
 
 /* Configures open boundaries on a handle whose geometry has boundary faces

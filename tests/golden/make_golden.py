@@ -91,6 +91,14 @@ OPEN_SPECS = {
         outlet_beta_t=-1.0, outlet_one_minus_beta=False,
         bc=("periodic", "periodic", "periodic", "periodic", "inflow_static_nscbc",
             "outflow_nscbc"), sponge=(0, 0, 0, 0, 0, 1), **_OPEN),
+    # Total-condition inflow (relaxing total pressure, total temperature and the
+    # flow direction) with the outgoing amplitude kept, outflow on i-max with a
+    # sponge and the matching layer, flow at an angle in the x-y plane.
+    "pulse_p3_5x3x2_total": cases.CaseSpec(
+        name="pulse_p3_5x3x2_total", n_elem=(5, 3, 2), p=3, hi=(5.0, 3.0, 2.0),
+        center=(0.7, 1.5, 1.0), vel_dir=(1.0, 0.25, 0.0), seed=7, inlet_incoming=True,
+        bc=("inflow_total_nscbc", "outflow_nscbc", "periodic", "periodic", "periodic",
+            "periodic"), sponge=(0, 1, 0, 0, 0, 0), cml=True, **_OPEN),
 }
 
 
@@ -108,6 +116,19 @@ SYNC_SPECS = {
                                    "Pressure pulse center": "5.2 0.8 1.0",
                                    "Pressure pulse strength": "1.0e-2",
                                    "Pressure pulse width": "0.5"}, 2),
+    # The configuration of the reference's own total-inflow test case (8x4x4
+    # elements of degree 3 on [0,2]x[0,1]x[0,1], total inflow / outflow in i,
+    # periodic in j and k, a pressure pulse on the free stream), generated here.
+    "total_p3_8x4x4": (cases.CaseSpec(
+        name="total_p3_8x4x4", kind="uniform", n_elem=(8, 4, 4), p=3, hi=(2.0, 1.0, 1.0),
+        mach=0.1, reynolds=60.0e3, grid_map="none", inlet_sigma=1.0, outlet_sigma=0.25,
+        outlet_beta_l=1.0, outlet_beta_t=-1.0, inlet_incoming=False,
+        bc=("inflow_total_nscbc", "outflow_nscbc", "periodic", "periodic", "periodic",
+            "periodic")),
+        {"Synchronization time step": "2.5e-5", "Restart": "no", "CFL number": "2.0",
+         "Fluctuations to add to initial solution": "Pressure pulse",
+         "Pressure pulse center": "1.0 0.5 0.5", "Pressure pulse strength": "0.1",
+         "Pressure pulse width": "0.1"}, 3),
 }
 
 

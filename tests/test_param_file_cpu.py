@@ -99,8 +99,8 @@ def test_wall_boundary_is_reported():
 
 @pytest.mark.skipif(not os.path.isdir(REF_TESTS), reason="reference test cases not present")
 def test_reference_own_parameter_files():
-    """The reference's own test cases: the NSCBC case with static inflow runs,
-    the others name what is outside the path; the stale n3_10x5x5 file has an
+    """The reference's own test cases: the NSCBC cases with static and total
+    inflow run, the duct names what is outside the path; the stale n3_10x5x5 file has an
     unknown keyword, which the reference rejects as well."""
     seen = {}
     for path in sorted(glob.glob(os.path.join(REF_TESTS, "**", "*.cfg"), recursive=True)):
@@ -116,5 +116,6 @@ def test_reference_own_parameter_files():
         except param_file.UnsupportedOption as e:
             seen[rel] = f"unsupported: {e}"
     assert seen["n3_8x4x4/param_static.cfg"] == "runs"
-    assert "BCInflowTotalNSCBC" in seen["n3_8x4x4/param_total.cfg"]
+    assert seen["n3_8x4x4/param_total.cfg"] == "runs"
+    assert "BCInflowSubsonic" in seen["n5_15x8x8/duct/param.cfg"]
     assert "Unknown keyword" in seen["n3_10x5x5/param.cfg"]

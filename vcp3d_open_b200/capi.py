@@ -18,7 +18,7 @@ ERRORS = {1: "VCPG_E_CUDA", 2: "VCPG_E_CG_NOCONV", 3: "VCPG_E_NEG_A2", 4: "VCPG_
 ROE, ISMAIL_ROE = 0, 1
 FP64, MIXED = 0, 1
 SSPRK3, LSRK4 = 0, 1
-BC_NONE, BC_OUTFLOW_NSCBC, BC_INFLOW_STATIC_NSCBC = 0, 1, 2
+BC_NONE, BC_OUTFLOW_NSCBC, BC_INFLOW_STATIC_NSCBC, BC_INFLOW_TOTAL_NSCBC = 0, 1, 2, 3
 
 # Every symbol include/vcp3d_b200.h declares.
 EXPORTED = [
@@ -61,7 +61,8 @@ class OpenBoundary(C.Structure):
                 ("inlet_incoming", C.c_int32), ("inlet_len", C.c_double),
                 ("inlet_sigma", C.c_double), ("sponge_elems", C.c_int32 * 6),
                 ("sponge_sigma", C.c_double * 6), ("sponge_alpha", C.c_double * 6),
-                ("cml", C.c_int32), ("sponge_state", C.c_double * 5)]
+                ("cml", C.c_int32), ("sponge_state", C.c_double * 5),
+                ("inflow_total", (C.c_double * 5) * 6)]
 
 
 class EnsembleConfig(C.Structure):

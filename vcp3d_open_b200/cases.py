@@ -34,7 +34,8 @@ GAMMA = 1.4
 R_GAS = 287.058
 # Boundary-condition names of the subface table (src/InputParamClass.cpp:1441-1580).
 BC_NAMES = {"periodic": "Periodic1to1Trans", "outflow_nscbc": "BCOutflowNSCBC",
-            "inflow_static_nscbc": "BCInflowStaticNSCBC"}
+            "inflow_static_nscbc": "BCInflowStaticNSCBC",
+            "inflow_total_nscbc": "BCInflowTotalNSCBC"}
 MU_DIM = 1.716e-5
 SU2_MAGIC = 535532
 NAME_LEN = 33
@@ -122,7 +123,9 @@ class CaseSpec:
     pulse_width: float = 0.5
     # Block-face boundary conditions (iMin, iMax, jMin, jMax, kMin, kMax): "periodic",
     # "outflow_nscbc" (BCOutflowNSCBC, prescribed static pressure) or
-    # "inflow_static_nscbc" (BCInflowStaticNSCBC, prescribed density and velocity).
+    # "inflow_static_nscbc" (BCInflowStaticNSCBC, prescribed density and velocity) or
+    # "inflow_total_nscbc" (BCInflowTotalNSCBC, prescribed total pressure, total
+    # temperature and velocity direction).
     bc: Tuple[str, ...] = ("periodic",) * 6
     p_inf: float = 101325.0          # free-stream static pressure of open cases (Pa)
     # NSCBC tuning parameters (src/InputParamClass.cpp:406-424).
@@ -144,6 +147,9 @@ class CaseSpec:
     # face: outflow pressure and inflow (rho, u, v, w); None: the free stream.
     prescribed_p: Optional[Tuple[float, ...]] = None
     prescribed_inflow: Optional[Tuple[Tuple[float, float, float, float], ...]] = None
+    # Total inflow per block face: (p_t, T_t, direction x, y, z); None: from the
+    # free stream (total_inflow_values).
+    prescribed_total: Optional[Tuple[Tuple[float, float, float, float, float], ...]] = None
     # Sponge-layer target state (rho, u, v, w, p, dimensional); None: the free stream.
     sponge_state: Optional[Tuple[float, ...]] = None
 
@@ -214,6 +220,10 @@ def reference_conditions(spec: CaseSpec) -> RefConditions:
     if "outflow_nscbc" in spec.bc and "inflow_static_nscbc" in spec.bc:
         p_ref = spec.p_inf
         rho_ref = spec.p_inf / (R_GAS * spec.t_inf)
+    elif "outflow_nscbc" in spec.bc and "inflow_total_nscbc" in spec.bc:
+        # Static outflow pressure and total temperature: rho_ref = p / (R T_t).
+        p_ref = spec.p_inf
+        rho_ref = spec.p_inf / (R_GAS * total_inflow_values(spec)[1])
     else:
         rho_ref = spec.reynolds * MU_DIM / (spec.reynolds_length * v_inf)
         p_ref = rho_ref * R_GAS * spec.t_inf
@@ -475,10 +485,25 @@ Sponge layer information
         elif bc == "inflow_static_nscbc":
             lines.append(f"    {f + 1}    1    1    Density VelocityX VelocityY VelocityZ")
             lines.append(f"        {rho_in!r} {vel_in[0]!r} {vel_in[1]!r} {vel_in[2]!r}")
+        elif bc == "inflow_total_nscbc":
+            t = total_inflow_values(spec)
+            lines.append(f"    {f + 1}    1    1    TotalPressure TotalTemperature VelocityDirX "
+                         "VelocityDirY VelocityDirZ")
+            lines.append("        " + " ".join(repr(float(v)) for v in t))
     presc = ""
     if lines:
         presc = "\nPrescribed boundary data\n" + "\n".join(lines) + "\n"
     return params, sponge, presc
+
+
+def total_inflow_values(spec: CaseSpec):
+    """Total pressure and temperature of the free stream (p_inf, t_inf, Mach) and
+    the flow direction: the prescribed data of a generated total inflow."""
+    ff = 1.0 + 0.5 * (GAMMA - 1.0) * spec.mach ** 2
+    d = np.asarray(spec.vel_dir, dtype=float)
+    d = d / math.sqrt(float(d @ d))
+    return (spec.p_inf * ff ** (GAMMA / (GAMMA - 1.0)), spec.t_inf * ff,
+            float(d[0]), float(d[1]), float(d[2]))
 
 
 def prescribed_values(spec: CaseSpec, ref: "RefConditions"):

@@ -9,7 +9,7 @@
 //                        number of its block face (SolverClass::AverageDataNSCBC,
 //                        src/SolverClass.cpp:2492-2581), the boundary state and
 //                        gradient (ConvertEntropyToPrimitive, the outflow / static
-//                        inflow LODI corrections and ReconstructBoundaryStateAndGradient,
+//                        / total inflow LODI corrections and ReconstructBoundaryStateAndGradient,
 //                        src/BoundaryState.cpp:1002-1289, 1300-1568, 1579-1847), and
 //                        the face fluxes of FluxesBoundaryFace (src/FluxesFace.cpp:16-214).
 //
@@ -33,7 +33,7 @@ struct BoundaryArgs {
   const double *face_metric;   // [nE][6][13][M^2]
   const double *elem_scalars;  // [nE][15]
   const int *bface;            // [nB][kBfStride]
-  const double *bpresc;        // [nB][4]
+  const double *bpresc;        // [nB][kPrescStride]
   const double *pc;            // [M^2][M^2]
   const double *dlq;           // [M][M]
   double *btrace;              // [nB][4][5][M^2]: value, d/dr, d/ds, d/dt
@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(NT) BoundaryFluxKernel(const BoundaryArgs a) {
   const double factNorm = (f % 2 == 0) ? -1.0 : 1.0;
   const double *fm = a.face_metric + ((size_t)e * 6 + f) * 13 * M2;
   const double *tr = a.btrace + (size_t)b * 4 * 5 * M2;
-  const double *pres = a.bpresc + (size_t)b * 4;
+  const double *pres = a.bpresc + (size_t)b * kPrescStride;
 
   // Boundary-averaged projected Mach number of this block face (sum in element order).
   if (threadIdx.x == 0) {
@@ -215,6 +215,8 @@ __global__ void __launch_bounds__(NT) BoundaryFluxKernel(const BoundaryArgs a) {
     const double dw3dr = rn[0] * dvdr - rn[1] * dudr;
     const double durdr = rn[0] * dudr + rn[1] * dvdr + rn[2] * dwdr;
     double LL[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    // Inverses of the acoustic eigenvalues that rebuild the normal derivative.
+    double ov1 = ovlmb1, ov3 = ovlmb3;
     if (type == VCPG_BC_OUTFLOW_NSCBC) {
       // BCOutflowCharacteristicSubfaceClass::ComputeBoundaryState (src/BoundaryState.cpp:1300-1568).
       const double sign = (c.iPhi == 0) ? -1.0 : 1.0;
@@ -246,6 +248,75 @@ __global__ void __launch_bounds__(NT) BoundaryFluxKernel(const BoundaryArgs a) {
       const double TT = -0.5 * aa * (ss[0] * duds + ss[1] * dvds + ss[2] * dwds +
                                      tt[0] * dudt + tt[1] * dvdt + tt[2] * dwdt);
       LL[c.iPhi] = kk * ovrho * magrr * (p - pInf) - cbl * LT + cbt * TT;
+    } else if (type == VCPG_BC_INFLOW_TOTAL_NSCBC) {
+      // BCInflowTotalCharacteristicSubfaceClass::ComputeBoundaryState
+      // (src/BoundaryState.cpp:1848-2238): the incoming amplitudes relax the total
+      // pressure, total temperature and the two direction cosines v/|u|, w/|u|
+      // towards the prescribed values; the 4x4 system is solved in closed form by
+      // elimination in the order of the reference (E, F, G, H coefficients). The
+      // eigenvalues use the unit normal here.
+      const int iPsi = c.iPhi == 0 ? 4 : 0;
+      const double kk = -c.sigma / c.len;
+      const double urn = u * rn[0] + v * rn[1] + w * rn[2];
+      const double l1 = urn - aa, l3 = urn + aa;
+      ov1 = 1.0 / l1;
+      ov3 = 1.0 / l3;
+      const double ovl2 = 1.0 / urn;
+      const double w1 = rn[1] * w - rn[2] * v, w2 = rn[2] * u - rn[0] * w,
+                   w3 = rn[0] * v - rn[1] * u;
+      const double ova = 1.0 / aa, ovrg = 1.0 / kRGas, ovcp = 1.0 / kCp;
+      if (c.incoming) {
+        LL[0] = 0.5 * l1 * (ovrhoa * dpdr - durdr);
+        LL[4] = 0.5 * l3 * (ovrhoa * dpdr + durdr);
+      }
+      const double magU2 = 2.0 * ek, magU = sqrt(magU2);
+      const double ff = 1.0 + 0.5 * gm1 * magU2 / aa2;
+      const double T = p * ovrho * ovrg;
+      const double Pt = p * pow(ff, kGam * ovgm1), Tt = T * ff;
+      const double Zt = v / magU, Zp = w / magU;
+      const double ka = kk * aa;
+      const double X1 = ka * (Pt - pres[0]), X2 = ka * (Tt - pres[1]);
+      const double X3 = ka * (Zt - pres[3]), X4 = ka * (Zp - pres[4]);
+      const double rPtTt = ovrg * Pt / Tt, Ttovrho = Tt * ovrho, gaPt = kGam * ova * Pt;
+      const double ekovrho = ek * ovrho, gm1eka = gm1 * ek * ova, gm1aTt = gm1 * ova * Tt;
+      const double ovU2 = 1.0 / magU2;
+      const double gp = gm1eka + urn, gmn = gm1eka - urn;
+      const double f1 = w1 - rn[0] * ekovrho, f2 = w2 - rn[1] * ekovrho, f3 = w3 - rn[2] * ekovrho;
+      const double A1 = gp * rPtTt - gaPt, A2 = f1 * rPtTt, A3 = f2 * rPtTt, A4 = f3 * rPtTt,
+                   A5 = gmn * rPtTt - gaPt;
+      const double B1 = gp * ovcp - gm1aTt, B2 = f1 * ovcp + rn[0] * Ttovrho,
+                   B3 = f2 * ovcp + rn[1] * Ttovrho, B4 = f3 * ovcp + rn[2] * Ttovrho,
+                   B5 = gmn * ovcp - gm1aTt;
+      const double C1 = (rn[1] * magU - urn * Zt) * ovU2, C2 = -(rn[2] * magU + w1 * Zt) * ovU2,
+                   C3 = (-w2 * Zt) * ovU2, C4 = (rn[0] * magU - w3 * Zt) * ovU2, C5 = -C1;
+      const double D1 = (rn[2] * magU - urn * Zp) * ovU2, D2 = (rn[1] * magU - w1 * Zp) * ovU2,
+                   D3 = -(rn[0] * magU + w2 * Zp) * ovU2, D4 = (-w3 * Zp) * ovU2, D5 = -D1;
+      const double Y1 = LL[iPsi] * A1, Y2 = LL[iPsi] * B1, Y3 = LL[iPsi] * C1,
+                   Y4 = LL[iPsi] * D1;
+      const double ovA2 = 1.0 / A2;
+      const double E0 = ovA2 * X1, E3 = -ovA2 * A3, E4 = -ovA2 * A4, E5 = -ovA2 * A5,
+                   P2 = -ovA2 * Y1;
+      const double ovF = 1.0 / (D3 + D2 * E3);
+      const double F0 = ovF * (X4 - D2 * E0), F4 = -ovF * (D4 + D2 * E4),
+                   F5 = -ovF * (D5 + D2 * E5), P3 = -ovF * (Y4 + D2 * P2);
+      const double ovG = 1.0 / (C4 + C2 * E4 + C3 * F4 + C2 * E3 * F4);
+      const double G0 = ovG * (X3 - C2 * E0 - C3 * F0 - C2 * E3 * F0),
+                   G5 = -ovG * (C5 + C2 * E5 + C3 * F5 + C2 * E3 * F5),
+                   P4 = -ovG * (Y3 + C2 * P2 + C3 * P3 + C2 * E3 * P3);
+      const double ovH = 1.0 / (B5 + B2 * E5 + B3 * F5 + B4 * G5 + B2 * E3 * F5 + B2 * E4 * G5 +
+                                B3 * F4 * G5 + B2 * E3 * F4 * G5);
+      const double H0 = ovH * (X2 - B2 * E0 - B3 * F0 - B4 * G0 - B2 * E3 * F0 - B2 * E4 * G0 -
+                               B3 * F4 * G0 - B2 * E3 * F4 * G0);
+      const double P5 = -ovH * (Y2 + B2 * P2 + B3 * P3 + B4 * P4 + B2 * E3 * P3 + B2 * E4 * P4 +
+                                B3 * F4 * P4 + B2 * E3 * F4 * P4);
+      LL[c.iPhi] = H0 + P5;
+      LL[3] = G0 + G5 * LL[c.iPhi] + P4;
+      LL[2] = F0 + F4 * LL[3] + F5 * LL[c.iPhi] + P3;
+      LL[1] = E0 + E3 * LL[2] + E4 * LL[3] + E5 * LL[c.iPhi] + P2;
+      LL[1] *= ovl2;
+      LL[2] *= ovl2;
+      LL[3] *= ovl2;
+      (void)dsdr; (void)dw1dr; (void)dw2dr; (void)dw3dr;
     } else {
       // BCInflowStaticCharacteristicSubfaceClass::ComputeBoundaryState
       // (src/BoundaryState.cpp:1579-1847).
@@ -267,12 +338,12 @@ __global__ void __launch_bounds__(NT) BoundaryFluxKernel(const BoundaryArgs a) {
     }
     // Boundary-conforming normal derivative of the primitive variables.
     double dn[5];
-    dn[0] = ovlmb1 * rhova * LL[0] + rn[0] * LL[1] + rn[1] * LL[2] + rn[2] * LL[3] +
-            ovlmb3 * rhova * LL[4];
-    dn[1] = -ovlmb1 * rn[0] * LL[0] - rn[2] * LL[2] + rn[1] * LL[3] + ovlmb3 * rn[0] * LL[4];
-    dn[2] = -ovlmb1 * rn[1] * LL[0] + rn[2] * LL[1] - rn[0] * LL[3] + ovlmb3 * rn[1] * LL[4];
-    dn[3] = -ovlmb1 * rn[2] * LL[0] - rn[1] * LL[1] + rn[0] * LL[2] + ovlmb3 * rn[2] * LL[4];
-    dn[4] = ovlmb1 * rhoa * LL[0] + ovlmb3 * rhoa * LL[4];
+    dn[0] = ov1 * rhova * LL[0] + rn[0] * LL[1] + rn[1] * LL[2] + rn[2] * LL[3] +
+            ov3 * rhova * LL[4];
+    dn[1] = -ov1 * rn[0] * LL[0] - rn[2] * LL[2] + rn[1] * LL[3] + ov3 * rn[0] * LL[4];
+    dn[2] = -ov1 * rn[1] * LL[0] + rn[2] * LL[1] - rn[0] * LL[3] + ov3 * rn[1] * LL[4];
+    dn[3] = -ov1 * rn[2] * LL[0] - rn[1] * LL[1] + rn[0] * LL[2] + ov3 * rn[2] * LL[4];
+    dn[4] = ov1 * rhoa * LL[0] + ov3 * rhoa * LL[4];
     const double q[5] = {rho, u, v, w, p};
     const double dqr[5] = {drhodr, dudr, dvdr, dwdr, dpdr};
 #pragma unroll

@@ -15,6 +15,8 @@ constexpr double kPrTurb = 0.90;
 constexpr double kFactHFLam = kGam / kPrLam;    // factHeatFlux_Lam
 constexpr double kFactHFTurb = kGam / kPrTurb;  // factHeatFlux_Turb
 constexpr double kLamOverMu = -2.0 / 3.0;       // lambdaOverMu
+constexpr double kRGas = 287.058;                 // RGas (include/VCP3D_CurviLinear.hpp:177)
+constexpr double kCp = kGam * kRGas / (kGam - 1.0);  // Cp
 
 // Math in the compute precision T (double for the FP64 form, float for the mixed form).
 __device__ __forceinline__ double Exp(double x) { return exp(x); }

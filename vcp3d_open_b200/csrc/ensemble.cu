@@ -233,7 +233,7 @@ int AllocBucket(vcpg_ensemble *e, Bucket &b, int deg, int64_t capE, int64_t capB
       (rc = alloc((void **)&b.sc, 8 * E * 15)) || (rc = alloc((void **)&b.nbr, 4 * E * 6)) ||
       (rc = alloc((void **)&b.elemCase, 4 * E)) || (rc = alloc((void **)&b.spongeIdx, 4 * E)) ||
       (rc = alloc((void **)&b.bface, 4 * B * kBfStride)) ||
-      (rc = alloc((void **)&b.bpresc, 8 * B * 4)) ||
+      (rc = alloc((void **)&b.bpresc, 8 * B * kPrescStride)) ||
       (rc = alloc((void **)&b.btrace, 8 * B * 4 * 5 * b.M2)) ||
       (rc = alloc((void **)&b.bmach, 8 * B)) ||
       (rc = alloc((void **)&b.bflux, 8 * B * 4 * 5 * b.M2)) ||
@@ -593,7 +593,8 @@ int vcpg_ensemble_submit(vcpg_ensemble *ens, const vcpg_params *params,
   if (ce == cudaSuccess) ce = cp(b.nbr + (size_t)eFirst * 6, nbr.data(), 4 * E * 6);
   if (ce == cudaSuccess) ce = cp(b.spongeIdx + eFirst, sidx.data(), 4 * E);
   if (ce == cudaSuccess && nB) ce = cp(b.bface + (size_t)bFirst * kBfStride, brows.data(), 4 * brows.size());
-  if (ce == cudaSuccess && nB) ce = cp(b.bpresc + (size_t)bFirst * 4, obh.bpresc.data(), 8 * obh.bpresc.size());
+  if (ce == cudaSuccess && nB)
+    ce = cp(b.bpresc + (size_t)bFirst * kPrescStride, obh.bpresc.data(), 8 * obh.bpresc.size());
   if (ce == cudaSuccess && nS) ce = cp(b.dampFn + (size_t)sFirst * 3 * MD, obh.dampFn.data(), 8 * obh.dampFn.size());
   if (ce == cudaSuccess && nS) ce = cp(b.dampSt + (size_t)sFirst * 5 * MD, obh.dampState.data(), 8 * obh.dampState.size());
   if (ce == cudaSuccess && nS) ce = cp(b.cml + (size_t)sFirst * 6, obh.cml.data(), 8 * obh.cml.size());

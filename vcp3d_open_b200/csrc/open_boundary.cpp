@@ -113,7 +113,7 @@ int BuildOpenBoundary(const vcpg_params &prm, const vcpg_open_boundary &ob,
     const int64_t nE = (int64_t)nI * nJ * nK;
     if (!geom.face_metric || !geom.neighbors) { err = "geometry arrays missing"; return VCPG_E_INVALID; }
     for (int f = 0; f < 6; ++f)
-      if (ob.bc[f] < VCPG_BC_NONE || ob.bc[f] > VCPG_BC_INFLOW_STATIC_NSCBC) {
+      if (ob.bc[f] < VCPG_BC_NONE || ob.bc[f] > VCPG_BC_INFLOW_TOTAL_NSCBC) {
         err = "unknown boundary condition on face " + std::to_string(f);
         return VCPG_E_INVALID;
       }
@@ -182,9 +182,18 @@ int BuildOpenBoundary(const vcpg_params &prm, const vcpg_open_boundary &ob,
         c.sigma = ob.outlet_sigma; c.len = ob.outlet_len;
         c.betaL = ob.outlet_beta_l; c.betaT = ob.outlet_beta_t;
         c.oneMinusBeta = ob.outlet_one_minus_beta ? 1 : 0;
-      } else if (c.type == VCPG_BC_INFLOW_STATIC_NSCBC) {
+      } else if (c.type == VCPG_BC_INFLOW_STATIC_NSCBC || c.type == VCPG_BC_INFLOW_TOTAL_NSCBC) {
         c.sigma = ob.inlet_sigma; c.len = ob.inlet_len;
         c.incoming = ob.inlet_incoming ? 1 : 0;
+      }
+      if (c.type == VCPG_BC_INFLOW_TOTAL_NSCBC) {
+        const double *t = ob.inflow_total[f];
+        const double dl = std::sqrt(t[2] * t[2] + t[3] * t[3] + t[4] * t[4]);
+        if (!(t[0] > 0.0) || !(t[1] > 0.0) || !(dl > 0.0)) {
+          err = "total inflow needs a positive total pressure, total temperature and a "
+                "velocity direction on face " + std::to_string(f);
+          return VCPG_E_INVALID;
+        }
       }
       if (c.type != VCPG_BC_NONE && !(c.len > 0.0)) {
         err = "characteristic length must be positive on face " + std::to_string(f);
@@ -204,16 +213,27 @@ int BuildOpenBoundary(const vcpg_params &prm, const vcpg_open_boundary &ob,
         const int b = out.nB++;
         int row[kBfStride] = {(int)e, f, c.type, grad[0], grad[1], grad[2], 0, 0};
         out.bface.insert(out.bface.end(), row, row + kBfStride);
-        double pres[4] = {0.0, 0.0, 0.0, 0.0};
+        double pres[kPrescStride] = {0.0, 0.0, 0.0, 0.0, 0.0};
         if (c.type == VCPG_BC_OUTFLOW_NSCBC) {
           pres[0] = ob.p_out[f] / prm.p_ref;
-        } else {
+        } else if (c.type == VCPG_BC_INFLOW_STATIC_NSCBC) {
           pres[0] = ob.inflow[f][0] / prm.rho_ref;
           pres[1] = ob.inflow[f][1] / prm.u_ref;
           pres[2] = ob.inflow[f][2] / prm.u_ref;
           pres[3] = ob.inflow[f][3] / prm.u_ref;
+        } else {
+          // BCInflowTotalCharacteristicSubfaceClass::ConvertPrescribedData
+          // (src/SubfaceClasses.cpp:1577-1608): p_t / p_ref, T_t / (p_ref / rho_ref)
+          // (the gas constant stays in the boundary formulas), unit direction.
+          const double *t = ob.inflow_total[f];
+          const double dl = std::sqrt(t[2] * t[2] + t[3] * t[3] + t[4] * t[4]);
+          pres[0] = t[0] / prm.p_ref;
+          pres[1] = t[1] / (prm.p_ref / prm.rho_ref);
+          pres[2] = t[2] / dl;
+          pres[3] = t[3] / dl;
+          pres[4] = t[4] / dl;
         }
-        out.bpresc.insert(out.bpresc.end(), pres, pres + 4);
+        out.bpresc.insert(out.bpresc.end(), pres, pres + kPrescStride);
         out.nbrCode[e * 6 + f] = -2 - b;
         for (int l = 0; l < M2; ++l) c.area += wInt[l % M] * wInt[l / M] * fm[3 * M2 + l];
       }

@@ -34,10 +34,14 @@ enum BFaceField {
   kBfStride = 8
 };
 
+// Non-dimensional prescribed values per boundary face: outflow p; static inflow
+// rho, u, v, w; total inflow p_t, T_t (scaled by p_ref / rho_ref), direction x, y, z.
+constexpr int kPrescStride = 5;
+
 struct OpenBoundaryHost {
   int nB = 0;                       // boundary faces with a characteristic BC
   std::vector<int> bface;           // [nB][kBfStride]
-  std::vector<double> bpresc;       // [nB][4] non-dimensional prescribed data
+  std::vector<double> bpresc;       // [nB][kPrescStride] non-dimensional prescribed data
   std::vector<double> pc;           // [M^2][M^2] polynomial-correction matrix
   std::vector<double> dlq;          // [M][M]: dlq[i * M + k] = dL_k(q_i), Lagrange basis
                                     // on the Gauss points

@@ -15,7 +15,8 @@ GPU path supports:
   DetermineNonDimPrimVarFreeStream :991-1192).
 
 Options outside the path (conservative working variables, subgrid-scale and
-wall models, walls, far field and the remaining boundary conditions, random or
+wall models, walls, far field and the non-characteristic in- and outflow
+conditions, random or
 synthetic fluctuations, several subfaces per block face, spatially varying
 prescribed data) raise UnsupportedOption with the option named.
 """
@@ -115,7 +116,8 @@ _ALL_BCS = ("internal1to1", "periodic1to1trans", "bcfarfield", "bcwallisothermal
             "bcoutflowsupersonic", "bcinflowstaticnscbc", "bcinflowtotalnscbc",
             "bcoutflownscbc")
 _BC_TO_CASE = {"periodic1to1trans": "periodic", "bcoutflownscbc": "outflow_nscbc",
-               "bcinflowstaticnscbc": "inflow_static_nscbc"}
+               "bcinflowstaticnscbc": "inflow_static_nscbc",
+               "bcinflowtotalnscbc": "inflow_total_nscbc"}
 _NSCBC = ("bcinflowstaticnscbc", "bcinflowtotalnscbc", "bcoutflownscbc")
 
 
@@ -566,6 +568,16 @@ def outflow_pressure(pf: ParamFile, face: int) -> float:
     if "Pressure" not in data:
         raise ParamFileError(f"face {face + 1}: BCOutflowNSCBC needs a prescribed Pressure")
     return data["Pressure"]
+
+
+def inflow_total(pf: ParamFile, face: int) -> Tuple[float, float, float, float, float]:
+    data = pf.prescribed.get((face, 0), {})
+    names = ("TotalPressure", "TotalTemperature", "VelocityDirX", "VelocityDirY",
+             "VelocityDirZ")
+    if not all(nm in data for nm in names):
+        raise ParamFileError(f"face {face + 1}: BCInflowTotalNSCBC needs TotalPressure, "
+                             "TotalTemperature and VelocityDirX/Y/Z")
+    return tuple(data[nm] for nm in names)
 
 
 def inflow_static(pf: ParamFile, face: int) -> Tuple[float, float, float, float]:

@@ -144,6 +144,8 @@ def load_case(pf: ParamFile) -> cases.CaseData:
                          for f, b in enumerate(bcs))
     prescribed_in = tuple(param_file.inflow_static(pf, f) if b == "inflow_static_nscbc"
                           else (0.0, 0.0, 0.0, 0.0) for f, b in enumerate(bcs))
+    prescribed_tot = tuple(param_file.inflow_total(pf, f) if b == "inflow_total_nscbc"
+                           else (0.0, 0.0, 1.0, 0.0, 0.0) for f, b in enumerate(bcs))
     sponge = tuple(r[0] for r in pf.sponge) if pf.sponge else (0,) * 6
     sponge_state = None
     if any(sponge):
@@ -164,7 +166,7 @@ def load_case(pf: ParamFile) -> cases.CaseData:
         sponge_sigma=tuple(r[1] for r in pf.sponge) if pf.sponge else 20.0,
         sponge_alpha=tuple(r[2] for r in pf.sponge) if pf.sponge else 2.0,
         cml=pf.cml and any(sponge), prescribed_p=prescribed_p, prescribed_inflow=prescribed_in,
-        sponge_state=sponge_state)
+        prescribed_total=prescribed_tot, sponge_state=sponge_state)
     refc = cases.RefConditions(ref.p_ref, ref.rho_ref, ref.u_ref, ref.mu_nondim, speed, vel_dir)
     return cases.CaseData(spec, refc, grid, nodes, xyz, np.ascontiguousarray(cons))
 

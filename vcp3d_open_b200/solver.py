@@ -106,11 +106,12 @@ def nodal_to_modal(case: CaseData, params: capi.Params) -> np.ndarray:
 def open_boundary(case: CaseData) -> capi.OpenBoundary:
     """vcpg_open_boundary of a case: its boundary conditions with the free stream
     as prescribed data, NSCBC tuning parameters, sponge layers and matching layer."""
-    from .cases import prescribed_values
+    from .cases import prescribed_values, total_inflow_values
     s, ref = case.spec, case.ref
     ob = capi.OpenBoundary()
     codes = {"periodic": capi.BC_NONE, "outflow_nscbc": capi.BC_OUTFLOW_NSCBC,
-             "inflow_static_nscbc": capi.BC_INFLOW_STATIC_NSCBC}
+             "inflow_static_nscbc": capi.BC_INFLOW_STATIC_NSCBC,
+             "inflow_total_nscbc": capi.BC_INFLOW_TOTAL_NSCBC}
     p_out, rho_in, vel_in = prescribed_values(s, ref)
     per_face = lambda v, f: v[f] if isinstance(v, (tuple, list)) else v
     for f, bc in enumerate(s.bc):
@@ -118,6 +119,10 @@ def open_boundary(case: CaseData) -> capi.OpenBoundary:
         ob.p_out[f] = s.prescribed_p[f] if s.prescribed_p else p_out
         inflow = s.prescribed_inflow[f] if s.prescribed_inflow else (rho_in, *vel_in)
         ob.inflow[f][0], ob.inflow[f][1], ob.inflow[f][2], ob.inflow[f][3] = inflow
+        if bc == "inflow_total_nscbc":
+            total = s.prescribed_total[f] if s.prescribed_total else total_inflow_values(s)
+            for q in range(5):
+                ob.inflow_total[f][q] = total[q]
         ob.sponge_elems[f] = s.sponge[f]
         ob.sponge_sigma[f] = per_face(s.sponge_sigma, f)
         ob.sponge_alpha[f] = per_face(s.sponge_alpha, f)
