@@ -215,10 +215,22 @@ enum vcpg_bc {
   VCPG_BC_INFLOW_STATIC_NSCBC = 2,  /* "BCInflowStaticNSCBC": prescribed density and
                                        velocity, BCInflowStaticCharacteristicSubfaceClass
                                        (src/BoundaryState.cpp:1579-1847)              */
-  VCPG_BC_INFLOW_TOTAL_NSCBC = 3    /* "BCInflowTotalNSCBC": prescribed total pressure,
+  VCPG_BC_INFLOW_TOTAL_NSCBC = 3,   /* "BCInflowTotalNSCBC": prescribed total pressure,
                                        total temperature and velocity direction,
                                        BCInflowTotalCharacteristicSubfaceClass
                                        (src/BoundaryState.cpp:1848-2238)              */
+  /* Boundary conditions through a boundary state (FluxesBoundaryFace,
+   * src/FluxesFace.cpp:16-214, with the subface's ComputeBoundaryState,
+   * src/BoundaryState.cpp:124-828); no wall model. */
+  VCPG_BC_WALL_HEAT_FLUX = 4,       /* "BCWallHeatFlux": wall_data = heat flux (W/m^2)  */
+  VCPG_BC_WALL_ISOTHERMAL = 5,      /* "BCWallIsothermal": wall_data = temperature (K)  */
+  VCPG_BC_WALL_INVISCID = 6,        /* "BCWallInviscid"                                 */
+  VCPG_BC_FARFIELD = 7,             /* "BCFarfield": the free stream (free_stream)      */
+  VCPG_BC_INFLOW_SUBSONIC = 8,      /* "BCInflowSubsonic": total pressure, total
+                                       temperature and direction in inflow_total        */
+  VCPG_BC_INFLOW_SUPERSONIC = 9,    /* "BCInflowSupersonic": inflow_super               */
+  VCPG_BC_OUTFLOW_SUBSONIC = 10,    /* "BCOutflowSubsonic": static pressure in p_out    */
+  VCPG_BC_OUTFLOW_SUPERSONIC = 11   /* "BCOutflowSupersonic"                            */
 };
 
 /* The reference's "NSCBC tuning parameters", "Prescribed boundary data" and
@@ -244,8 +256,15 @@ typedef struct vcpg_open_boundary {
   int32_t cml;                    /* "Characteristic matching layer" in sponge elements */
   double sponge_state[5];         /* damping (averaged) state: density, velocity x, y,
                                      z, pressure, dimensional                          */
-  double inflow_total[6][5];      /* total inflow: total pressure (Pa), total
-                                     temperature (K), velocity direction x, y, z      */
+  double inflow_total[6][5];      /* total inflow (characteristic or subsonic): total
+                                     pressure (Pa), total temperature (K), velocity
+                                     direction x, y, z                                 */
+  double wall_data[6];            /* heat-flux wall: heat flux (W/m^2); isothermal
+                                     wall: wall temperature (K)                        */
+  double inflow_super[6][5];      /* supersonic inflow: density, velocity x, y, z,
+                                     pressure                                          */
+  double free_stream[5];          /* far field: density, velocity x, y, z, pressure
+                                     (the reference's free stream, dimensional)        */
 } vcpg_open_boundary;
 
 /* Configures open boundaries on a handle whose geometry has boundary faces

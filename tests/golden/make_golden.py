@@ -99,6 +99,26 @@ OPEN_SPECS = {
         center=(0.7, 1.5, 1.0), vel_dir=(1.0, 0.25, 0.0), seed=7, inlet_incoming=True,
         bc=("inflow_total_nscbc", "outflow_nscbc", "periodic", "periodic", "periodic",
             "periodic"), sponge=(0, 1, 0, 0, 0, 0), cml=True, **_OPEN),
+    # Walls through a boundary state: a heat-flux wall with a non-zero flux on j-min,
+    # an isothermal wall on j-max, flow along the walls; i and k periodic.
+    "wall_p3_4x3x3": cases.CaseSpec(
+        name="wall_p3_4x3x3", n_elem=(4, 3, 3), p=3, hi=(4.0, 3.0, 3.0), center=(2.0, 0.6, 1.5),
+        seed=8, wall_data=(0.0, 0.0, 50.0, 300.0, 0.0, 0.0),
+        bc=("periodic", "periodic", "wall_heat_flux", "wall_isothermal", "periodic",
+            "periodic"), **_OPEN),
+    # Subsonic inflow (total conditions) and outflow (back pressure) through a
+    # boundary state, inviscid walls on the j faces, k periodic.
+    "subsonic_p3_5x3x2": cases.CaseSpec(
+        name="subsonic_p3_5x3x2", n_elem=(5, 3, 2), p=3, hi=(5.0, 3.0, 2.0),
+        center=(0.8, 1.5, 1.0), seed=9,
+        bc=("inflow_subsonic", "outflow_subsonic", "wall_inviscid", "wall_inviscid", "periodic",
+            "periodic"), **_OPEN),
+    # Supersonic inflow / outflow states and far field on the j faces, Roe flux, degree 2.
+    "farfield_p2_4x4x2_roe": cases.CaseSpec(
+        name="farfield_p2_4x4x2_roe", n_elem=(4, 4, 2), p=2, hi=(4.0, 4.0, 2.0),
+        center=(2.0, 3.3, 1.0), seed=10, riemann="Roe",
+        bc=("inflow_supersonic", "outflow_supersonic", "farfield", "farfield", "periodic",
+            "periodic"), **_OPEN),
 }
 
 
@@ -129,6 +149,19 @@ SYNC_SPECS = {
          "Fluctuations to add to initial solution": "Pressure pulse",
          "Pressure pulse center": "1.0 0.5 0.5", "Pressure pulse strength": "0.1",
          "Pressure pulse width": "0.1"}, 3),
+    # A duct in the manner of the reference's n5_15x8x8 case, reduced: degree 5,
+    # subsonic inflow, characteristic outflow with a sponge layer, adiabatic walls
+    # on the j and k faces, a pressure pulse on the free stream of the boundary data.
+    "duct_p5_5x3x3": (cases.CaseSpec(
+        name="duct_p5_5x3x3", kind="uniform", n_elem=(5, 3, 3), p=5, hi=(5.0, 1.5, 1.5),
+        mach=0.2, grid_map="none", outlet_sigma=0.25, outlet_beta_l=1.0, outlet_beta_t=-1.0,
+        sponge=(0, 1, 0, 0, 0, 0), sponge_sigma=10.0,
+        bc=("inflow_subsonic", "outflow_nscbc", "wall_heat_flux", "wall_heat_flux",
+            "wall_heat_flux", "wall_heat_flux")),
+        {"Synchronization time step": "2.0e-5", "Restart": "no", "CFL number": "1.0",
+         "Fluctuations to add to initial solution": "Pressure pulse",
+         "Pressure pulse center": "2.5 0.75 0.75", "Pressure pulse strength": "0.05",
+         "Pressure pulse width": "0.2"}, 2),
 }
 
 
@@ -178,8 +211,15 @@ def spec_to_json(spec: cases.CaseSpec) -> str:
 
 def spec_from_json(text: str) -> cases.CaseSpec:
     d = json.loads(text)
-    for k in ("n_elem", "lo", "hi", "vel_dir", "center", "bc", "sponge"):
-        if k in d:
+    for k in ("n_elem", "lo", "hi", "vel_dir", "center", "bc", "sponge", "wall_data",
+              "prescribed_p", "sponge_state", "free_stream"):
+        if d.get(k) is not None:
+            d[k] = tuple(d[k])
+    for k in ("prescribed_inflow", "prescribed_total", "prescribed_super"):
+        if d.get(k) is not None:
+            d[k] = tuple(tuple(v) for v in d[k])
+    for k in ("sponge_sigma", "sponge_alpha"):
+        if isinstance(d.get(k), list):
             d[k] = tuple(d[k])
     return cases.CaseSpec(**d)
 

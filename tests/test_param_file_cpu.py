@@ -87,20 +87,29 @@ def test_options_outside_the_path(edit, what):
         param_file.check_supported(pf)
 
 
-def test_wall_boundary_is_reported():
-    text = _base_text()
+def _replace_subface(text, k, line):
     lines = text.split("\n")
-    k = next(n for n, ln in enumerate(lines) if ln.strip().startswith("Periodic1to1Trans"))
-    lines[k] = "        BCWallHeatFlux 1 1 1 3 1 3"
-    pf = param_file.parse("\n".join(lines))
-    with pytest.raises(param_file.UnsupportedOption, match="BCWallHeatFlux"):
-        param_file.check_supported(pf)
+    idx = [n for n, ln in enumerate(lines) if ln.strip().startswith("Periodic1to1Trans")]
+    lines[idx[k]] = line
+    return "\n".join(lines)
+
+
+def test_boundary_conditions_outside_the_path():
+    # The symmetry plane terminates in the reference as well.
+    text = _replace_subface(_replace_subface(_base_text(), 2, "  BCSymmetryPlane 1 3 1 1 1 3"),
+                            3, "  BCSymmetryPlane 1 3 3 3 1 3")
+    with pytest.raises(param_file.UnsupportedOption, match="BCSymmetryPlane"):
+        param_file.check_supported(param_file.parse(text))
+    # A wall facing a periodic face.
+    text = _replace_subface(_base_text(), 0, "        BCWallHeatFlux 1 1 1 3 1 3")
+    with pytest.raises(param_file.UnsupportedOption, match="periodic on one face only"):
+        param_file.check_supported(param_file.parse(text))
 
 
 @pytest.mark.skipif(not os.path.isdir(REF_TESTS), reason="reference test cases not present")
 def test_reference_own_parameter_files():
     """The reference's own test cases: the NSCBC cases with static and total
-    inflow run, the duct names what is outside the path; the stale n3_10x5x5 file has an
+    inflow and the duct (walls, subsonic inflow) parse and are supported; the stale n3_10x5x5 file has an
     unknown keyword, which the reference rejects as well."""
     seen = {}
     for path in sorted(glob.glob(os.path.join(REF_TESTS, "**", "*.cfg"), recursive=True)):
@@ -117,5 +126,5 @@ def test_reference_own_parameter_files():
             seen[rel] = f"unsupported: {e}"
     assert seen["n3_8x4x4/param_static.cfg"] == "runs"
     assert seen["n3_8x4x4/param_total.cfg"] == "runs"
-    assert "BCInflowSubsonic" in seen["n5_15x8x8/duct/param.cfg"]
+    assert seen["n5_15x8x8/duct/param.cfg"] == "runs"
     assert "Unknown keyword" in seen["n3_10x5x5/param.cfg"]

@@ -19,6 +19,8 @@ ROE, ISMAIL_ROE = 0, 1
 FP64, MIXED = 0, 1
 SSPRK3, LSRK4 = 0, 1
 BC_NONE, BC_OUTFLOW_NSCBC, BC_INFLOW_STATIC_NSCBC, BC_INFLOW_TOTAL_NSCBC = 0, 1, 2, 3
+(BC_WALL_HEAT_FLUX, BC_WALL_ISOTHERMAL, BC_WALL_INVISCID, BC_FARFIELD, BC_INFLOW_SUBSONIC,
+ BC_INFLOW_SUPERSONIC, BC_OUTFLOW_SUBSONIC, BC_OUTFLOW_SUPERSONIC) = range(4, 12)
 
 # Every symbol include/vcp3d_b200.h declares.
 EXPORTED = [
@@ -62,7 +64,8 @@ class OpenBoundary(C.Structure):
                 ("inlet_sigma", C.c_double), ("sponge_elems", C.c_int32 * 6),
                 ("sponge_sigma", C.c_double * 6), ("sponge_alpha", C.c_double * 6),
                 ("cml", C.c_int32), ("sponge_state", C.c_double * 5),
-                ("inflow_total", (C.c_double * 5) * 6)]
+                ("inflow_total", (C.c_double * 5) * 6), ("wall_data", C.c_double * 6),
+                ("inflow_super", (C.c_double * 5) * 6), ("free_stream", C.c_double * 5)]
 
 
 class EnsembleConfig(C.Structure):

@@ -35,7 +35,11 @@ R_GAS = 287.058
 # Boundary-condition names of the subface table (src/InputParamClass.cpp:1441-1580).
 BC_NAMES = {"periodic": "Periodic1to1Trans", "outflow_nscbc": "BCOutflowNSCBC",
             "inflow_static_nscbc": "BCInflowStaticNSCBC",
-            "inflow_total_nscbc": "BCInflowTotalNSCBC"}
+            "inflow_total_nscbc": "BCInflowTotalNSCBC",
+            "wall_heat_flux": "BCWallHeatFlux", "wall_isothermal": "BCWallIsothermal",
+            "wall_inviscid": "BCWallInviscid", "farfield": "BCFarfield",
+            "inflow_subsonic": "BCInflowSubsonic", "inflow_supersonic": "BCInflowSupersonic",
+            "outflow_subsonic": "BCOutflowSubsonic", "outflow_supersonic": "BCOutflowSupersonic"}
 MU_DIM = 1.716e-5
 SU2_MAGIC = 535532
 NAME_LEN = 33
@@ -125,7 +129,10 @@ class CaseSpec:
     # "outflow_nscbc" (BCOutflowNSCBC, prescribed static pressure) or
     # "inflow_static_nscbc" (BCInflowStaticNSCBC, prescribed density and velocity) or
     # "inflow_total_nscbc" (BCInflowTotalNSCBC, prescribed total pressure, total
-    # temperature and velocity direction).
+    # temperature and velocity direction), or a condition through a boundary
+    # state: "wall_heat_flux", "wall_isothermal", "wall_inviscid", "farfield",
+    # "inflow_subsonic" (total conditions), "inflow_supersonic",
+    # "outflow_subsonic" (static pressure), "outflow_supersonic".
     bc: Tuple[str, ...] = ("periodic",) * 6
     p_inf: float = 101325.0          # free-stream static pressure of open cases (Pa)
     # NSCBC tuning parameters (src/InputParamClass.cpp:406-424).
@@ -152,6 +159,13 @@ class CaseSpec:
     prescribed_total: Optional[Tuple[Tuple[float, float, float, float, float], ...]] = None
     # Sponge-layer target state (rho, u, v, w, p, dimensional); None: the free stream.
     sponge_state: Optional[Tuple[float, ...]] = None
+    # Per block face: heat flux (W/m^2) of heat-flux walls or temperature (K) of
+    # isothermal walls; None: adiabatic walls and walls at t_inf.
+    wall_data: Optional[Tuple[float, ...]] = None
+    # Supersonic inflow state per face (rho, u, v, w, p) and the far-field state,
+    # dimensional; None: the free stream.
+    prescribed_super: Optional[Tuple[Tuple[float, ...], ...]] = None
+    free_stream: Optional[Tuple[float, ...]] = None
 
     def __post_init__(self):
         if self.p_grid is None:
@@ -217,13 +231,18 @@ def reference_conditions(spec: CaseSpec) -> RefConditions:
     v_inf = spec.mach * math.sqrt(GAMMA * R_GAS * spec.t_inf)
     d = np.asarray(spec.vel_dir, dtype=float)
     d = d / math.sqrt(float(d @ d))
-    if "outflow_nscbc" in spec.bc and "inflow_static_nscbc" in spec.bc:
+    outflow_p = any(b in ("outflow_nscbc", "outflow_subsonic") for b in spec.bc)
+    total_in = any(b in ("inflow_total_nscbc", "inflow_subsonic") for b in spec.bc)
+    if outflow_p and "inflow_static_nscbc" in spec.bc:
         p_ref = spec.p_inf
         rho_ref = spec.p_inf / (R_GAS * spec.t_inf)
-    elif "outflow_nscbc" in spec.bc and "inflow_total_nscbc" in spec.bc:
+    elif outflow_p and total_in:
         # Static outflow pressure and total temperature: rho_ref = p / (R T_t).
         p_ref = spec.p_inf
         rho_ref = spec.p_inf / (R_GAS * total_inflow_values(spec)[1])
+    elif outflow_p or total_in:
+        raise NotImplementedError("generated cases pair a pressure outflow with a static "
+                                  "or total-condition inflow")
     else:
         rho_ref = spec.reynolds * MU_DIM / (spec.reynolds_length * v_inf)
         p_ref = rho_ref * R_GAS * spec.t_inf
@@ -485,7 +504,20 @@ Sponge layer information
         elif bc == "inflow_static_nscbc":
             lines.append(f"    {f + 1}    1    1    Density VelocityX VelocityY VelocityZ")
             lines.append(f"        {rho_in!r} {vel_in[0]!r} {vel_in[1]!r} {vel_in[2]!r}")
-        elif bc == "inflow_total_nscbc":
+        elif bc == "outflow_subsonic":
+            lines.append(f"    {f + 1}    1    1    Pressure")
+            lines.append(f"        {p_out!r}")
+        elif bc in ("wall_heat_flux", "wall_isothermal"):
+            val = spec.wall_data[f] if spec.wall_data else (
+                0.0 if bc == "wall_heat_flux" else spec.t_inf)
+            name = "HeatFlux" if bc == "wall_heat_flux" else "Temperature"
+            lines.append(f"    {f + 1}    1    1    {name}")
+            lines.append(f"        {float(val)!r}")
+        elif bc == "inflow_supersonic":
+            q = spec.prescribed_super[f] if spec.prescribed_super else (rho_in, *vel_in, p_out)
+            lines.append(f"    {f + 1}    1    1    Density VelocityX VelocityY VelocityZ Pressure")
+            lines.append("        " + " ".join(repr(float(v)) for v in q))
+        elif bc in ("inflow_total_nscbc", "inflow_subsonic"):
             t = total_inflow_values(spec)
             lines.append(f"    {f + 1}    1    1    TotalPressure TotalTemperature VelocityDirX "
                          "VelocityDirY VelocityDirZ")

@@ -129,7 +129,165 @@ __global__ void __launch_bounds__(NT) BoundaryTraceKernel(const BoundaryArgs a) 
   }
 }
 
-// Boundary state and fluxes of one characteristic boundary face.
+// Fluxes of one boundary face whose condition is a boundary state
+// (FluxesBoundaryFace, src/FluxesFace.cpp:16-214, without wall model or NSCBC):
+// the Cartesian gradient of the interior state (metric indexed as in the
+// parity mode), the right state of the subface's ComputeBoundaryState
+// (src/BoundaryState.cpp:124-828, entropy-variable branches), the Riemann flux
+// with the wall factor (0 on walls), the viscous, penalty and symmetrizing fluxes
+// with the interior gradient (heat-flux walls: no conduction, the prescribed
+// flux added), and the four distribution inputs per face point.
+template <int K, int M, int NT>
+__device__ __forceinline__ void WeakBoundaryFlux(const BoundaryArgs &a, const int b,
+                                                 const int e, const int f, const int type,
+                                                 const double mu, const double *fm,
+                                                 const double *tr, const double *pres) {
+  constexpr int SLOT = Slot<K, M>::value;
+  constexpr int M2 = M * M;
+  const int d = f / 2;
+  const double factNorm = (f % 2 == 0) ? -1.0 : 1.0;
+  const double gm1 = kGam - 1.0, ovgm1 = 1.0 / gm1, govgm1 = kGam * ovgm1, ovg = 1.0 / kGam;
+  const double lenScale = a.elem_scalars[(size_t)e * 15 + d];
+  double *out = a.bflux + (size_t)b * 4 * 5 * M2;
+  const int pFast = BFastParam(d), pSlow = 3 - d - pFast;
+  for (int l = threadIdx.x; l < M2; l += NT) {
+    const int li = l / M, lj = l - li * M;
+    double VL[5], VR[5], gx[5], gy[5], gz[5];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) {
+      VL[n] = tr[n * M2 + l];
+      const int mi = a.metric_compat ? n : l;
+      const double dvdr = tr[(5 + n) * M2 + l], dvds = tr[(10 + n) * M2 + l],
+                   dvdt = tr[(15 + n) * M2 + l];
+      gx[n] = dvdr * fm[4 * M2 + mi] + dvds * fm[7 * M2 + mi] + dvdt * fm[10 * M2 + mi];
+      gy[n] = dvdr * fm[5 * M2 + mi] + dvds * fm[8 * M2 + mi] + dvdt * fm[11 * M2 + mi];
+      gz[n] = dvdr * fm[6 * M2 + mi] + dvds * fm[9 * M2 + mi] + dvdt * fm[12 * M2 + mi];
+    }
+    const double nx = factNorm * fm[0 * M2 + l], ny = factNorm * fm[1 * M2 + l],
+                 nz = factNorm * fm[2 * M2 + l];
+    double factU = 1.0, hfMult = 1.0, qWall = 0.0;
+    switch (type) {
+      case VCPG_BC_WALL_HEAT_FLUX:
+      case VCPG_BC_WALL_ISOTHERMAL: {
+        VR[0] = VL[0] - 0.5 * (VL[1] * VL[1] + VL[2] * VL[2] + VL[3] * VL[3]) / VL[4];
+        VR[1] = VR[2] = VR[3] = 0.0;
+        VR[4] = type == VCPG_BC_WALL_HEAT_FLUX ? VL[4] : pres[0];
+        factU = 0.0;
+        if (type == VCPG_BC_WALL_HEAT_FLUX) { hfMult = 0.0; qWall = pres[0]; }
+        break;
+      }
+      case VCPG_BC_WALL_INVISCID: {
+        // ApplyInviscidWallBC (src/BoundaryState.cpp:40-118): the normal part of
+        // V1..V3 removed with the face's unit normal.
+        const double m0 = fm[0 * M2 + l], m1 = fm[1 * M2 + l], m2 = fm[2 * M2 + l];
+        const double Vn = VL[1] * m0 + VL[2] * m1 + VL[3] * m2;
+        VR[0] = VL[0] - 0.5 * Vn * Vn / VL[4];
+        VR[1] = VL[1] - Vn * m0;
+        VR[2] = VL[2] - Vn * m1;
+        VR[3] = VL[3] - Vn * m2;
+        VR[4] = VL[4];
+        factU = 0.0;
+        break;
+      }
+      case VCPG_BC_FARFIELD:
+      case VCPG_BC_INFLOW_SUPERSONIC:
+#pragma unroll
+        for (int n = 0; n < 5; ++n) VR[n] = pres[n];
+        break;
+      case VCPG_BC_INFLOW_SUBSONIC: {
+        // Riemann invariant extrapolated, scaled by the total enthalpy; the
+        // velocity magnitude from the quadratic with the prescribed direction,
+        // the Mach number clipped to 1 (src/BoundaryState.cpp:505-590).
+        const double V4Inv = 1.0 / VL[4];
+        const double u = -V4Inv * VL[1], v = -V4Inv * VL[2], w = -V4Inv * VL[3];
+        const double a2 = -kGam * V4Inv, aa = sqrt(a2);
+        const double un = u * nx + v * ny + w * nz;
+        double riemann = 2.0 * aa * ovgm1 + un;
+        const double H = a2 * ovgm1 + 0.5 * (u * u + v * v + w * w);
+        riemann *= sqrt(pres[1] / H);
+        const double alpha = nx * pres[2] + ny * pres[3] + nz * pres[4];
+        const double qa = 1.0 + 0.5 * gm1 * alpha * alpha;
+        const double qb = -gm1 * alpha * riemann;
+        const double qc = 0.5 * gm1 * riemann * riemann - 2.0 * pres[1];
+        double dd = qb * qb - 4.0 * qa * qc;
+        dd = sqrt(fmax(0.0, dd));
+        double qR = (-qb + dd) / (2.0 * qa);
+        qR = fmax(0.0, qR);
+        double qR2 = qR * qR;
+        double aR2 = gm1 * (pres[1] - 0.5 * qR2);
+        double MR2 = qR2 / aR2;
+        MR2 = fmin(1.0, MR2);
+        const double tmp = 1.0 / (1.0 + 0.5 * gm1 * MR2);
+        aR2 = gm1 * pres[1] * tmp;
+        qR2 = MR2 * aR2;
+        qR = sqrt(qR2);
+        const double pR = pres[0] * pow(tmp, govgm1);
+        const double rhoR = kGam * pR / aR2;
+        const double pRInv = 1.0 / pR;
+        const double sR = log(pR / pow(rhoR, kGam));
+        VR[0] = (kGam - sR) * ovgm1 - 0.5 * pRInv * rhoR * qR2;
+        VR[1] = rhoR * pRInv * qR * pres[2];
+        VR[2] = rhoR * pRInv * qR * pres[3];
+        VR[3] = rhoR * pRInv * qR * pres[4];
+        VR[4] = -rhoR * pRInv;
+        break;
+      }
+      case VCPG_BC_OUTFLOW_SUBSONIC: {
+        // Entropy, tangential velocity and the acoustic Riemann invariant
+        // extrapolated, the back pressure imposed (src/BoundaryState.cpp:736-785).
+        const double V4Inv = 1.0 / VL[4];
+        const double u = -V4Inv * VL[1], v = -V4Inv * VL[2], w = -V4Inv * VL[3];
+        const double eKin = 0.5 * (u * u + v * v + w * w);
+        const double sL = kGam - gm1 * (VL[0] - VL[4] * eKin);
+        const double aa = sqrt(-kGam * V4Inv);
+        const double un = u * nx + v * ny + w * nz;
+        const double riemann = 2.0 * aa * ovgm1 + un;
+        const double pR = pres[0];
+        const double rhoR = pow(pR / exp(sL), ovg);
+        const double aR = sqrt(kGam * pR / rhoR);
+        const double unR = riemann - 2.0 * aR * ovgm1;
+        const double uR = u + (unR - un) * nx, vR = v + (unR - un) * ny, wR = w + (unR - un) * nz;
+        const double pRInv = 1.0 / pR;
+        VR[0] = (kGam - sL) * ovgm1 - 0.5 * pRInv * rhoR * (uR * uR + vR * vR + wR * wR);
+        VR[1] = rhoR * pRInv * uR;
+        VR[2] = rhoR * pRInv * vR;
+        VR[3] = rhoR * pRInv * wR;
+        VR[4] = -rhoR * pRInv;
+        break;
+      }
+      default:  // VCPG_BC_OUTFLOW_SUPERSONIC: the interior state
+#pragma unroll
+        for (int n = 0; n < 5; ++n) VR[n] = VL[n];
+        break;
+    }
+    const double wf = c_ops[SLOT].w[lj] * c_ops[SLOT].w[li];
+    const double area = fm[3 * M2 + l];
+    double flux[5], sx[5], sy[5], sz[5];
+    if (a.riemann == 1)
+      IsmailRoeFlux(VL, VR, nx, ny, nz, wf * area, flux, factU);
+    else
+      RoeFlux(VL, VR, nx, ny, nz, 0.5 * wf * area, flux, factU);
+    ViscousPenaltySymFlux(VL, VR, gx, gy, gz, nx, ny, nz, wf, area, mu,
+                          a.tau_num / lenScale, a.theta_sym, flux, sx, sy, sz, hfMult,
+                          wf * area * qWall);
+#pragma unroll
+    for (int n = 0; n < 5; ++n) {
+      const int mi = a.metric_compat ? n : l;
+      double sym[3];
+#pragma unroll
+      for (int p = 0; p < 3; ++p)
+        sym[p] = sx[n] * fm[(4 + 3 * p) * M2 + mi] + sy[n] * fm[(5 + 3 * p) * M2 + mi] +
+                 sz[n] * fm[(6 + 3 * p) * M2 + mi];
+      out[(0 * 5 + n) * M2 + l] = sym[pFast];
+      out[(1 * 5 + n) * M2 + l] = flux[n];
+      out[(2 * 5 + n) * M2 + l] = sym[d];
+      out[(3 * 5 + n) * M2 + l] = sym[pSlow];
+    }
+  }
+}
+
+// Boundary state and fluxes of one boundary face (characteristic conditions
+// here, the others in WeakBoundaryFlux).
 template <int K, int M, int NT>
 __global__ void __launch_bounds__(NT) BoundaryFluxKernel(const BoundaryArgs a) {
   constexpr int SLOT = Slot<K, M>::value;
@@ -149,6 +307,10 @@ __global__ void __launch_bounds__(NT) BoundaryFluxKernel(const BoundaryArgs a) {
   const double *fm = a.face_metric + ((size_t)e * 6 + f) * 13 * M2;
   const double *tr = a.btrace + (size_t)b * 4 * 5 * M2;
   const double *pres = a.bpresc + (size_t)b * kPrescStride;
+  if (type >= VCPG_BC_WALL_HEAT_FLUX) {   // the same branch for every thread of the CTA
+    WeakBoundaryFlux<K, M, NT>(a, b, e, f, type, mu, fm, tr, pres);
+    return;
+  }
 
   // Boundary-averaged projected Mach number of this block face (sum in element order).
   if (threadIdx.x == 0) {

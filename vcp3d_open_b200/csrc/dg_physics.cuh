@@ -81,7 +81,7 @@ __device__ __forceinline__ void FaceStatePrim(const T *V, T &rho, T &u, T &v,
 template <typename T>
 __device__ __forceinline__ void IsmailRoeFlux(const T *VL, const T *VR, const T nx,
                                               const T ny, const T nz, const T Area,
-                                              T *f) {
+                                              T *f, const T factU = T(1.0)) {
   const T gam = T(kGam), gm1 = gam - T(1.0), ovgm1 = T(1.0) / (gam - T(1.0));
   const T gp1Ovg = (gam + T(1.0)) / gam, gm1Ovg = gm1 / gam;
   const T beta = T(1.0) / T(6.0), alphaMax = T(0.0);
@@ -141,17 +141,18 @@ __device__ __forceinline__ void IsmailRoeFlux(const T *VL, const T *VR, const T 
   const T abv5 = nx * dru + ny * drv + nz * drw - vnAvg * dr;
   const T abv6 = abv3 * abv4 * ova2Avg + abv2 * abv5 * ovaAvg;
   const T abv7 = abv2 * abv4 * ovaAvg + abv3 * abv5;
-  // factUNorm == 1 for internal faces and the boundary faces handled here.
-  T f0 = rhoAvg * vnAvg;
-  T f1 = rhoAvg * vnAvg * vxAvg + p1Avg * nx;
-  T f2 = rhoAvg * vnAvg * vyAvg + p1Avg * ny;
-  T f3 = rhoAvg * vnAvg * vzAvg + p1Avg * nz;
-  T f4 = rhoAvg * vnAvg * HAvg;
-  f0 -= (lam3 * dr + abv6);
-  f1 -= (lam3 * dru + vxAvg * abv6 + nx * abv7);
-  f2 -= (lam3 * drv + vyAvg * abv6 + ny * abv7);
-  f3 -= (lam3 * drw + vzAvg * abv6 + nz * abv7);
-  f4 -= (lam3 * drE + HAvg * abv6 + vnAvg * abv7);
+  // factU (the reference's factUNorm): 1 for internal faces and open boundaries,
+  // 0 for walls (no mass and convective transport through the face).
+  T f0 = factU * rhoAvg * vnAvg;
+  T f1 = factU * rhoAvg * vnAvg * vxAvg + p1Avg * nx;
+  T f2 = factU * rhoAvg * vnAvg * vyAvg + p1Avg * ny;
+  T f3 = factU * rhoAvg * vnAvg * vzAvg + p1Avg * nz;
+  T f4 = factU * rhoAvg * vnAvg * HAvg;
+  f0 -= factU * (lam3 * dr + abv6);
+  f1 -= factU * (lam3 * dru + vxAvg * abv6 + nx * abv7);
+  f2 -= factU * (lam3 * drv + vyAvg * abv6 + ny * abv7);
+  f3 -= factU * (lam3 * drw + vzAvg * abv6 + nz * abv7);
+  f4 -= factU * (lam3 * drE + HAvg * abv6 + vnAvg * abv7);
   f[0] = f0 * Area; f[1] = f1 * Area; f[2] = f2 * Area; f[3] = f3 * Area; f[4] = f4 * Area;
 }
 
@@ -160,7 +161,7 @@ __device__ __forceinline__ void IsmailRoeFlux(const T *VL, const T *VR, const T 
 template <typename T>
 __device__ __forceinline__ void RoeFlux(const T *VL, const T *VR, const T nx,
                                         const T ny, const T nz, const T halfArea,
-                                        T *f) {
+                                        T *f, const T factU = T(1.0)) {
   const T gam = T(kGam), gm1 = gam - T(1.0), ovgm1 = T(1.0) / (gam - T(1.0));
   const T Delta = T(0.001);
   T rhoL, vxL, vyL, vzL, pL, v2L, rhoR, vxR, vyR, vzR, pR, v2R;
@@ -199,7 +200,7 @@ __device__ __forceinline__ void RoeFlux(const T *VL, const T *VR, const T nx,
   const T vnL = vxL * nx + vyL * ny + vzL * nz;
   const T vnR = vxR * nx + vyR * ny + vzR * nz;
   const T pa = halfArea * (pL + pR);
-  const T fact = halfArea;
+  const T fact = factU * halfArea;
   f[0] = fact * (rhoL * vnL + rhoR * vnR - (lam3 * dr + abv6));
   f[1] = fact * (rhoL * vxL * vnL + rhoR * vxR * vnR - (lam3 * dru + uAvg * abv6 + nx * abv7)) + pa * nx;
   f[2] = fact * (rhoL * vyL * vnL + rhoR * vyR * vnR - (lam3 * drv + vAvg * abv6 + ny * abv7)) + pa * ny;
@@ -209,8 +210,10 @@ __device__ __forceinline__ void RoeFlux(const T *VL, const T *VR, const T nx,
 
 // Viscous normal flux, interior penalty and symmetrizing fluxes of one face
 // point for entropy variables: ViscousFluxesFace (src/FluxesFace.cpp:1290-1651,
-// entropy branch, no SGS model, no prescribed heat flux) followed by
-// PenAndSymFluxesSymmVar (src/FluxesFace.cpp:1152-1284).
+// entropy branch, no SGS model) followed by PenAndSymFluxesSymmVar
+// (src/FluxesFace.cpp:1152-1284). hfMult = 0 for a wall with a prescribed heat
+// flux (the conductive terms vanish) and qWallArea = w * area * q_wall is then
+// added to the energy flux between the two, as the reference does.
 //   VL, VR      left/right entropy variables
 //   gx, gy, gz  averaged Cartesian gradients of the entropy variables
 //   nnx..nnz    unit normal times factNorm (-1 when the own element is on the
@@ -223,7 +226,8 @@ __device__ __forceinline__ void ViscousPenaltySymFlux(
     const T *VL, const T *VR, const T *gx, const T *gy, const T *gz,
     const T nnx, const T nny, const T nnz, const T wf,
     const T area, const T mu, const T tau, const T thetaSym, T *f,
-    T *sx, T *sy, T *sz) {
+    T *sx, T *sy, T *sz, const T hfMult = T(1.0), const T qWallArea = T(0.0)) {
+  const T factHFLam = hfMult * T(kFactHFLam);
   const T gm1 = T(kGam) - T(1.0), ovgm1 = T(1.0) / gm1, ov1mg = -ovgm1;
   const T V1 = T(0.5) * (VL[1] + VR[1]);
   const T V2 = T(0.5) * (VL[2] + VR[2]), V3 = T(0.5) * (VL[3] + VR[3]);
@@ -259,7 +263,7 @@ __device__ __forceinline__ void ViscousPenaltySymFlux(
     const T tauxy = muTot * (dudy + dvdx);
     const T tauxz = muTot * (dudz + dwdx);
     const T tauyz = muTot * (dvdz + dwdy);
-    const T factHeatTot = mu * T(kFactHFLam) + T(0.0) * T(kFactHFTurb);
+    const T factHeatTot = mu * factHFLam + T(0.0) * (hfMult * T(kFactHFTurb));
     const T qx = -factHeatTot * dedx, qy = -factHeatTot * dedy, qz = -factHeatTot * dedz;
     f[1] -= tauxx * nx + tauxy * ny + tauxz * nz;
     f[2] -= tauxy * nx + tauyy * ny + tauyz * nz;
@@ -267,6 +271,7 @@ __device__ __forceinline__ void ViscousPenaltySymFlux(
     f[4] -= (u * tauxx + v * tauxy + w * tauxz - qx) * nx +
             (u * tauxy + v * tauyy + w * tauyz - qy) * ny +
             (u * tauxz + v * tauyz + w * tauzz - qz) * nz;
+    if (hfMult == T(0.0)) f[4] += qWallArea;
   }
 
   // Penalty and symmetrizing fluxes (src/FluxesFace.cpp:1180-1283).
@@ -274,7 +279,7 @@ __device__ __forceinline__ void ViscousPenaltySymFlux(
   const T e = pOvRho * ovgm1;
   const T factFlux = pOvRho * wf * area * (mu + T(0.0));
   T nx = factFlux * nnx, ny = factFlux * nny, nz = factFlux * nnz;
-  const T factHeatFlux = (mu * T(kFactHFLam) + T(0.0) * T(kFactHFTurb)) / (mu + T(0.0));
+  const T factHeatFlux = (mu * factHFLam + T(0.0) * (hfMult * T(kFactHFTurb))) / (mu + T(0.0));
   const T abvE = u * u + v * v + w * w + factHeatFlux * e;
   const T K11_11 = lamp2, K11_14 = u * lamp2, K11_22 = T(1.0), K11_24 = v, K11_33 = T(1.0),
                K11_34 = w, K11_44 = abvE + u * u * lamp1;

@@ -25,6 +25,8 @@ namespace vcpg {
 namespace {
 
 constexpr double kGamma = 1.4;
+constexpr double kRGas = 287.058;                      // RGas (include/VCP3D_CurviLinear.hpp:177)
+constexpr double kCp = kGamma * kRGas / (kGamma - 1.0);  // Cp
 constexpr double kEpsThreshold = 1.e-10;  // include/VCP3D_CurviLinear.hpp:137
 
 // Lagrange basis on `nodes` at `pts`: val[j * nP + i] = L_j(pts[i]) and its
@@ -104,6 +106,68 @@ bool IdentifyBoundaryIndices(const double *fm, int M2, int grad[3]) {
 
 }  // namespace
 
+// Non-dimensional prescribed data of a boundary condition through a boundary
+// state, as the subfaces' ConvertPrescribedData / PrescribedDataFromFreeStream
+// produce them (src/SubfaceClasses.cpp:542-620, 739-751, 863-915, 1026-1109,
+// 1169-1180): heat flux / (p_ref u_ref); for the isothermal wall the value
+// -p_ref / (R rho_ref T_wall) that becomes the wall's V4; for the far field and
+// the supersonic inflow the entropy variables of the state; for the subsonic
+// inflow p_t / p_ref, the total enthalpy Cp T_t / u_ref^2 and the unit
+// direction; for the subsonic outflow p / p_ref.
+static void EntropyFromPrimitive(double rho, double u, double v, double w, double p,
+                                 double *V) {
+  const double ovgm1 = 1.0 / (kGamma - 1.0);
+  const double s = std::log(p / std::pow(rho, kGamma));
+  const double pInv = 1.0 / p;
+  V[0] = (kGamma - s) * ovgm1 - 0.5 * pInv * rho * (u * u + v * v + w * w);
+  V[1] = rho * u * pInv;
+  V[2] = rho * v * pInv;
+  V[3] = rho * w * pInv;
+  V[4] = -rho * pInv;
+}
+
+static void WeakBoundaryData(int type, const vcpg_open_boundary &ob, int f,
+                             const vcpg_params &prm, double *pres) {
+  const double rhoRefInv = 1.0 / prm.rho_ref, uRefInv = 1.0 / prm.u_ref,
+               pRefInv = 1.0 / prm.p_ref;
+  switch (type) {
+    case VCPG_BC_WALL_HEAT_FLUX:
+      pres[0] = ob.wall_data[f] * (1.0 / (prm.p_ref * prm.u_ref));
+      break;
+    case VCPG_BC_WALL_ISOTHERMAL:
+      pres[0] = (-prm.p_ref / (kRGas * prm.rho_ref)) / ob.wall_data[f];
+      break;
+    case VCPG_BC_FARFIELD: {
+      const double *q = ob.free_stream;
+      EntropyFromPrimitive(q[0] / prm.rho_ref, q[1] / prm.u_ref, q[2] / prm.u_ref,
+                           q[3] / prm.u_ref, q[4] / prm.p_ref, pres);
+      break;
+    }
+    case VCPG_BC_INFLOW_SUPERSONIC: {
+      const double *q = ob.inflow_super[f];
+      EntropyFromPrimitive(q[0] * rhoRefInv, q[1] * uRefInv, q[2] * uRefInv, q[3] * uRefInv,
+                           q[4] * pRefInv, pres);
+      break;
+    }
+    case VCPG_BC_INFLOW_SUBSONIC: {
+      const double *t = ob.inflow_total[f];
+      const double len2 = t[2] * t[2] + t[3] * t[3] + t[4] * t[4];
+      const double lenInv = 1.0 / std::sqrt(len2);
+      pres[0] = t[0] * pRefInv;
+      pres[1] = t[1] * (kCp * uRefInv * uRefInv);
+      pres[2] = t[2] * lenInv;
+      pres[3] = t[3] * lenInv;
+      pres[4] = t[4] * lenInv;
+      break;
+    }
+    case VCPG_BC_OUTFLOW_SUBSONIC:
+      pres[0] = ob.p_out[f] * pRefInv;
+      break;
+    default:
+      break;
+  }
+}
+
 int BuildOpenBoundary(const vcpg_params &prm, const vcpg_open_boundary &ob,
                       const vcpg_geometry &geom, int pGrid, int dofLocation,
                       const double *gridNodes, OpenBoundaryHost &out, std::string &err) {
@@ -113,7 +177,7 @@ int BuildOpenBoundary(const vcpg_params &prm, const vcpg_open_boundary &ob,
     const int64_t nE = (int64_t)nI * nJ * nK;
     if (!geom.face_metric || !geom.neighbors) { err = "geometry arrays missing"; return VCPG_E_INVALID; }
     for (int f = 0; f < 6; ++f)
-      if (ob.bc[f] < VCPG_BC_NONE || ob.bc[f] > VCPG_BC_INFLOW_TOTAL_NSCBC) {
+      if (ob.bc[f] < VCPG_BC_NONE || ob.bc[f] > VCPG_BC_OUTFLOW_SUPERSONIC) {
         err = "unknown boundary condition on face " + std::to_string(f);
         return VCPG_E_INVALID;
       }
@@ -186,7 +250,7 @@ int BuildOpenBoundary(const vcpg_params &prm, const vcpg_open_boundary &ob,
         c.sigma = ob.inlet_sigma; c.len = ob.inlet_len;
         c.incoming = ob.inlet_incoming ? 1 : 0;
       }
-      if (c.type == VCPG_BC_INFLOW_TOTAL_NSCBC) {
+      if (c.type == VCPG_BC_INFLOW_TOTAL_NSCBC || c.type == VCPG_BC_INFLOW_SUBSONIC) {
         const double *t = ob.inflow_total[f];
         const double dl = std::sqrt(t[2] * t[2] + t[3] * t[3] + t[4] * t[4]);
         if (!(t[0] > 0.0) || !(t[1] > 0.0) || !(dl > 0.0)) {
@@ -195,7 +259,8 @@ int BuildOpenBoundary(const vcpg_params &prm, const vcpg_open_boundary &ob,
           return VCPG_E_INVALID;
         }
       }
-      if (c.type != VCPG_BC_NONE && !(c.len > 0.0)) {
+      const bool weak = c.type >= VCPG_BC_WALL_HEAT_FLUX;
+      if (c.type != VCPG_BC_NONE && !weak && !(c.len > 0.0)) {
         err = "characteristic length must be positive on face " + std::to_string(f);
         return VCPG_E_INVALID;
       }
@@ -203,8 +268,9 @@ int BuildOpenBoundary(const vcpg_params &prm, const vcpg_open_boundary &ob,
         if (geom.neighbors[e * 6 + f] >= 0) continue;
         if (c.type == VCPG_BC_NONE) continue;  // stays -1: flagged by the residual kernel
         const double *fm = geom.face_metric + ((size_t)e * 6 + f) * 13 * M2;
-        int grad[3];
-        if (!IdentifyBoundaryIndices(fm, M2, grad)) {
+        const int fd = f / 2;
+        int grad[3] = {fd, fd == 0 ? 1 : 0, fd == 2 ? 1 : 2};
+        if (!weak && !IdentifyBoundaryIndices(fm, M2, grad)) {
           err = "could not identify the boundary indices of element " + std::to_string(e) +
                 " face " + std::to_string(f) + " (characteristic faces must be aligned with "
                 "a parametric direction)";
@@ -221,7 +287,7 @@ int BuildOpenBoundary(const vcpg_params &prm, const vcpg_open_boundary &ob,
           pres[1] = ob.inflow[f][1] / prm.u_ref;
           pres[2] = ob.inflow[f][2] / prm.u_ref;
           pres[3] = ob.inflow[f][3] / prm.u_ref;
-        } else {
+        } else if (c.type == VCPG_BC_INFLOW_TOTAL_NSCBC) {
           // BCInflowTotalCharacteristicSubfaceClass::ConvertPrescribedData
           // (src/SubfaceClasses.cpp:1577-1608): p_t / p_ref, T_t / (p_ref / rho_ref)
           // (the gas constant stays in the boundary formulas), unit direction.
@@ -232,6 +298,8 @@ int BuildOpenBoundary(const vcpg_params &prm, const vcpg_open_boundary &ob,
           pres[2] = t[2] / dl;
           pres[3] = t[3] / dl;
           pres[4] = t[4] / dl;
+        } else {
+          WeakBoundaryData(c.type, ob, f, prm, pres);
         }
         out.bpresc.insert(out.bpresc.end(), pres, pres + kPrescStride);
         out.nbrCode[e * 6 + f] = -2 - b;

@@ -15,8 +15,7 @@ GPU path supports:
   DetermineNonDimPrimVarFreeStream :991-1192).
 
 Options outside the path (conservative working variables, subgrid-scale and
-wall models, walls, far field and the non-characteristic in- and outflow
-conditions, random or
+wall models, the symmetry plane, random or
 synthetic fluctuations, several subfaces per block face, spatially varying
 prescribed data) raise UnsupportedOption with the option named.
 """
@@ -117,7 +116,17 @@ _ALL_BCS = ("internal1to1", "periodic1to1trans", "bcfarfield", "bcwallisothermal
             "bcoutflownscbc")
 _BC_TO_CASE = {"periodic1to1trans": "periodic", "bcoutflownscbc": "outflow_nscbc",
                "bcinflowstaticnscbc": "inflow_static_nscbc",
-               "bcinflowtotalnscbc": "inflow_total_nscbc"}
+               "bcinflowtotalnscbc": "inflow_total_nscbc",
+               "bcwallheatflux": "wall_heat_flux", "bcwallisothermal": "wall_isothermal",
+               "bcwallinviscid": "wall_inviscid", "bcfarfield": "farfield",
+               "bcinflowsubsonic": "inflow_subsonic", "bcinflowsupersonic": "inflow_supersonic",
+               "bcoutflowsubsonic": "outflow_subsonic",
+               "bcoutflowsupersonic": "outflow_supersonic"}
+_WHY_NOT = {"bcsymmetryplane": "BCSymmetryPlane (the reference terminates on it: not "
+                               "implemented there either)",
+            "bcwallisothermalwm": "BCWallIsothermalWM (wall model)",
+            "bcwallheatfluxwm": "BCWallHeatFluxWM (wall model)",
+            "internal1to1": "Internal1to1 (multi-block grids)"}
 _NSCBC = ("bcinflowstaticnscbc", "bcinflowtotalnscbc", "bcoutflownscbc")
 
 
@@ -545,7 +554,8 @@ def check_supported(pf: ParamFile) -> None:
         if len(subs) != 1:
             raise UnsupportedOption(f"face {face + 1}: {len(subs)} subfaces (one per face runs)")
         if subs[0].kind not in _BC_TO_CASE:
-            raise UnsupportedOption(f"face {face + 1}: boundary condition {subs[0].bc}")
+            why = _WHY_NOT.get(subs[0].kind, subs[0].bc)
+            raise UnsupportedOption(f"face {face + 1}: boundary condition {why}")
     for d in range(3):
         a, b = pf.subfaces[2 * d][0].kind, pf.subfaces[2 * d + 1][0].kind
         if (a == "periodic1to1trans") != (b == "periodic1to1trans"):
@@ -564,20 +574,33 @@ def case_bcs(pf: ParamFile) -> Tuple[str, ...]:
 
 
 def outflow_pressure(pf: ParamFile, face: int) -> float:
+    return _need(pf, face, ("Pressure",), pf.subfaces[face][0].bc)[0]
+
+
+def _need(pf: ParamFile, face: int, names: Sequence[str], what: str) -> Tuple[float, ...]:
     data = pf.prescribed.get((face, 0), {})
-    if "Pressure" not in data:
-        raise ParamFileError(f"face {face + 1}: BCOutflowNSCBC needs a prescribed Pressure")
-    return data["Pressure"]
+    if not all(nm in data for nm in names):
+        raise ParamFileError(f"face {face + 1}: {what} needs the prescribed data "
+                             + ", ".join(names))
+    return tuple(data[nm] for nm in names)
 
 
 def inflow_total(pf: ParamFile, face: int) -> Tuple[float, float, float, float, float]:
-    data = pf.prescribed.get((face, 0), {})
-    names = ("TotalPressure", "TotalTemperature", "VelocityDirX", "VelocityDirY",
-             "VelocityDirZ")
-    if not all(nm in data for nm in names):
-        raise ParamFileError(f"face {face + 1}: BCInflowTotalNSCBC needs TotalPressure, "
-                             "TotalTemperature and VelocityDirX/Y/Z")
-    return tuple(data[nm] for nm in names)
+    """Total conditions of BCInflowTotalNSCBC or BCInflowSubsonic (the latter's
+    density/velocity data set is not run: its boundary state uses the totals)."""
+    return _need(pf, face, ("TotalPressure", "TotalTemperature", "VelocityDirX",
+                            "VelocityDirY", "VelocityDirZ"), pf.subfaces[face][0].bc)
+
+
+def wall_value(pf: ParamFile, face: int) -> float:
+    kind = pf.subfaces[face][0].kind
+    name = "HeatFlux" if kind == "bcwallheatflux" else "Temperature"
+    return _need(pf, face, (name,), pf.subfaces[face][0].bc)[0]
+
+
+def inflow_supersonic(pf: ParamFile, face: int) -> Tuple[float, ...]:
+    return _need(pf, face, ("Density", "VelocityX", "VelocityY", "VelocityZ", "Pressure"),
+                 "BCInflowSupersonic")
 
 
 def inflow_static(pf: ParamFile, face: int) -> Tuple[float, float, float, float]:

@@ -140,12 +140,19 @@ def load_case(pf: ParamFile) -> cases.CaseData:
         cons = np.ascontiguousarray(_add_pressure_pulse(pf, xyz, cons.transpose(1, 0, 2))
                                     .transpose(1, 0, 2))
     bcs = param_file.case_bcs(pf)
-    prescribed_p = tuple(param_file.outflow_pressure(pf, f) if b == "outflow_nscbc" else 0.0
+    prescribed_p = tuple(param_file.outflow_pressure(pf, f)
+                         if b in ("outflow_nscbc", "outflow_subsonic") else 0.0
                          for f, b in enumerate(bcs))
     prescribed_in = tuple(param_file.inflow_static(pf, f) if b == "inflow_static_nscbc"
                           else (0.0, 0.0, 0.0, 0.0) for f, b in enumerate(bcs))
-    prescribed_tot = tuple(param_file.inflow_total(pf, f) if b == "inflow_total_nscbc"
+    prescribed_tot = tuple(param_file.inflow_total(pf, f)
+                           if b in ("inflow_total_nscbc", "inflow_subsonic")
                            else (0.0, 0.0, 1.0, 0.0, 0.0) for f, b in enumerate(bcs))
+    wall_data = tuple(param_file.wall_value(pf, f)
+                      if b in ("wall_heat_flux", "wall_isothermal") else 0.0
+                      for f, b in enumerate(bcs))
+    prescribed_sup = tuple(param_file.inflow_supersonic(pf, f) if b == "inflow_supersonic"
+                           else (1.0, 0.0, 0.0, 0.0, 1.0) for f, b in enumerate(bcs))
     sponge = tuple(r[0] for r in pf.sponge) if pf.sponge else (0,) * 6
     sponge_state = None
     if any(sponge):
@@ -166,7 +173,8 @@ def load_case(pf: ParamFile) -> cases.CaseData:
         sponge_sigma=tuple(r[1] for r in pf.sponge) if pf.sponge else 20.0,
         sponge_alpha=tuple(r[2] for r in pf.sponge) if pf.sponge else 2.0,
         cml=pf.cml and any(sponge), prescribed_p=prescribed_p, prescribed_inflow=prescribed_in,
-        prescribed_total=prescribed_tot, sponge_state=sponge_state)
+        prescribed_total=prescribed_tot, sponge_state=sponge_state, wall_data=wall_data,
+        prescribed_super=prescribed_sup, free_stream=tuple(ref.free_stream))
     refc = cases.RefConditions(ref.p_ref, ref.rho_ref, ref.u_ref, ref.mu_nondim, speed, vel_dir)
     return cases.CaseData(spec, refc, grid, nodes, xyz, np.ascontiguousarray(cons))
 

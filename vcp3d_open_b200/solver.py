@@ -111,7 +111,13 @@ def open_boundary(case: CaseData) -> capi.OpenBoundary:
     ob = capi.OpenBoundary()
     codes = {"periodic": capi.BC_NONE, "outflow_nscbc": capi.BC_OUTFLOW_NSCBC,
              "inflow_static_nscbc": capi.BC_INFLOW_STATIC_NSCBC,
-             "inflow_total_nscbc": capi.BC_INFLOW_TOTAL_NSCBC}
+             "inflow_total_nscbc": capi.BC_INFLOW_TOTAL_NSCBC,
+             "wall_heat_flux": capi.BC_WALL_HEAT_FLUX, "wall_isothermal": capi.BC_WALL_ISOTHERMAL,
+             "wall_inviscid": capi.BC_WALL_INVISCID, "farfield": capi.BC_FARFIELD,
+             "inflow_subsonic": capi.BC_INFLOW_SUBSONIC,
+             "inflow_supersonic": capi.BC_INFLOW_SUPERSONIC,
+             "outflow_subsonic": capi.BC_OUTFLOW_SUBSONIC,
+             "outflow_supersonic": capi.BC_OUTFLOW_SUPERSONIC}
     p_out, rho_in, vel_in = prescribed_values(s, ref)
     per_face = lambda v, f: v[f] if isinstance(v, (tuple, list)) else v
     for f, bc in enumerate(s.bc):
@@ -119,10 +125,17 @@ def open_boundary(case: CaseData) -> capi.OpenBoundary:
         ob.p_out[f] = s.prescribed_p[f] if s.prescribed_p else p_out
         inflow = s.prescribed_inflow[f] if s.prescribed_inflow else (rho_in, *vel_in)
         ob.inflow[f][0], ob.inflow[f][1], ob.inflow[f][2], ob.inflow[f][3] = inflow
-        if bc == "inflow_total_nscbc":
+        if bc in ("inflow_total_nscbc", "inflow_subsonic"):
             total = s.prescribed_total[f] if s.prescribed_total else total_inflow_values(s)
             for q in range(5):
                 ob.inflow_total[f][q] = total[q]
+        if bc in ("wall_heat_flux", "wall_isothermal"):
+            ob.wall_data[f] = (s.wall_data[f] if s.wall_data else
+                               (0.0 if bc == "wall_heat_flux" else s.t_inf))
+        if bc == "inflow_supersonic":
+            sup = s.prescribed_super[f] if s.prescribed_super else (rho_in, *vel_in, p_out)
+            for q in range(5):
+                ob.inflow_super[f][q] = sup[q]
         ob.sponge_elems[f] = s.sponge[f]
         ob.sponge_sigma[f] = per_face(s.sponge_sigma, f)
         ob.sponge_alpha[f] = per_face(s.sponge_alpha, f)
@@ -134,6 +147,8 @@ def open_boundary(case: CaseData) -> capi.OpenBoundary:
     ob.cml = 1 if s.cml else 0
     ob.sponge_state[:] = (list(s.sponge_state) if s.sponge_state else
                           [rho_in, vel_in[0], vel_in[1], vel_in[2], p_out])
+    ob.free_stream[:] = (list(s.free_stream) if s.free_stream else
+                         [rho_in, vel_in[0], vel_in[1], vel_in[2], p_out])
     return ob
 
 
