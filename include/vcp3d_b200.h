@@ -114,6 +114,17 @@ int vcpg_setup_geometry(const vcpg_params *params, int32_t p_grid, int32_t dof_l
                         double *basis_center, double *vol_metric, double *face_metric,
                         double *elem_scalars, int32_t *neighbors);
 
+/* The same set-up with the metric terms computed on the current CUDA device (one
+ * CTA per element; the same doubles as vcpg_setup_geometry, which runs the
+ * identical arithmetic on the host). Same arguments and outputs; the grid nodes
+ * go to the device in passes of at most about 1 GiB of buffers. */
+int vcpg_setup_geometry_device(const vcpg_params *params, int32_t p_grid, int32_t dof_location,
+                               const int32_t periodic[3], const double *grid_nodes,
+                               double *leg_int, double *dleg_int, double *leg_face,
+                               double *dleg_face, double *w_int, double *leg_dofs,
+                               double *basis_center, double *vol_metric, double *face_metric,
+                               double *elem_scalars, int32_t *neighbors);
+
 /* Converts dimensional conservative variables at the nodal DOFs
  * ([n_elem][5][K^3]) to modal entropy-variable coefficients, as
  * SolverClass::ReadRestartSolution does (src/SolverClass.cpp:3310-3366).

@@ -16,8 +16,11 @@ ROOT = os.path.dirname(PKG)
 BUILD = os.path.join(ROOT, "_build")
 LIB = os.path.join(PKG, "libvcp3d_b200.so")
 SOURCES = ["kernels.cu", "capi.cu", "capi_setup.cpp", "host_setup.cpp", "open_boundary.cpp",
-           "ensemble.cu",
+           "ensemble.cu", "geometry.cu",
            "noalloc.cu"]
+# Per-file flags: the device metric terms round every product and sum separately,
+# as the host set-up does (explicit fma calls stay fused).
+EXTRA = {"geometry.cu": ["-fmad=false"]}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
          "-diag-suppress", "177"]
@@ -40,8 +43,8 @@ def _compile(src: str, force: bool) -> str:
     if (not force and os.path.exists(obj)
             and os.path.getmtime(obj) >= max(os.path.getmtime(path), _headers_mtime())):
         return obj
-    cmd = [_nvcc(), *ARCH, *FLAGS, "-x", "cu" if src.endswith(".cu") else "c++", "-c", path,
-           "-o", obj]
+    cmd = [_nvcc(), *ARCH, *FLAGS, *EXTRA.get(src, []), "-x", "cu" if src.endswith(".cu") else "c++",
+           "-c", path, "-o", obj]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError(f"nvcc failed for {src}:\n{res.stdout}\n{res.stderr}")

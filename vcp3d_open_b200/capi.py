@@ -25,6 +25,7 @@ BC_NONE, BC_OUTFLOW_NSCBC, BC_INFLOW_STATIC_NSCBC, BC_INFLOW_TOTAL_NSCBC = 0, 1,
 # Every symbol include/vcp3d_b200.h declares.
 EXPORTED = [
     "vcpg_create", "vcpg_destroy", "vcpg_last_error", "vcpg_setup_geometry",
+    "vcpg_setup_geometry_device",
     "vcpg_nodal_conservative_to_modal", "vcpg_set_state", "vcpg_get_state",
     "vcpg_get_residual", "vcpg_residual", "vcpg_get_raw_residual", "vcpg_time_step",
     "vcpg_step", "vcpg_synchronization_step", "vcpg_sync", "vcpg_stream", "vcpg_launch_count", "vcpg_stats",
@@ -102,6 +103,8 @@ def load() -> C.CDLL:
     lib.vcpg_last_error.argtypes = [hp]
     lib.vcpg_last_error.restype = C.c_char_p
     lib.vcpg_setup_geometry.argtypes = [C.POINTER(Params), C.c_int32, C.c_int32, ip, dp, dp, dp,
+                                        dp, dp, dp, dp, dp, dp, dp, dp, ip]
+    lib.vcpg_setup_geometry_device.argtypes = [C.POINTER(Params), C.c_int32, C.c_int32, ip, dp, dp, dp,
                                         dp, dp, dp, dp, dp, dp, dp, dp, ip]
     lib.vcpg_nodal_conservative_to_modal.argtypes = [C.POINTER(Params), dp, dp, dp, C.c_int64]
     for name in ("vcpg_set_state", "vcpg_get_state", "vcpg_get_residual", "vcpg_get_raw_residual"):

@@ -42,27 +42,7 @@ int vcpg_setup_geometry(const vcpg_params *params, int32_t p_grid, int32_t dof_l
                                  params->n_poly);
       if (elem_scalars) std::memcpy(elem_scalars + e * 15, sc, sizeof(sc));
     }
-    if (neighbors) {
-      const int n[3] = {nI, nJ, nK};
-      for (int k = 0; k < nK; ++k)
-        for (int j = 0; j < nJ; ++j)
-          for (int i = 0; i < nI; ++i) {
-            const int64_t e = ((int64_t)k * nJ + j) * nI + i;
-            const int idx[3] = {i, j, k};
-            for (int d = 0; d < 3; ++d)
-              for (int s = 0; s < 2; ++s) {
-                int c[3] = {idx[0], idx[1], idx[2]};
-                c[d] += s == 0 ? -1 : 1;
-                int32_t nb = -1;
-                if (c[d] < 0 || c[d] >= n[d]) {
-                  if (periodic && periodic[d]) c[d] = (c[d] + n[d]) % n[d];
-                  else c[d] = -1;
-                }
-                if (c[d] >= 0) nb = (int32_t)(((int64_t)c[2] * nJ + c[1]) * nI + c[0]);
-                neighbors[e * 6 + 2 * d + s] = nb;
-              }
-          }
-    }
+    if (neighbors) vcpg::host::BlockNeighbors(nI, nJ, nK, periodic, neighbors);
   } catch (const std::exception &) {
     return VCPG_E_INVALID;
   }

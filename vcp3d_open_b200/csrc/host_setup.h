@@ -1,6 +1,7 @@
 // Host-side pre-processing of the hot path's inputs (see host_setup.cpp).
 #pragma once
 
+#include <cstdint>
 #include <vector>
 
 namespace vcpg {
@@ -32,6 +33,10 @@ StdElement BuildStdElement(int K, int M, int Kg, int dofLgl, int gridLgl);
 // vol[10][M^3] (J, dr/dx .. dt/dz), face[6][13][M^2], scalars[15].
 void ElementMetrics(const StdElement &se, const double *gridNodes, double *vol, double *face,
                     double *scalars, int nPoly);
+
+// Face neighbours of a single block, elements i fastest: [nE][6] (iMin, iMax,
+// jMin, jMax, kMin, kMax), -1 on a non-periodic block face.
+void BlockNeighbors(int nI, int nJ, int nK, const int32_t periodic[3], int32_t *neighbors);
 
 }  // namespace host
 }  // namespace vcpg

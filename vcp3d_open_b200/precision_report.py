@@ -47,7 +47,7 @@ def run(workload: str, steps: int, every: int, scheme: int = capi.LSRK4) -> dict
     spec = workloads.make_spec(workload)
     case = cases.build_case(spec)
     p64 = solver.make_params(case, metric_compat=True, precision=capi.FP64)
-    disc = solver.setup_discretization(case, p64)
+    disc = solver.setup_discretization(case, p64, device=True)
     s64 = solver.create(case, precision=capi.FP64, disc=disc)
     s32 = solver.create(case, precision=capi.MIXED, disc=disc)
     u0 = s64.get_state()

@@ -52,7 +52,7 @@ def run(workload: str = "pulse40_p4_lsrk4", steps: int = 2000, every: int = 100,
     spec = workloads.make_spec(workload)
     case = cases.build_case(spec)
     p64 = solver.make_params(case, precision=capi.FP64)
-    disc = solver.setup_discretization(case, p64)
+    disc = solver.setup_discretization(case, p64, device=True)
     s64 = solver.create(case, precision=capi.FP64, disc=disc)
     s32 = solver.create(case, precision=capi.MIXED, disc=disc) if mixed else None
     mask = probe_mask(case.dof_xyz, box_lo, box_hi)

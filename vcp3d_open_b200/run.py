@@ -249,7 +249,7 @@ def run(path: str, precision: int = capi.FP64, steps: Optional[int] = None,
     pf = param_file.read(path)
     case = load_case(pf)
     params = solver.make_params(case, precision=precision)
-    disc = solver.setup_discretization(case, params)
+    disc = solver.setup_discretization(case, params, device=True)
     s = solver.Solver(params, disc)
     files, history = [], []
     try:

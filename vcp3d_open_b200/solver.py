@@ -64,9 +64,11 @@ def make_params(case: CaseData, metric_compat: bool = True,
 
 
 def setup_discretization(case: CaseData, params: capi.Params,
-                         periodic=None) -> Discretization:
-    """Operators and metric terms from the case grid (host C++ in the library).
-    periodic defaults to the case's periodic directions."""
+                         periodic=None, device: bool = False) -> Discretization:
+    """Operators and metric terms from the case grid: host C++ in the library
+    (vcpg_setup_geometry) or, with device=True, the same arithmetic on the GPU
+    (vcpg_setup_geometry_device). periodic defaults to the case's periodic
+    directions."""
     if periodic is None:
         periodic = case.spec.periodic
     lib = capi.load()
@@ -81,13 +83,15 @@ def setup_discretization(case: CaseData, params: capi.Params,
         neighbors=np.zeros((nE, 6), dtype=np.int32))
     per = np.asarray(periodic, dtype=np.int32)
     nodes = np.ascontiguousarray(case.elem_nodes, dtype=np.float64)
-    rc = lib.vcpg_setup_geometry(
+    setup = lib.vcpg_setup_geometry_device if device else lib.vcpg_setup_geometry
+    rc = setup(
         C.byref(params), s.p_grid, 1, capi.ptr(per), capi.ptr(nodes), capi.ptr(d.leg_int),
         capi.ptr(d.dleg_int), capi.ptr(d.leg_face), capi.ptr(d.dleg_face), capi.ptr(d.w_int),
         capi.ptr(d.leg_dofs), capi.ptr(d.basis_center), capi.ptr(d.vol_metric),
         capi.ptr(d.face_metric), capi.ptr(d.elem_scalars), capi.ptr(d.neighbors))
     if rc != capi.VCPG_OK:
-        raise capi.VcpgError(rc, "vcpg_setup_geometry failed")
+        raise capi.VcpgError(rc, ("vcpg_setup_geometry_device" if device else
+                                  "vcpg_setup_geometry") + " failed")
     return d
 
 
@@ -276,15 +280,16 @@ class Solver:
 
 
 def create(case: CaseData, metric_compat: bool = True, precision: int = capi.FP64,
-           disc: Optional[Discretization] = None) -> Solver:
-    """Set-up + handle + initial state for a generated case.
+           disc: Optional[Discretization] = None, device_setup: bool = False) -> Solver:
+    """Set-up + handle + initial state for a generated case (device_setup: the
+    metric terms computed on the GPU).
 
     precision: capi.FP64 (the reference's arithmetic) or capi.MIXED (residual in
     FP32, state and time integration in FP64). A Discretization of the same case
     may be passed to share the host-side set-up between handles."""
     params = make_params(case, metric_compat=metric_compat, precision=precision)
     if disc is None:
-        disc = setup_discretization(case, params)
+        disc = setup_discretization(case, params, device=device_setup)
     s = Solver(params, disc)
     if case.spec.is_open:
         s.set_open_boundary(case)
