@@ -50,6 +50,9 @@ enum vcpg_status {
 enum vcpg_riemann { VCPG_ROE = 0, VCPG_ISMAIL_ROE = 1 };
 enum vcpg_precision { VCPG_FP64 = 0, VCPG_MIXED = 1 };
 enum vcpg_scheme { VCPG_SSPRK3 = 0, VCPG_LSRK4 = 1 };
+/* "Subgrid scale model" (src/SGSModel.cpp): WALE (C_w = 0.325) or Vreman (c = 0.07),
+ * with the element's LES length scale (elem_scalars[3]). */
+enum vcpg_sgs { VCPG_SGS_NONE = 0, VCPG_SGS_WALE = 1, VCPG_SGS_VREMAN = 2 };
 
 /* Face numbering used by every per-face array: 0 iMin, 1 iMax, 2 jMin, 3 jMax, 4 kMin, 5 kMax. */
 
@@ -71,6 +74,8 @@ typedef struct vcpg_params {
   double cfl;                 /* "CFL number"                                        */
   double mu;                  /* non-dimensional laminar viscosity                   */
   double p_ref, u_ref, rho_ref; /* reference conditions (dimensional)                */
+  int32_t sgs_model;          /* enum vcpg_sgs; a model needs ops->dleg_dofs and
+                                 geom->vol_metric_dofs (vcpg_setup_nodal_metrics)  */
 } vcpg_params;
 
 /* Standard-element operators (StandardElementClass, src/StandardElementClass.cpp:105-911). */
@@ -82,6 +87,8 @@ typedef struct vcpg_operators {
   const double *w_int;        /* [M]    1-D Gauss weights                                   */
   const double *leg_dofs;     /* [K][K] basis at the 1-D nodal DOFs (time-step conversion)  */
   const double *basis_center; /* [K^3]  3-D basis at the element centre (CG preconditioner) */
+  const double *dleg_dofs;    /* [K][K] derivative of basis k at nodal DOF i (time step with
+                                 an SGS model; may be NULL without one)                    */
 } vcpg_operators;
 
 /* Per-element geometry (ElementClass::ComputeMetricTerms, src/ElementClass.cpp:1027-1407). */
@@ -91,6 +98,9 @@ typedef struct vcpg_geometry {
   const double *elem_scalars; /* [n_elem][15]: lenI lenJ lenK lenLES lenVol volElem,
                                  averaged unit normals of the i, j, k directions (9)       */
   const int32_t *neighbors;   /* [n_elem][6]: neighbour element per face, -1 = boundary    */
+  const double *vol_metric_dofs; /* [n_elem][10][K^3]: J and the inverse-Jacobian terms at
+                                 the nodal solution DOFs (mVolMetricSolDOFs); needed with
+                                 an SGS model (time step), may be NULL without one       */
 } vcpg_geometry;
 
 typedef struct vcpg_handle vcpg_handle;
@@ -113,6 +123,14 @@ int vcpg_setup_geometry(const vcpg_params *params, int32_t p_grid, int32_t dof_l
                         double *dleg_face, double *w_int, double *leg_dofs,
                         double *basis_center, double *vol_metric, double *face_metric,
                         double *elem_scalars, int32_t *neighbors);
+
+/* Metric terms at the nodal solution DOFs (ElementClass::ComputeCoorNodalSolDOFs,
+ * src/ElementClass.cpp:816-918) and the derivative of the modal basis at the 1-D
+ * nodal DOFs: the inputs an SGS model's time step needs. vol_metric_dofs
+ * [n_elem][10][K^3], dleg_dofs [K][K]; host computation. */
+int vcpg_setup_nodal_metrics(const vcpg_params *params, int32_t p_grid, int32_t dof_location,
+                             const double *grid_nodes, double *dleg_dofs,
+                             double *vol_metric_dofs);
 
 /* The same set-up with the metric terms computed on the current CUDA device (one
  * CTA per element; the same doubles as vcpg_setup_geometry, which runs the

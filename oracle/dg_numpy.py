@@ -15,6 +15,8 @@ Follows, function by function:
                                                               src/SolverClass.cpp:3616-3732
   mass solve        CG_EntropyVarMassMatrix                   src/CG_MassMatrix.cpp:250-504
   time step         ElementClass::ComputeTimeStep             src/ElementClass.cpp:1522-1644
+  nodal gradients   ComputeVelocityGradientsNodalDOFs         src/ElementClass.cpp:1647-1795
+  SGS models        CWALEModel / CVremanModel::EddyViscosity  src/SGSModel.cpp:35-202
   Runge-Kutta       ExecuteTimeSynchronizationStep stages     src/SolverClass.cpp:2368-2396
 The metric-index behaviour of the reference (gradient and symmetrizing-flux
 transforms take the metric of point l = variable index) is reproduced when
@@ -32,7 +34,10 @@ import numpy as np
 GAM = 1.4
 GM1 = GAM - 1.0
 FHF_LAM = GAM / 0.72
+FHF_TURB = GAM / 0.90          # turbulent Prandtl number 0.9
 LAM_OVER_MU = -2.0 / 3.0
+EPS_SMALL = 1e-30
+SGS_NONE, SGS_WALE, SGS_VREMAN = 0, 1, 2
 
 
 @dataclasses.dataclass
@@ -60,6 +65,9 @@ class Disc:
     rho_ref: float
     cfl: float
     n_poly: int
+    sgs: int = SGS_NONE      # subgrid-scale model
+    dlegdof: np.ndarray = None   # [K, K] basis derivative at the 1-D nodal DOFs
+    vmd: np.ndarray = None       # [nE, 10, K^3] metric terms at the nodal DOFs
 
 
 # ---------------------------------------------------------------------------
@@ -119,6 +127,41 @@ def _cart_grad(dr, ds, dt, met, off, compat):
     return gx, gy, gz
 
 
+def eddy_viscosity(model, length, rho, G):
+    """Dynamic eddy viscosity of the WALE (C_w = 0.325) or Vreman (c = 0.07)
+    model, src/SGSModel.cpp:35-202. G[i][j] = d u_i / d x_j, length = the
+    element's LES length scale (broadcastable against rho)."""
+    if model == SGS_NONE:
+        return np.zeros_like(rho)
+    if model == SGS_WALE:
+        lw = 0.325 * length
+        S = [[0.5 * (G[i][j] + G[j][i]) for j in range(3)] for i in range(3)]
+        G2 = [[G[i][0] * G[0][j] + G[i][1] * G[1][j] + G[i][2] * G[2][j] for j in range(3)]
+              for i in range(3)]
+        Sd = [[0.5 * (G2[i][j] + G2[j][i]) for j in range(3)] for i in range(3)]
+        tr = (Sd[0][0] + Sd[1][1] + Sd[2][2]) / 3.0
+        for i in range(3):
+            Sd[i][i] = Sd[i][i] - tr
+        sumS = (S[0][0] ** 2 + S[1][1] ** 2 + S[2][2] ** 2
+                + 2.0 * (S[0][1] ** 2 + S[0][2] ** 2 + S[1][2] ** 2))
+        sumSd = (Sd[0][0] ** 2 + Sd[1][1] ** 2 + Sd[2][2] ** 2
+                 + 2.0 * (Sd[0][1] ** 2 + Sd[0][2] ** 2 + Sd[1][2] ** 2))
+        sd32 = sumSd * np.sqrt(sumSd)
+        denom = sumS * sumS * np.sqrt(sumS) + np.sqrt(sd32 * sumSd)
+        return rho * (lw * lw) * sd32 / np.maximum(denom, EPS_SMALL)
+    # Vreman: alpha = G with its trace removed from the diagonal.
+    tr = (G[0][0] + G[1][1] + G[2][2]) / 3.0
+    a = [[G[i][j] - (tr if i == j else 0.0) for j in range(3)] for i in range(3)]
+    l2 = length * length
+    b = [[l2 * (a[i][0] * a[j][0] + a[i][1] * a[j][1] + a[i][2] * a[j][2]) for j in range(3)]
+         for i in range(3)]
+    B = (b[0][0] * b[1][1] - b[0][1] ** 2 + b[0][0] * b[2][2] - b[0][2] ** 2
+         + b[1][1] * b[2][2] - b[1][2] ** 2)
+    B = np.maximum(B, 0.0)
+    denom = sum(a[i][j] ** 2 for i in range(3) for j in range(3))
+    return rho * 0.07 * np.sqrt(B / np.maximum(denom, EPS_SMALL))
+
+
 def volume_residual(U, d: Disc, compat=True):
     """Volume part of the residual and the CG point data (src/ElementClass.cpp:3809-4443)."""
     nE, M = U.shape[0], d.M
@@ -139,12 +182,14 @@ def volume_residual(U, d: Disc, compat=True):
     W3 = _weights3(d.w).reshape(MD)
     J = d.vol[:, 0]
     weight = -J * W3
-    mu = d.mu
+    eddy = eddy_viscosity(d.sgs, d.scal[:, 3:4], rho, [[dudx, dudy, dudz], [dvdx, dvdy, dvdz],
+                                                       [dwdx, dwdy, dwdz]])
+    mu = d.mu + eddy
     ru, rv, rw = rho * u, rho * v, rho * w
     div = LAM_OVER_MU * (dudx + dvdy + dwdz)
     txx, tyy, tzz = mu * (2 * dudx + div), mu * (2 * dvdy + div), mu * (2 * dwdz + div)
     txy, txz, tyz = mu * (dudy + dvdx), mu * (dudz + dwdx), mu * (dvdz + dwdy)
-    kq = mu * FHF_LAM
+    kq = d.mu * FHF_LAM + eddy * FHF_TURB
     qx, qy, qz = -kq * dedx, -kq * dedy, -kq * dedz
     fx = [ru, ru * u - txx + p, rv * u - txy, rw * u - txz,
           (rE + p) * u - (u * txx + v * txy + w * txz - qx)]
@@ -160,7 +205,7 @@ def volume_residual(U, d: Disc, compat=True):
                  .reshape(nE, 5, M, M, M))
     R = (vol_project(F[0], d.leg, d.leg, d.dleg) + vol_project(F[1], d.leg, d.dleg, d.leg)
          + vol_project(F[2], d.dleg, d.leg, d.leg))
-    cg = dict(rho=rho, u=u, v=v, w=w, p=p, rE=rE, eKin=eKin, JW=J * W3)
+    cg = dict(rho=rho, u=u, v=v, w=w, p=p, rE=rE, eKin=eKin, JW=J * W3, eddy_max=eddy.max())
     return R, cg
 
 
@@ -281,15 +326,24 @@ def roe(VL, VR, nx, ny, nz, halfArea):
                         - (l3 * drE + H * b6 + vn * b7))]
 
 
-def viscous_face(VL, VR, gx, gy, gz, nnx, nny, nnz, wf, area, mu, tau, theta, f):
+def viscous_face(VL, VR, gx, gy, gz, nnx, nny, nnz, wf, area, mu_lam, tau, theta, f,
+                 sgs=SGS_NONE, len_les=None):
     """ViscousFluxesFace + PenAndSymFluxesSymmVar (src/FluxesFace.cpp:1152-1651), entropy
-    variables, no SGS model. Updates f in place; returns Cartesian symmetrizing fluxes."""
+    variables; the eddy viscosity of the averaged state when an SGS model is used.
+    Updates f in place; returns Cartesian symmetrizing fluxes and the eddy viscosity."""
     V = [0.5 * (VL[n] + VR[n]) for n in range(5)]
     V4Inv = 1.0 / V[4]
     u, v, w = -V4Inv * V[1], -V4Inv * V[2], -V4Inv * V[3]
     du = [-V4Inv * (g[1] + u * g[4]) for g in (gx, gy, gz)]
     dv = [-V4Inv * (g[2] + v * g[4]) for g in (gx, gy, gz)]
     dw = [-V4Inv * (g[3] + w * g[4]) for g in (gx, gy, gz)]
+    if sgs != SGS_NONE:
+        rho = (-V[4] * np.exp(GAM - GM1 * (V[0] - V[4] * 0.5 * (u * u + v * v + w * w)))) \
+            ** (-1.0 / GM1)
+        eddy = eddy_viscosity(sgs, len_les, rho, [du, dv, dw])
+    else:
+        eddy = np.zeros_like(u)
+    mu = mu_lam + eddy
     fe = V4Inv * V4Inv / GM1
     de = [fe * g[4] for g in (gx, gy, gz)]
     dV = [VL[n] - VR[n] for n in range(5)]
@@ -299,7 +353,7 @@ def viscous_face(VL, VR, gx, gy, gz, nnx, nny, nnz, wf, area, mu, tau, theta, f)
     div = LAM_OVER_MU * (du[0] + dv[1] + dw[2])
     txx, tyy, tzz = mu * (2 * du[0] + div), mu * (2 * dv[1] + div), mu * (2 * dw[2] + div)
     txy, txz, tyz = mu * (du[1] + dv[0]), mu * (du[2] + dw[0]), mu * (dv[2] + dw[1])
-    kq = mu * FHF_LAM
+    kq = mu_lam * FHF_LAM + eddy * FHF_TURB
     qx, qy, qz = -kq * de[0], -kq * de[1], -kq * de[2]
     f[1] = f[1] - (txx * nx + txy * ny + txz * nz)
     f[2] = f[2] - (txy * nx + tyy * ny + tyz * nz)
@@ -309,7 +363,7 @@ def viscous_face(VL, VR, gx, gy, gz, nnx, nny, nnz, wf, area, mu, tau, theta, f)
     lam, lp1, lp2 = LAM_OVER_MU, LAM_OVER_MU + 1, LAM_OVER_MU + 2
     e = pOvRho / GM1
     ff = pOvRho * wf * area * mu
-    abvE = u * u + v * v + w * w + FHF_LAM * e
+    abvE = u * u + v * v + w * w + (mu_lam * FHF_LAM + eddy * FHF_TURB) / mu * e
     un = u * nnx + v * nny + w * nnz
     dVn = dV[1] * nnx + dV[2] * nny + dV[3] * nnz
     tt = tau * ff
@@ -340,7 +394,7 @@ def viscous_face(VL, VR, gx, gy, gz, nnx, nny, nnz, wf, area, mu, tau, theta, f)
           -(lam * d1 + u * lam * d4) * nx - (lam * d2 + v * lam * d4) * ny - (lp2 * d3 + K33[3] * d4) * nz,
           -(w * lam * d1 + u * d3 + u * w * lp1 * d4) * nx - (w * lam * d2 + v * d3 + v * w * lp1 * d4) * ny
           - (u * d1 + v * d2 + K33[3] * d3 + K33[4] * d4) * nz]
-    return sx, sy, sz
+    return sx, sy, sz, eddy
 
 
 def _face_expand(B, d: Disc, dd, g, q):
@@ -387,9 +441,10 @@ def face_residual(U, d: Disc, compat=True):
             f = roe(VL, VR, nx, ny, nz, 0.5 * wf * area)
         lenScale = np.minimum(d.scal[:, dd], d.scal[L, dd])
         tau = d.tau_num / lenScale[:, None]
-        sx, sy, sz = viscous_face(VL, VR, [gx[:, n] for n in range(5)], [gy[:, n] for n in range(5)],
-                                  [gz[:, n] for n in range(5)], nx, ny, nz, wf, area, d.mu, tau,
-                                  d.theta, f)
+        len_les = 0.5 * (d.scal[:, 3] + d.scal[L, 3])[:, None]
+        sx, sy, sz, _ = viscous_face(VL, VR, [gx[:, n] for n in range(5)],
+                                     [gy[:, n] for n in range(5)], [gz[:, n] for n in range(5)],
+                                     nx, ny, nz, wf, area, d.mu, tau, d.theta, f, d.sgs, len_les)
         flux = np.stack(f, axis=1)
         SX, SY, SZ = np.stack(sx, axis=1), np.stack(sy, axis=1), np.stack(sz, axis=1)
 
@@ -504,16 +559,40 @@ def time_step(U, d: Disc):
     li, lj, lk = 1.0 / sc[:, 0:1], 1.0 / sc[:, 1:2], 1.0 / sc[:, 2:3]
     muDim = d.mu * d.p_ref / d.u_ref
     radVisNu = max(max(1.0, 2.0 + LAM_OVER_MU), FHF_LAM) * (li * li + lj * lj + lk * lk)
+    if d.sgs != SGS_NONE:
+        eddy = _nodal_eddy_viscosity(U, d, rho, u, v, w, p)
+        radVisTurb = max(max(1.0, 2.0 + LAM_OVER_MU), FHF_TURB) * (li * li + lj * lj + lk * lk)
+        radVis = (1.0 / rho * (muDim * radVisNu + eddy * radVisTurb)).max(axis=1)
+    else:
+        radVis = (1.0 / rho * muDim * radVisNu).max(axis=1)
     a = np.sqrt(np.abs(GAM * p / rho))
     vI = u * sc[:, 6:7] + v * sc[:, 7:8] + w * sc[:, 8:9]
     vJ = u * sc[:, 9:10] + v * sc[:, 10:11] + w * sc[:, 11:12]
     vK = u * sc[:, 12:13] + v * sc[:, 13:14] + w * sc[:, 14:15]
     radInv = ((np.abs(vI) + a) * li + (np.abs(vJ) + a) * lj + (np.abs(vK) + a) * lk).max(axis=1)
-    radVis = (1.0 / rho * muDim * radVisNu).max(axis=1)
     f1 = [2.0, 6.0, 12.0, 20.0, 28.0, 38.0, 50.0, 64.0, 80.0, 98.0]
     f2 = [6.0, 36.0, 150.0, 420.0, 980.0, 1975.0, 3575.0, 7000.0, 14000.0, 28000.0]
     dt = d.cfl * d.u_ref / (f1[d.n_poly] * radInv + f2[d.n_poly] * radVis)
     return float(dt.min())
+
+
+def _nodal_eddy_viscosity(U, d: Disc, rho, u, v, w, p):
+    """Eddy viscosity in the nodal DOFs from the dimensional primitive variables
+    (ComputeVelocityGradientsNodalDOFs, entropy branch, src/ElementClass.cpp:1647-1795,
+    then EddyViscosity with the element's LES length scale)."""
+    nE = U.shape[0]
+    _, dr, ds, dt = vol_interp(U, d.legdof, d.dlegdof)
+    dr, ds, dt = (a.reshape(nE, 5, -1) for a in (dr, ds, dt))
+    uRefInv = 1.0 / d.u_ref
+    un, vn, wn = u * uRefInv, v * uRefInv, w * uRefInv
+    V4Inv = -p * uRefInv * uRefInv / rho
+    comp = []
+    for c, vel in ((1, un), (2, vn), (3, wn)):
+        comp.append([-V4Inv * (g[:, c] + vel * g[:, 4]) for g in (dr, ds, dt)])
+    m = d.vmd
+    G = [[d.u_ref * (comp[i][0] * m[:, 1 + j] + comp[i][1] * m[:, 4 + j] + comp[i][2] * m[:, 7 + j])
+          for j in range(3)] for i in range(3)]
+    return eddy_viscosity(d.sgs, d.scal[:, 3:4], rho, G)
 
 
 LS_A = [0.0, -567301805773.0 / 1357537059087.0, -2404267990393.0 / 2016746695238.0,
@@ -557,4 +636,5 @@ def from_discretization(disc, params) -> Disc:
                 tau_num=float((params.n_poly + 1) ** 2) * params.rel_penalty,
                 theta=params.theta_sym, riemann=params.riemann, p_ref=params.p_ref,
                 u_ref=params.u_ref, rho_ref=params.rho_ref, cfl=params.cfl,
-                n_poly=params.n_poly)
+                n_poly=params.n_poly, sgs=params.sgs_model, dlegdof=disc.dleg_dofs,
+                vmd=disc.vol_metric_dofs)

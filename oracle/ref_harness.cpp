@@ -177,7 +177,13 @@ su2double GlobalTimeStep(SolverClass &s) {
     for (int m = 0; m <= nVar; ++m)
       solNodal[m] = (su2double *)AllocateMemory(s.mStandardHex.mNDOFsPad * sizeof(su2double));
     (void)nDOFs;
+    // Gradients of the nodal solution, used by the eddy viscosity of an SGS model.
     std::vector<su2double *> gradSolNodal;
+    if (s.mInputParam->mSGSModelType != NO_SGS_MODEL) {
+      gradSolNodal.resize(3 * nVar);
+      for (auto &p : gradSolNodal)
+        p = (su2double *)AllocateMemory(s.mStandardHex.mNDOFsPad * sizeof(su2double));
+    }
 #pragma omp for schedule(static), collapse(3), reduction(min : deltaT)
     for (int k = 1; k <= s.mNElemPerRankK; ++k)
       for (int j = 1; j <= s.mNElemPerRankJ; ++j)
@@ -187,6 +193,7 @@ su2double GlobalTimeStep(SolverClass &s) {
           deltaT = std::min(deltaT, dt);
         }
     for (auto &p : solNodal) FreeMemory((void **)&p);
+    for (auto &p : gradSolNodal) FreeMemory((void **)&p);
   }
   return deltaT;
 }

@@ -60,6 +60,16 @@ GOLDEN_SPECS = {
     "tgv_p5_2x2x2": cases.CaseSpec(name="tgv_p5_2x2x2", kind="tgv", n_elem=(2, 2, 2), p=5,
                                    hi=(TWO_PI,) * 3, mach=0.1, reynolds=1600.0,
                                    grid_map="random", grid_amp=0.01, seed=3),
+    # WALE subgrid-scale model, Taylor-Green vortex at a high Reynolds number on a
+    # perturbed grid, degree 4.
+    "tgv_p4_3x3x3_wale": cases.CaseSpec(name="tgv_p4_3x3x3_wale", kind="tgv", n_elem=(3, 3, 3),
+                                        p=4, hi=(TWO_PI,) * 3, mach=0.1, reynolds=1.0e5,
+                                        grid_map="random", grid_amp=0.005, seed=11, sgs="wale"),
+    # Vreman model, isentropic vortex, degree 3, Roe flux, anisotropic block.
+    "vortex_p3_4x3x3_vreman": cases.CaseSpec(name="vortex_p3_4x3x3_vreman", kind="vortex",
+                                             n_elem=(4, 3, 3), p=3, riemann="Roe",
+                                             hi=(10.0, 7.5, 7.5), center=(5.0, 3.75, 3.75),
+                                             reynolds=1.0e5, seed=12, sgs="vreman"),
 }
 
 
@@ -119,6 +129,23 @@ OPEN_SPECS = {
         center=(2.0, 3.3, 1.0), seed=10, riemann="Roe",
         bc=("inflow_supersonic", "outflow_supersonic", "farfield", "farfield", "periodic",
             "periodic"), **_OPEN),
+    # WALE model with walls (isothermal on j-min, heat flux on j-max), static inflow
+    # and characteristic outflow in i with a sponge layer, k periodic, degree 4; an
+    # isentropic vortex next to the isothermal wall gives the wall faces velocity
+    # gradients and so an eddy viscosity.
+    "wale_p4_4x3x2_walls": cases.CaseSpec(
+        name="wale_p4_4x3x2_walls", n_elem=(4, 3, 2), p=4, hi=(4.0, 3.0, 2.0),
+        center=(1.5, 0.7, 1.0), seed=13, reynolds=1.0e5, sgs="wale",
+        wall_data=(0.0, 0.0, 310.0, 20.0, 0.0, 0.0), sponge=(0, 1, 0, 0, 0, 0),
+        bc=("inflow_static_nscbc", "outflow_nscbc", "wall_isothermal", "wall_heat_flux",
+            "periodic", "periodic"), **dict(_OPEN, kind="vortex", beta=2.0)),
+    # Vreman model with the subsonic inflow / outflow states and far field, a
+    # vortex next to the j-max far field.
+    "vreman_p3_4x4x2_farfield": cases.CaseSpec(
+        name="vreman_p3_4x4x2_farfield", n_elem=(4, 4, 2), p=3, hi=(4.0, 4.0, 2.0),
+        center=(2.0, 3.3, 1.0), seed=14, reynolds=1.0e5, sgs="vreman",
+        bc=("inflow_subsonic", "outflow_subsonic", "farfield", "farfield", "periodic",
+            "periodic"), **dict(_OPEN, kind="vortex", beta=2.0)),
 }
 
 
@@ -130,6 +157,12 @@ OPEN_SPECS = {
 SYNC_SPECS = {
     "vortex_p3_4x4x4": (GOLDEN_SPECS["vortex_p3_4x4x4"],
                         {"Synchronization time step": "1.0e-4"}, 3),
+    # Vreman model at degree 3: the reference's synchronisation step sizes its
+    # nodal SGS buffers by the unpadded DOF count and fills them up to the padded
+    # count, which stays inside the buffers only where the two agree (K^3 a
+    # multiple of the padding, as for degree 3).
+    "vortex_p3_4x3x3_vreman": (GOLDEN_SPECS["vortex_p3_4x3x3_vreman"],
+                               {"Synchronization time step": "2.0e-4"}, 2),
     "pulse_p3_6x4x2_sponge_cml": (OPEN_SPECS["pulse_p3_6x4x2_sponge_cml"],
                                   {"Synchronization time step": "5.0e-5", "Restart": "no",
                                    "Fluctuations to add to initial solution": "Pressure pulse",

@@ -74,3 +74,21 @@ def test_reference_build_reproduces_fixture():
         r = records.read_records(out)
     assert rel_l2(r["res"][:, :, :K ** 3], g["res"]) < 1e-15
     assert r["dt"][0] == pytest.approx(g["dt0"][0], rel=1e-15)
+
+
+@pytest.mark.parametrize("model", [dn.SGS_WALE, dn.SGS_VREMAN])
+def test_eddy_viscosity_vanishes_in_pure_shear_and_scales_with_length(model):
+    """Both models are built to give no eddy viscosity in a pure shear flow;
+    both scale with the square of the length scale."""
+    rng = np.random.default_rng(5)
+    n = 64
+    rho = 1.0 + rng.random(n)
+    z = np.zeros(n)
+    shear = rng.standard_normal(n)
+    G = [[z, shear, z], [z, z, z], [z, z, z]]
+    assert np.all(dn.eddy_viscosity(model, 0.1, rho, G) < 1e-12 * np.abs(shear).max())
+    G = [[rng.standard_normal(n) for _ in range(3)] for _ in range(3)]
+    a = dn.eddy_viscosity(model, 0.1, rho, G)
+    b = dn.eddy_viscosity(model, 0.2, rho, G)
+    assert np.all(a > 0.0)
+    np.testing.assert_allclose(b, 4.0 * a, rtol=1e-13)

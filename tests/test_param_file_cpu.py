@@ -76,7 +76,7 @@ def test_unknown_keyword_and_bad_values():
 
 
 @pytest.mark.parametrize("edit, what", [
-    (("Subgrid scale model: None", "Subgrid scale model: WALE"), "Subgrid"),
+    (("Wall modeling: No wall model", "Wall modeling: Logarithmic wall model"), "Wall"),
     (("FEM working variables: Entropy", "FEM working variables: Conservative"), "Conservative"),
     (("Fluctuations to add to initial solution: No fluctuations",
       "Fluctuations to add to initial solution: Random fluctuations"), "(?i)random"),

@@ -40,6 +40,8 @@ def test_gpu_matches_reference_fixtures(gpu_available, path):
         assert rel_l2(s.get_raw_residual(), g["res_raw"]) < TOL_RES
         assert rel_l2(s.get_residual(), g["res"]) < TOL_RES
         assert mon[6] == pytest.approx(g["monitor"][6], rel=1e-13)
+        # Largest eddy viscosity of the volume and face points (0 without a model).
+        assert mon[7] == pytest.approx(max(g["monitor"][7], 0.0), rel=1e-10)
         assert s.time_step() == pytest.approx(g["dt0"][0], rel=TOL_DT)
         n = int(g["n_steps"])
         for scheme, key in ((capi.SSPRK3, "ssp"), (capi.LSRK4, "ls")):

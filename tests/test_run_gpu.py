@@ -4,6 +4,7 @@ same files, the written restart files, the mixed form and the command line."""
 from __future__ import annotations
 
 import os
+import re
 
 import numpy as np
 import pytest
@@ -54,5 +55,6 @@ def test_command_line(gpu_available, tmp_path):
     with open(cfg) as f:
         text = f.read()
     with open(cfg, "w") as f:
-        f.write(text.replace("Subgrid scale model: None", "Subgrid scale model: Vreman"))
+        f.write(re.sub(r"(?m)^Fluctuations to add to initial solution:.*$",
+                       "Fluctuations to add to initial solution: Random fluctuations", text))
     assert run.main([cfg, "--no-write"]) == 3

@@ -17,6 +17,7 @@ ERRORS = {1: "VCPG_E_CUDA", 2: "VCPG_E_CG_NOCONV", 3: "VCPG_E_NEG_A2", 4: "VCPG_
           5: "VCPG_E_OOM", 6: "VCPG_E_UNSUPPORTED_KM", 7: "VCPG_E_ADMISSION", 8: "VCPG_E_INVALID"}
 ROE, ISMAIL_ROE = 0, 1
 FP64, MIXED = 0, 1
+SGS_NONE, SGS_WALE, SGS_VREMAN = 0, 1, 2
 SSPRK3, LSRK4 = 0, 1
 BC_NONE, BC_OUTFLOW_NSCBC, BC_INFLOW_STATIC_NSCBC, BC_INFLOW_TOTAL_NSCBC = 0, 1, 2, 3
 (BC_WALL_HEAT_FLUX, BC_WALL_ISOTHERMAL, BC_WALL_INVISCID, BC_FARFIELD, BC_INFLOW_SUBSONIC,
@@ -25,7 +26,7 @@ BC_NONE, BC_OUTFLOW_NSCBC, BC_INFLOW_STATIC_NSCBC, BC_INFLOW_TOTAL_NSCBC = 0, 1,
 # Every symbol include/vcp3d_b200.h declares.
 EXPORTED = [
     "vcpg_create", "vcpg_destroy", "vcpg_last_error", "vcpg_setup_geometry",
-    "vcpg_setup_geometry_device",
+    "vcpg_setup_geometry_device", "vcpg_setup_nodal_metrics",
     "vcpg_nodal_conservative_to_modal", "vcpg_set_state", "vcpg_get_state",
     "vcpg_get_residual", "vcpg_residual", "vcpg_get_raw_residual", "vcpg_time_step",
     "vcpg_step", "vcpg_synchronization_step", "vcpg_sync", "vcpg_stream", "vcpg_launch_count", "vcpg_stats",
@@ -41,18 +42,20 @@ class Params(C.Structure):
                 ("riemann", C.c_int32), ("metric_index_compat", C.c_int32),
                 ("precision", C.c_int32), ("theta_sym", C.c_double),
                 ("rel_penalty", C.c_double), ("cfl", C.c_double), ("mu", C.c_double),
-                ("p_ref", C.c_double), ("u_ref", C.c_double), ("rho_ref", C.c_double)]
+                ("p_ref", C.c_double), ("u_ref", C.c_double), ("rho_ref", C.c_double),
+                ("sgs_model", C.c_int32)]
 
 
 class Operators(C.Structure):
     _fields_ = [(n, C.POINTER(C.c_double)) for n in
                 ("leg_int", "dleg_int", "leg_face", "dleg_face", "w_int", "leg_dofs",
-                 "basis_center")]
+                 "basis_center", "dleg_dofs")]
 
 
 class Geometry(C.Structure):
     _fields_ = [("vol_metric", C.POINTER(C.c_double)), ("face_metric", C.POINTER(C.c_double)),
-                ("elem_scalars", C.POINTER(C.c_double)), ("neighbors", C.POINTER(C.c_int32))]
+                ("elem_scalars", C.POINTER(C.c_double)), ("neighbors", C.POINTER(C.c_int32)),
+                ("vol_metric_dofs", C.POINTER(C.c_double))]
 
 
 class OpenBoundary(C.Structure):
@@ -106,6 +109,7 @@ def load() -> C.CDLL:
                                         dp, dp, dp, dp, dp, dp, dp, dp, ip]
     lib.vcpg_setup_geometry_device.argtypes = [C.POINTER(Params), C.c_int32, C.c_int32, ip, dp, dp, dp,
                                         dp, dp, dp, dp, dp, dp, dp, dp, ip]
+    lib.vcpg_setup_nodal_metrics.argtypes = [C.POINTER(Params), C.c_int32, C.c_int32, dp, dp, dp]
     lib.vcpg_nodal_conservative_to_modal.argtypes = [C.POINTER(Params), dp, dp, dp, C.c_int64]
     for name in ("vcpg_set_state", "vcpg_get_state", "vcpg_get_residual", "vcpg_get_raw_residual"):
         getattr(lib, name).argtypes = [hp, dp]

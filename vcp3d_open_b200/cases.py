@@ -166,6 +166,8 @@ class CaseSpec:
     # dimensional; None: the free stream.
     prescribed_super: Optional[Tuple[Tuple[float, ...], ...]] = None
     free_stream: Optional[Tuple[float, ...]] = None
+    # Subgrid-scale model: "none", "wale" or "vreman" (src/SGSModel.cpp).
+    sgs: str = "none"
 
     def __post_init__(self):
         if self.p_grid is None:
@@ -544,6 +546,19 @@ def prescribed_values(spec: CaseSpec, ref: "RefConditions"):
     return float(ref.p_ref), float(ref.rho_ref), vel
 
 
+_SGS_NAMES = {"none": "None", "wale": "WALE", "vreman": "Vreman"}
+
+
+def free_stream_values(spec: CaseSpec) -> Tuple[float, float, float, float, float]:
+    """Dimensional free stream (rho, u, v, w, p) of a generated case as the
+    reference derives it from the prescribed boundary data of its parameter file
+    (DetermineNonDimPrimVarFreeStream, src/InputParamClass.cpp:991-1192): the
+    far-field state and the default of CaseSpec.free_stream."""
+    from . import param_file
+    pf = param_file.parse(param_cfg_text(spec))
+    return param_file.reference_conditions(pf).free_stream
+
+
 def param_cfg_text(spec: CaseSpec, grid_file="grid.xyz", restart_file="restart.dat",
                    restart=True) -> str:
     d = spec.vel_dir
@@ -565,7 +580,7 @@ Save solution every: 100000000
 Write time history info every: 1
 FEM working variables: Entropy
 Riemann solver: {spec.riemann}
-Subgrid scale model: None
+Subgrid scale model: {_SGS_NAMES[spec.sgs.lower()]}
 Wall modeling: No wall model
 Theta parameter symmetrizing terms: {spec.theta_sym!r}
 Relative penalty parameter: {spec.penalty!r}

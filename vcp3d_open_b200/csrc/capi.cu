@@ -27,7 +27,8 @@ struct vcpg_handle {
   double *d_sol = nullptr, *d_solOld = nullptr, *d_res = nullptr, *d_resRaw = nullptr;
   double *d_vol = nullptr, *d_face = nullptr, *d_sc = nullptr;
   int *d_nbr = nullptr;
-  unsigned long long *d_dtbits = nullptr, *d_mach2 = nullptr;
+  unsigned long long *d_dtbits = nullptr, *d_mach2 = nullptr, *d_eddymax = nullptr;
+  double *d_nmetric = nullptr;   // [nE][10][K^3] metric at the nodal DOFs (SGS model)
   double *d_dt = nullptr, *d_fixed = nullptr, *d_hist = nullptr;
   int *d_status = nullptr, *d_counter = nullptr;
   unsigned long long *d_cgstats = nullptr;
@@ -91,6 +92,8 @@ ResidualArgs MakeResidualArgs(vcpg_handle *h, double *rawOut, unsigned long long
   a.riemann = h->prm.riemann;
   a.metric_compat = h->prm.metric_index_compat;
   a.mach2max = mach;
+  a.sgs = h->prm.sgs_model;
+  a.eddymax = mach ? h->d_eddymax : nullptr;   // with the monitoring data
   a.status = h->d_status;
   a.cg_stats = h->d_cgstats;
   // The mixed form computes the residual in FP32; its mass-matrix CG stops at a
@@ -121,6 +124,8 @@ TimeStepArgs MakeTimeStepArgs(vcpg_handle *h) {
   t.rho_ref = h->prm.rho_ref;
   t.dt_bits = h->d_dtbits;
   t.status = h->d_status;
+  t.sgs = h->prm.sgs_model;
+  t.vol_metric_dofs = h->d_nmetric;
   return t;
 }
 
@@ -156,6 +161,7 @@ BoundaryArgs MakeBoundaryArgs(vcpg_handle *h) {
   b.theta_sym = h->prm.theta_sym;
   b.riemann = h->prm.riemann;
   b.metric_compat = h->prm.metric_index_compat;
+  b.sgs = h->prm.sgs_model;
   b.cfgs = h->d_cfg;
   return b;
 }
@@ -165,7 +171,9 @@ BoundaryArgs MakeBoundaryArgs(vcpg_handle *h) {
 int EnqueueResidual(vcpg_handle *h, const ResidualArgs &a, int *launches) {
   int n = 0;
   if (h->open && h->nB > 0) {
-    VCPG_CUDA(h, LaunchBoundary(h->K, h->M, MakeBoundaryArgs(h), h->stream));
+    BoundaryArgs b = MakeBoundaryArgs(h);
+    b.eddymax = a.eddymax;
+    VCPG_CUDA(h, LaunchBoundary(h->K, h->M, b, h->stream));
     n += 2;
   }
   VCPG_CUDA(h, LaunchResidual(h->K, h->M, a, h->stream));
@@ -220,7 +228,7 @@ int vcpg_destroy(vcpg_handle *h) {
                   h->d_nbr, h->d_dtbits, h->d_mach2, h->d_dt, h->d_fixed, h->d_hist,
                   h->d_status, h->d_counter, h->d_cgstats, h->d_bface, h->d_bpresc, h->d_pc,
                   h->d_dlq, h->d_btrace, h->d_bmach, h->d_bflux, h->d_sponge, h->d_dampfn,
-                  h->d_dampst, h->d_cml, h->d_cfg, h->d_fflux};
+                  h->d_dampst, h->d_cml, h->d_cfg, h->d_fflux, h->d_eddymax, h->d_nmetric};
   for (void *p : bufs)
     if (p) cudaFree(p);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -256,6 +264,13 @@ int vcpg_create(const vcpg_params *params, const vcpg_operators *ops, const vcpg
     *out = h;
     return rc;
   }
+  if (params->sgs_model < VCPG_SGS_NONE || params->sgs_model > VCPG_SGS_VREMAN ||
+      (params->sgs_model != VCPG_SGS_NONE && (!ops->dleg_dofs || !geom->vol_metric_dofs))) {
+    int rc = Fail(h, VCPG_E_INVALID, "sgs_model must be VCPG_SGS_NONE, _WALE or _VREMAN; a model "
+                                     "needs ops->dleg_dofs and geom->vol_metric_dofs");
+    *out = h;
+    return rc;
+  }
   *out = h;
   const int K = h->K, M = h->M;
   // Operator table into the (K, M) constant slot.
@@ -264,6 +279,7 @@ int vcpg_create(const vcpg_params *params, const vcpg_operators *ops, const vcpg
   VCPG_CUDA(h, UploadOpTable(SlotOf(K, M), t));
 
   VCPG_CUDA(h, ConfigureResidual(K, M));
+  if (params->sgs_model != VCPG_SGS_NONE) VCPG_CUDA(h, ConfigureTimeStep(K, M));
   VCPG_CUDA(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
   const size_t nState = (size_t)h->nE * 5 * h->KD;
   auto alloc = [&](void **p, size_t bytes) -> int {
@@ -282,6 +298,12 @@ int vcpg_create(const vcpg_params *params, const vcpg_operators *ops, const vcpg
   if ((rc = alloc((void **)&h->d_nbr, (size_t)h->nE * 6 * sizeof(int)))) return rc;
   if ((rc = alloc((void **)&h->d_dtbits, sizeof(unsigned long long)))) return rc;
   if ((rc = alloc((void **)&h->d_mach2, sizeof(unsigned long long)))) return rc;
+  if ((rc = alloc((void **)&h->d_eddymax, sizeof(unsigned long long)))) return rc;
+  if (params->sgs_model != VCPG_SGS_NONE) {
+    if ((rc = alloc((void **)&h->d_nmetric, (size_t)h->nE * 10 * h->KD * 8))) return rc;
+    VCPG_CUDA(h, cudaMemcpy(h->d_nmetric, geom->vol_metric_dofs, (size_t)h->nE * 10 * h->KD * 8,
+                            cudaMemcpyHostToDevice));
+  }
   if ((rc = alloc((void **)&h->d_dt, sizeof(double)))) return rc;
   if ((rc = alloc((void **)&h->d_fixed, sizeof(double)))) return rc;
   if ((rc = alloc((void **)&h->d_status, 4 * sizeof(int)))) return rc;
@@ -350,7 +372,10 @@ int vcpg_residual(vcpg_handle *h, double *monitoring, int32_t keep_raw) {
     cudaError_t e = cudaMalloc((void **)&h->d_resRaw, (size_t)h->nE * 5 * h->KD * 8);
     if (e != cudaSuccess) return Fail(h, VCPG_E_OOM, "cudaMalloc raw residual");
   }
-  if (monitoring) VCPG_CUDA(h, cudaMemsetAsync(h->d_mach2, 0, 8, h->stream));
+  if (monitoring) {
+    VCPG_CUDA(h, cudaMemsetAsync(h->d_mach2, 0, 8, h->stream));
+    VCPG_CUDA(h, cudaMemsetAsync(h->d_eddymax, 0, 8, h->stream));
+  }
   ResidualArgs a = MakeResidualArgs(h, keep_raw ? h->d_resRaw : nullptr,
                                     monitoring ? h->d_mach2 : nullptr);
   int nl = 0;
@@ -364,10 +389,13 @@ int vcpg_residual(vcpg_handle *h, double *monitoring, int32_t keep_raw) {
     VCPG_CUDA(h, cudaMemcpy(&bits, h->d_mach2, 8, cudaMemcpyDeviceToHost));
     double m2;
     std::memcpy(&m2, &bits, 8);
-    // Periodic blocks carry no walls: force coefficients are zero and no SGS model is used.
+    VCPG_CUDA(h, cudaMemcpy(&bits, h->d_eddymax, 8, cudaMemcpyDeviceToHost));
+    double eddyMax;
+    std::memcpy(&eddyMax, &bits, 8);
+    // Force coefficients are not computed (no wall forces): zero.
     for (int i = 0; i < 6; ++i) monitoring[i] = 0.0;
     monitoring[6] = m2;
-    monitoring[7] = 0.0;
+    monitoring[7] = eddyMax;   // maximum eddy viscosity of the volume and face points
   }
   return rc;
 }

@@ -49,6 +49,26 @@ int vcpg_setup_geometry(const vcpg_params *params, int32_t p_grid, int32_t dof_l
   return VCPG_OK;
 }
 
+int vcpg_setup_nodal_metrics(const vcpg_params *params, int32_t p_grid, int32_t dof_location,
+                             const double *grid_nodes, double *dleg_dofs,
+                             double *vol_metric_dofs) {
+  if (!params || !grid_nodes || p_grid < 1) return VCPG_E_INVALID;
+  try {
+    const int K = params->n_poly + 1, M = params->n_int_1d, Kg = p_grid + 1;
+    const int64_t nE = (int64_t)params->n_elem[0] * params->n_elem[1] * params->n_elem[2];
+    if (K < 2 || M < 1 || nE < 1) return VCPG_E_INVALID;
+    StdElement se = vcpg::host::BuildStdElement(K, M, Kg, dof_location, dof_location);
+    if (dleg_dofs) std::memcpy(dleg_dofs, se.dlegdof.data(), sizeof(double) * K * K);
+    const int KD = K * K * K, KG3 = Kg * Kg * Kg;
+    if (vol_metric_dofs)
+      for (int64_t e = 0; e < nE; ++e)
+        vcpg::host::NodalMetrics(se, grid_nodes + e * 3 * KG3, vol_metric_dofs + e * 10 * KD);
+  } catch (const std::exception &) {
+    return VCPG_E_INVALID;
+  }
+  return VCPG_OK;
+}
+
 int vcpg_nodal_conservative_to_modal(const vcpg_params *params, const double *vand_inv,
                                      const double *cons, double *modal, int64_t n_elem) {
   if (!params || !cons || !modal || n_elem < 0) return VCPG_E_INVALID;

@@ -42,6 +42,8 @@ struct BoundaryArgs {
   int nB;
   double mu, tau_num, theta_sym;
   int riemann, metric_compat;
+  int sgs;                     // enum vcpg_sgs
+  unsigned long long *eddymax; // optional: bits of the max eddy viscosity
   const BlockFaceCfg *cfgs;    // [nCases][6] per case and block face
   // Several cases per launch (null case_state: one case): the case slot is entry
   // kBfCase of the boundary-face row; only faces of cases in state `require` run.
@@ -267,9 +269,12 @@ __device__ __forceinline__ void WeakBoundaryFlux(const BoundaryArgs &a, const in
       IsmailRoeFlux(VL, VR, nx, ny, nz, wf * area, flux, factU);
     else
       RoeFlux(VL, VR, nx, ny, nz, 0.5 * wf * area, flux, factU);
+    double eddy = 0.0;
     ViscousPenaltySymFlux(VL, VR, gx, gy, gz, nx, ny, nz, wf, area, mu,
                           a.tau_num / lenScale, a.theta_sym, flux, sx, sy, sz, hfMult,
-                          wf * area * qWall);
+                          wf * area * qWall, a.sgs, a.elem_scalars[(size_t)e * 15 + 3], &eddy);
+    if (a.sgs && a.eddymax && eddy > 0.0)
+      atomicMax(a.eddymax, (unsigned long long)__double_as_longlong(eddy));
 #pragma unroll
     for (int n = 0; n < 5; ++n) {
       const int mi = a.metric_compat ? n : l;
@@ -602,8 +607,12 @@ __global__ void __launch_bounds__(NT) BoundaryFluxKernel(const BoundaryArgs a) {
       IsmailRoeFlux(VL, VR, nx, ny, nz, wf * area, flux);
     else
       RoeFlux(VL, VR, nx, ny, nz, 0.5 * wf * area, flux);
+    double eddy = 0.0;
     ViscousPenaltySymFlux(VL, VR, gx, gy, gz, nx, ny, nz, wf, area, mu,
-                          a.tau_num / lenScale, a.theta_sym, flux, sx, sy, sz);
+                          a.tau_num / lenScale, a.theta_sym, flux, sx, sy, sz, 1.0, 0.0, a.sgs,
+                          a.elem_scalars[(size_t)e * 15 + 3], &eddy);
+    if (a.sgs && a.eddymax && eddy > 0.0)
+      atomicMax(a.eddymax, (unsigned long long)__double_as_longlong(eddy));
     double *out = a.bflux + (size_t)b * 4 * 5 * M2;
     const int pFast = BFastParam(d), pSlow = 3 - d - pFast;
 #pragma unroll

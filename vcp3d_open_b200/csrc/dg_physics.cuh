@@ -22,6 +22,8 @@ constexpr double kCp = kGam * kRGas / (kGam - 1.0);  // Cp
 __device__ __forceinline__ double Exp(double x) { return exp(x); }
 __device__ __forceinline__ float Exp(float x) { return expf(x); }
 __device__ __forceinline__ double Log(double x) { return log(x); }
+__device__ __forceinline__ double Pow(double x, double y) { return pow(x, y); }
+__device__ __forceinline__ float Pow(float x, float y) { return powf(x, y); }
 __device__ __forceinline__ float Log(float x) { return logf(x); }
 __device__ __forceinline__ double Sqrt(double x) { return sqrt(x); }
 __device__ __forceinline__ float Sqrt(float x) { return sqrtf(x); }
@@ -74,6 +76,65 @@ __device__ __forceinline__ void FaceStatePrim(const T *V, T &rho, T &u, T &v,
   // rho = (-V4 exp(s))^(-1/(gam-1)), as in EntropyToPrim.
   rho = Exp(ov1mg * (Log(-V[4]) + s));
   p = -V4Inv * rho;
+}
+
+// Eddy viscosity of the subgrid-scale models (src/SGSModel.cpp): sgs 1 WALE
+// (C_w = 0.325), sgs 2 Vreman (c = 0.07), 0 none. g holds the velocity gradient
+// du/dx, dv/dx, dw/dx, du/dy, dv/dy, dw/dy, du/dz, dv/dz, dw/dz; the result is
+// rho times the model's kinematic eddy viscosity.
+template <typename T>
+__device__ __forceinline__ T EddyViscosity(const int sgs, const T lenScale, const T rho,
+                                           const T *g) {
+  const T third = T(1.0) / T(3.0), epsSmall = T(1.e-30);
+  const T dudx = g[0], dvdx = g[1], dwdx = g[2], dudy = g[3], dvdy = g[4], dwdy = g[5];
+  const T dudz = g[6], dvdz = g[7], dwdz = g[8];
+  if (sgs == 1) {
+    const T len = T(0.325) * lenScale, len2 = len * len;
+    const T S11 = dudx, S22 = dvdy, S33 = dwdz;
+    const T S12 = T(0.5) * (dudy + dvdx), S13 = T(0.5) * (dudz + dwdx), S23 = T(0.5) * (dvdz + dwdy);
+    T Sd11 = dudx * dudx + dudy * dvdx + dudz * dwdx;
+    T Sd22 = dvdx * dudy + dvdy * dvdy + dvdz * dwdy;
+    T Sd33 = dwdx * dudz + dwdy * dvdz + dwdz * dwdz;
+    const T Sd12 = T(0.5) * (dudx * dudy + dudy * dvdy + dudz * dwdy + dvdx * dudx + dvdy * dvdx +
+                             dvdz * dwdx);
+    const T Sd13 = T(0.5) * (dudx * dudz + dudy * dvdz + dudz * dwdz + dwdx * dudx + dwdy * dvdx +
+                             dwdz * dwdx);
+    const T Sd23 = T(0.5) * (dvdx * dudz + dvdy * dvdz + dvdz * dwdz + dwdx * dudy + dwdy * dvdy +
+                             dwdz * dwdy);
+    const T thirdTrace = third * (Sd11 + Sd22 + Sd33);
+    Sd11 -= thirdTrace;
+    Sd22 -= thirdTrace;
+    Sd33 -= thirdTrace;
+    const T sumS = S11 * S11 + S22 * S22 + S33 * S33 + T(2.0) * (S12 * S12 + S13 * S13 + S23 * S23);
+    const T sumSd = Sd11 * Sd11 + Sd22 * Sd22 + Sd33 * Sd33 +
+                    T(2.0) * (Sd12 * Sd12 + Sd13 * Sd13 + Sd23 * Sd23);
+    const T sumSdPow3_2 = sumSd * Sqrt(sumSd);
+    const T sumSdPow5_4 = Sqrt(sumSdPow3_2 * sumSd);
+    const T sumSPow5_2 = sumS * sumS * Sqrt(sumS);
+    const T denom = sumSPow5_2 + sumSdPow5_4;
+    return rho * (len2 * sumSdPow3_2 / Fmax(denom, epsSmall));
+  }
+  if (sgs == 2) {
+    const T len2 = lenScale * lenScale;
+    T a11 = dudx, a22 = dvdy, a33 = dwdz;
+    const T tmp = third * (a11 + a22 + a33);
+    a11 -= tmp;
+    a22 -= tmp;
+    a33 -= tmp;
+    const T a12 = dudy, a13 = dudz, a23 = dvdz, a21 = dvdx, a31 = dwdx, a32 = dwdy;
+    const T b11 = len2 * (a11 * a11 + a12 * a12 + a13 * a13);
+    const T b12 = len2 * (a11 * a21 + a12 * a22 + a13 * a23);
+    const T b13 = len2 * (a11 * a31 + a12 * a32 + a13 * a33);
+    const T b22 = len2 * (a21 * a21 + a22 * a22 + a23 * a23);
+    const T b23 = len2 * (a21 * a31 + a22 * a32 + a23 * a33);
+    const T b33 = len2 * (a31 * a31 + a32 * a32 + a33 * a33);
+    T B = b11 * b22 - b12 * b12 + b11 * b33 - b13 * b13 + b22 * b33 - b23 * b23;
+    B = (B + Fabs(B)) * T(0.5);
+    const T denom = a11 * a11 + a22 * a22 + a33 * a33 + a12 * a12 + a13 * a13 + a23 * a23 +
+                    a21 * a21 + a31 * a31 + a32 * a32;
+    return rho * T(0.07) * Sqrt(B / Fmax(denom, epsSmall));
+  }
+  return T(0.0);
 }
 
 // Ismail-Roe entropy-stable flux, entropy-variable branch of InviscidFluxesFace
@@ -226,15 +287,15 @@ __device__ __forceinline__ void ViscousPenaltySymFlux(
     const T *VL, const T *VR, const T *gx, const T *gy, const T *gz,
     const T nnx, const T nny, const T nnz, const T wf,
     const T area, const T mu, const T tau, const T thetaSym, T *f,
-    T *sx, T *sy, T *sz, const T hfMult = T(1.0), const T qWallArea = T(0.0)) {
-  const T factHFLam = hfMult * T(kFactHFLam);
+    T *sx, T *sy, T *sz, const T hfMult = T(1.0), const T qWallArea = T(0.0),
+    const int sgs = 0, const T lenLES = T(0.0), T *eddyOut = nullptr) {
+  const T factHFLam = hfMult * T(kFactHFLam), factHFTurb = hfMult * T(kFactHFTurb);
   const T gm1 = T(kGam) - T(1.0), ovgm1 = T(1.0) / gm1, ov1mg = -ovgm1;
   const T V1 = T(0.5) * (VL[1] + VR[1]);
   const T V2 = T(0.5) * (VL[2] + VR[2]), V3 = T(0.5) * (VL[3] + VR[3]);
   const T V4 = T(0.5) * (VL[4] + VR[4]);
   const T V4Inv = T(1.0) / V4;
   const T u = -V4Inv * V1, v = -V4Inv * V2, w = -V4Inv * V3;
-  // (rho of the averaged state is only needed by an SGS model.)
   const T dudx = -V4Inv * (gx[1] + u * gx[4]);
   const T dvdx = -V4Inv * (gx[2] + v * gx[4]);
   const T dwdx = -V4Inv * (gx[3] + w * gx[4]);
@@ -244,6 +305,17 @@ __device__ __forceinline__ void ViscousPenaltySymFlux(
   const T dudz = -V4Inv * (gz[1] + u * gz[4]);
   const T dvdz = -V4Inv * (gz[2] + v * gz[4]);
   const T dwdz = -V4Inv * (gz[3] + w * gz[4]);
+  // Eddy viscosity of the averaged state (ViscousFluxesFace step 2).
+  T eddy = T(0.0);
+  if (sgs) {
+    const T V0 = T(0.5) * (VL[0] + VR[0]);
+    const T eKin = T(0.5) * (u * u + v * v + w * w);
+    const T s = T(kGam) - gm1 * (V0 - V4 * eKin);
+    const T rho = Pow(-V4 * Exp(s), ov1mg);
+    const T gv[9] = {dudx, dvdx, dwdx, dudy, dvdy, dwdy, dudz, dvdz, dwdz};
+    eddy = EddyViscosity(sgs, lenLES, rho, gv);
+    if (eddyOut) *eddyOut = eddy;
+  }
   const T fe = -V4Inv * V4Inv * ov1mg;
   const T dedx = fe * gx[4], dedy = fe * gy[4], dedz = fe * gz[4];
   const T dV1 = VL[1] - VR[1], dV2 = VL[2] - VR[2], dV3 = VL[3] - VR[3];
@@ -256,14 +328,14 @@ __device__ __forceinline__ void ViscousPenaltySymFlux(
     const T Area = wf * area;
     const T nx = Area * nnx, ny = Area * nny, nz = Area * nnz;
     const T lamDivVel = T(kLamOverMu) * (dudx + dvdy + dwdz);
-    const T muTot = mu + T(0.0);
+    const T muTot = mu + eddy;
     const T tauxx = muTot * (T(2.0) * dudx + lamDivVel);
     const T tauyy = muTot * (T(2.0) * dvdy + lamDivVel);
     const T tauzz = muTot * (T(2.0) * dwdz + lamDivVel);
     const T tauxy = muTot * (dudy + dvdx);
     const T tauxz = muTot * (dudz + dwdx);
     const T tauyz = muTot * (dvdz + dwdy);
-    const T factHeatTot = mu * factHFLam + T(0.0) * (hfMult * T(kFactHFTurb));
+    const T factHeatTot = mu * factHFLam + eddy * factHFTurb;
     const T qx = -factHeatTot * dedx, qy = -factHeatTot * dedy, qz = -factHeatTot * dedz;
     f[1] -= tauxx * nx + tauxy * ny + tauxz * nz;
     f[2] -= tauxy * nx + tauyy * ny + tauyz * nz;
@@ -277,9 +349,9 @@ __device__ __forceinline__ void ViscousPenaltySymFlux(
   // Penalty and symmetrizing fluxes (src/FluxesFace.cpp:1180-1283).
   const T lam = T(kLamOverMu), lamp1 = T(kLamOverMu) + T(1.0), lamp2 = T(kLamOverMu) + T(2.0);
   const T e = pOvRho * ovgm1;
-  const T factFlux = pOvRho * wf * area * (mu + T(0.0));
+  const T factFlux = pOvRho * wf * area * (mu + eddy);
   T nx = factFlux * nnx, ny = factFlux * nny, nz = factFlux * nnz;
-  const T factHeatFlux = (mu * factHFLam + T(0.0) * (hfMult * T(kFactHFTurb))) / (mu + T(0.0));
+  const T factHeatFlux = (mu * factHFLam + eddy * factHFTurb) / (mu + eddy);
   const T abvE = u * u + v * v + w * w + factHeatFlux * e;
   const T K11_11 = lamp2, K11_14 = u * lamp2, K11_22 = T(1.0), K11_24 = v, K11_33 = T(1.0),
                K11_34 = w, K11_44 = abvE + u * u * lamp1;

@@ -52,6 +52,8 @@ struct ResidualArgs {
   int riemann;                 // 0 Roe, 1 Ismail-Roe
   int metric_compat;           // 1: metric indexed by the variable index
   unsigned long long *mach2max;  // optional: bits of max Mach^2 (non-negative double)
+  int sgs;                     // enum vcpg_sgs: subgrid-scale model
+  unsigned long long *eddymax;   // optional: bits of the max eddy viscosity
   int *status;                 // [0] CG iteration cap hits, [1] boundary face without BC
   unsigned long long *cg_stats;  // [0] CG iterations, [1] element solves (cumulative)
   double cg_tol;               // relative CG stopping tolerance (1e-10 in the FP64 form)
@@ -81,6 +83,8 @@ struct TimeStepArgs {
   unsigned long long *dt_bits;  // per case: bits of the minimum over its elements
   int *status;  // [2]: negative a^2 seen
   CaseView cases;  // several cases: per-case parameters and time steps
+  int sgs;                          // enum vcpg_sgs
+  const double *vol_metric_dofs;    // [nE][10][K^3] metric at the nodal DOFs (with sgs)
 };
 
 template <int NT, typename T>
@@ -334,7 +338,7 @@ __device__ __forceinline__ void VolumePhase(const ResidualArgs &a, const int e, 
 
   const double *vm = a.vol_metric + (size_t)e * 10 * MD;
   const T gm1 = T(kGam) - T(1.0), ov1mg = -T(1.0) / gm1;
-  T mach2 = T(0.0);
+  T mach2 = T(0.0), eddyMax = T(0.0);
   for (int l = threadIdx.x; l < MD; l += NT) {
     const int i = l % M, j = (l / M) % M, k = l / M2;
     // Parametric -> Cartesian gradients (src/ElementClass.cpp:3856-3875). In the
@@ -385,8 +389,15 @@ __device__ __forceinline__ void VolumePhase(const ResidualArgs &a, const int e, 
     s_jw[l] = Wl * Jl;
     const T weight = -Jl * Wl;
     const T ru = rho * u, rv = rho * v, rw = rho * w;
-    const T muTot = T(mu) + T(0.0);
-    const T factHeatFluxTot = T(mu) * T(kFactHFLam) + T(0.0) * T(kFactHFTurb);
+    T eddy = T(0.0);
+    if (a.sgs) {
+      // Eddy viscosity at the point (src/ElementClass.cpp:4272-4310).
+      const T gv[9] = {dudx, dvdx, dwdx, dudy, dvdy, dwdy, dudz, dvdz, dwdz};
+      eddy = EddyViscosity(a.sgs, T(a.elem_scalars[(size_t)e * 15 + 3]), rho, gv);
+      eddyMax = Fmax(eddyMax, eddy);
+    }
+    const T muTot = T(mu) + eddy;
+    const T factHeatFluxTot = T(mu) * T(kFactHFLam) + eddy * T(kFactHFTurb);
     const T divVelTerm = T(kLamOverMu) * (dudx + dvdy + dwdz);
     const T tauxx = muTot * (T(2.0) * dudx + divVelTerm);
     const T tauyy = muTot * (T(2.0) * dvdy + divVelTerm);
@@ -418,6 +429,10 @@ __device__ __forceinline__ void VolumePhase(const ResidualArgs &a, const int e, 
   if (a.mach2max) {
     const T m = BlockMax<NT>(mach2, s_red);
     if (threadIdx.x == 0) atomicMax(a.mach2max, (unsigned long long)__double_as_longlong((double)m));
+  }
+  if (a.sgs && a.eddymax) {
+    const T m = BlockMax<NT>(eddyMax, s_red);
+    if (threadIdx.x == 0) atomicMax(a.eddymax, (unsigned long long)__double_as_longlong((double)m));
   }
   __syncthreads();
 
@@ -570,7 +585,8 @@ template <int K, int M, typename T>
 __device__ __forceinline__ void FacePointFlux(const ResidualArgs &a, const double mu, const int d,
                                               const int pt, const T *TR, const int tL,
                                               const int tR, const double *fmL,
-                                              const double *fmR, const T lenScale, T *out) {
+                                              const double *fmR, const T lenScale, T *out,
+                                              const T lenLES, T &eddy) {
   constexpr int SLOT = Slot<K, M>::value;
   constexpr int M2 = M * M;
   T VL[5], VR[5], gxL[5], gyL[5], gzL[5], gxR[5], gyR[5], gzR[5];
@@ -600,7 +616,8 @@ __device__ __forceinline__ void FacePointFlux(const ResidualArgs &a, const doubl
     RoeFlux(VL, VR, nx, ny, nz, T(0.5) * wf * area, flux);
   T sx[5], sy[5], sz[5];
   ViscousPenaltySymFlux(VL, VR, gx, gy, gz, nx, ny, nz, wf, area, T(mu),
-                        T(a.tau_num) / lenScale, T(a.theta_sym), flux, sx, sy, sz);
+                        T(a.tau_num) / lenScale, T(a.theta_sym), flux, sx, sy, sz, T(1.0),
+                        T(0.0), a.sgs, lenLES, &eddy);
 #pragma unroll
   for (int n = 0; n < 5; ++n) {
     out[n * M2 + pt] = flux[n];
@@ -678,16 +695,28 @@ __device__ __forceinline__ void MinFaceFluxes(const ResidualArgs &a, const int e
   __syncthreads();
   const double *sc = a.elem_scalars + (size_t)e * 15;
   T *out = reinterpret_cast<T *>(a.face_flux) + (size_t)e * 3 * 20 * M2;
+  T eddyMax = T(0.0);
   for (int idx = threadIdx.x; idx < 3 * M2; idx += NT) {
     const int d = idx / M2, pt = idx - d * M2;
     const int nb = d == 0 ? nb0 : (d == 1 ? nb1 : nb2);
     if (nb < 0) continue;
     const T lenScale = Fmin(T(sc[d]), T(a.elem_scalars[(size_t)nb * 15 + d]));
+    // LES length of the face: the mean of both elements' (src/ElementClass.cpp:2655).
+    const T lenLES = T(0.5) * (T(sc[3]) + T(a.elem_scalars[(size_t)nb * 15 + 3]));
     const double *fmOwn = a.face_metric + ((size_t)e * 6 + 2 * d) * 13 * M2;
     const double *fmNb = a.face_metric + ((size_t)nb * 6 + 2 * d + 1) * 13 * M2;
     // The lower element (the neighbour, trace slot 2d+1) is the left state.
+    T eddy = T(0.0);
     FacePointFlux<K, M>(a, mu, d, pt, TR, 2 * d + 1, 2 * d, fmNb, fmOwn, lenScale,
-                        out + d * 20 * M2);
+                        out + d * 20 * M2, lenLES, eddy);
+    eddyMax = Fmax(eddyMax, eddy);
+  }
+  if (a.sgs && a.eddymax) {
+    // Largest eddy viscosity of the faces for the monitoring data.
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) eddyMax = Fmax(eddyMax, __shfl_xor_sync(0xffffffffu, eddyMax, o));
+    if ((threadIdx.x & 31) == 0 && eddyMax > T(0.0))
+      atomicMax(a.eddymax, (unsigned long long)__double_as_longlong((double)eddyMax));
   }
 }
 

@@ -33,6 +33,7 @@ struct OpTable {
   double dface[2 * kKMax];
   double w[kMMax];                  // 1-D Gauss weights
   double legdof[kKMax * kKMax];     // legdof[k * K + i]: basis k at nodal DOF i
+  double dlegdof[kKMax * kKMax];    // its derivative (time step with an SGS model)
   double center[kKMax * kKMax * kKMax];
   // FP32 copies for the mixed-precision form.
   float legf[kKMax * kMMax];
@@ -62,7 +63,8 @@ enum OpSel {
   kDLeg = 1,   // K -> M with the derivative
   kLegT = 2,   // M -> K: out[k] = sum_m leg[k][m] in[m]   (transposed operator)
   kDLegT = 3,  // M -> K with the derivative
-  kLegDof = 4  // K -> K: out[i] = sum_k legdof[k][i] in[k]   (modal -> nodal)
+  kLegDof = 4,  // K -> K: out[i] = sum_k legdof[k][i] in[k]   (modal -> nodal)
+  kDLegDof = 5  // K -> K with the derivative
 };
 
 template <int SLOT, int K, int M, int OP, typename T = double>
@@ -77,6 +79,7 @@ __device__ __forceinline__ T Coef(const int c, const int o) {
     if (OP == kDLeg) return c_ops[SLOT].dleg[c * M + o];
     if (OP == kLegT) return c_ops[SLOT].leg[o * M + c];
     if (OP == kLegDof) return c_ops[SLOT].legdof[c * K + o];
+    if (OP == kDLegDof) return c_ops[SLOT].dlegdof[c * K + o];
     return c_ops[SLOT].dleg[o * M + c];
   }
 }

@@ -461,6 +461,8 @@ int vcpg_ensemble_submit(vcpg_ensemble *ens, const vcpg_params *params,
   if (!ens || !params || !ops || !geom || !modal_state || !case_id || n_steps < 0)
     return VCPG_E_INVALID;
   vcpg_ensemble *e = ens;
+  if (params->sgs_model != VCPG_SGS_NONE)
+    return Fail(e, VCPG_E_INVALID, "subgrid-scale models run on single-case handles");
   const int deg = params->n_poly;
   if (deg < 1 || deg > 6 || e->b[deg].deg != deg)
     return Fail(e, VCPG_E_INVALID, "no bucket for degree " + std::to_string(deg));

@@ -245,6 +245,16 @@ StdElement BuildStdElement(int K, int M, int Kg, int dofLgl, int gridLgl) {
         se.lagInt[j * M + m] += NormJacobi(k, 0, 0, se.rInt[m]) * Vg[k * Kg + j];
         se.dlagInt[j * M + m] += GradNormJacobi(k, 0, 0, se.rInt[m]) * Vg[k * Kg + j];
       }
+  se.lagDof.assign(Kg * K, 0.0); se.dlagDof.assign(Kg * K, 0.0);
+  for (int j = 0; j < Kg; ++j)
+    for (int m = 0; m < K; ++m)
+      for (int k = 0; k < Kg; ++k) {
+        se.lagDof[j * K + m] += NormJacobi(k, 0, 0, se.rDof[m]) * Vg[k * Kg + j];
+        se.dlagDof[j * K + m] += GradNormJacobi(k, 0, 0, se.rDof[m]) * Vg[k * Kg + j];
+      }
+  se.dlegdof.resize(K * K);
+  for (int k = 0; k < K; ++k)
+    for (int i = 0; i < K; ++i) se.dlegdof[k * K + i] = GradNormJacobi(k, 0, 0, se.rDof[i]);
   se.lagFace.assign(2 * Kg, 0.0); se.dlagFace.assign(2 * Kg, 0.0);
   se.lagFace[0] = 1.0;
   se.lagFace[Kg + Kg - 1] = 1.0;
@@ -366,6 +376,39 @@ void ElementMetrics(const StdElement &se, const double *gridNodes, double *vol, 
     scalars[6 + 3 * d] = a0 / s;
     scalars[7 + 3 * d] = a1 / s;
     scalars[8 + 3 * d] = a2 / s;
+  }
+}
+
+void NodalMetrics(const StdElement &se, const double *gridNodes, double *out) {
+  const int Kg = se.Kg, K = se.K, KD = K * K * K, KG3 = Kg * Kg * Kg;
+  std::vector<double> dc((size_t)9 * KD);  // [param][coord][DOF]
+  for (int x = 0; x < 3; ++x) {
+    std::vector<double> g(gridNodes + x * KG3, gridNodes + (x + 1) * KG3);
+    for (int q = 0; q < 3; ++q) {
+      std::vector<double> t = ApplyAxis(g, Kg, Kg, Kg, 2, (q == 2 ? se.dlagDof : se.lagDof).data(), K);
+      t = ApplyAxis(t, Kg, Kg, K, 1, (q == 1 ? se.dlagDof : se.lagDof).data(), K);
+      t = ApplyAxis(t, Kg, K, K, 0, (q == 0 ? se.dlagDof : se.lagDof).data(), K);
+      for (int l = 0; l < KD; ++l) dc[((size_t)q * 3 + x) * KD + l] = t[l];
+    }
+  }
+  for (int l = 0; l < KD; ++l) {
+    const double dxdr = dc[0 * KD + l], dydr = dc[1 * KD + l], dzdr = dc[2 * KD + l];
+    const double dxds = dc[3 * KD + l], dyds = dc[4 * KD + l], dzds = dc[5 * KD + l];
+    const double dxdt = dc[6 * KD + l], dydt = dc[7 * KD + l], dzdt = dc[8 * KD + l];
+    const double J = dxdr * (dyds * dzdt - dzds * dydt) - dxds * (dydr * dzdt - dzdr * dydt) +
+                     dxdt * (dydr * dzds - dzdr * dyds);
+    if (!(J > 0.0)) throw std::runtime_error("negative or zero Jacobian at a nodal DOF");
+    const double Jinv = 1.0 / J;
+    out[0 * KD + l] = J;
+    out[1 * KD + l] = Jinv * (dyds * dzdt - dzds * dydt);
+    out[2 * KD + l] = Jinv * (dzds * dxdt - dxds * dzdt);
+    out[3 * KD + l] = Jinv * (dxds * dydt - dyds * dxdt);
+    out[4 * KD + l] = Jinv * (dzdr * dydt - dydr * dzdt);
+    out[5 * KD + l] = Jinv * (dxdr * dzdt - dzdr * dxdt);
+    out[6 * KD + l] = Jinv * (dydr * dxdt - dxdr * dydt);
+    out[7 * KD + l] = Jinv * (dydr * dzds - dzdr * dyds);
+    out[8 * KD + l] = Jinv * (dzdr * dxds - dxdr * dzds);
+    out[9 * KD + l] = Jinv * (dxdr * dyds - dydr * dxds);
   }
 }
 

@@ -25,6 +25,8 @@ struct StdElement {
   std::vector<double> vandInv;           // [K][K]   nodal c -> modal o
   std::vector<double> lagInt, dlagInt;   // [Kg][M]  grid Lagrange basis at the Gauss points
   std::vector<double> lagFace, dlagFace; // [2][Kg]  grid Lagrange basis at r = -1, +1
+  std::vector<double> lagDof, dlagDof;   // [Kg][K]  grid Lagrange basis at the nodal DOFs
+  std::vector<double> dlegdof;           // [K][K]   derivative of modal basis k at DOF i
 };
 
 StdElement BuildStdElement(int K, int M, int Kg, int dofLgl, int gridLgl);
@@ -33,6 +35,10 @@ StdElement BuildStdElement(int K, int M, int Kg, int dofLgl, int gridLgl);
 // vol[10][M^3] (J, dr/dx .. dt/dz), face[6][13][M^2], scalars[15].
 void ElementMetrics(const StdElement &se, const double *gridNodes, double *vol, double *face,
                     double *scalars, int nPoly);
+
+// Metric terms at the nodal solution DOFs (ComputeCoorNodalSolDOFs): out[10][K^3]
+// with J and the nine inverse-Jacobian terms, in the layout of the volume metric.
+void NodalMetrics(const StdElement &se, const double *gridNodes, double *out);
 
 // Face neighbours of a single block, elements i fastest: [nE][6] (iMin, iMax,
 // jMin, jMax, kMin, kMax), -1 on a non-periodic block face.

@@ -82,6 +82,130 @@ __global__ void __launch_bounds__(NT) TimeStepKernel(const TimeStepArgs a) {
   }
 }
 
+// The time step with a subgrid-scale model (the SGS branch of
+// ElementClass::ComputeTimeStep): the eddy viscosity at the nodal DOFs from
+// ComputeVelocityGradientsNodalDOFs (src/ElementClass.cpp:1649-1800; gradients of
+// the entropy variables V1..V4 at the DOFs, the metric at the DOFs, dimensional
+// velocity gradients) and the model, added to the viscous spectral radius.
+// Dynamic shared memory: state, nodal values, two stage buffers (5 K^3 each)
+// and the three parametric gradients of V1..V4 (12 K^3).
+template <int K, int M, int NT>
+__global__ void __launch_bounds__(NT) TimeStepSgsKernel(const TimeStepArgs a) {
+  constexpr int SLOT = Slot<K, M>::value;
+  constexpr int KD = K * K * K;
+  extern __shared__ __align__(16) double sm_ts[];
+  double *s_sol = sm_ts, *s_val = s_sol + 5 * KD, *tA = s_val + 5 * KD, *tB = tA + 5 * KD;
+  double *gr = tB + 5 * KD;  // [3][4][KD]: d/dr, d/ds, d/dt of V1..V4
+  __shared__ double s_red[64];
+  const int e = blockIdx.x;
+  if (e >= a.n_elem) return;
+  int cs = 0;
+  double cfl = a.cfl, mu = a.mu, pRef = a.p_ref, uRef = a.u_ref, rhoRef = a.rho_ref;
+  if (a.cases.elem_case) {
+    cs = a.cases.elem_case[e];
+    if (cs < 0) return;
+    const int st = a.cases.state[cs];
+    if (st != kCasePending && st != kCaseRunning) return;
+    const double *pc = a.cases.par + cs * kCasePar;
+    mu = pc[kParMu]; pRef = pc[kParPRef]; uRef = pc[kParURef]; rhoRef = pc[kParRhoRef];
+    cfl = pc[kParCfl];
+  }
+  const double *src = a.sol + (size_t)e * 5 * KD;
+  for (int i = threadIdx.x; i < 5 * KD; i += NT) s_sol[i] = src[i];
+  __syncthreads();
+  Contract<NT, SLOT, K, M, kLegDof, 2, 5, K, K, K, K, K, false>(s_sol, tA);
+  __syncthreads();
+  Contract<NT, SLOT, K, M, kLegDof, 1, 5, K, K, K, K, K, false>(tA, tB);
+  __syncthreads();
+  Contract<NT, SLOT, K, M, kLegDof, 0, 5, K, K, K, K, K, false>(tB, s_val);
+  __syncthreads();
+  const double *V1 = s_sol + KD;  // entropy variables 1..4
+  // d/dr: derivative along i (the last stage).
+  Contract<NT, SLOT, K, M, kLegDof, 2, 4, K, K, K, K, K, false>(V1, tA);
+  __syncthreads();
+  Contract<NT, SLOT, K, M, kLegDof, 1, 4, K, K, K, K, K, false>(tA, tB);
+  __syncthreads();
+  Contract<NT, SLOT, K, M, kDLegDof, 0, 4, K, K, K, K, K, false>(tB, gr);
+  __syncthreads();
+  // d/ds: derivative along j.
+  Contract<NT, SLOT, K, M, kLegDof, 2, 4, K, K, K, K, K, false>(V1, tA);
+  __syncthreads();
+  Contract<NT, SLOT, K, M, kDLegDof, 1, 4, K, K, K, K, K, false>(tA, tB);
+  __syncthreads();
+  Contract<NT, SLOT, K, M, kLegDof, 0, 4, K, K, K, K, K, false>(tB, gr + 4 * KD);
+  __syncthreads();
+  // d/dt: derivative along k.
+  Contract<NT, SLOT, K, M, kDLegDof, 2, 4, K, K, K, K, K, false>(V1, tA);
+  __syncthreads();
+  Contract<NT, SLOT, K, M, kLegDof, 1, 4, K, K, K, K, K, false>(tA, tB);
+  __syncthreads();
+  Contract<NT, SLOT, K, M, kLegDof, 0, 4, K, K, K, K, K, false>(tB, gr + 8 * KD);
+  __syncthreads();
+  const double *sc = a.elem_scalars + (size_t)e * 15;
+  const double *nm = a.vol_metric_dofs + (size_t)e * 10 * KD;
+  const double muDim = mu * pRef / uRef;
+  const double uRefInv = 1.0 / uRef;
+  const double dliInv = 1.0 / sc[0], dljInv = 1.0 / sc[1], dlkInv = 1.0 / sc[2];
+  const double dli2Inv = dliInv * dliInv, dlj2Inv = dljInv * dljInv, dlk2Inv = dlkInv * dlkInv;
+  const double dLen2Inv = dli2Inv + dlj2Inv + dlk2Inv;
+  const double radVisOverNuLam = fmax(fmax(1.0, 2.0 + kLamOverMu), kFactHFLam) * dLen2Inv;
+  const double radVisOverNuTurb = fmax(fmax(1.0, 2.0 + kLamOverMu), kFactHFTurb) * dLen2Inv;
+  double radInvMax = 0.0, radVisMax = 0.0, a2Min = 1.e+10;
+  for (int l = threadIdx.x; l < KD; l += NT) {
+    double rho, u, v, w, p, eKin;
+    EntropyToPrim(s_val[l], s_val[KD + l], s_val[2 * KD + l], s_val[3 * KD + l],
+                  s_val[4 * KD + l], rho, u, v, w, p, eKin);
+    rho *= rhoRef; u *= uRef; v *= uRef; w *= uRef; p *= pRef;
+    // Velocity gradients in computational space from the entropy-variable
+    // gradients, then Cartesian and dimensional.
+    const double un = u * uRefInv, vn = v * uRefInv, wn = w * uRefInv;
+    const double V4Inv = -p * uRefInv * uRefInv / rho;
+    double dv[3][3];  // [velocity][parameter]
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const double *G = gr + q * 4 * KD;
+      const double d4 = G[3 * KD + l];
+      dv[0][q] = -V4Inv * (G[l] + un * d4);
+      dv[1][q] = -V4Inv * (G[KD + l] + vn * d4);
+      dv[2][q] = -V4Inv * (G[2 * KD + l] + wn * d4);
+    }
+    const double drdx = nm[1 * KD + l], drdy = nm[2 * KD + l], drdz = nm[3 * KD + l];
+    const double dsdx = nm[4 * KD + l], dsdy = nm[5 * KD + l], dsdz = nm[6 * KD + l];
+    const double dtdx = nm[7 * KD + l], dtdy = nm[8 * KD + l], dtdz = nm[9 * KD + l];
+    double g[9];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      g[c] = uRef * (dv[c][0] * drdx + dv[c][1] * dsdx + dv[c][2] * dtdx);
+      g[3 + c] = uRef * (dv[c][0] * drdy + dv[c][1] * dsdy + dv[c][2] * dtdy);
+      g[6 + c] = uRef * (dv[c][0] * drdz + dv[c][1] * dsdz + dv[c][2] * dtdz);
+    }
+    const double eddy = EddyViscosity(a.sgs, sc[3], rho, g);
+    const double rhoInv = 1.0 / rho;
+    const double a2 = kGam * p * rhoInv;
+    const double velI = u * sc[6] + v * sc[7] + w * sc[8];
+    const double velJ = u * sc[9] + v * sc[10] + w * sc[11];
+    const double velK = u * sc[12] + v * sc[13] + w * sc[14];
+    const double aa = sqrt(fabs(a2));
+    const double radInv = (fabs(velI) + aa) * dliInv + (fabs(velJ) + aa) * dljInv +
+                          (fabs(velK) + aa) * dlkInv;
+    const double radVis = rhoInv * (muDim * radVisOverNuLam + eddy * radVisOverNuTurb);
+    radInvMax = fmax(radInvMax, radInv);
+    radVisMax = fmax(radVisMax, radVis);
+    a2Min = fmin(a2Min, a2);
+  }
+  radInvMax = BlockMax<NT>(radInvMax, s_red);
+  radVisMax = BlockMax<NT>(radVisMax, s_red);
+  a2Min = -BlockMax<NT>(-a2Min, s_red);
+  if (threadIdx.x == 0) {
+    if (a2Min < 0.0) atomicAdd(a.status + 2, 1);
+    const double f1[] = {2.0, 6.0, 12.0, 20.0, 28.0, 38.0, 50.0, 64.0, 80.0, 98.0};
+    const double f2[] = {6.0, 36.0, 150.0, 420.0, 980.0, 1975.0, 3575.0, 7000.0, 14000.0, 28000.0};
+    const double dtInv = f1[a.n_poly] * radInvMax + f2[a.n_poly] * radVisMax;
+    const double dtElem = cfl * uRef / dtInv;
+    atomicMin(a.dt_bits + cs, (unsigned long long)__double_as_longlong(dtElem));
+  }
+}
+
 // Reads the reduced time step (or the fixed one), records it and re-arms the reduction.
 __global__ void FinalizeDtKernel(unsigned long long *dt_bits, const double *fixed_dt, double *d_dt,
                                  double *hist, int hist_cap, int *counter) {
@@ -232,8 +356,21 @@ static cudaError_t LaunchBoundaryKM(const BoundaryArgs &a, cudaStream_t st) {
 
 template <int K, int M>
 static cudaError_t LaunchTimeStepKM(const TimeStepArgs &a, cudaStream_t st) {
-  TimeStepKernel<K, M, 64><<<a.n_elem, 64, 0, st>>>(a);
+  if (a.sgs) {
+    constexpr size_t smem = sizeof(double) * 32 * K * K * K;
+    TimeStepSgsKernel<K, M, 64><<<a.n_elem, 64, smem, st>>>(a);
+  } else {
+    TimeStepKernel<K, M, 64><<<a.n_elem, 64, 0, st>>>(a);
+  }
   return cudaGetLastError();
+}
+
+// The SGS time-step kernel's dynamic shared memory (before any capture).
+template <int K, int M>
+static cudaError_t ConfigureTimeStepKM() {
+  return cudaFuncSetAttribute(TimeStepSgsKernel<K, M, 64>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)(sizeof(double) * 32 * K * K * K));
 }
 
 #define VCPG_DISPATCH(K_, M_, CALL) \
@@ -276,6 +413,15 @@ cudaError_t LaunchResidual(int K, int M, const ResidualArgs &a, cudaStream_t st)
   if (K == 4 && M == 5) return LaunchResidualKM<4, 5>(a, st);
   if (K == 5 && M == 7) return LaunchResidualKM<5, 7>(a, st);
   if (K == 6 && M == 8) return LaunchResidualKM<6, 8>(a, st);
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t ConfigureTimeStep(int K, int M) {
+  if (K == 2 && M == 3) return ConfigureTimeStepKM<2, 3>();
+  if (K == 3 && M == 4) return ConfigureTimeStepKM<3, 4>();
+  if (K == 4 && M == 5) return ConfigureTimeStepKM<4, 5>();
+  if (K == 5 && M == 7) return ConfigureTimeStepKM<5, 7>();
+  if (K == 6 && M == 8) return ConfigureTimeStepKM<6, 8>();
   return cudaErrorInvalidValue;
 }
 
@@ -354,6 +500,8 @@ void FillOpTable(const vcpg_operators *ops, int K, int M, OpTable *t) {
   }
   for (int m = 0; m < M; ++m) t->w[m] = ops->w_int[m];
   for (int i = 0; i < K * K; ++i) t->legdof[i] = ops->leg_dofs[i];
+  if (ops->dleg_dofs)
+    for (int i = 0; i < K * K; ++i) t->dlegdof[i] = ops->dleg_dofs[i];
   for (int i = 0; i < K * K * K; ++i) t->center[i] = ops->basis_center[i];
   // FP32 copies, rounded once from the FP64 operators, for the mixed form.
   for (int i = 0; i < K * M; ++i) { t->legf[i] = (float)t->leg[i]; t->dlegf[i] = (float)t->dleg[i]; }

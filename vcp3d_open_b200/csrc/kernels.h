@@ -32,6 +32,8 @@ cudaError_t LaunchResidual(int K, int M, const ResidualArgs &a, cudaStream_t st)
 // Sets the shared-memory limits of all residual-kernel variants of a (K, M) pair;
 // call before capturing launches into a CUDA graph.
 cudaError_t ConfigureResidual(int K, int M);
+// Dynamic shared memory of the time-step kernel with an SGS model.
+cudaError_t ConfigureTimeStep(int K, int M);
 // Boundary traces + Mach weights, then the boundary states and fluxes (2 launches).
 cudaError_t LaunchBoundary(int K, int M, const BoundaryArgs &a, cudaStream_t st);
 cudaError_t LaunchTimeStep(int K, int M, const TimeStepArgs &a, cudaStream_t st);

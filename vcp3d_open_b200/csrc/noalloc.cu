@@ -135,6 +135,8 @@ extern "C" int vcpg_time_step_noalloc(const vcpg_params *params, const vcpg_oper
   if (!params || !ops || !d_sol || !d_elem_scalars || !d_dt) return VCPG_E_INVALID;
   const int K = params->n_poly + 1, M = params->n_int_1d;
   const int64_t nE = (int64_t)params->n_elem[0] * params->n_elem[1] * params->n_elem[2];
+  // The eddy viscosity of an SGS model needs the nodal-DOF metric of a handle.
+  if (params->sgs_model != VCPG_SGS_NONE) return VCPG_E_INVALID;
   if (nE <= 0) return VCPG_E_INVALID;
   if (nE > kMaxElems) return VCPG_E_ADMISSION;  // beyond the static scratch array
   if (!Supported(K, M) || K > kKMax || M > kMMax) return VCPG_E_UNSUPPORTED_KM;

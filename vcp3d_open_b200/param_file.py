@@ -538,8 +538,6 @@ def check_supported(pf: ParamFile) -> None:
     """Raise UnsupportedOption for an option outside the path."""
     if pf.fem_variables != "entropy":
         raise UnsupportedOption("FEM working variables: Conservative")
-    if pf.sgs_model != "none":
-        raise UnsupportedOption(f"Subgrid scale model: {pf.sgs_model}")
     if pf.wall_model != "no wall model":
         raise UnsupportedOption(f"Wall modeling: {pf.wall_model}")
     if pf.fluctuations not in ("no fluctuations", "pressure pulse"):

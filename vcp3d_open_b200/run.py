@@ -165,6 +165,7 @@ def load_case(pf: ParamFile) -> cases.CaseData:
         p_grid=pf.p_grid, n_poly_int=pf.n_poly_int, mach=pf.mach, reynolds=pf.reynolds,
         reynolds_length=pf.reynolds_length, t_inf=pf.t_inf,
         vel_dir=vel_dir, riemann="IsmailRoe" if pf.riemann == "ismailroe" else "Roe",
+        sgs=pf.sgs_model,
         theta_sym=pf.theta_sym, penalty=pf.penalty, cfl=pf.cfl, grid_map="none",
         bc=bcs, p_inf=ref.p_ref, outlet_len=pf.outlet_len, outlet_sigma=pf.outlet_sigma,
         outlet_beta_l=pf.outlet_beta_l, outlet_beta_t=pf.outlet_beta_t,

@@ -39,6 +39,10 @@ class Discretization:
     face_metric: np.ndarray     # [nE][6][13][M^2]
     elem_scalars: np.ndarray    # [nE][15]
     neighbors: np.ndarray       # [nE][6] int32
+    # With a subgrid-scale model: basis derivative at the nodal DOFs [K][K] and
+    # the metric terms at the nodal DOFs [nE][10][K^3] (vcpg_setup_nodal_metrics).
+    dleg_dofs: Optional[np.ndarray] = None
+    vol_metric_dofs: Optional[np.ndarray] = None
 
     @property
     def n_elements(self) -> int:
@@ -60,7 +64,11 @@ def make_params(case: CaseData, metric_compat: bool = True,
     p.cfl = s.cfl
     p.mu = r.mu_nondim
     p.p_ref, p.u_ref, p.rho_ref = r.p_ref, r.u_ref, r.rho_ref
+    p.sgs_model = SGS_CODES[s.sgs.lower()]
     return p
+
+
+SGS_CODES = {"none": capi.SGS_NONE, "wale": capi.SGS_WALE, "vreman": capi.SGS_VREMAN}
 
 
 def setup_discretization(case: CaseData, params: capi.Params,
@@ -92,6 +100,13 @@ def setup_discretization(case: CaseData, params: capi.Params,
     if rc != capi.VCPG_OK:
         raise capi.VcpgError(rc, ("vcpg_setup_geometry_device" if device else
                                   "vcpg_setup_geometry") + " failed")
+    if params.sgs_model != capi.SGS_NONE:
+        d.dleg_dofs = np.zeros((K, K))
+        d.vol_metric_dofs = np.zeros((nE, 10, K ** 3))
+        rc = lib.vcpg_setup_nodal_metrics(C.byref(params), s.p_grid, 1, capi.ptr(nodes),
+                                          capi.ptr(d.dleg_dofs), capi.ptr(d.vol_metric_dofs))
+        if rc != capi.VCPG_OK:
+            raise capi.VcpgError(rc, "vcpg_setup_nodal_metrics failed")
     return d
 
 
@@ -110,7 +125,7 @@ def nodal_to_modal(case: CaseData, params: capi.Params) -> np.ndarray:
 def open_boundary(case: CaseData) -> capi.OpenBoundary:
     """vcpg_open_boundary of a case: its boundary conditions with the free stream
     as prescribed data, NSCBC tuning parameters, sponge layers and matching layer."""
-    from .cases import prescribed_values, total_inflow_values
+    from .cases import free_stream_values, prescribed_values, total_inflow_values
     s, ref = case.spec, case.ref
     ob = capi.OpenBoundary()
     codes = {"periodic": capi.BC_NONE, "outflow_nscbc": capi.BC_OUTFLOW_NSCBC,
@@ -151,8 +166,7 @@ def open_boundary(case: CaseData) -> capi.OpenBoundary:
     ob.cml = 1 if s.cml else 0
     ob.sponge_state[:] = (list(s.sponge_state) if s.sponge_state else
                           [rho_in, vel_in[0], vel_in[1], vel_in[2], p_out])
-    ob.free_stream[:] = (list(s.free_stream) if s.free_stream else
-                         [rho_in, vel_in[0], vel_in[1], vel_in[2], p_out])
+    ob.free_stream[:] = list(s.free_stream if s.free_stream else free_stream_values(s))
     return ob
 
 
@@ -167,11 +181,14 @@ class Solver:
             disc.leg_int, disc.dleg_int, disc.leg_face, disc.dleg_face, disc.w_int,
             disc.leg_dofs, disc.basis_center, disc.vol_metric, disc.face_metric,
             disc.elem_scalars)]
-        ops = capi.Operators(*[capi.ptr(a) for a in self._keep[:7]])
         nbr = np.ascontiguousarray(disc.neighbors, dtype=np.int32)
         self._keep.append(nbr)
+        nodal = [None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+                 for a in (disc.dleg_dofs, disc.vol_metric_dofs)]
+        self._keep_nodal = nodal
+        ops = capi.Operators(*[capi.ptr(a) for a in self._keep[:7]], capi.ptr(nodal[0]))
         geom = capi.Geometry(capi.ptr(self._keep[7]), capi.ptr(self._keep[8]),
-                             capi.ptr(self._keep[9]), capi.ptr(nbr))
+                             capi.ptr(self._keep[9]), capi.ptr(nbr), capi.ptr(nodal[1]))
         h = C.c_void_p()
         rc = self.lib.vcpg_create(C.byref(params), C.byref(ops), C.byref(geom), C.byref(h))
         self.h = h
