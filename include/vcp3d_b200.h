@@ -76,6 +76,13 @@ typedef struct vcpg_params {
   double p_ref, u_ref, rho_ref; /* reference conditions (dimensional)                */
   int32_t sgs_model;          /* enum vcpg_sgs; a model needs ops->dleg_dofs and
                                  geom->vol_metric_dofs (vcpg_setup_nodal_metrics)  */
+  int32_t monitor_forces;     /* "Monitor forces": with wall faces (heat flux,
+                                 isothermal, inviscid) the monitoring data's entries
+                                 0-2 are the pressure and 3-5 the viscous force
+                                 coefficients in x, y, z (src/FluxesFace.cpp:997-1011,
+                                 1586-1612, src/SolverClass.cpp:3754-3783); else 0 */
+  double mach;                /* "Mach number" (force coefficients)                  */
+  double ref_area;            /* "Reference area force coefficients" (default 1)     */
 } vcpg_params;
 
 /* Standard-element operators (StandardElementClass, src/StandardElementClass.cpp:105-911). */

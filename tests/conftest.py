@@ -56,6 +56,25 @@ def rel_l2(a, b):
     return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
 
 
+def assert_forces_match(mon, ref, spec, rel=1e-10):
+    """Wall force coefficients (monitoring entries 0-2 pressure, 3-5 viscous)
+    against the reference's. Components that cancel across walls are rounding
+    noise, so each group is compared on an absolute scale: the pressure group
+    to rel times the coefficient of a unit pressure on all wall area, the viscous
+    group to rel times its largest component."""
+    mon, ref = np.asarray(mon, dtype=float), np.asarray(ref, dtype=float)
+    ext = np.asarray(spec.hi, dtype=float) - np.asarray(spec.lo, dtype=float)
+    area = sum(float(np.prod(np.delete(ext, f // 2))) for f, b in enumerate(spec.bc)
+               if b.startswith("wall_"))
+    if not (spec.monitor_forces and area > 0.0):
+        assert np.all(mon[:6] == 0.0)
+        return
+    scale_p = 2.0 / (1.4 * spec.mach ** 2 * spec.ref_area) * area
+    assert np.max(np.abs(mon[:3] - ref[:3])) <= rel * scale_p, (mon[:3], ref[:3])
+    tol_v = rel * np.max(np.abs(ref[3:6])) + 1e-16 * scale_p
+    assert np.max(np.abs(mon[3:6] - ref[3:6])) <= tol_v, (mon[3:6], ref[3:6])
+
+
 @pytest.fixture(scope="session")
 def gpu_available():
     import torch

@@ -113,14 +113,14 @@ OPEN_SPECS = {
     # an isothermal wall on j-max, flow along the walls; i and k periodic.
     "wall_p3_4x3x3": cases.CaseSpec(
         name="wall_p3_4x3x3", n_elem=(4, 3, 3), p=3, hi=(4.0, 3.0, 3.0), center=(2.0, 0.6, 1.5),
-        seed=8, wall_data=(0.0, 0.0, 50.0, 300.0, 0.0, 0.0),
+        seed=8, wall_data=(0.0, 0.0, 50.0, 300.0, 0.0, 0.0), monitor_forces=True,
         bc=("periodic", "periodic", "wall_heat_flux", "wall_isothermal", "periodic",
             "periodic"), **_OPEN),
     # Subsonic inflow (total conditions) and outflow (back pressure) through a
     # boundary state, inviscid walls on the j faces, k periodic.
     "subsonic_p3_5x3x2": cases.CaseSpec(
         name="subsonic_p3_5x3x2", n_elem=(5, 3, 2), p=3, hi=(5.0, 3.0, 2.0),
-        center=(0.8, 1.5, 1.0), seed=9,
+        center=(0.8, 1.5, 1.0), seed=9, monitor_forces=True, ref_area=2.5,
         bc=("inflow_subsonic", "outflow_subsonic", "wall_inviscid", "wall_inviscid", "periodic",
             "periodic"), **_OPEN),
     # Supersonic inflow / outflow states and far field on the j faces, Roe flux, degree 2.
@@ -135,7 +135,7 @@ OPEN_SPECS = {
     # gradients and so an eddy viscosity.
     "wale_p4_4x3x2_walls": cases.CaseSpec(
         name="wale_p4_4x3x2_walls", n_elem=(4, 3, 2), p=4, hi=(4.0, 3.0, 2.0),
-        center=(1.5, 0.7, 1.0), seed=13, reynolds=1.0e5, sgs="wale",
+        center=(1.5, 0.7, 1.0), seed=13, reynolds=1.0e5, sgs="wale", monitor_forces=True,
         wall_data=(0.0, 0.0, 310.0, 20.0, 0.0, 0.0), sponge=(0, 1, 0, 0, 0, 0),
         bc=("inflow_static_nscbc", "outflow_nscbc", "wall_isothermal", "wall_heat_flux",
             "periodic", "periodic"), **dict(_OPEN, kind="vortex", beta=2.0)),
@@ -192,6 +192,7 @@ SYNC_SPECS = {
         bc=("inflow_subsonic", "outflow_nscbc", "wall_heat_flux", "wall_heat_flux",
             "wall_heat_flux", "wall_heat_flux")),
         {"Synchronization time step": "2.0e-5", "Restart": "no", "CFL number": "1.0",
+         "Monitor forces": "yes",
          "Fluctuations to add to initial solution": "Pressure pulse",
          "Pressure pulse center": "2.5 0.75 0.75", "Pressure pulse strength": "0.05",
          "Pressure pulse width": "0.2"}, 2),

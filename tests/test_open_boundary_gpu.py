@@ -14,7 +14,7 @@ import tempfile
 import numpy as np
 import pytest
 
-from conftest import load_golden, open_golden_files, rel_l2
+from conftest import assert_forces_match, load_golden, open_golden_files, rel_l2
 from oracle import records
 from vcp3d_open_b200 import capi, cases, solver, workloads
 
@@ -48,6 +48,7 @@ def test_open_boundary_residual_matches_reference(gpu_available, path):
         # face arrays, where a characteristic face reconstructs a gradient from
         # placeholder data, so with such faces its value bounds the maximum
         # over the integration points from above.
+        assert_forces_match(mon, g["monitor"], g["spec"])
         ref_eddy = max(g["monitor"][7], 0.0)
         if any(b.endswith("_nscbc") for b in g["spec"].bc):
             assert mon[7] <= ref_eddy * (1.0 + 1e-12)

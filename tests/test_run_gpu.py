@@ -3,13 +3,14 @@ synchronisation steps against the reference main program's own loop on the
 same files, the written restart files, the mixed form and the command line."""
 from __future__ import annotations
 
+import dataclasses
 import os
 import re
 
 import numpy as np
 import pytest
 
-from conftest import load_golden, rel_l2, sync_golden_files, write_sync_case
+from conftest import assert_forces_match, load_golden, rel_l2, sync_golden_files, write_sync_case
 from vcp3d_open_b200 import capi, cases, param_file, run, solver
 
 pytestmark = pytest.mark.gpu
@@ -25,6 +26,10 @@ def test_synchronization_steps_match_reference(gpu_available, path, tmp_path):
     n, _, mach, _ = res.history[-1]
     assert n == int(g["n_sync"])
     assert mach ** 2 == pytest.approx(float(g["monitor"][6]), rel=1e-10)
+    pf = param_file.read(cfg)
+    assert_forces_match(res.monitoring, g["monitor"],
+                        dataclasses.replace(g["spec"], monitor_forces=pf.monitor_forces,
+                                            ref_area=pf.reference_area))
     # The restart files: the initial state and the final one, as the reference
     # writes them (dimensional conservative variables at the nodal DOFs).
     pf = param_file.read(cfg)

@@ -168,6 +168,10 @@ class CaseSpec:
     free_stream: Optional[Tuple[float, ...]] = None
     # Subgrid-scale model: "none", "wale" or "vreman" (src/SGSModel.cpp).
     sgs: str = "none"
+    # Wall force coefficients in the monitoring data ("Monitor forces") and their
+    # reference area.
+    monitor_forces: bool = False
+    ref_area: float = 1.0
 
     def __post_init__(self):
         if self.p_grid is None:
@@ -590,7 +594,8 @@ Reynolds length: {spec.reynolds_length!r}
 Free stream temperature: {spec.t_inf!r}
 Free stream velocity direction: {d[0]!r} {d[1]!r} {d[2]!r}
 Fluctuations to add to initial solution: No fluctuations
-Monitor forces: no
+Monitor forces: {"yes" if spec.monitor_forces else "no"}
+Reference area force coefficients: {spec.ref_area!r}
 Number of synchronization time steps: 1
 Synchronization time step: 1.0
 CFL number: {spec.cfl!r}

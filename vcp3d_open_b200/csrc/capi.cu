@@ -44,6 +44,7 @@ struct vcpg_handle {
   int *d_bface = nullptr;
   double *d_bpresc = nullptr, *d_pc = nullptr, *d_dlq = nullptr;
   double *d_btrace = nullptr, *d_bmach = nullptr, *d_bflux = nullptr;
+  double *d_bforce = nullptr;   // [nB][6] wall-face forces of a monitored residual
   BlockFaceCfg *d_cfg = nullptr;
   void *d_fflux = nullptr;  // fluxes of every element's Min faces (FaceFluxKernel)
   int *d_sponge = nullptr;
@@ -173,6 +174,8 @@ int EnqueueResidual(vcpg_handle *h, const ResidualArgs &a, int *launches) {
   if (h->open && h->nB > 0) {
     BoundaryArgs b = MakeBoundaryArgs(h);
     b.eddymax = a.eddymax;
+    // Wall forces only for a residual with monitoring data (mach2max set).
+    b.bforce = (a.mach2max && h->prm.monitor_forces) ? h->d_bforce : nullptr;
     VCPG_CUDA(h, LaunchBoundary(h->K, h->M, b, h->stream));
     n += 2;
   }
@@ -228,7 +231,8 @@ int vcpg_destroy(vcpg_handle *h) {
                   h->d_nbr, h->d_dtbits, h->d_mach2, h->d_dt, h->d_fixed, h->d_hist,
                   h->d_status, h->d_counter, h->d_cgstats, h->d_bface, h->d_bpresc, h->d_pc,
                   h->d_dlq, h->d_btrace, h->d_bmach, h->d_bflux, h->d_sponge, h->d_dampfn,
-                  h->d_dampst, h->d_cml, h->d_cfg, h->d_fflux, h->d_eddymax, h->d_nmetric};
+                  h->d_dampst, h->d_cml, h->d_cfg, h->d_fflux, h->d_eddymax, h->d_nmetric,
+                  h->d_bforce};
   for (void *p : bufs)
     if (p) cudaFree(p);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -261,6 +265,11 @@ int vcpg_create(const vcpg_params *params, const vcpg_operators *ops, const vcpg
   }
   if (params->precision != VCPG_FP64 && params->precision != VCPG_MIXED) {
     int rc = Fail(h, VCPG_E_INVALID, "precision must be VCPG_FP64 or VCPG_MIXED");
+    *out = h;
+    return rc;
+  }
+  if (params->monitor_forces && !(params->mach > 0.0 && params->ref_area > 0.0)) {
+    int rc = Fail(h, VCPG_E_INVALID, "force monitoring needs mach > 0 and ref_area > 0");
     *out = h;
     return rc;
   }
@@ -372,9 +381,12 @@ int vcpg_residual(vcpg_handle *h, double *monitoring, int32_t keep_raw) {
     cudaError_t e = cudaMalloc((void **)&h->d_resRaw, (size_t)h->nE * 5 * h->KD * 8);
     if (e != cudaSuccess) return Fail(h, VCPG_E_OOM, "cudaMalloc raw residual");
   }
+  const bool forces = monitoring && h->prm.monitor_forces && h->d_bforce && h->nB > 0;
   if (monitoring) {
     VCPG_CUDA(h, cudaMemsetAsync(h->d_mach2, 0, 8, h->stream));
     VCPG_CUDA(h, cudaMemsetAsync(h->d_eddymax, 0, 8, h->stream));
+    if (forces)   // faces that are no walls keep zeros
+      VCPG_CUDA(h, cudaMemsetAsync(h->d_bforce, 0, sizeof(double) * 6 * h->nB, h->stream));
   }
   ResidualArgs a = MakeResidualArgs(h, keep_raw ? h->d_resRaw : nullptr,
                                     monitoring ? h->d_mach2 : nullptr);
@@ -392,8 +404,19 @@ int vcpg_residual(vcpg_handle *h, double *monitoring, int32_t keep_raw) {
     VCPG_CUDA(h, cudaMemcpy(&bits, h->d_eddymax, 8, cudaMemcpyDeviceToHost));
     double eddyMax;
     std::memcpy(&eddyMax, &bits, 8);
-    // Force coefficients are not computed (no wall forces): zero.
+    // Force coefficients (src/SolverClass.cpp:3754-3783): pressure and viscous
+    // forces of the wall faces, summed in boundary-face order and scaled by
+    // 2 / (gamma M^2 A_ref); zero without force monitoring or walls.
     for (int i = 0; i < 6; ++i) monitoring[i] = 0.0;
+    if (forces) {
+      std::vector<double> bf((size_t)6 * h->nB);
+      VCPG_CUDA(h, cudaMemcpy(bf.data(), h->d_bforce, sizeof(double) * bf.size(),
+                              cudaMemcpyDeviceToHost));
+      for (int b = 0; b < h->nB; ++b)
+        for (int i = 0; i < 6; ++i) monitoring[i] += bf[(size_t)b * 6 + i];
+      const double factCoef = 2.0 / (1.4 * h->prm.mach * h->prm.mach * h->prm.ref_area);
+      for (int i = 0; i < 6; ++i) monitoring[i] *= factCoef;
+    }
     monitoring[6] = m2;
     monitoring[7] = eddyMax;   // maximum eddy viscosity of the volume and face points
   }
@@ -542,6 +565,7 @@ int vcpg_set_open_boundary(vcpg_handle *h, const vcpg_open_boundary *ob,
       (rc = upload((void **)&h->d_dlq, ob_host.dlq.data(), sizeof(double) * ob_host.dlq.size())) ||
       (rc = upload((void **)&h->d_btrace, nullptr, sizeof(double) * nB * 4 * 5 * M2)) ||
       (rc = upload((void **)&h->d_bmach, nullptr, sizeof(double) * nB)) ||
+      (rc = upload((void **)&h->d_bforce, nullptr, sizeof(double) * nB * 6)) ||
       (rc = upload((void **)&h->d_bflux, nullptr, sizeof(double) * nB * 4 * 5 * M2)) ||
       (rc = upload((void **)&h->d_sponge, ob_host.spongeIdx.data(), sizeof(int) * ob_host.spongeIdx.size())) ||
       (rc = upload((void **)&h->d_dampfn, ob_host.dampFn.data(), sizeof(double) * nS * 3 * MD)) ||

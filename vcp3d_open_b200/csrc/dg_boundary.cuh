@@ -44,6 +44,8 @@ struct BoundaryArgs {
   int riemann, metric_compat;
   int sgs;                     // enum vcpg_sgs
   unsigned long long *eddymax; // optional: bits of the max eddy viscosity
+  double *bforce;              // optional [nB][6]: pressure (0-2) and viscous (3-5)
+                               // force of each wall face, monitoring only
   const BlockFaceCfg *cfgs;    // [nCases][6] per case and block face
   // Several cases per launch (null case_state: one case): the case slot is entry
   // kBfCase of the boundary-face row; only faces of cases in state `require` run.
@@ -152,6 +154,10 @@ __device__ __forceinline__ void WeakBoundaryFlux(const BoundaryArgs &a, const in
   const double lenScale = a.elem_scalars[(size_t)e * 15 + d];
   double *out = a.bflux + (size_t)b * 4 * 5 * M2;
   const int pFast = BFastParam(d), pSlow = 3 - d - pFast;
+  const bool forces = a.bforce && (type == VCPG_BC_WALL_HEAT_FLUX ||
+                                   type == VCPG_BC_WALL_ISOTHERMAL ||
+                                   type == VCPG_BC_WALL_INVISCID);
+  double force[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   for (int l = threadIdx.x; l < M2; l += NT) {
     const int li = l / M, lj = l - li * M;
     double VL[5], VR[5], gx[5], gy[5], gz[5];
@@ -269,12 +275,27 @@ __device__ __forceinline__ void WeakBoundaryFlux(const BoundaryArgs &a, const in
       IsmailRoeFlux(VL, VR, nx, ny, nz, wf * area, flux, factU);
     else
       RoeFlux(VL, VR, nx, ny, nz, 0.5 * wf * area, flux, factU);
-    double eddy = 0.0;
+    double eddy = 0.0, visc[3];
     ViscousPenaltySymFlux(VL, VR, gx, gy, gz, nx, ny, nz, wf, area, mu,
                           a.tau_num / lenScale, a.theta_sym, flux, sx, sy, sz, hfMult,
-                          wf * area * qWall, a.sgs, a.elem_scalars[(size_t)e * 15 + 3], &eddy);
+                          wf * area * qWall, a.sgs, a.elem_scalars[(size_t)e * 15 + 3], &eddy,
+                          forces ? visc : nullptr);
     if (a.sgs && a.eddymax && eddy > 0.0)
       atomicMax(a.eddymax, (unsigned long long)__double_as_longlong(eddy));
+    if (forces) {
+      // Pressure force: the mean of both states' pressures on the normal
+      // pointing into the boundary (src/FluxesFace.cpp:997-1011).
+      double r, uu, vv, ww, pL, pR, q2;
+      FaceStatePrim(VL, r, uu, vv, ww, pL, q2);
+      FaceStatePrim(VR, r, uu, vv, ww, pR, q2);
+      const double abv = 0.5 * wf * area * (pL + pR);
+      force[0] += abv * nx;
+      force[1] += abv * ny;
+      force[2] += abv * nz;
+      force[3] += visc[0];
+      force[4] += visc[1];
+      force[5] += visc[2];
+    }
 #pragma unroll
     for (int n = 0; n < 5; ++n) {
       const int mi = a.metric_compat ? n : l;
@@ -287,6 +308,22 @@ __device__ __forceinline__ void WeakBoundaryFlux(const BoundaryArgs &a, const in
       out[(1 * 5 + n) * M2 + l] = flux[n];
       out[(2 * 5 + n) * M2 + l] = sym[d];
       out[(3 * 5 + n) * M2 + l] = sym[pSlow];
+    }
+  }
+  if (forces) {
+    // Face sums of the six force components (warp shuffles, then warp order).
+    __shared__ double s_force[6][NT / 32];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      double v = force[c];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      if ((threadIdx.x & 31) == 0) s_force[c][threadIdx.x >> 5] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+      double v = 0.0;
+      for (int w = 0; w < NT / 32; ++w) v += s_force[threadIdx.x][w];
+      a.bforce[(size_t)b * 6 + threadIdx.x] = v;
     }
   }
 }

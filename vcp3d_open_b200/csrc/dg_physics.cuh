@@ -288,7 +288,8 @@ __device__ __forceinline__ void ViscousPenaltySymFlux(
     const T nnx, const T nny, const T nnz, const T wf,
     const T area, const T mu, const T tau, const T thetaSym, T *f,
     T *sx, T *sy, T *sz, const T hfMult = T(1.0), const T qWallArea = T(0.0),
-    const int sgs = 0, const T lenLES = T(0.0), T *eddyOut = nullptr) {
+    const int sgs = 0, const T lenLES = T(0.0), T *eddyOut = nullptr,
+    T *viscForce = nullptr) {
   const T factHFLam = hfMult * T(kFactHFLam), factHFTurb = hfMult * T(kFactHFTurb);
   const T gm1 = T(kGam) - T(1.0), ovgm1 = T(1.0) / gm1, ov1mg = -ovgm1;
   const T V1 = T(0.5) * (VL[1] + VR[1]);
@@ -340,6 +341,12 @@ __device__ __forceinline__ void ViscousPenaltySymFlux(
     f[1] -= tauxx * nx + tauxy * ny + tauxz * nz;
     f[2] -= tauxy * nx + tauyy * ny + tauyz * nz;
     f[3] -= tauxz * nx + tauyz * ny + tauzz * nz;
+    if (viscForce) {
+      // Viscous wall force of the point (src/FluxesFace.cpp:1590-1612).
+      viscForce[0] = -(tauxx * nx + tauxy * ny + tauxz * nz);
+      viscForce[1] = -(tauxy * nx + tauyy * ny + tauyz * nz);
+      viscForce[2] = -(tauxz * nx + tauyz * ny + tauzz * nz);
+    }
     f[4] -= (u * tauxx + v * tauxy + w * tauxz - qx) * nx +
             (u * tauxy + v * tauyy + w * tauyz - qy) * ny +
             (u * tauxz + v * tauyz + w * tauzz - qz) * nz;

@@ -165,7 +165,7 @@ def load_case(pf: ParamFile) -> cases.CaseData:
         p_grid=pf.p_grid, n_poly_int=pf.n_poly_int, mach=pf.mach, reynolds=pf.reynolds,
         reynolds_length=pf.reynolds_length, t_inf=pf.t_inf,
         vel_dir=vel_dir, riemann="IsmailRoe" if pf.riemann == "ismailroe" else "Roe",
-        sgs=pf.sgs_model,
+        sgs=pf.sgs_model, monitor_forces=pf.monitor_forces, ref_area=pf.reference_area,
         theta_sym=pf.theta_sym, penalty=pf.penalty, cfl=pf.cfl, grid_map="none",
         bc=bcs, p_inf=ref.p_ref, outlet_len=pf.outlet_len, outlet_sigma=pf.outlet_sigma,
         outlet_beta_l=pf.outlet_beta_l, outlet_beta_t=pf.outlet_beta_t,
@@ -243,6 +243,18 @@ class RunResult:
     rk_steps: int
     history: list                # (step, time, mach_max, rk_steps)
     files: list
+    monitoring: Optional[np.ndarray] = None   # the last step's 8 monitoring values
+
+
+def _force_directions(pf: ParamFile):
+    """Free-stream and lift directions of the force coefficients
+    (src/InputParamClass.cpp:697-736): unit vectors, the lift direction by default
+    normal to the free stream without a z component."""
+    v = np.asarray(pf.vel_dir if pf.vel_dir is not None else (1.0, 0.0, 0.0), dtype=float)
+    v = v / np.linalg.norm(v)
+    lift = np.asarray(pf.lift_dir if pf.lift_dir is not None else (-v[1], v[0], 0.0),
+                      dtype=float)
+    return v, lift / np.linalg.norm(lift)
 
 
 def run(path: str, precision: int = capi.FP64, steps: Optional[int] = None,
@@ -261,18 +273,32 @@ def run(path: str, precision: int = capi.FP64, steps: Optional[int] = None,
         dt_sync = pf.dt_sync * case.ref.u_ref       # non-dimensional (reference length 1)
         if write:
             files.append(write_solution(pf, case, disc, s.get_state(), 0))
-        print(f"#{'step':>9}{'wall (s)':>13}{'time (s)':>13}{'Mach max':>13}{'RK steps':>10}",
+        sgs = case.spec.sgs != "none"
+        forces = params.monitor_forces != 0
+        vel_dir, lift_dir = _force_directions(pf)
+        print(f"#{'step':>9}{'wall (s)':>13}{'time (s)':>13}{'Mach max':>13}{'RK steps':>10}"
+              + (f"{'mu_t/mu':>13}" if sgs else "")
+              + (f"{'CL':>13}{'CD':>13}{'CL visc':>13}{'CD visc':>13}" if forces else ""),
               file=out)
+        last_mon = None
         t0 = time.perf_counter()
         total_rk, saved = 0, True
         for n in range(1, n_sync + 1):
             saved = False
             if n % pf.n_history == 0:
                 rk, mon = s.synchronization_step(dt_sync, monitoring=True)
+                last_mon = mon
                 mach = math.sqrt(max(mon[6], 0.0))
                 history.append((n, n * pf.dt_sync, mach, rk))
-                print(f"{n:>10}{time.perf_counter() - t0:>13.5e}{n * pf.dt_sync:>13.5e}"
-                      f"{mach:>13.5e}{rk:>10}", file=out, flush=True)
+                line = (f"{n:>10}{time.perf_counter() - t0:>13.5e}{n * pf.dt_sync:>13.5e}"
+                        f"{mach:>13.5e}{rk:>10}")
+                if sgs:   # eddy over laminar viscosity (WriteTimeStepData)
+                    line += f"{mon[7] / case.ref.mu_nondim:>13.5e}"
+                if forces:
+                    cl_i, cl_v = float(mon[0:3] @ lift_dir), float(mon[3:6] @ lift_dir)
+                    cd_i, cd_v = float(mon[0:3] @ vel_dir), float(mon[3:6] @ vel_dir)
+                    line += f"{cl_i + cl_v:>13.5e}{cd_i + cd_v:>13.5e}{cl_v:>13.5e}{cd_v:>13.5e}"
+                print(line, file=out, flush=True)
             else:
                 rk = s.synchronization_step(dt_sync)
             total_rk += rk
@@ -282,7 +308,7 @@ def run(path: str, precision: int = capi.FP64, steps: Optional[int] = None,
         state = s.get_state()
         if write and not saved:
             files.append(write_solution(pf, case, disc, state, n_sync))
-        return RunResult(state, total_rk, history, files)
+        return RunResult(state, total_rk, history, files, last_mon)
     finally:
         s.close()
 

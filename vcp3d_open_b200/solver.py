@@ -65,6 +65,11 @@ def make_params(case: CaseData, metric_compat: bool = True,
     p.mu = r.mu_nondim
     p.p_ref, p.u_ref, p.rho_ref = r.p_ref, r.u_ref, r.rho_ref
     p.sgs_model = SGS_CODES[s.sgs.lower()]
+    # The reference monitors forces only where wall faces exist
+    # (src/InputParamClass.cpp:1574-1575).
+    walls = any(b.startswith("wall_") for b in s.bc)
+    p.monitor_forces = 1 if (s.monitor_forces and walls) else 0
+    p.mach, p.ref_area = s.mach, s.ref_area
     return p
 
 
