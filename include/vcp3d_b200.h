@@ -206,6 +206,33 @@ int vcpg_sync(vcpg_handle *h);
 /* The handle's CUDA stream (cudaStream_t) for callers that time or order work. */
 void *vcpg_stream(vcpg_handle *h);
 
+/* ---- A block split across GPUs (the reference's DistributeGrid,
+ * src/SolverClass.cpp:1537-1584, with the halo exchange of Residual). ----
+ * A rank's handle holds its owned elements first, then ghost copies of the
+ * neighbouring ranks' elements. vcpg_set_partition declares elements
+ * [0, n_owned) owned: residual, time step (local minimum) and stages run on
+ * them. Elements [n_owned, n_owned + n_face_ghost) are ghosts whose Min faces
+ * towards owned elements are evaluated here (their other lower neighbours -1);
+ * the remaining elements are ghosts that only provide their state. Periodic
+ * blocks only (open boundaries are rejected); vcpg_step and
+ * vcpg_synchronization_step are rejected, a step being: vcpg_time_step, the
+ * minimum over ranks, then per stage vcpg_rk_stage, the exchange of the ghost
+ * states (vcpg_pack_states / vcpg_unpack_states around the transport) and
+ * vcpg_residual. */
+int vcpg_set_partition(vcpg_handle *h, int32_t n_owned, int32_t n_face_ghost);
+
+/* Device-to-device copies, on the handle's stream, between the states of
+ * elements [first, first + count) and a device buffer of count * 5 K^3
+ * doubles (element-major, as the state). */
+int vcpg_pack_states(vcpg_handle *h, int32_t first, int32_t count, double *d_buf);
+int vcpg_unpack_states(vcpg_handle *h, int32_t first, int32_t count, const double *d_buf);
+
+/* One Runge-Kutta stage of step dt with the current residual on the owned
+ * elements (the stage loop of ExecuteTimeSynchronizationStep,
+ * src/SolverClass.cpp:2368-2396): SSP-RK3 stage 0-2 (stage 0 keeps the state
+ * as the step's start) or LSRK4 stage 0-4. */
+int vcpg_rk_stage(vcpg_handle *h, int32_t scheme, int32_t stage, double dt);
+
 /* Number of this library's kernel launches issued since creation. */
 int64_t vcpg_launch_count(const vcpg_handle *h);
 

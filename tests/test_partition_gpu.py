@@ -1,0 +1,93 @@
+"""A periodic block split into k slabs, all slabs driven by one process on one
+GPU (LocalTransport): residuals and steps of the partitioned block against the
+single-handle path on the same block. Every face is evaluated from the same
+inputs in both, so the results are equal bit for bit."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from vcp3d_open_b200 import capi, cases, partition, solver
+
+pytestmark = pytest.mark.gpu
+
+TWO_PI = 6.283185307179586
+
+SPECS = [
+    cases.CaseSpec(name="tgv_p3_3x4x6", kind="tgv", n_elem=(3, 4, 6), p=3, hi=(TWO_PI,) * 3,
+                   mach=0.1, reynolds=1600.0, grid_map="random", grid_amp=0.01, seed=2),
+    cases.CaseSpec(name="vortex_p2_roe_4x3x5", kind="vortex", n_elem=(4, 3, 5), p=2,
+                   riemann="Roe", hi=(10.0, 7.5, 12.5), center=(5.0, 3.75, 6.25)),
+    cases.CaseSpec(name="tgv_p4_wale_3x3x4", kind="tgv", n_elem=(3, 3, 4), p=4,
+                   hi=(TWO_PI,) * 3, mach=0.1, reynolds=1.0e5, grid_map="random",
+                   grid_amp=0.005, seed=11, sgs="wale"),
+]
+
+
+def _setup(spec, world, precision=capi.FP64):
+    case = cases.build_case(spec)
+    prm = solver.make_params(case, precision=precision)
+    disc = solver.setup_discretization(case, prm)
+    modal = solver.nodal_to_modal(case, prm)
+    whole = solver.Solver(prm, disc)
+    whole.set_state(modal)
+    shards = [partition.Shard(sl, prm, disc, modal) for sl in partition.slabs(spec.n_elem, world)]
+    return whole, partition.ShardedSolver(partition.LocalTransport(shards))
+
+
+def _gather(sharded, what):
+    out = []
+    for s in sharded.shards:
+        a = s.solver.get_residual() if what == "res" else s.solver.get_state()
+        out.append(a[:s.slab.n_owned])
+    return np.concatenate(out)
+
+
+@pytest.mark.parametrize("world", [2, 3])
+@pytest.mark.parametrize("spec", SPECS, ids=lambda s: s.name)
+def test_partitioned_residual_and_steps_equal_the_block(gpu_available, spec, world):
+    whole, sharded = _setup(spec, world)
+    try:
+        mon_w = whole.residual(monitoring=True)
+        mon_s = sharded.residual(monitoring=True)
+        assert np.array_equal(_gather(sharded, "res"), whole.get_residual())
+        assert mon_s[6] == mon_w[6] and mon_s[7] == mon_w[7]
+        assert sharded.time_step() == whole.time_step()
+        for scheme in (capi.LSRK4, capi.SSPRK3):
+            hw = whole.step(2, scheme)
+            hs = sharded.step(2, scheme)
+            assert np.array_equal(hs, hw)
+            assert np.array_equal(_gather(sharded, "state"), whole.get_state())
+    finally:
+        whole.close()
+        for s in sharded.shards:
+            s.solver.close()
+
+
+def test_partitioned_mixed_form(gpu_available):
+    whole, sharded = _setup(SPECS[0], 2, precision=capi.MIXED)
+    try:
+        hw = whole.step(3, capi.LSRK4)
+        hs = sharded.step(3, capi.LSRK4)
+        np.testing.assert_allclose(hs, hw, rtol=1e-14)
+        assert rel_l2(_gather(sharded, "state"), whole.get_state()) < 1e-14
+    finally:
+        whole.close()
+        for s in sharded.shards:
+            s.solver.close()
+
+
+def test_partitioned_handle_refuses_whole_block_calls(gpu_available):
+    _, sharded = _setup(SPECS[1], 2)
+    try:
+        s = sharded.shards[0].solver
+        with pytest.raises(capi.VcpgError, match="stage by stage"):
+            s.step(1)
+        with pytest.raises(capi.VcpgError, match="partition"):
+            s.set_partition(0, 0)
+        with pytest.raises(capi.VcpgError):
+            s.rk_stage(capi.SSPRK3, 3, 1e-3)
+    finally:
+        for sh in sharded.shards:
+            sh.solver.close()

@@ -27,6 +27,7 @@ BC_NONE, BC_OUTFLOW_NSCBC, BC_INFLOW_STATIC_NSCBC, BC_INFLOW_TOTAL_NSCBC = 0, 1,
 EXPORTED = [
     "vcpg_create", "vcpg_destroy", "vcpg_last_error", "vcpg_setup_geometry",
     "vcpg_setup_geometry_device", "vcpg_setup_nodal_metrics",
+    "vcpg_set_partition", "vcpg_pack_states", "vcpg_unpack_states", "vcpg_rk_stage",
     "vcpg_nodal_conservative_to_modal", "vcpg_set_state", "vcpg_get_state",
     "vcpg_get_residual", "vcpg_residual", "vcpg_get_raw_residual", "vcpg_time_step",
     "vcpg_step", "vcpg_synchronization_step", "vcpg_sync", "vcpg_stream", "vcpg_launch_count", "vcpg_stats",
@@ -120,6 +121,10 @@ def load() -> C.CDLL:
     lib.vcpg_synchronization_step.argtypes = [hp, C.c_double, C.c_int32,
                                               C.POINTER(C.c_int32), dp]
     lib.vcpg_sync.argtypes = [hp]
+    lib.vcpg_set_partition.argtypes = [hp, C.c_int32, C.c_int32]
+    lib.vcpg_pack_states.argtypes = [hp, C.c_int32, C.c_int32, C.c_void_p]
+    lib.vcpg_unpack_states.argtypes = [hp, C.c_int32, C.c_int32, C.c_void_p]
+    lib.vcpg_rk_stage.argtypes = [hp, C.c_int32, C.c_int32, C.c_double]
     lib.vcpg_stream.argtypes = [hp]
     lib.vcpg_stream.restype = C.c_void_p
     lib.vcpg_launch_count.argtypes = [hp]

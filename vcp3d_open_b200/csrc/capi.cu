@@ -23,6 +23,9 @@ struct vcpg_handle {
   vcpg_params prm{};
   int K = 0, M = 0, KD = 0, MD = 0, M2 = 0;
   int64_t nE = 0;
+  // Partition (vcpg_set_partition): residual, time step and stages run on the
+  // first nOwned elements, face fluxes on the first nFace; both nE otherwise.
+  int64_t nOwned = 0, nFace = 0;
   cudaStream_t stream = nullptr;
   double *d_sol = nullptr, *d_solOld = nullptr, *d_res = nullptr, *d_resRaw = nullptr;
   double *d_vol = nullptr, *d_face = nullptr, *d_sc = nullptr;
@@ -86,7 +89,8 @@ ResidualArgs MakeResidualArgs(vcpg_handle *h, double *rawOut, unsigned long long
   a.face_metric = h->d_face;
   a.elem_scalars = h->d_sc;
   a.nbr = h->d_nbr;
-  a.n_elem = (int)h->nE;
+  a.n_elem = (int)h->nOwned;
+  a.n_face_elem = (int)h->nFace;
   a.mu = h->prm.mu;
   a.tau_num = (double)((h->prm.n_poly + 1) * (h->prm.n_poly + 1)) * h->prm.rel_penalty;
   a.theta_sym = h->prm.theta_sym;
@@ -116,7 +120,7 @@ TimeStepArgs MakeTimeStepArgs(vcpg_handle *h) {
   TimeStepArgs t{};
   t.sol = h->d_sol;
   t.elem_scalars = h->d_sc;
-  t.n_elem = (int)h->nE;
+  t.n_elem = (int)h->nOwned;
   t.n_poly = h->prm.n_poly;
   t.cfl = h->prm.cfl;
   t.mu = h->prm.mu;
@@ -188,7 +192,7 @@ int EnqueueResidual(vcpg_handle *h, const ResidualArgs &a, int *launches) {
 int ResidualLaunches(const vcpg_handle *h) { return (h->open && h->nB > 0) ? 4 : 2; }
 
 int EnqueueStep(vcpg_handle *h, int scheme) {
-  const size_t n = (size_t)h->nE * 5 * h->KD;
+  const size_t n = (size_t)h->nOwned * 5 * h->KD;
   TimeStepArgs t = MakeTimeStepArgs(h);
   VCPG_CUDA(h, LaunchTimeStep(h->K, h->M, t, h->stream));
   // The fixed step lives in device memory (d_fixed); a non-positive value selects the CFL step.
@@ -257,6 +261,7 @@ int vcpg_create(const vcpg_params *params, const vcpg_operators *ops, const vcpg
     *out = h;
     return rc;
   }
+  h->nOwned = h->nFace = h->nE;
   if (!Supported(h->K, h->M) || h->K > kKMax || h->M > kMMax) {
     int rc = Fail(h, VCPG_E_UNSUPPORTED_KM, "no kernel for K=" + std::to_string(h->K) +
                                                 " M=" + std::to_string(h->M));
@@ -441,6 +446,9 @@ int vcpg_time_step(vcpg_handle *h, double *dt) {
 int vcpg_step(vcpg_handle *h, int32_t scheme, int32_t n_steps, double fixed_dt,
               double *dt_history) {
   if (!h || n_steps < 0 || (scheme != VCPG_SSPRK3 && scheme != VCPG_LSRK4)) return VCPG_E_INVALID;
+  if (h->nOwned != h->nE)
+    return Fail(h, VCPG_E_INVALID, "a partitioned block steps stage by stage (vcpg_rk_stage) "
+                                   "with the halo exchanged before every residual");
   if (n_steps == 0) return VCPG_OK;
   if (n_steps > h->hist_cap) {
     // Grow the history buffer; graphs hold the old pointer and are rebuilt.
@@ -524,6 +532,64 @@ int vcpg_sync(vcpg_handle *h) {
   return CheckStatus(h);
 }
 
+int vcpg_set_partition(vcpg_handle *h, int32_t n_owned, int32_t n_face_ghost) {
+  if (!h) return VCPG_E_INVALID;
+  if (n_owned < 1 || n_face_ghost < 0 || (int64_t)n_owned + n_face_ghost > h->nE)
+    return Fail(h, VCPG_E_INVALID, "partition: need 1 <= n_owned and n_owned + n_face_ghost "
+                                   "<= the handle's elements");
+  if (h->open)
+    return Fail(h, VCPG_E_INVALID, "partition: blocks with open boundaries are not partitioned");
+  h->nOwned = n_owned;
+  h->nFace = (int64_t)n_owned + n_face_ghost;
+  h->res_valid = false;
+  for (int s = 0; s < 2; ++s) {
+    if (h->exec[s]) { cudaGraphExecDestroy(h->exec[s]); h->exec[s] = nullptr; }
+    if (h->graph[s]) { cudaGraphDestroy(h->graph[s]); h->graph[s] = nullptr; }
+  }
+  return VCPG_OK;
+}
+
+int vcpg_pack_states(vcpg_handle *h, int32_t first, int32_t count, double *d_buf) {
+  if (!h || !d_buf || first < 0 || count < 0 || (int64_t)first + count > h->nE)
+    return VCPG_E_INVALID;
+  const size_t per = (size_t)5 * h->KD;
+  VCPG_CUDA(h, cudaMemcpyAsync(d_buf, h->d_sol + (size_t)first * per, sizeof(double) * per * count,
+                               cudaMemcpyDeviceToDevice, h->stream));
+  return VCPG_OK;
+}
+
+int vcpg_unpack_states(vcpg_handle *h, int32_t first, int32_t count, const double *d_buf) {
+  if (!h || !d_buf || first < 0 || count < 0 || (int64_t)first + count > h->nE)
+    return VCPG_E_INVALID;
+  const size_t per = (size_t)5 * h->KD;
+  VCPG_CUDA(h, cudaMemcpyAsync(h->d_sol + (size_t)first * per, d_buf, sizeof(double) * per * count,
+                               cudaMemcpyDeviceToDevice, h->stream));
+  h->res_valid = false;
+  return VCPG_OK;
+}
+
+int vcpg_rk_stage(vcpg_handle *h, int32_t scheme, int32_t stage, double dt) {
+  if (!h || !(dt > 0.0)) return VCPG_E_INVALID;
+  if (!((scheme == VCPG_SSPRK3 && stage >= 0 && stage < 3) ||
+        (scheme == VCPG_LSRK4 && stage >= 0 && stage < 5)))
+    return Fail(h, VCPG_E_INVALID, "rk stage: SSP-RK3 stages 0-2, LSRK4 stages 0-4");
+  // The stage kernels read the step from device memory.
+  VCPG_CUDA(h, cudaMemcpyAsync(h->d_dt, &dt, 8, cudaMemcpyHostToDevice, h->stream));
+  const size_t n = (size_t)h->nOwned * 5 * h->KD;
+  if (scheme == VCPG_SSPRK3) {
+    const double alphaRK[] = {1.0, 3.0 / 4.0, 1.0 / 3.0};
+    const double betaRK[] = {1.0, 1.0 / 4.0, 2.0 / 3.0};
+    VCPG_CUDA(h, LaunchSspStage(h->d_sol, h->d_solOld, h->d_res, h->d_dt, alphaRK[stage],
+                                betaRK[stage], stage == 0, n, h->stream, CaseView{}, 5 * h->KD));
+  } else {
+    VCPG_CUDA(h, LaunchLsrkStage(h->d_sol, h->d_solOld, h->d_res, h->d_dt, kLsA[stage],
+                                 kLsB[stage], n, h->stream, CaseView{}, 5 * h->KD));
+  }
+  h->launches += 1;
+  h->res_valid = false;
+  return VCPG_OK;
+}
+
 void *vcpg_stream(vcpg_handle *h) { return h ? (void *)h->stream : nullptr; }
 
 int64_t vcpg_launch_count(const vcpg_handle *h) { return h ? h->launches : 0; }
@@ -543,6 +609,8 @@ int vcpg_set_open_boundary(vcpg_handle *h, const vcpg_open_boundary *ob,
                            const double *grid_nodes) {
   if (!h || !ob || !geom) return VCPG_E_INVALID;
   if (h->open) return Fail(h, VCPG_E_INVALID, "open boundaries are already configured");
+  if (h->nOwned != h->nE)
+    return Fail(h, VCPG_E_INVALID, "open boundaries: the block is partitioned");
   OpenBoundaryHost ob_host;
   std::string err;
   int rc = BuildOpenBoundary(h->prm, *ob, *geom, p_grid, dof_location, grid_nodes, ob_host, err);

@@ -45,7 +45,10 @@ struct ResidualArgs {
   const double *face_metric;   // [nE][6][13][M^2]
   const double *elem_scalars;  // [nE][15]
   const int *nbr;              // [nE][6]
-  int n_elem;
+  int n_elem;                  // elements whose residual is computed
+  // Elements whose Min-face fluxes FaceFluxKernel computes (0: n_elem). More than
+  // n_elem in a partitioned block: the ghost elements above the owned ones.
+  int n_face_elem;
   double mu;                   // non-dimensional viscosity
   double tau_num;              // (p+1)^2 * relative penalty parameter
   double theta_sym;
@@ -1161,7 +1164,7 @@ __global__ void __launch_bounds__(NT, (FluxPlan<K, M, T>::MIN_BLOCKS)) FaceFluxK
   T *smem = reinterpret_cast<T *>(smem_raw);
   T *s_sol = smem, *s_fv = s_sol + 5 * KD, *work = s_fv + 4 * kKMax;
   const int e = blockIdx.x;
-  if (e >= a.n_elem) return;
+  if (e >= (a.n_face_elem > 0 ? a.n_face_elem : a.n_elem)) return;
   double mu = a.mu;
   if (a.cases.elem_case) {
     const int cs = a.cases.elem_case[e];

@@ -329,7 +329,8 @@ static cudaError_t LaunchResidualKMT(const ResidualArgs &a, cudaStream_t st) {
   cudaError_t err = ConfigureKMT<K, M, T, OPEN>();
   if (err == cudaSuccess) err = ConfigureFluxKMT<K, M, T>();
   if (err != cudaSuccess) return err;
-  FaceFluxKernel<K, M, PF::NT, T><<<a.n_elem, PF::NT, PF::BYTES, st>>>(a);
+  FaceFluxKernel<K, M, PF::NT, T>
+      <<<a.n_face_elem > 0 ? a.n_face_elem : a.n_elem, PF::NT, PF::BYTES, st>>>(a);
   ResidualKernel<K, M, P::NT, T, OPEN><<<a.n_elem, P::NT, P::BYTES, st>>>(a);
   return cudaGetLastError();
 }

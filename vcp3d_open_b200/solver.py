@@ -286,6 +286,24 @@ class Solver:
     def sync(self):
         self._check(self.lib.vcpg_sync(self.h), "sync")
 
+    # A block split across GPUs (vcp3d_open_b200.partition).
+    def set_partition(self, n_owned: int, n_face_ghost: int):
+        self._check(self.lib.vcpg_set_partition(self.h, int(n_owned), int(n_face_ghost)),
+                    "set_partition")
+
+    def pack_states(self, first: int, count: int, d_buf: int):
+        """States of elements [first, first + count) into the device buffer d_buf."""
+        self._check(self.lib.vcpg_pack_states(self.h, int(first), int(count), C.c_void_p(d_buf)),
+                    "pack_states")
+
+    def unpack_states(self, first: int, count: int, d_buf: int):
+        self._check(self.lib.vcpg_unpack_states(self.h, int(first), int(count),
+                                                C.c_void_p(d_buf)), "unpack_states")
+
+    def rk_stage(self, scheme: int, stage: int, dt: float):
+        self._check(self.lib.vcpg_rk_stage(self.h, int(scheme), int(stage), float(dt)),
+                    "rk_stage")
+
     @property
     def stream(self) -> int:
         return self.lib.vcpg_stream(self.h)
