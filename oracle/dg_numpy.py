@@ -118,7 +118,10 @@ def _cart_grad(dr, ds, dt, met, off, compat):
     dr, ds, dt: [e, 5, P]. compat: variable n uses the metric of point n.
     """
     if compat:
-        m = met[:, off:off + 9, :5][:, :, :, None]      # [e, 9, n, 1]
+        # Fewer than 5 points (faces with M = 2): variable 4 reads the padding,
+        # a copy of point 0 (src/ElementClass.cpp:1163-1173).
+        idx = [n if n < met.shape[2] else 0 for n in range(5)]
+        m = met[:, off:off + 9, idx][:, :, :, None]     # [e, 9, n, 1]
     else:
         m = met[:, off:off + 9, None, :]                 # [e, 9, 1, P]
     gx = dr * m[:, 0] + ds * m[:, 3] + dt * m[:, 6]
@@ -450,7 +453,7 @@ def face_residual(U, d: Disc, compat=True):
 
         def param(fm):
             if compat:
-                m = fm[:, 4:13, :5][:, :, :, None]
+                m = fm[:, 4:13, [n if n < M2 else 0 for n in range(5)]][:, :, :, None]
             else:
                 m = fm[:, 4:13, None, :]
             return [SX * m[:, 3 * q] + SY * m[:, 3 * q + 1] + SZ * m[:, 3 * q + 2] for q in range(3)]

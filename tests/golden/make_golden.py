@@ -60,6 +60,23 @@ GOLDEN_SPECS = {
     "tgv_p5_2x2x2": cases.CaseSpec(name="tgv_p5_2x2x2", kind="tgv", n_elem=(2, 2, 2), p=5,
                                    hi=(TWO_PI,) * 3, mach=0.1, reynolds=1600.0,
                                    grid_map="random", grid_amp=0.01, seed=3),
+    # The other degrees of the reference's tensor-product dispatch: p1 (M = 2),
+    # p6 with a 16th-order rule (M = 9), p7 with a 22nd-order rule (M = 12), p8
+    # and p9 with the default rule (M = 13, 14).
+    "tgv_p1_4x4x4": cases.CaseSpec(name="tgv_p1_4x4x4", kind="tgv", n_elem=(4, 4, 4), p=1,
+                                   hi=(TWO_PI,) * 3, mach=0.1, reynolds=1600.0,
+                                   grid_map="random", grid_amp=0.01, seed=21),
+    "tgv_p6_2x2x2": cases.CaseSpec(name="tgv_p6_2x2x2", kind="tgv", n_elem=(2, 2, 2), p=6,
+                                   n_poly_int=16, hi=(TWO_PI,) * 3, mach=0.1, reynolds=1600.0,
+                                   grid_map="random", grid_amp=0.005, seed=22),
+    "vortex_p7_2x2x2": cases.CaseSpec(name="vortex_p7_2x2x2", kind="vortex", n_elem=(2, 2, 2),
+                                      p=7, n_poly_int=22, beta=2.0),
+    "tgv_p8_2x2x2": cases.CaseSpec(name="tgv_p8_2x2x2", kind="tgv", n_elem=(2, 2, 2), p=8,
+                                   hi=(TWO_PI,) * 3, mach=0.1, reynolds=1600.0,
+                                   grid_map="random", grid_amp=0.005, seed=23),
+    "tgv_p9_2x2x2_roe": cases.CaseSpec(name="tgv_p9_2x2x2_roe", kind="tgv", n_elem=(2, 2, 2),
+                                       p=9, riemann="Roe", hi=(TWO_PI,) * 3, mach=0.1,
+                                       reynolds=1600.0, grid_map="sine", grid_amp=0.05),
     # WALE subgrid-scale model, Taylor-Green vortex at a high Reynolds number on a
     # perturbed grid, degree 4.
     "tgv_p4_3x3x3_wale": cases.CaseSpec(name="tgv_p4_3x3x3_wale", kind="tgv", n_elem=(3, 3, 3),

@@ -1,6 +1,6 @@
 """Metric terms computed on the GPU (vcpg_setup_geometry_device) against the
 host set-up (vcpg_setup_geometry): the same arithmetic, the same doubles, on
-curvilinear, randomly perturbed and open-boundary grids of degrees 2 to 5."""
+curvilinear, randomly perturbed and open-boundary grids of degrees 1 to 9."""
 from __future__ import annotations
 
 import numpy as np
@@ -17,6 +17,11 @@ SPECS = [
     cases.CaseSpec(name="vortex_p2", kind="vortex", n_elem=(5, 2, 3), p=2),
     cases.CaseSpec(name="tgv_p5", kind="tgv", n_elem=(2, 2, 2), p=5, hi=(6.283185307179586,) * 3,
                    grid_map="random", grid_amp=0.02, seed=3),
+    cases.CaseSpec(name="tgv_p1", kind="tgv", n_elem=(3, 3, 3), p=1, hi=(6.283185307179586,) * 3,
+                   grid_map="random", grid_amp=0.02, seed=5),
+    cases.CaseSpec(name="vortex_p7", kind="vortex", n_elem=(2, 2, 2), p=7, n_poly_int=22),
+    cases.CaseSpec(name="tgv_p8", kind="tgv", n_elem=(2, 2, 2), p=8, hi=(6.283185307179586,) * 3,
+                   grid_map="random", grid_amp=0.005, seed=6),
     cases.CaseSpec(name="pulse_p3", kind="pulse", n_elem=(4, 3, 2), p=3, hi=(4.0, 3.0, 2.0),
                    grid_map="random", grid_amp=0.01, seed=4,
                    bc=("inflow_static_nscbc", "outflow_nscbc", "periodic", "periodic",

@@ -48,6 +48,9 @@ struct vcpg_handle {
   double *d_bpresc = nullptr, *d_pc = nullptr, *d_dlq = nullptr;
   double *d_btrace = nullptr, *d_bmach = nullptr, *d_bflux = nullptr;
   double *d_bforce = nullptr;   // [nB][6] wall-face forces of a monitored residual
+  double *d_center = nullptr;   // [K^3] 3-D basis at the element centre
+  void *d_scratch = nullptr;    // element arrays of degrees above one CTA's shared memory
+  int scratch_ctas = 0;
   BlockFaceCfg *d_cfg = nullptr;
   void *d_fflux = nullptr;  // fluxes of every element's Min faces (FaceFluxKernel)
   int *d_sponge = nullptr;
@@ -89,6 +92,9 @@ ResidualArgs MakeResidualArgs(vcpg_handle *h, double *rawOut, unsigned long long
   a.face_metric = h->d_face;
   a.elem_scalars = h->d_sc;
   a.nbr = h->d_nbr;
+  a.center = h->d_center;
+  a.scratch = h->d_scratch;
+  a.scratch_ctas = h->scratch_ctas;
   a.n_elem = (int)h->nOwned;
   a.n_face_elem = (int)h->nFace;
   a.mu = h->prm.mu;
@@ -236,7 +242,7 @@ int vcpg_destroy(vcpg_handle *h) {
                   h->d_status, h->d_counter, h->d_cgstats, h->d_bface, h->d_bpresc, h->d_pc,
                   h->d_dlq, h->d_btrace, h->d_bmach, h->d_bflux, h->d_sponge, h->d_dampfn,
                   h->d_dampst, h->d_cml, h->d_cfg, h->d_fflux, h->d_eddymax, h->d_nmetric,
-                  h->d_bforce};
+                  h->d_bforce, h->d_center, h->d_scratch};
   for (void *p : bufs)
     if (p) cudaFree(p);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -285,15 +291,18 @@ int vcpg_create(const vcpg_params *params, const vcpg_operators *ops, const vcpg
     *out = h;
     return rc;
   }
+  if (params->sgs_model != VCPG_SGS_NONE && h->K > 9) {
+    int rc = Fail(h, VCPG_E_UNSUPPORTED_KM, "the SGS time step runs up to degree 8");
+    *out = h;
+    return rc;
+  }
   *out = h;
   const int K = h->K, M = h->M;
   // Operator table into the (K, M) constant slot.
-  OpTable t;
-  FillOpTable(ops, K, M, &t);
-  VCPG_CUDA(h, UploadOpTable(SlotOf(K, M), t));
+  VCPG_CUDA(h, UploadOperatorTable(ops, K, M));
 
   VCPG_CUDA(h, ConfigureResidual(K, M));
-  if (params->sgs_model != VCPG_SGS_NONE) VCPG_CUDA(h, ConfigureTimeStep(K, M));
+  VCPG_CUDA(h, ConfigureTimeStep(K, M));
   VCPG_CUDA(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
   const size_t nState = (size_t)h->nE * 5 * h->KD;
   auto alloc = [&](void **p, size_t bytes) -> int {
@@ -317,6 +326,20 @@ int vcpg_create(const vcpg_params *params, const vcpg_operators *ops, const vcpg
     if ((rc = alloc((void **)&h->d_nmetric, (size_t)h->nE * 10 * h->KD * 8))) return rc;
     VCPG_CUDA(h, cudaMemcpy(h->d_nmetric, geom->vol_metric_dofs, (size_t)h->nE * 10 * h->KD * 8,
                             cudaMemcpyHostToDevice));
+  }
+  if ((rc = alloc((void **)&h->d_center, (size_t)h->KD * 8))) return rc;
+  VCPG_CUDA(h, cudaMemcpy(h->d_center, ops->basis_center, (size_t)h->KD * 8,
+                          cudaMemcpyHostToDevice));
+  {
+    // Degrees 7-9 (FP64) loop one CTA per SM over the elements with global scratch.
+    int dev = 0, sms = 0;
+    VCPG_CUDA(h, cudaGetDevice(&dev));
+    VCPG_CUDA(h, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const size_t sb = ResidualScratchBytes(K, M, sms);
+    if (sb > 0) {
+      if ((rc = alloc(&h->d_scratch, sb))) return rc;
+      h->scratch_ctas = sms;
+    }
   }
   if ((rc = alloc((void **)&h->d_dt, sizeof(double)))) return rc;
   if ((rc = alloc((void **)&h->d_fixed, sizeof(double)))) return rc;
@@ -611,6 +634,8 @@ int vcpg_set_open_boundary(vcpg_handle *h, const vcpg_open_boundary *ob,
   if (h->open) return Fail(h, VCPG_E_INVALID, "open boundaries are already configured");
   if (h->nOwned != h->nE)
     return Fail(h, VCPG_E_INVALID, "open boundaries: the block is partitioned");
+  if (!SupportsOpenBoundaries(h->K, h->M))
+    return Fail(h, VCPG_E_UNSUPPORTED_KM, "open boundaries run up to degree 6");
   OpenBoundaryHost ob_host;
   std::string err;
   int rc = BuildOpenBoundary(h->prm, *ob, *geom, p_grid, dof_location, grid_nodes, ob_host, err);

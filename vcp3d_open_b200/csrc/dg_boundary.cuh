@@ -90,8 +90,8 @@ __global__ void __launch_bounds__(NT) BoundaryTraceKernel(const BoundaryArgs a) 
 #pragma unroll
     for (int n = 0; n < K; ++n) {
       const double x = bsrc[n * ns];
-      a0 = fma(c_ops[SLOT].face[side * K + n], x, a0);
-      d0 = fma(c_ops[SLOT].dface[side * K + n], x, d0);
+      a0 = fma(Ops<SLOT>().face[side * K + n], x, a0);
+      d0 = fma(Ops<SLOT>().dface[side * K + n], x, d0);
     }
     s_bn[line] = a0;
     s_bnd[line] = d0;
@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(NT) BoundaryTraceKernel(const BoundaryArgs a) 
   const int I0 = 4 + 3 * bf[kBfGrad];
   for (int l = threadIdx.x; l < M2; l += NT) {
     const double magn = fm[3 * M2 + l];
-    const double wts = c_ops[SLOT].w[l % M] * c_ops[SLOT].w[l / M];
+    const double wts = Ops<SLOT>().w[l % M] * Ops<SLOT>().w[l / M];
     const double rrx = fm[I0 * M2 + l], rry = fm[(I0 + 1) * M2 + l], rrz = fm[(I0 + 2) * M2 + l];
     const double magrr = sqrt(rrx * rrx + rry * rry + rrz * rrz);
     const double V4Inv = 1.0 / s_tr[4 * M2 + l];
@@ -164,7 +164,7 @@ __device__ __forceinline__ void WeakBoundaryFlux(const BoundaryArgs &a, const in
 #pragma unroll
     for (int n = 0; n < 5; ++n) {
       VL[n] = tr[n * M2 + l];
-      const int mi = a.metric_compat ? n : l;
+      const int mi = a.metric_compat ? (n < M2 ? n : 0) : l;
       const double dvdr = tr[(5 + n) * M2 + l], dvds = tr[(10 + n) * M2 + l],
                    dvdt = tr[(15 + n) * M2 + l];
       gx[n] = dvdr * fm[4 * M2 + mi] + dvds * fm[7 * M2 + mi] + dvdt * fm[10 * M2 + mi];
@@ -268,7 +268,7 @@ __device__ __forceinline__ void WeakBoundaryFlux(const BoundaryArgs &a, const in
         for (int n = 0; n < 5; ++n) VR[n] = VL[n];
         break;
     }
-    const double wf = c_ops[SLOT].w[lj] * c_ops[SLOT].w[li];
+    const double wf = Ops<SLOT>().w[lj] * Ops<SLOT>().w[li];
     const double area = fm[3 * M2 + l];
     double flux[5], sx[5], sy[5], sz[5];
     if (a.riemann == 1)
@@ -298,7 +298,7 @@ __device__ __forceinline__ void WeakBoundaryFlux(const BoundaryArgs &a, const in
     }
 #pragma unroll
     for (int n = 0; n < 5; ++n) {
-      const int mi = a.metric_compat ? n : l;
+      const int mi = a.metric_compat ? (n < M2 ? n : 0) : l;
       double sym[3];
 #pragma unroll
       for (int p = 0; p < 3; ++p)
@@ -621,7 +621,7 @@ __global__ void __launch_bounds__(NT) BoundaryFluxKernel(const BoundaryArgs a) {
     double gx[5], gy[5], gz[5];
 #pragma unroll
     for (int n = 0; n < 5; ++n) {
-      const int mi = a.metric_compat ? n : l;
+      const int mi = a.metric_compat ? (n < M2 ? n : 0) : l;
       const double drdx = fm[4 * M2 + mi], dsdx = fm[7 * M2 + mi], dtdx = fm[10 * M2 + mi];
       const double drdy = fm[5 * M2 + mi], dsdy = fm[8 * M2 + mi], dtdy = fm[11 * M2 + mi];
       const double drdz = fm[6 * M2 + mi], dsdz = fm[9 * M2 + mi], dtdz = fm[12 * M2 + mi];
@@ -635,7 +635,7 @@ __global__ void __launch_bounds__(NT) BoundaryFluxKernel(const BoundaryArgs a) {
       gy[n] = 0.5 * (yL + yR);
       gz[n] = 0.5 * (zL + zR);
     }
-    const double wf = c_ops[SLOT].w[lj] * c_ops[SLOT].w[li];
+    const double wf = Ops<SLOT>().w[lj] * Ops<SLOT>().w[li];
     const double nx = factNorm * fm[0 * M2 + l], ny = factNorm * fm[1 * M2 + l],
                  nz = factNorm * fm[2 * M2 + l];
     const double area = fm[3 * M2 + l];
@@ -654,7 +654,7 @@ __global__ void __launch_bounds__(NT) BoundaryFluxKernel(const BoundaryArgs a) {
     const int pFast = BFastParam(d), pSlow = 3 - d - pFast;
 #pragma unroll
     for (int n = 0; n < 5; ++n) {
-      const int mi = a.metric_compat ? n : l;
+      const int mi = a.metric_compat ? (n < M2 ? n : 0) : l;
       double sym[3];
 #pragma unroll
       for (int p = 0; p < 3; ++p)

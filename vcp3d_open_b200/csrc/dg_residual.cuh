@@ -74,6 +74,11 @@ struct ResidualArgs {
   // [nE][3][20][M^2] fluxes of every element's Min faces in the compute precision
   // (FaceFluxKernel writes them, the residual kernel reads them).
   void *face_flux;
+  const double *center;        // [K^3] 3-D basis at the element centre (CG preconditioner)
+  // Degrees whose element arrays exceed the shared memory of one CTA: one
+  // global scratch area per CTA of a grid that loops over the elements.
+  void *scratch;
+  int scratch_ctas;            // CTAs the scratch areas hold (the grid of those degrees)
 };
 
 // Arguments of the CFL time-step kernel (kernels.cu).
@@ -192,9 +197,16 @@ template <int K, int M, typename T = double, bool OPEN = false> struct Plan {
   static constexpr int WORK = VOL > OTHER ? VOL : OTHER;
   // Persistent: sol, R, CG point data (rho, u, v, w, p per point), J*w, reduction scratch,
   // face vectors (basis and derivative at r = -1, +1).
-  static constexpr int PERSIST = 10 * KD + 6 * MD + 64 + 4 * kKMax;
+  // Face vectors: basis and derivative at r = -1, +1 (4 K values, room for 28 at least).
+  static constexpr int FV = 4 * (K > 7 ? K : 7);
+  static constexpr int PERSIST = 10 * KD + 6 * MD + 64 + FV;
   static constexpr int TOTAL = PERSIST + WORK;
   static constexpr size_t BYTES = sizeof(T) * (size_t)TOTAL;
+  // Above the 227 KB of one CTA (degrees 7-9 in FP64): the arrays live in a
+  // global scratch area per CTA (stride SCRATCH, 16-byte aligned) of a grid that
+  // loops over the elements.
+  static constexpr bool BIG = BYTES > 227 * 1024;
+  static constexpr int SCRATCH = (TOTAL + 3) / 4 * 4;
   // Threads per CTA and the CTAs per SM that the shared memory allows (227 KB).
   // Threads per CTA and CTAs per SM (through __launch_bounds__ they bound the
   // registers per thread). FP64: 128 threads cover the widest contraction stage
@@ -565,7 +577,9 @@ __device__ __forceinline__ void TraceCartesianGrad(const T *TR, const int t, con
   const int qr = DerivSlot(d, 0), qs = DerivSlot(d, 1), qt = DerivSlot(d, 2);
 #pragma unroll
   for (int n = 0; n < 5; ++n) {
-    const int mi = compat ? n : pt;
+    // With fewer than 5 face points (M = 2) variable 4 reads the padding, which
+    // holds point 0's metric (src/ElementClass.cpp:1163-1173).
+    const int mi = compat ? (n < M2 ? n : 0) : pt;
     const T dvdr = TR[((qr * 6 + t) * 5 + n) * M2 + pt];
     const T dvds = TR[((qs * 6 + t) * 5 + n) * M2 + pt];
     const T dvdt = TR[((qt * 6 + t) * 5 + n) * M2 + pt];
@@ -656,7 +670,7 @@ __device__ __forceinline__ void FaceRoles(const ResidualArgs &a, const int g, co
   const int pFast = FastParam(d);
 #pragma unroll
   for (int n = 0; n < 5; ++n) {
-    const int mi = a.metric_compat ? n : pt;
+    const int mi = a.metric_compat ? (n < M2 ? n : 0) : pt;
     const T flux = F[n * M2 + pt], sx = F[(5 + n) * M2 + pt], sy = F[(10 + n) * M2 + pt],
             sz = F[(15 + n) * M2 + pt];
     T sym[3];
@@ -938,7 +952,7 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
   // Entropy variables at the element centre and dV/dU there (src/CG_MassMatrix.cpp:313-361).
   if (threadIdx.x < 5) {
     T V = T(0.0);
-    for (int l = 0; l < KD; ++l) V += CenterBasis<SLOT, T>(l) * s_sol[threadIdx.x * KD + l];
+    for (int l = 0; l < KD; ++l) V += T(a.center[l]) * s_sol[threadIdx.x * KD + l];
     dvdu[threadIdx.x + 16] = V;
   }
   __syncthreads();
@@ -1105,16 +1119,14 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
 // ---------------------------------------------------------------------------
 // The fused kernel.
 // ---------------------------------------------------------------------------
+// One element's residual: volume terms, face distribution and mass solve, with
+// the element arrays at smem (shared memory, or the CTA's global scratch area).
 template <int K, int M, int NT, typename T, bool OPEN>
-__global__ void __launch_bounds__(NT, (Plan<K, M, T, OPEN>::MIN_BLOCKS)) ResidualKernel(const ResidualArgs a) {
+__device__ __forceinline__ void ResidualElement(const ResidualArgs &a, const int e, T *smem) {
   using P = Plan<K, M, T, OPEN>;
   constexpr int KD = P::KD, MD = P::MD;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T *smem = reinterpret_cast<T *>(smem_raw);
   T *s_sol = smem, *s_R = s_sol + 5 * KD, *s_cgp = s_R + 5 * KD, *s_jw = s_cgp + 5 * MD;
-  T *s_red = s_jw + MD, *s_fv = s_red + 64, *work = s_fv + 4 * kKMax;
-  const int e = blockIdx.x;
-  if (e >= a.n_elem) return;
+  T *s_red = s_jw + MD, *s_fv = s_red + 64, *work = s_fv + P::FV;
   // Several cases per launch: skip unused elements and cases in another state.
   double mu = a.mu;
   if (a.cases.elem_case) {
@@ -1139,11 +1151,31 @@ __global__ void __launch_bounds__(NT, (Plan<K, M, T, OPEN>::MIN_BLOCKS)) Residua
   MassSolve<NT, K, M>(a, e, s_sol, s_R, s_cgp, s_jw, work, s_red, a.res + (size_t)e * 5 * KD);
 }
 
+template <int K, int M, int NT, typename T, bool OPEN>
+__global__ void __launch_bounds__(NT, (Plan<K, M, T, OPEN>::MIN_BLOCKS)) ResidualKernel(const ResidualArgs a) {
+  using P = Plan<K, M, T, OPEN>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  if constexpr (P::BIG) {
+    T *base = reinterpret_cast<T *>(a.scratch) + (size_t)blockIdx.x * P::SCRATCH;
+    for (int e = blockIdx.x; e < a.n_elem; e += gridDim.x) {
+      ResidualElement<K, M, NT, T, OPEN>(a, e, base);
+      __syncthreads();
+    }
+  } else {
+    if ((int)blockIdx.x >= a.n_elem) return;
+    ResidualElement<K, M, NT, T, OPEN>(a, blockIdx.x, reinterpret_cast<T *>(smem_raw));
+  }
+}
+
 // Shared memory (in T) and launch shape of the face-flux kernel.
 template <int K, int M, typename T = double> struct FluxPlan {
   static constexpr int KD = K * K * K, M2 = M * M;
-  static constexpr int TOTAL = 5 * KD + 4 * kKMax + 90 * K * M + 120 * M2;
+  static constexpr int FV = 4 * (K > 7 ? K : 7);
+  static constexpr int TOTAL = 5 * KD + FV + 90 * K * M + 120 * M2;
   static constexpr size_t BYTES = sizeof(T) * (size_t)TOTAL;
+  // Above one CTA's shared memory: global scratch per CTA, elements in a loop.
+  static constexpr bool BIG = BYTES > 227 * 1024;
+  static constexpr int SCRATCH = (TOTAL + 3) / 4 * 4;
   // Launch shape measured best on B200 over 96..192 threads and 2..4 CTAs per SM:
   // 128 threads and up to 4 CTAs (<= 128 registers) for degree <= 3; from degree
   // 4 on, 160 threads (the 3 M^2 face points of a group in one pass) with up to
@@ -1158,13 +1190,9 @@ template <int K, int M, typename T = double> struct FluxPlan {
 // The fluxes of every interior face, computed once by the face's upper element
 // (its Min faces), before the residual kernel distributes them to both sides.
 template <int K, int M, int NT, typename T>
-__global__ void __launch_bounds__(NT, (FluxPlan<K, M, T>::MIN_BLOCKS)) FaceFluxKernel(const ResidualArgs a) {
+__device__ __forceinline__ void FaceFluxElement(const ResidualArgs &a, const int e, T *smem) {
   constexpr int KD = K * K * K;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T *smem = reinterpret_cast<T *>(smem_raw);
-  T *s_sol = smem, *s_fv = s_sol + 5 * KD, *work = s_fv + 4 * kKMax;
-  const int e = blockIdx.x;
-  if (e >= (a.n_face_elem > 0 ? a.n_face_elem : a.n_elem)) return;
+  T *s_sol = smem, *s_fv = s_sol + 5 * KD, *work = s_fv + FluxPlan<K, M, T>::FV;
   double mu = a.mu;
   if (a.cases.elem_case) {
     const int cs = a.cases.elem_case[e];
@@ -1179,6 +1207,23 @@ __global__ void __launch_bounds__(NT, (FluxPlan<K, M, T>::MIN_BLOCKS)) FaceFluxK
   }
   __syncthreads();
   MinFaceFluxes<NT, K, M, T>(a, e, mu, s_sol, s_fv, work);
+}
+
+template <int K, int M, int NT, typename T>
+__global__ void __launch_bounds__(NT, (FluxPlan<K, M, T>::MIN_BLOCKS)) FaceFluxKernel(const ResidualArgs a) {
+  using P = FluxPlan<K, M, T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int n = a.n_face_elem > 0 ? a.n_face_elem : a.n_elem;
+  if constexpr (P::BIG) {
+    T *base = reinterpret_cast<T *>(a.scratch) + (size_t)blockIdx.x * P::SCRATCH;
+    for (int e = blockIdx.x; e < n; e += gridDim.x) {
+      FaceFluxElement<K, M, NT, T>(a, e, base);
+      __syncthreads();
+    }
+  } else {
+    if ((int)blockIdx.x >= n) return;
+    FaceFluxElement<K, M, NT, T>(a, blockIdx.x, reinterpret_cast<T *>(smem_raw));
+  }
 }
 
 }  // namespace vcpg

@@ -12,9 +12,9 @@
 //  include/TensorProductVolumeResidual.hpp:5-96,
 //  include/TensorProductSolAndGrad[IJK]Face.hpp, include/TensorProductRes[IJK]Face.hpp).
 //
-// The 1-D operator values sit in constant memory, one table per (K, M) pair;
-// with compile-time indices every coefficient is a uniform constant-bank
-// operand of the FMA.
+// The 1-D operator values sit in constant memory, one exactly sized table per
+// (K, M) pair; with compile-time indices every coefficient is a uniform
+// constant-bank operand of the FMA.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -23,39 +23,91 @@
 
 namespace vcpg {
 
-constexpr int kKMax = 7;   // up to polynomial degree 6
-constexpr int kMMax = 10;
+constexpr int kKMax = 10;   // up to polynomial degree 9
+constexpr int kMMax = 14;
 
-struct OpTable {
-  double leg[kKMax * kMMax];        // leg[k * M + m]: basis k at Gauss point m
-  double dleg[kKMax * kMMax];       // derivative
-  double face[2 * kKMax];           // [side][k], side 0: r = -1, side 1: r = +1
-  double dface[2 * kKMax];
-  double w[kMMax];                  // 1-D Gauss weights
-  double legdof[kKMax * kKMax];     // legdof[k * K + i]: basis k at nodal DOF i
-  double dlegdof[kKMax * kKMax];    // its derivative (time step with an SGS model)
-  double center[kKMax * kKMax * kKMax];
+// The 1-D operators of one (K, M) pair, sized exactly (constant memory holds
+// every supported pair's table).
+template <int K, int M> struct OpTableKM {
+  double leg[K * M];           // leg[k * M + m]: basis k at Gauss point m
+  double dleg[K * M];          // derivative
+  double face[2 * K];          // [side][k], side 0: r = -1, side 1: r = +1
+  double dface[2 * K];
+  double w[M];                 // 1-D Gauss weights
+  double legdof[K * K];        // legdof[k * K + i]: basis k at nodal DOF i
+  double dlegdof[K * K];       // its derivative (time step with an SGS model)
   // FP32 copies for the mixed-precision form.
-  float legf[kKMax * kMMax];
-  float dlegf[kKMax * kMMax];
-  float facef[2 * kKMax];
-  float dfacef[2 * kKMax];
-  float wf[kMMax];
-  float centerf[kKMax * kKMax * kKMax];
+  float legf[K * M];
+  float dlegf[K * M];
+  float facef[2 * K];
+  float dfacef[2 * K];
+  float wf[M];
 };
 
-// Supported (K, M) pairs and their constant-memory slot.
-template <int K, int M> struct Slot;
-template <> struct Slot<2, 3> { static constexpr int value = 0; };
-template <> struct Slot<3, 4> { static constexpr int value = 1; };
-template <> struct Slot<4, 5> { static constexpr int value = 2; };
-template <> struct Slot<5, 7> { static constexpr int value = 3; };
-template <> struct Slot<6, 8> { static constexpr int value = 4; };
-template <> struct Slot<7, 10> { static constexpr int value = 5; };
-constexpr int kNumSlots = 6;
+// Supported (K, M) pairs -- the reference's tensor-product dispatch
+// (src/TensorProductVolumeResidualK2.cpp ... K10.cpp) -- and their slots.
+#define VCPG_SLOTS(X) \
+  X(0, 2, 2) X(1, 2, 3) X(2, 3, 4) X(3, 4, 5) X(4, 5, 7) X(5, 6, 8) X(6, 7, 9) X(7, 8, 12) \
+  X(8, 9, 13) X(9, 10, 14)
+constexpr int kNumSlots = 10;
 
-// One copy per translation unit; only kernels.cu launches kernels and uploads it.
-static __constant__ OpTable c_ops[kNumSlots];
+template <int K, int M> struct Slot;
+template <int SLOT> struct SlotOps;
+// One copy per translation unit: every unit that launches kernels uploads its
+// own (UploadOperators).
+#define VCPG_SLOT_DECL(S_, K_, M_)                                                          \
+  template <> struct Slot<K_, M_> { static constexpr int value = S_; };                     \
+  static __constant__ OpTableKM<K_, M_> c_ops##S_;                                          \
+  template <> struct SlotOps<S_> {                                                          \
+    __device__ static __forceinline__ const OpTableKM<K_, M_> &get() { return c_ops##S_; } \
+  };
+VCPG_SLOTS(VCPG_SLOT_DECL)
+#undef VCPG_SLOT_DECL
+
+template <int SLOT> __device__ __forceinline__ decltype(auto) Ops() { return SlotOps<SLOT>::get(); }
+
+// Fills and uploads the table of one pair from the C-ABI operator arrays of
+// this unit's copy (legdof / dlegdof may be absent: zeros).
+template <int K, int M, typename Sym>
+static inline cudaError_t UploadOperatorsKM(const Sym &sym, const double *leg, const double *dleg,
+                                            const double *face, const double *dface,
+                                            const double *w, const double *legdof,
+                                            const double *dlegdof) {
+  OpTableKM<K, M> t{};
+  for (int i = 0; i < K * M; ++i) {
+    t.leg[i] = leg[i];
+    t.dleg[i] = dleg[i];
+    t.legf[i] = (float)leg[i];    // rounded once from the FP64 operators
+    t.dlegf[i] = (float)dleg[i];
+  }
+  for (int i = 0; i < 2 * K; ++i) {
+    t.face[i] = face[i];
+    t.dface[i] = dface[i];
+    t.facef[i] = (float)face[i];
+    t.dfacef[i] = (float)dface[i];
+  }
+  for (int m = 0; m < M; ++m) {
+    t.w[m] = w[m];
+    t.wf[m] = (float)w[m];
+  }
+  for (int i = 0; i < K * K; ++i) {
+    t.legdof[i] = legdof ? legdof[i] : 0.0;
+    t.dlegdof[i] = dlegdof ? dlegdof[i] : 0.0;
+  }
+  return cudaMemcpyToSymbol(sym, &t, sizeof(t), 0, cudaMemcpyHostToDevice);
+}
+
+static inline cudaError_t UploadOperators(int K, int M, const double *leg, const double *dleg,
+                                          const double *face, const double *dface,
+                                          const double *w, const double *legdof,
+                                          const double *dlegdof) {
+#define VCPG_SLOT_UPLOAD(S_, K_, M_)                                                  \
+  if (K == K_ && M == M_)                                                             \
+    return UploadOperatorsKM<K_, M_>(c_ops##S_, leg, dleg, face, dface, w, legdof, dlegdof);
+  VCPG_SLOTS(VCPG_SLOT_UPLOAD)
+#undef VCPG_SLOT_UPLOAD
+  return cudaErrorInvalidValue;
+}
 
 // Operator selection for a line transform.
 enum OpSel {
@@ -70,41 +122,36 @@ enum OpSel {
 template <int SLOT, int K, int M, int OP, typename T = double>
 __device__ __forceinline__ T Coef(const int c, const int o) {
   if constexpr (std::is_same<T, float>::value) {
-    if (OP == kLeg) return c_ops[SLOT].legf[c * M + o];
-    if (OP == kDLeg) return c_ops[SLOT].dlegf[c * M + o];
-    if (OP == kLegT) return c_ops[SLOT].legf[o * M + c];
-    return c_ops[SLOT].dlegf[o * M + c];
+    if (OP == kLeg) return Ops<SLOT>().legf[c * M + o];
+    if (OP == kDLeg) return Ops<SLOT>().dlegf[c * M + o];
+    if (OP == kLegT) return Ops<SLOT>().legf[o * M + c];
+    return Ops<SLOT>().dlegf[o * M + c];
   } else {
-    if (OP == kLeg) return c_ops[SLOT].leg[c * M + o];
-    if (OP == kDLeg) return c_ops[SLOT].dleg[c * M + o];
-    if (OP == kLegT) return c_ops[SLOT].leg[o * M + c];
-    if (OP == kLegDof) return c_ops[SLOT].legdof[c * K + o];
-    if (OP == kDLegDof) return c_ops[SLOT].dlegdof[c * K + o];
-    return c_ops[SLOT].dleg[o * M + c];
+    if (OP == kLeg) return Ops<SLOT>().leg[c * M + o];
+    if (OP == kDLeg) return Ops<SLOT>().dleg[c * M + o];
+    if (OP == kLegT) return Ops<SLOT>().leg[o * M + c];
+    if (OP == kLegDof) return Ops<SLOT>().legdof[c * K + o];
+    if (OP == kDLegDof) return Ops<SLOT>().dlegdof[c * K + o];
+    return Ops<SLOT>().dleg[o * M + c];
   }
 }
 
-// Face basis values (side 0: r = -1, side 1: r = +1), 1-D weights and the centre
-// basis in the compute precision.
+// Face basis values (side 0: r = -1, side 1: r = +1) and 1-D weights in the
+// compute precision.
 template <int SLOT, typename T>
 __device__ __forceinline__ T FaceVal(const int i) {
-  if constexpr (std::is_same<T, float>::value) return c_ops[SLOT].facef[i];
-  else return c_ops[SLOT].face[i];
+  if constexpr (std::is_same<T, float>::value) return Ops<SLOT>().facef[i];
+  else return Ops<SLOT>().face[i];
 }
 template <int SLOT, typename T>
 __device__ __forceinline__ T FaceDer(const int i) {
-  if constexpr (std::is_same<T, float>::value) return c_ops[SLOT].dfacef[i];
-  else return c_ops[SLOT].dface[i];
+  if constexpr (std::is_same<T, float>::value) return Ops<SLOT>().dfacef[i];
+  else return Ops<SLOT>().dface[i];
 }
 template <int SLOT, typename T>
 __device__ __forceinline__ T Weight1D(const int i) {
-  if constexpr (std::is_same<T, float>::value) return c_ops[SLOT].wf[i];
-  else return c_ops[SLOT].w[i];
-}
-template <int SLOT, typename T>
-__device__ __forceinline__ T CenterBasis(const int i) {
-  if constexpr (std::is_same<T, float>::value) return c_ops[SLOT].centerf[i];
-  else return c_ops[SLOT].center[i];
+  if constexpr (std::is_same<T, float>::value) return Ops<SLOT>().wf[i];
+  else return Ops<SLOT>().w[i];
 }
 
 // Strides (in elements) of an array [NV][D2][D1][D0] with unit stride along D0:

@@ -121,6 +121,7 @@ struct Bucket {
   double *bpresc = nullptr, *btrace = nullptr, *bmach = nullptr, *bflux = nullptr;
   double *pc = nullptr, *dlq = nullptr;
   double *dampFn = nullptr, *dampSt = nullptr, *cml = nullptr;
+  double *center = nullptr;  // [K^3] 3-D basis at the element centre
   // Case slots.
   int *state = nullptr, *target = nullptr, *done = nullptr, *status = nullptr;
   double *par = nullptr, *dt = nullptr, *simTime = nullptr;
@@ -193,7 +194,7 @@ void FreeBucket(Bucket &b) {
   void *bufs[] = {b.fflux, b.sol, b.solOld, b.res, b.vol, b.face, b.sc, b.nbr, b.elemCase, b.spongeIdx,
                   b.bface, b.bpresc, b.btrace, b.bmach, b.bflux, b.pc, b.dlq, b.dampFn,
                   b.dampSt, b.cml, b.state, b.target, b.done, b.status, b.par, b.dt,
-                  b.simTime, b.dtBits, b.cgStats, b.cfgs};
+                  b.simTime, b.dtBits, b.cgStats, b.cfgs, b.center};
   for (void *p : bufs)
     if (p) cudaFree(p);
   if (b.stream) cudaStreamDestroy(b.stream);
@@ -209,7 +210,10 @@ int AllocBucket(vcpg_ensemble *e, Bucket &b, int deg, int64_t capE, int64_t capB
   b.MD = b.M * b.M * b.M;
   b.M2 = b.M * b.M;
   b.capE = capE; b.capB = capB; b.capS = capS; b.capC = capC;
-  if (!Supported(b.K, b.M) || b.K > kKMax || b.M > kMMax)
+  // Buckets hold degrees whose kernels run in shared memory and have the
+  // open-boundary kernels (up to degree 6).
+  if (!Supported(b.K, b.M) || !SupportsOpenBoundaries(b.K, b.M) ||
+      ResidualScratchBytes(b.K, b.M, 1) > 0)
     return Fail(e, VCPG_E_UNSUPPORTED_KM, "no kernel for degree " + std::to_string(deg));
   ENS_CUDA(e, ConfigureResidual(b.K, b.M));
   ENS_CUDA(e, cudaStreamCreateWithFlags(&b.stream, cudaStreamNonBlocking));
@@ -246,7 +250,8 @@ int AllocBucket(vcpg_ensemble *e, Bucket &b, int deg, int64_t capE, int64_t capB
       (rc = alloc((void **)&b.status, 4 * 4)) || (rc = alloc((void **)&b.par, 8 * C * kCasePar)) ||
       (rc = alloc((void **)&b.dt, 8 * C)) || (rc = alloc((void **)&b.simTime, 8 * C)) ||
       (rc = alloc((void **)&b.dtBits, 8 * C)) || (rc = alloc((void **)&b.cgStats, 8 * 2)) ||
-      (rc = alloc((void **)&b.cfgs, sizeof(BlockFaceCfg) * C * 6)))
+      (rc = alloc((void **)&b.cfgs, sizeof(BlockFaceCfg) * C * 6)) ||
+      (rc = alloc((void **)&b.center, 8 * (size_t)b.KD)))
     return rc;
   // Unused elements and faces carry case -1; every slot starts free.
   ENS_CUDA(e, cudaMemsetAsync(b.elemCase, 0xFF, 4 * E, b.stream));
@@ -294,6 +299,7 @@ ResidualArgs BucketResidualArgs(const vcpg_ensemble *e, const Bucket &b, int req
   a.cml_on = b.capS > 0 ? 1 : 0;
   a.cases = CaseView{b.elemCase, b.state, b.par, require};
   a.face_flux = b.fflux;
+  a.center = b.center;
   return a;
 }
 
@@ -538,9 +544,9 @@ int vcpg_ensemble_submit(vcpg_ensemble *ens, const vcpg_params *params,
 
   // Bucket-wide operators on first use.
   if (!b.opsReady) {
-    OpTable t;
-    FillOpTable(ops, b.K, b.M, &t);
-    cudaError_t ce = UploadOpTable(SlotOf(b.K, b.M), t);
+    cudaError_t ce = UploadOperatorTable(ops, b.K, b.M);
+    if (ce == cudaSuccess)
+      ce = cudaMemcpy(b.center, ops->basis_center, 8 * (size_t)b.KD, cudaMemcpyHostToDevice);
     if (ce != cudaSuccess) { rollback(); return Fail(e, VCPG_E_CUDA, cudaGetErrorString(ce)); }
     b.opsReady = true;
   }

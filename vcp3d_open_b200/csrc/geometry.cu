@@ -229,6 +229,14 @@ int vcpg_setup_geometry_device(const vcpg_params *params, int32_t p_grid, int32_
 
   const int64_t nE = (int64_t)nI * nJ * nK;
   const int KG3 = Kg * Kg * Kg, MD = M * M * M, M2 = M * M;
+  const size_t smem = sizeof(double) * ((size_t)3 * KG3 + Kg * Kg * std::max(Kg, M) +
+                                        Kg * M * M + Kg * M + 9 * MD + 2 * Kg * M + 4 * Kg + M);
+  // One element's arrays above the shared memory of a CTA (degree 9 with 14
+  // points per direction): the host set-up, whose doubles the kernel reproduces.
+  if (smem > 227 * 1024)
+    return vcpg_setup_geometry(params, p_grid, dof_location, periodic, grid_nodes, leg_int,
+                               dleg_int, leg_face, dleg_face, w_int, leg_dofs, basis_center,
+                               vol_metric, face_metric, elem_scalars, neighbors);
   // Elements per pass: device buffers of at most about 1 GiB.
   const size_t perElem = sizeof(double) * ((size_t)3 * KG3 + 10 * MD + 78 * M2 + 15);
   const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(nE, (int64_t)((1ull << 30) / perElem)));
@@ -249,8 +257,6 @@ int vcpg_setup_geometry_device(const vcpg_params *params, int32_t p_grid, int32_
   if (ce == cudaSuccess) ce = cudaMalloc((void **)&dBad, sizeof(int));
   if (ce == cudaSuccess) ce = cudaMemcpy(dOps, ops.data(), sizeof(double) * ops.size(), cudaMemcpyHostToDevice);
   if (ce == cudaSuccess) ce = cudaMemset(dBad, 0, sizeof(int));
-  const size_t smem = sizeof(double) * ((size_t)3 * KG3 + Kg * Kg * std::max(Kg, M) +
-                                        Kg * M * M + Kg * M + 9 * MD + 2 * Kg * M + 4 * Kg + M);
   if (ce == cudaSuccess && smem > 48 * 1024)
     ce = cudaFuncSetAttribute(vcpg::ElementMetricsKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)smem);
@@ -272,7 +278,10 @@ int vcpg_setup_geometry_device(const vcpg_params *params, int32_t p_grid, int32_
   }
   if (ce == cudaSuccess) ce = cudaMemcpy(&bad, dBad, sizeof(int), cudaMemcpyDeviceToHost);
   cudaFree(dOps); cudaFree(dNodes); cudaFree(dVol); cudaFree(dFace); cudaFree(dSc); cudaFree(dBad);
-  if (ce != cudaSuccess) return VCPG_E_CUDA;
+  if (ce != cudaSuccess) {
+    cudaGetLastError();   // a failed call leaves no error behind for later launches
+    return VCPG_E_CUDA;
+  }
   if (bad) rc = VCPG_E_INVALID;   // a non-positive Jacobian, as the host version rejects
   // The volume length scale: cube root on the host, as vcpg_setup_geometry takes it.
   for (int64_t e = 0; e < nE; ++e) {

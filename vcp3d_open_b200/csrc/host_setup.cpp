@@ -271,21 +271,20 @@ void ElementMetrics(const StdElement &se, const double *gridNodes, double *vol, 
   const int Kg = se.Kg, M = se.M, MD = M * M * M, M2 = M * M;
   const int KG3 = Kg * Kg * Kg;
   // Volume: coordinates derivatives at the integration points (k, then j, then i).
-  double dc[3][3][512 * 2];  // [param][coord][point]
-  if (MD > 1024) throw std::runtime_error("too many integration points");
+  std::vector<double> dc((size_t)9 * MD);  // [param][coord][point]
   for (int x = 0; x < 3; ++x) {
     std::vector<double> g(gridNodes + x * KG3, gridNodes + (x + 1) * KG3);
     for (int q = 0; q < 3; ++q) {
       std::vector<double> t = ApplyAxis(g, Kg, Kg, Kg, 2, (q == 2 ? se.dlagInt : se.lagInt).data(), M);
       t = ApplyAxis(t, Kg, Kg, M, 1, (q == 1 ? se.dlagInt : se.lagInt).data(), M);
       t = ApplyAxis(t, Kg, M, M, 0, (q == 0 ? se.dlagInt : se.lagInt).data(), M);
-      for (int l = 0; l < MD; ++l) dc[q][x][l] = t[l];
+      for (int l = 0; l < MD; ++l) dc[(q * 3 + x) * MD + l] = t[l];
     }
   }
   for (int l = 0; l < MD; ++l) {
-    const double dxdr = dc[0][0][l], dydr = dc[0][1][l], dzdr = dc[0][2][l];
-    const double dxds = dc[1][0][l], dyds = dc[1][1][l], dzds = dc[1][2][l];
-    const double dxdt = dc[2][0][l], dydt = dc[2][1][l], dzdt = dc[2][2][l];
+    const double dxdr = dc[(0 * 3 + 0) * MD + l], dydr = dc[(0 * 3 + 1) * MD + l], dzdr = dc[(0 * 3 + 2) * MD + l];
+    const double dxds = dc[(1 * 3 + 0) * MD + l], dyds = dc[(1 * 3 + 1) * MD + l], dzds = dc[(1 * 3 + 2) * MD + l];
+    const double dxdt = dc[(2 * 3 + 0) * MD + l], dydt = dc[(2 * 3 + 1) * MD + l], dzdt = dc[(2 * 3 + 2) * MD + l];
     const double J = dxdr * (dyds * dzdt - dzds * dydt) - dxds * (dydr * dzdt - dzdr * dydt) +
                      dxdt * (dydr * dzds - dzdr * dyds);
     if (!(J > 0.0)) throw std::runtime_error("negative or zero Jacobian");
@@ -306,8 +305,7 @@ void ElementMetrics(const StdElement &se, const double *gridNodes, double *vol, 
     const int d = f / 2, side = f % 2;
     const double *fv = se.lagFace.data() + side * Kg, *dfv = se.dlagFace.data() + side * Kg;
     const int fastAx = d == 0 ? 1 : 0, slowAx = d == 2 ? 1 : 2;
-    double fdc[3][3][128];
-    if (M2 > 128) throw std::runtime_error("too many face points");
+    std::vector<double> fdc((size_t)9 * M2);  // [param][coord][point]
     for (int x = 0; x < 3; ++x) {
       std::vector<double> g(gridNodes + x * KG3, gridNodes + (x + 1) * KG3);
       for (int q = 0; q < 3; ++q) {
@@ -317,14 +315,14 @@ void ElementMetrics(const StdElement &se, const double *gridNodes, double *vol, 
         t = ApplyAxis(t, n[0], n[1], n[2], fastAx, (q == fastAx ? se.dlagInt : se.lagInt).data(), M);
         n[fastAx] = M;
         t = ApplyAxis(t, n[0], n[1], n[2], slowAx, (q == slowAx ? se.dlagInt : se.lagInt).data(), M);
-        for (int l = 0; l < M2; ++l) fdc[q][x][l] = t[l];
+        for (int l = 0; l < M2; ++l) fdc[(q * 3 + x) * M2 + l] = t[l];
       }
     }
     double *fm = face + (size_t)f * 13 * M2;
     for (int l = 0; l < M2; ++l) {
-      const double dxdr = fdc[0][0][l], dydr = fdc[0][1][l], dzdr = fdc[0][2][l];
-      const double dxds = fdc[1][0][l], dyds = fdc[1][1][l], dzds = fdc[1][2][l];
-      const double dxdt = fdc[2][0][l], dydt = fdc[2][1][l], dzdt = fdc[2][2][l];
+      const double dxdr = fdc[(0 * 3 + 0) * M2 + l], dydr = fdc[(0 * 3 + 1) * M2 + l], dzdr = fdc[(0 * 3 + 2) * M2 + l];
+      const double dxds = fdc[(1 * 3 + 0) * M2 + l], dyds = fdc[(1 * 3 + 1) * M2 + l], dzds = fdc[(1 * 3 + 2) * M2 + l];
+      const double dxdt = fdc[(2 * 3 + 0) * M2 + l], dydt = fdc[(2 * 3 + 1) * M2 + l], dzdt = fdc[(2 * 3 + 2) * M2 + l];
       double nx, ny, nz;
       if (d == 0) {
         nx = dyds * dzdt - dydt * dzds; ny = dxdt * dzds - dxds * dzdt; nz = dxds * dydt - dxdt * dyds;

@@ -16,11 +16,22 @@ namespace vcpg {
 // ---------------------------------------------------------------------------
 
 
+// Shared memory of TimeStepKernel in doubles; above the 48 KB of static shared
+// memory (degrees 7-9) it is dynamic.
+template <int K> struct TimeStepSmem {
+  static constexpr int N = 15 * K * K * K + 64;
+  static constexpr bool DYN = N * 8 > 48 * 1024;
+};
+
 template <int K, int M, int NT>
 __global__ void __launch_bounds__(NT) TimeStepKernel(const TimeStepArgs a) {
   constexpr int SLOT = Slot<K, M>::value;
   constexpr int KD = K * K * K;
-  __shared__ double s_sol[5 * KD], s_t1[5 * KD], s_t2[5 * KD], s_red[64];
+  using SM = TimeStepSmem<K>;
+  __shared__ double s_static[SM::DYN ? 1 : SM::N];
+  extern __shared__ __align__(16) double sm_ts[];
+  double *s_sol = SM::DYN ? sm_ts : s_static;
+  double *s_t1 = s_sol + 5 * KD, *s_t2 = s_t1 + 5 * KD, *s_red = s_t2 + 5 * KD;
   const int e = blockIdx.x;
   if (e >= a.n_elem) return;
   // Several cases per launch: per-case parameters, pending and running cases only.
@@ -290,7 +301,7 @@ template <int K, int M, typename T, bool OPEN>
 static cudaError_t ConfigureKMT() {
   using P = Plan<K, M, T, OPEN>;
   static bool configured = false;
-  if (configured) return cudaSuccess;
+  if (configured || P::BIG) return cudaSuccess;
   cudaError_t err = cudaFuncSetAttribute(ResidualKernel<K, M, P::NT, T, OPEN>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)P::BYTES);
@@ -302,7 +313,7 @@ template <int K, int M, typename T>
 static cudaError_t ConfigureFluxKMT() {
   using P = FluxPlan<K, M, T>;
   static bool configured = false;
-  if (configured) return cudaSuccess;
+  if (configured || P::BIG) return cudaSuccess;
   cudaError_t err = cudaFuncSetAttribute(FaceFluxKernel<K, M, P::NT, T>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)P::BYTES);
@@ -329,9 +340,17 @@ static cudaError_t LaunchResidualKMT(const ResidualArgs &a, cudaStream_t st) {
   cudaError_t err = ConfigureKMT<K, M, T, OPEN>();
   if (err == cudaSuccess) err = ConfigureFluxKMT<K, M, T>();
   if (err != cudaSuccess) return err;
-  FaceFluxKernel<K, M, PF::NT, T>
-      <<<a.n_face_elem > 0 ? a.n_face_elem : a.n_elem, PF::NT, PF::BYTES, st>>>(a);
-  ResidualKernel<K, M, P::NT, T, OPEN><<<a.n_elem, P::NT, P::BYTES, st>>>(a);
+  const int nFace = a.n_face_elem > 0 ? a.n_face_elem : a.n_elem;
+  if ((P::BIG || PF::BIG) && (!a.scratch || a.scratch_ctas < 1)) return cudaErrorInvalidValue;
+  if constexpr (PF::BIG)
+    FaceFluxKernel<K, M, PF::NT, T><<<nFace < a.scratch_ctas ? nFace : a.scratch_ctas, PF::NT, 0, st>>>(a);
+  else
+    FaceFluxKernel<K, M, PF::NT, T><<<nFace, PF::NT, PF::BYTES, st>>>(a);
+  if constexpr (P::BIG)
+    ResidualKernel<K, M, P::NT, T, OPEN>
+        <<<a.n_elem < a.scratch_ctas ? a.n_elem : a.scratch_ctas, P::NT, 0, st>>>(a);
+  else
+    ResidualKernel<K, M, P::NT, T, OPEN><<<a.n_elem, P::NT, P::BYTES, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -357,48 +376,84 @@ static cudaError_t LaunchBoundaryKM(const BoundaryArgs &a, cudaStream_t st) {
 
 template <int K, int M>
 static cudaError_t LaunchTimeStepKM(const TimeStepArgs &a, cudaStream_t st) {
+  constexpr size_t sgsSmem = sizeof(double) * 32 * K * K * K;
   if (a.sgs) {
-    constexpr size_t smem = sizeof(double) * 32 * K * K * K;
-    TimeStepSgsKernel<K, M, 64><<<a.n_elem, 64, smem, st>>>(a);
+    if constexpr (sgsSmem <= 227 * 1024)
+      TimeStepSgsKernel<K, M, 64><<<a.n_elem, 64, sgsSmem, st>>>(a);
+    else
+      return cudaErrorInvalidValue;   // no SGS time step at degree 9
   } else {
-    TimeStepKernel<K, M, 64><<<a.n_elem, 64, 0, st>>>(a);
+    using SM = TimeStepSmem<K>;
+    TimeStepKernel<K, M, 64><<<a.n_elem, 64, SM::DYN ? sizeof(double) * SM::N : 0, st>>>(a);
   }
   return cudaGetLastError();
 }
 
-// The SGS time-step kernel's dynamic shared memory (before any capture).
+// Dynamic shared memory of the time-step kernels (before any capture).
 template <int K, int M>
 static cudaError_t ConfigureTimeStepKM() {
-  return cudaFuncSetAttribute(TimeStepSgsKernel<K, M, 64>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)(sizeof(double) * 32 * K * K * K));
+  constexpr size_t sgsSmem = sizeof(double) * 32 * K * K * K;
+  cudaError_t e = cudaSuccess;
+  if constexpr (sgsSmem <= 227 * 1024)
+    e = cudaFuncSetAttribute(TimeStepSgsKernel<K, M, 64>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sgsSmem);
+  using SM = TimeStepSmem<K>;
+  if (e == cudaSuccess && SM::DYN)
+    e = cudaFuncSetAttribute(TimeStepKernel<K, M, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(sizeof(double) * SM::N));
+  return e;
 }
 
-#define VCPG_DISPATCH(K_, M_, CALL) \
-  if (K == K_ && M == M_) return CALL<K_, M_>
+// Every supported (K, M) pair; the open-boundary kernels (static shared memory
+// sized by the pair) exist up to degree 6.
+#define VCPG_PAIRS(X) \
+  X(2, 2) X(2, 3) X(3, 4) X(4, 5) X(5, 7) X(6, 8) X(7, 9) X(8, 12) X(9, 13) X(10, 14)
+#define VCPG_PAIRS_OPEN(X) X(2, 2) X(2, 3) X(3, 4) X(4, 5) X(5, 7) X(6, 8) X(7, 9)
 
 bool Supported(int K, int M) {
-  return (K == 2 && M == 3) || (K == 3 && M == 4) || (K == 4 && M == 5) || (K == 5 && M == 7) ||
-         (K == 6 && M == 8) || (K == 7 && M == 10);
+#define VCPG_IS(K_, M_) if (K == K_ && M == M_) return true;
+  VCPG_PAIRS(VCPG_IS)
+#undef VCPG_IS
+  return false;
+}
+
+bool SupportsOpenBoundaries(int K, int M) {
+#define VCPG_IS(K_, M_) if (K == K_ && M == M_) return true;
+  VCPG_PAIRS_OPEN(VCPG_IS)
+#undef VCPG_IS
+  return false;
 }
 
 int SlotOf(int K, int M) {
-  if (K == 2 && M == 3) return Slot<2, 3>::value;
-  if (K == 3 && M == 4) return Slot<3, 4>::value;
-  if (K == 4 && M == 5) return Slot<4, 5>::value;
-  if (K == 5 && M == 7) return Slot<5, 7>::value;
-  if (K == 6 && M == 8) return Slot<6, 8>::value;
-  if (K == 7 && M == 10) return Slot<7, 10>::value;
+#define VCPG_SLOT_OF(K_, M_) if (K == K_ && M == M_) return Slot<K_, M_>::value;
+  VCPG_PAIRS(VCPG_SLOT_OF)
+#undef VCPG_SLOT_OF
   return -1;
 }
 
 size_t ResidualSmemBytes(int K, int M) {
-  if (K == 2 && M == 3) return Plan<2, 3>::BYTES;
-  if (K == 3 && M == 4) return Plan<3, 4>::BYTES;
-  if (K == 4 && M == 5) return Plan<4, 5>::BYTES;
-  if (K == 5 && M == 7) return Plan<5, 7>::BYTES;
-  if (K == 6 && M == 8) return Plan<6, 8>::BYTES;
-  if (K == 7 && M == 10) return Plan<7, 10>::BYTES;
+#define VCPG_SMEM(K_, M_) if (K == K_ && M == M_) return Plan<K_, M_>::BIG ? 0 : Plan<K_, M_>::BYTES;
+  VCPG_PAIRS(VCPG_SMEM)
+#undef VCPG_SMEM
+  return 0;
+}
+
+template <int K, int M> static size_t ScratchBytesKM(int ctas) {
+  size_t b = 0;
+  auto take = [&b, ctas](bool big, size_t per) { if (big && per * ctas > b) b = per * ctas; };
+  take(Plan<K, M, double, false>::BIG, sizeof(double) * Plan<K, M, double, false>::SCRATCH);
+  take(Plan<K, M, double, true>::BIG, sizeof(double) * Plan<K, M, double, true>::SCRATCH);
+  take(Plan<K, M, float, false>::BIG, sizeof(float) * Plan<K, M, float, false>::SCRATCH);
+  take(Plan<K, M, float, true>::BIG, sizeof(float) * Plan<K, M, float, true>::SCRATCH);
+  take(FluxPlan<K, M, double>::BIG, sizeof(double) * FluxPlan<K, M, double>::SCRATCH);
+  take(FluxPlan<K, M, float>::BIG, sizeof(float) * FluxPlan<K, M, float>::SCRATCH);
+  return b;
+}
+
+size_t ResidualScratchBytes(int K, int M, int ctas) {
+#define VCPG_SCRATCH(K_, M_) if (K == K_ && M == M_) return ScratchBytesKM<K_, M_>(ctas);
+  VCPG_PAIRS(VCPG_SCRATCH)
+#undef VCPG_SCRATCH
   return 0;
 }
 
@@ -409,49 +464,39 @@ size_t FaceFluxBytesPerElement(int K, int M) {
 
 cudaError_t LaunchResidual(int K, int M, const ResidualArgs &a, cudaStream_t st) {
   if (a.n_elem <= 0) return cudaSuccess;
-  if (K == 2 && M == 3) return LaunchResidualKM<2, 3>(a, st);
-  if (K == 3 && M == 4) return LaunchResidualKM<3, 4>(a, st);
-  if (K == 4 && M == 5) return LaunchResidualKM<4, 5>(a, st);
-  if (K == 5 && M == 7) return LaunchResidualKM<5, 7>(a, st);
-  if (K == 6 && M == 8) return LaunchResidualKM<6, 8>(a, st);
+#define VCPG_LAUNCH(K_, M_) if (K == K_ && M == M_) return LaunchResidualKM<K_, M_>(a, st);
+  VCPG_PAIRS(VCPG_LAUNCH)
+#undef VCPG_LAUNCH
   return cudaErrorInvalidValue;
 }
 
 cudaError_t ConfigureTimeStep(int K, int M) {
-  if (K == 2 && M == 3) return ConfigureTimeStepKM<2, 3>();
-  if (K == 3 && M == 4) return ConfigureTimeStepKM<3, 4>();
-  if (K == 4 && M == 5) return ConfigureTimeStepKM<4, 5>();
-  if (K == 5 && M == 7) return ConfigureTimeStepKM<5, 7>();
-  if (K == 6 && M == 8) return ConfigureTimeStepKM<6, 8>();
+#define VCPG_CONF(K_, M_) if (K == K_ && M == M_) return ConfigureTimeStepKM<K_, M_>();
+  VCPG_PAIRS(VCPG_CONF)
+#undef VCPG_CONF
   return cudaErrorInvalidValue;
 }
 
 cudaError_t ConfigureResidual(int K, int M) {
-  if (K == 2 && M == 3) return ConfigureKM<2, 3>();
-  if (K == 3 && M == 4) return ConfigureKM<3, 4>();
-  if (K == 4 && M == 5) return ConfigureKM<4, 5>();
-  if (K == 5 && M == 7) return ConfigureKM<5, 7>();
-  if (K == 6 && M == 8) return ConfigureKM<6, 8>();
+#define VCPG_CONF(K_, M_) if (K == K_ && M == M_) return ConfigureKM<K_, M_>();
+  VCPG_PAIRS(VCPG_CONF)
+#undef VCPG_CONF
   return cudaErrorInvalidValue;
 }
 
 cudaError_t LaunchBoundary(int K, int M, const BoundaryArgs &a, cudaStream_t st) {
   if (a.nB <= 0) return cudaSuccess;
-  if (K == 2 && M == 3) return LaunchBoundaryKM<2, 3>(a, st);
-  if (K == 3 && M == 4) return LaunchBoundaryKM<3, 4>(a, st);
-  if (K == 4 && M == 5) return LaunchBoundaryKM<4, 5>(a, st);
-  if (K == 5 && M == 7) return LaunchBoundaryKM<5, 7>(a, st);
-  if (K == 6 && M == 8) return LaunchBoundaryKM<6, 8>(a, st);
+#define VCPG_LAUNCH(K_, M_) if (K == K_ && M == M_) return LaunchBoundaryKM<K_, M_>(a, st);
+  VCPG_PAIRS_OPEN(VCPG_LAUNCH)
+#undef VCPG_LAUNCH
   return cudaErrorInvalidValue;
 }
 
 cudaError_t LaunchTimeStep(int K, int M, const TimeStepArgs &a, cudaStream_t st) {
   if (a.n_elem <= 0) return cudaSuccess;
-  if (K == 2 && M == 3) return LaunchTimeStepKM<2, 3>(a, st);
-  if (K == 3 && M == 4) return LaunchTimeStepKM<3, 4>(a, st);
-  if (K == 4 && M == 5) return LaunchTimeStepKM<4, 5>(a, st);
-  if (K == 5 && M == 7) return LaunchTimeStepKM<5, 7>(a, st);
-  if (K == 6 && M == 8) return LaunchTimeStepKM<6, 8>(a, st);
+#define VCPG_LAUNCH(K_, M_) if (K == K_ && M == M_) return LaunchTimeStepKM<K_, M_>(a, st);
+  VCPG_PAIRS(VCPG_LAUNCH)
+#undef VCPG_LAUNCH
   return cudaErrorInvalidValue;
 }
 
@@ -488,32 +533,9 @@ cudaError_t LaunchLsrkStage(double *sol, double *du, const double *res, const do
   return cudaGetLastError();
 }
 
-void FillOpTable(const vcpg_operators *ops, int K, int M, OpTable *t) {
-  std::memset(t, 0, sizeof(*t));
-  for (int k = 0; k < K; ++k)
-    for (int m = 0; m < M; ++m) {
-      t->leg[k * M + m] = ops->leg_int[k * M + m];
-      t->dleg[k * M + m] = ops->dleg_int[k * M + m];
-    }
-  for (int i = 0; i < 2 * K; ++i) {
-    t->face[i] = ops->leg_face[i];
-    t->dface[i] = ops->dleg_face[i];
-  }
-  for (int m = 0; m < M; ++m) t->w[m] = ops->w_int[m];
-  for (int i = 0; i < K * K; ++i) t->legdof[i] = ops->leg_dofs[i];
-  if (ops->dleg_dofs)
-    for (int i = 0; i < K * K; ++i) t->dlegdof[i] = ops->dleg_dofs[i];
-  for (int i = 0; i < K * K * K; ++i) t->center[i] = ops->basis_center[i];
-  // FP32 copies, rounded once from the FP64 operators, for the mixed form.
-  for (int i = 0; i < K * M; ++i) { t->legf[i] = (float)t->leg[i]; t->dlegf[i] = (float)t->dleg[i]; }
-  for (int i = 0; i < 2 * K; ++i) { t->facef[i] = (float)t->face[i]; t->dfacef[i] = (float)t->dface[i]; }
-  for (int m = 0; m < M; ++m) t->wf[m] = (float)t->w[m];
-  for (int i = 0; i < K * K * K; ++i) t->centerf[i] = (float)t->center[i];
-}
-
-cudaError_t UploadOpTable(int slot, const OpTable &t) {
-  return cudaMemcpyToSymbol(c_ops, &t, sizeof(OpTable), sizeof(OpTable) * (size_t)slot,
-                            cudaMemcpyHostToDevice);
+cudaError_t UploadOperatorTable(const vcpg_operators *ops, int K, int M) {
+  return UploadOperators(K, M, ops->leg_int, ops->dleg_int, ops->leg_face, ops->dleg_face,
+                         ops->w_int, ops->leg_dofs, ops->dleg_dofs);
 }
 
 }  // namespace vcpg

@@ -19,9 +19,15 @@ int SlotOf(int K, int M);
 size_t ResidualSmemBytes(int K, int M);
 // Device bytes per element of the face-flux buffer (ResidualArgs::face_flux).
 size_t FaceFluxBytesPerElement(int K, int M);
-// Operator table of a (K, M) pair from the C-ABI operators (FP64 and FP32 copies).
-void FillOpTable(const vcpg_operators *ops, int K, int M, OpTable *t);
-cudaError_t UploadOpTable(int slot, const OpTable &t);
+// The open-boundary kernels exist for this pair (degrees up to 6).
+bool SupportsOpenBoundaries(int K, int M);
+// Global scratch of the residual kernels for degrees whose element arrays exceed
+// one CTA's shared memory (ResidualArgs::scratch), for a grid of `ctas` CTAs; 0
+// when every variant of the pair runs in shared memory.
+size_t ResidualScratchBytes(int K, int M, int ctas);
+// Uploads the 1-D operators of a (K, M) pair (FP64 and FP32 copies) to the
+// constant memory of this library's residual, boundary and time-step kernels.
+cudaError_t UploadOperatorTable(const vcpg_operators *ops, int K, int M);
 // Per-case step bookkeeping of a bucket holding several cases (csrc/ensemble.cu).
 cudaError_t LaunchEnsembleFinalize(int n_cases, int *state, const int *target, int *done,
                                    unsigned long long *dt_bits, double *dt, double *sim_time,
@@ -32,7 +38,7 @@ cudaError_t LaunchResidual(int K, int M, const ResidualArgs &a, cudaStream_t st)
 // Sets the shared-memory limits of all residual-kernel variants of a (K, M) pair;
 // call before capturing launches into a CUDA graph.
 cudaError_t ConfigureResidual(int K, int M);
-// Dynamic shared memory of the time-step kernel with an SGS model.
+// Dynamic shared memory of the time-step kernels (with an SGS model, or degree >= 7).
 cudaError_t ConfigureTimeStep(int K, int M);
 // Boundary traces + Mach weights, then the boundary states and fluxes (2 launches).
 cudaError_t LaunchBoundary(int K, int M, const BoundaryArgs &a, cudaStream_t st);

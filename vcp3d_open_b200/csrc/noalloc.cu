@@ -139,21 +139,15 @@ extern "C" int vcpg_time_step_noalloc(const vcpg_params *params, const vcpg_oper
   if (params->sgs_model != VCPG_SGS_NONE) return VCPG_E_INVALID;
   if (nE <= 0) return VCPG_E_INVALID;
   if (nE > kMaxElems) return VCPG_E_ADMISSION;  // beyond the static scratch array
-  if (!Supported(K, M) || K > kKMax || M > kMMax) return VCPG_E_UNSUPPORTED_KM;
+  // This kernel keeps 15 K^3 doubles in static shared memory: up to degree 6.
+  if (!Supported(K, M) || K > 7) return VCPG_E_UNSUPPORTED_KM;
   double *scratch = nullptr;
   int rc = ScratchForCurrentDevice(&scratch);
   if (rc != VCPG_OK) return rc;
   cudaStream_t st = (cudaStream_t)stream;
-  // Operator table of this (K, M) pair into this file's constant memory.
-  OpTable t;
-  memset(&t, 0, sizeof(t));
-  for (int i = 0; i < K * M; ++i) { t.leg[i] = ops->leg_int[i]; t.dleg[i] = ops->dleg_int[i]; }
-  for (int i = 0; i < 2 * K; ++i) { t.face[i] = ops->leg_face[i]; t.dface[i] = ops->dleg_face[i]; }
-  for (int i = 0; i < M; ++i) t.w[i] = ops->w_int[i];
-  for (int i = 0; i < K * K; ++i) t.legdof[i] = ops->leg_dofs[i];
-  for (int i = 0; i < K * K * K; ++i) t.center[i] = ops->basis_center[i];
-  if (cudaMemcpyToSymbol(c_ops, &t, sizeof(OpTable), sizeof(OpTable) * (size_t)SlotOf(K, M),
-                         cudaMemcpyHostToDevice) != cudaSuccess)
+  // Operators of this (K, M) pair into this file's constant memory.
+  if (UploadOperators(K, M, ops->leg_int, ops->dleg_int, ops->leg_face, ops->dleg_face,
+                      ops->w_int, ops->leg_dofs, nullptr) != cudaSuccess)
     return VCPG_E_CUDA;
   if (cudaMemsetAsync(scratch + kStatusSlot, 0, sizeof(double), st) != cudaSuccess)
     return VCPG_E_CUDA;
@@ -164,6 +158,8 @@ extern "C" int vcpg_time_step_noalloc(const vcpg_params *params, const vcpg_oper
   else if (K == 4 && M == 5) e = LaunchKM<4, 5>(params, d_sol, d_elem_scalars, n, scratch, d_dt, st);
   else if (K == 5 && M == 7) e = LaunchKM<5, 7>(params, d_sol, d_elem_scalars, n, scratch, d_dt, st);
   else if (K == 6 && M == 8) e = LaunchKM<6, 8>(params, d_sol, d_elem_scalars, n, scratch, d_dt, st);
+  else if (K == 2 && M == 2) e = LaunchKM<2, 2>(params, d_sol, d_elem_scalars, n, scratch, d_dt, st);
+  else if (K == 7 && M == 9) e = LaunchKM<7, 9>(params, d_sol, d_elem_scalars, n, scratch, d_dt, st);
   if (e != cudaSuccess) return VCPG_E_CUDA;
   double status = 0.0;
   if (cudaMemcpyAsync(&status, scratch + kStatusSlot, sizeof(double), cudaMemcpyDeviceToHost,
