@@ -23,6 +23,14 @@ WORKLOADS = {
     "tgv48_p4_lsrk4": dict(_TGV, n_elem=(48, 48, 48), p=4),
     # Profiling size: state + metrics ~200 MB (above the 126 MB L2), 8000 elements.
     "tgv20_p3_lsrk4": dict(_TGV, n_elem=(20, 20, 20), p=3),
+    # The reference's high degrees: p6 with a 16th-order rule (M = 9, 1.4M DOFs) and
+    # p9 with the default rule (M = 14, 1.7M DOFs); their element arrays exceed one
+    # CTA's shared memory from p7 on. A smooth sine map of amplitude 0.05 curves
+    # the grid (random node moves give the closely spaced nodes of these degrees
+    # non-positive Jacobians, which the reference rejects).
+    "tgv16_p6_lsrk4": dict(_TGV, n_elem=(16, 16, 16), p=6, n_poly_int=16, grid_map="sine",
+                           grid_amp=0.05),
+    "tgv12_p9_lsrk4": dict(_TGV, n_elem=(12, 12, 12), p=9, grid_map="sine", grid_amp=0.05),
     # Degree 4 on 16^3 elements: the mixed-versus-FP64 test case (fits a test's time).
     "tgv16_p4_lsrk4": dict(_TGV, n_elem=(16, 16, 16), p=4),
     # Acoustic pulse with open boundaries: [0,20]x[0,10]x[0,10], 40x20x20 elements of
