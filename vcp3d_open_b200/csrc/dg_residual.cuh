@@ -598,7 +598,7 @@ __device__ __forceinline__ void TraceCartesianGrad(const T *TR, const int t, con
 // normal is the left element's. Writes the normal flux and the Cartesian
 // symmetrizing fluxes (component 0 of those is zero) to out[20][M^2]:
 // 0-4 flux, 5-9 x, 10-14 y, 15-19 z.
-template <int K, int M, typename T>
+template <int K, int M, bool SGS, typename T>
 __device__ __forceinline__ void FacePointFlux(const ResidualArgs &a, const double mu, const int d,
                                               const int pt, const T *TR, const int tL,
                                               const int tR, const double *fmL,
@@ -634,7 +634,7 @@ __device__ __forceinline__ void FacePointFlux(const ResidualArgs &a, const doubl
   T sx[5], sy[5], sz[5];
   ViscousPenaltySymFlux(VL, VR, gx, gy, gz, nx, ny, nz, wf, area, T(mu),
                         T(a.tau_num) / lenScale, T(a.theta_sym), flux, sx, sy, sz, T(1.0),
-                        T(0.0), a.sgs, lenLES, &eddy);
+                        T(0.0), SGS ? a.sgs : 0, lenLES, &eddy);
 #pragma unroll
   for (int n = 0; n < 5; ++n) {
     out[n * M2 + pt] = flux[n];
@@ -689,7 +689,7 @@ __device__ __forceinline__ void FaceRoles(const ResidualArgs &a, const int g, co
 // once, by its upper element): the traces of both sides (TPSAG[IJK]) and the
 // pointwise fluxes, into face_flux[e][d][20][M^2]. Boundary faces are skipped
 // (their fluxes come from the boundary kernels).
-template <int NT, int K, int M, typename T>
+template <int NT, int K, int M, typename T, bool SGS>
 __device__ __forceinline__ void MinFaceFluxes(const ResidualArgs &a, const int e, const double mu,
                                               const T *s_sol, const T *s_fv, T *work) {
   constexpr int SLOT = Slot<K, M>::value;
@@ -724,11 +724,11 @@ __device__ __forceinline__ void MinFaceFluxes(const ResidualArgs &a, const int e
     const double *fmNb = a.face_metric + ((size_t)nb * 6 + 2 * d + 1) * 13 * M2;
     // The lower element (the neighbour, trace slot 2d+1) is the left state.
     T eddy = T(0.0);
-    FacePointFlux<K, M>(a, mu, d, pt, TR, 2 * d + 1, 2 * d, fmNb, fmOwn, lenScale,
+    FacePointFlux<K, M, SGS>(a, mu, d, pt, TR, 2 * d + 1, 2 * d, fmNb, fmOwn, lenScale,
                         out + d * 20 * M2, lenLES, eddy);
     eddyMax = Fmax(eddyMax, eddy);
   }
-  if (a.sgs && a.eddymax) {
+  if (SGS && a.eddymax) {
     // Largest eddy viscosity of the faces for the monitoring data.
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) eddyMax = Fmax(eddyMax, __shfl_xor_sync(0xffffffffu, eddyMax, o));
@@ -1189,7 +1189,7 @@ template <int K, int M, typename T = double> struct FluxPlan {
 
 // The fluxes of every interior face, computed once by the face's upper element
 // (its Min faces), before the residual kernel distributes them to both sides.
-template <int K, int M, int NT, typename T>
+template <int K, int M, int NT, typename T, bool SGS>
 __device__ __forceinline__ void FaceFluxElement(const ResidualArgs &a, const int e, T *smem) {
   constexpr int KD = K * K * K;
   T *s_sol = smem, *s_fv = s_sol + 5 * KD, *work = s_fv + FluxPlan<K, M, T>::FV;
@@ -1206,10 +1206,11 @@ __device__ __forceinline__ void FaceFluxElement(const ResidualArgs &a, const int
     s_fv[2 * K + threadIdx.x] = FaceDer<Slot<K, M>::value, T>(threadIdx.x);
   }
   __syncthreads();
-  MinFaceFluxes<NT, K, M, T>(a, e, mu, s_sol, s_fv, work);
+  MinFaceFluxes<NT, K, M, T, SGS>(a, e, mu, s_sol, s_fv, work);
 }
 
-template <int K, int M, int NT, typename T>
+// SGS: with a subgrid-scale model (without one the kernel carries none of its code).
+template <int K, int M, int NT, typename T, bool SGS>
 __global__ void __launch_bounds__(NT, (FluxPlan<K, M, T>::MIN_BLOCKS)) FaceFluxKernel(const ResidualArgs a) {
   using P = FluxPlan<K, M, T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1217,12 +1218,12 @@ __global__ void __launch_bounds__(NT, (FluxPlan<K, M, T>::MIN_BLOCKS)) FaceFluxK
   if constexpr (P::BIG) {
     T *base = reinterpret_cast<T *>(a.scratch) + (size_t)blockIdx.x * P::SCRATCH;
     for (int e = blockIdx.x; e < n; e += gridDim.x) {
-      FaceFluxElement<K, M, NT, T>(a, e, base);
+      FaceFluxElement<K, M, NT, T, SGS>(a, e, base);
       __syncthreads();
     }
   } else {
     if ((int)blockIdx.x >= n) return;
-    FaceFluxElement<K, M, NT, T>(a, blockIdx.x, reinterpret_cast<T *>(smem_raw));
+    FaceFluxElement<K, M, NT, T, SGS>(a, blockIdx.x, reinterpret_cast<T *>(smem_raw));
   }
 }
 

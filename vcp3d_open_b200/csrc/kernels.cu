@@ -314,9 +314,12 @@ static cudaError_t ConfigureFluxKMT() {
   using P = FluxPlan<K, M, T>;
   static bool configured = false;
   if (configured || P::BIG) return cudaSuccess;
-  cudaError_t err = cudaFuncSetAttribute(FaceFluxKernel<K, M, P::NT, T>,
+  cudaError_t err = cudaFuncSetAttribute(FaceFluxKernel<K, M, P::NT, T, false>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)P::BYTES);
+  if (err == cudaSuccess)
+    err = cudaFuncSetAttribute(FaceFluxKernel<K, M, P::NT, T, true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P::BYTES);
   if (err == cudaSuccess) configured = true;
   return err;
 }
@@ -342,10 +345,12 @@ static cudaError_t LaunchResidualKMT(const ResidualArgs &a, cudaStream_t st) {
   if (err != cudaSuccess) return err;
   const int nFace = a.n_face_elem > 0 ? a.n_face_elem : a.n_elem;
   if ((P::BIG || PF::BIG) && (!a.scratch || a.scratch_ctas < 1)) return cudaErrorInvalidValue;
-  if constexpr (PF::BIG)
-    FaceFluxKernel<K, M, PF::NT, T><<<nFace < a.scratch_ctas ? nFace : a.scratch_ctas, PF::NT, 0, st>>>(a);
+  const unsigned gridF = PF::BIG ? (nFace < a.scratch_ctas ? nFace : a.scratch_ctas) : nFace;
+  const size_t smemF = PF::BIG ? 0 : PF::BYTES;
+  if (a.sgs)
+    FaceFluxKernel<K, M, PF::NT, T, true><<<gridF, PF::NT, smemF, st>>>(a);
   else
-    FaceFluxKernel<K, M, PF::NT, T><<<nFace, PF::NT, PF::BYTES, st>>>(a);
+    FaceFluxKernel<K, M, PF::NT, T, false><<<gridF, PF::NT, smemF, st>>>(a);
   if constexpr (P::BIG)
     ResidualKernel<K, M, P::NT, T, OPEN>
         <<<a.n_elem < a.scratch_ctas ? a.n_elem : a.scratch_ctas, P::NT, 0, st>>>(a);
