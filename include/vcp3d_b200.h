@@ -83,6 +83,9 @@ typedef struct vcpg_params {
                                  1586-1612, src/SolverClass.cpp:3754-3783); else 0 */
   double mach;                /* "Mach number" (force coefficients)                  */
   double ref_area;            /* "Reference area force coefficients" (default 1)     */
+  double body_force[3];       /* "Body force per unit volume (x,y,z)", dimensional
+                                 (N/m^3): the source -J w (0, f, u.f) / p_ref of the
+                                 volume residual (src/ElementClass.cpp:4495-4533)    */
 } vcpg_params;
 
 /* Standard-element operators (StandardElementClass, src/StandardElementClass.cpp:105-911). */

@@ -66,6 +66,7 @@ class Disc:
     cfl: float
     n_poly: int
     sgs: int = SGS_NONE      # subgrid-scale model
+    fbody: tuple = None      # body force per unit volume / p_ref, or None
     dlegdof: np.ndarray = None   # [K, K] basis derivative at the 1-D nodal DOFs
     vmd: np.ndarray = None       # [nE, 10, K^3] metric terms at the nodal DOFs
 
@@ -208,6 +209,12 @@ def volume_residual(U, d: Disc, compat=True):
                  .reshape(nE, 5, M, M, M))
     R = (vol_project(F[0], d.leg, d.leg, d.dleg) + vol_project(F[1], d.leg, d.dleg, d.leg)
          + vol_project(F[2], d.dleg, d.leg, d.leg))
+    if d.fbody is not None:
+        # Body force: -J w (f, u . f) on momentum and energy (src/ElementClass.cpp:4495-4533).
+        fx, fy, fz = d.fbody
+        S = np.stack([weight * fx, weight * fy, weight * fz,
+                      weight * (u * fx + v * fy + w * fz)], axis=1).reshape(nE, 4, M, M, M)
+        R[:, 1:] = R[:, 1:] + vol_project(S, d.leg, d.leg, d.leg)
     cg = dict(rho=rho, u=u, v=v, w=w, p=p, rE=rE, eKin=eKin, JW=J * W3, eddy_max=eddy.max())
     return R, cg
 
@@ -640,4 +647,6 @@ def from_discretization(disc, params) -> Disc:
                 theta=params.theta_sym, riemann=params.riemann, p_ref=params.p_ref,
                 u_ref=params.u_ref, rho_ref=params.rho_ref, cfl=params.cfl,
                 n_poly=params.n_poly, sgs=params.sgs_model, dlegdof=disc.dleg_dofs,
-                vmd=disc.vol_metric_dofs)
+                vmd=disc.vol_metric_dofs,
+                fbody=(tuple(1.0 / params.p_ref * f for f in params.body_force)
+                       if any(params.body_force) else None))

@@ -77,6 +77,11 @@ GOLDEN_SPECS = {
     "tgv_p9_2x2x2_roe": cases.CaseSpec(name="tgv_p9_2x2x2_roe", kind="tgv", n_elem=(2, 2, 2),
                                        p=9, riemann="Roe", hi=(TWO_PI,) * 3, mach=0.1,
                                        reynolds=1600.0, grid_map="sine", grid_amp=0.05),
+    # A body force per unit volume (N/m^3) on the isentropic vortex, degree 3.
+    "vortex_p3_4x4x2_body": cases.CaseSpec(name="vortex_p3_4x4x2_body", kind="vortex",
+                                           n_elem=(4, 4, 2), p=3, hi=(10.0, 10.0, 5.0),
+                                           center=(5.0, 5.0, 2.5), seed=15,
+                                           body_force=(2.0, -1.0, 0.5)),
     # WALE subgrid-scale model, Taylor-Green vortex at a high Reynolds number on a
     # perturbed grid, degree 4.
     "tgv_p4_3x3x3_wale": cases.CaseSpec(name="tgv_p4_3x3x3_wale", kind="tgv", n_elem=(3, 3, 3),
@@ -263,7 +268,7 @@ def spec_to_json(spec: cases.CaseSpec) -> str:
 def spec_from_json(text: str) -> cases.CaseSpec:
     d = json.loads(text)
     for k in ("n_elem", "lo", "hi", "vel_dir", "center", "bc", "sponge", "wall_data",
-              "prescribed_p", "sponge_state", "free_stream"):
+              "prescribed_p", "sponge_state", "free_stream", "body_force"):
         if d.get(k) is not None:
             d[k] = tuple(d[k])
     for k in ("prescribed_inflow", "prescribed_total", "prescribed_super"):

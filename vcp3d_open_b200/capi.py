@@ -45,7 +45,8 @@ class Params(C.Structure):
                 ("rel_penalty", C.c_double), ("cfl", C.c_double), ("mu", C.c_double),
                 ("p_ref", C.c_double), ("u_ref", C.c_double), ("rho_ref", C.c_double),
                 ("sgs_model", C.c_int32), ("monitor_forces", C.c_int32),
-                ("mach", C.c_double), ("ref_area", C.c_double)]
+                ("mach", C.c_double), ("ref_area", C.c_double),
+                ("body_force", C.c_double * 3)]
 
 
 class Operators(C.Structure):

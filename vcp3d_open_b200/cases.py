@@ -172,6 +172,8 @@ class CaseSpec:
     # reference area.
     monitor_forces: bool = False
     ref_area: float = 1.0
+    # Body force per unit volume (N/m^3, x, y, z); None: none.
+    body_force: Optional[Tuple[float, float, float]] = None
 
     def __post_init__(self):
         if self.p_grid is None:
@@ -553,6 +555,13 @@ def prescribed_values(spec: CaseSpec, ref: "RefConditions"):
 _SGS_NAMES = {"none": "None", "wale": "WALE", "vreman": "Vreman"}
 
 
+def _body_force_line(spec: CaseSpec) -> str:
+    if spec.body_force is None:
+        return ""
+    f = spec.body_force
+    return f"Body force per unit volume (x,y,z): {f[0]!r} {f[1]!r} {f[2]!r}\n"
+
+
 def free_stream_values(spec: CaseSpec) -> Tuple[float, float, float, float, float]:
     """Dimensional free stream (rho, u, v, w, p) of a generated case as the
     reference derives it from the prescribed boundary data of its parameter file
@@ -596,7 +605,7 @@ Free stream velocity direction: {d[0]!r} {d[1]!r} {d[2]!r}
 Fluctuations to add to initial solution: No fluctuations
 Monitor forces: {"yes" if spec.monitor_forces else "no"}
 Reference area force coefficients: {spec.ref_area!r}
-Number of synchronization time steps: 1
+{_body_force_line(spec)}Number of synchronization time steps: 1
 Synchronization time step: 1.0
 CFL number: {spec.cfl!r}
 Compute average solution: no

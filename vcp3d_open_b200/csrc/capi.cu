@@ -97,6 +97,10 @@ ResidualArgs MakeResidualArgs(vcpg_handle *h, double *rawOut, unsigned long long
   a.scratch_ctas = h->scratch_ctas;
   a.n_elem = (int)h->nOwned;
   a.n_face_elem = (int)h->nFace;
+  a.body_force = (h->prm.body_force[0] != 0.0 || h->prm.body_force[1] != 0.0 ||
+                  h->prm.body_force[2] != 0.0) ? 1 : 0;
+  const double pRefInv = 1.0 / h->prm.p_ref;
+  for (int c = 0; c < 3; ++c) a.fbody[c] = pRefInv * h->prm.body_force[c];
   a.mu = h->prm.mu;
   a.tau_num = (double)((h->prm.n_poly + 1) * (h->prm.n_poly + 1)) * h->prm.rel_penalty;
   a.theta_sym = h->prm.theta_sym;

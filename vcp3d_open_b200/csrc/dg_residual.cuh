@@ -79,6 +79,8 @@ struct ResidualArgs {
   // global scratch area per CTA of a grid that loops over the elements.
   void *scratch;
   int scratch_ctas;            // CTAs the scratch areas hold (the grid of those degrees)
+  int body_force;              // 1: the body-force source with fbody
+  double fbody[3];             // body force per unit volume / p_ref
 };
 
 // Arguments of the CFL time-step kernel (kernels.cu).
@@ -501,6 +503,26 @@ __device__ __forceinline__ void VolumePhase(const ResidualArgs &a, const int e, 
     ContractL<NT, SLOT, K, M, kLegT, 1, 5, M, M, K, M, K, false, T, typename P::VD, typename P::VE>(tJ, tK);
     __syncthreads();
     ContractL<NT, SLOT, K, M, kLegT, 0, 5, M, K, K, M, K, true, T, typename P::VE, Dense<K, K, K>>(tK, s_R);
+    __syncthreads();
+  }
+  // Body force per unit volume (src/ElementClass.cpp:4495-4533): the source
+  // -J w (f, u . f) on the momentum and energy residuals.
+  if (a.body_force) {
+    const T fx = T(a.fbody[0]), fy = T(a.fbody[1]), fz = T(a.fbody[2]);
+    for (int l = threadIdx.x; l < MD; l += NT) {
+      const T weight = -s_jw[l];
+      const T u = s_cgp[1 * MD + l], v = s_cgp[2 * MD + l], w = s_cgp[3 * MD + l];
+      dX[0 * MD + l] = weight * fx;
+      dX[1 * MD + l] = weight * fy;
+      dX[2 * MD + l] = weight * fz;
+      dX[3 * MD + l] = weight * (u * fx + v * fy + w * fz);
+    }
+    __syncthreads();
+    ContractL<NT, SLOT, K, M, kLegT, 2, 4, M, M, M, M, K, false, T, Dense<M, M, M>, typename P::VD>(dX, tJ);
+    __syncthreads();
+    ContractL<NT, SLOT, K, M, kLegT, 1, 4, M, M, K, M, K, false, T, typename P::VD, typename P::VE>(tJ, tK);
+    __syncthreads();
+    ContractL<NT, SLOT, K, M, kLegT, 0, 4, M, K, K, M, K, true, T, typename P::VE, Dense<K, K, K>>(tK, s_R + KD);
     __syncthreads();
   }
 }

@@ -542,8 +542,6 @@ def check_supported(pf: ParamFile) -> None:
         raise UnsupportedOption(f"Wall modeling: {pf.wall_model}")
     if pf.fluctuations not in ("no fluctuations", "pressure pulse"):
         raise UnsupportedOption(f"Fluctuations to add to initial solution: {pf.fluctuations}")
-    if pf.body_force is not None and any(pf.body_force):
-        raise UnsupportedOption("Body force per unit volume")
     if pf.compute_average:
         raise UnsupportedOption("Compute average solution")
     if pf.outlet_local_mach:

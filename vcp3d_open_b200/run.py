@@ -166,6 +166,7 @@ def load_case(pf: ParamFile) -> cases.CaseData:
         reynolds_length=pf.reynolds_length, t_inf=pf.t_inf,
         vel_dir=vel_dir, riemann="IsmailRoe" if pf.riemann == "ismailroe" else "Roe",
         sgs=pf.sgs_model, monitor_forces=pf.monitor_forces, ref_area=pf.reference_area,
+        body_force=tuple(pf.body_force) if pf.body_force is not None else None,
         theta_sym=pf.theta_sym, penalty=pf.penalty, cfl=pf.cfl, grid_map="none",
         bc=bcs, p_inf=ref.p_ref, outlet_len=pf.outlet_len, outlet_sigma=pf.outlet_sigma,
         outlet_beta_l=pf.outlet_beta_l, outlet_beta_t=pf.outlet_beta_t,

@@ -70,6 +70,8 @@ def make_params(case: CaseData, metric_compat: bool = True,
     walls = any(b.startswith("wall_") for b in s.bc)
     p.monitor_forces = 1 if (s.monitor_forces and walls) else 0
     p.mach, p.ref_area = s.mach, s.ref_area
+    if s.body_force is not None:
+        p.body_force[:] = [float(v) for v in s.body_force]
     return p
 
 
