@@ -121,10 +121,20 @@ int vcpg_create(const vcpg_params *params, const vcpg_operators *ops,
 int vcpg_destroy(vcpg_handle *h);
 const char *vcpg_last_error(const vcpg_handle *h);
 
+/* Parametric positions of the nodal solution DOFs and of the grid nodes
+ * ("Location of the DOFs"; the reference detects the grid's own spacing,
+ * ElementClass::LGLDistribution, src/ElementClass.cpp:3406-3622). */
+enum vcpg_dof_location {
+  VCPG_DOFS_EQUIDISTANT = 0,     /* equidistant solution DOFs and grid nodes */
+  VCPG_DOFS_LGL = 1,             /* LGL solution DOFs and grid nodes         */
+  VCPG_DOFS_EQUI_GRID_LGL = 2,   /* equidistant solution DOFs, LGL grid      */
+  VCPG_DOFS_LGL_GRID_EQUI = 3    /* LGL solution DOFs, equidistant grid      */
+};
+
 /* Host-side set-up from a high-order grid (the product's own restatement of the
  * reference's operator and metric pre-processing). grid_nodes is the per-element
- * grid, [n_elem][3][(p_grid+1)^3], nodes at LGL (dof_location = 1) or
- * equidistant (0) parametric positions. Fills caller-allocated arrays with the
+ * grid, [n_elem][3][(p_grid+1)^3], nodes and solution DOFs at the parametric
+ * positions of dof_location (enum vcpg_dof_location). Fills caller-allocated arrays with the
  * shapes documented in vcpg_operators / vcpg_geometry; neighbors are filled for
  * a block that is periodic in every direction listed in periodic[3]. */
 int vcpg_setup_geometry(const vcpg_params *params, int32_t p_grid, int32_t dof_location,
@@ -159,6 +169,11 @@ int vcpg_setup_geometry_device(const vcpg_params *params, int32_t p_grid, int32_
  * vand_inv is the [K][K] inverse 1-D Vandermonde matrix of the nodal DOFs,
  * vand_inv[c * K + o] mapping nodal value c to mode o; NULL selects the LGL
  * nodal DOFs. */
+/* The [K][K] inverse 1-D Vandermonde matrix of the nodal solution DOFs of
+ * dof_location (StandardElementClass, src/StandardElementClass.cpp:860-880), the
+ * vand_inv argument of vcpg_nodal_conservative_to_modal. */
+int vcpg_vandermonde_inverse(int32_t n_poly, int32_t dof_location, double *vand_inv);
+
 int vcpg_nodal_conservative_to_modal(const vcpg_params *params, const double *vand_inv,
                                      const double *cons, double *modal, int64_t n_elem);
 

@@ -77,6 +77,10 @@ GOLDEN_SPECS = {
     "tgv_p9_2x2x2_roe": cases.CaseSpec(name="tgv_p9_2x2x2_roe", kind="tgv", n_elem=(2, 2, 2),
                                        p=9, riemann="Roe", hi=(TWO_PI,) * 3, mach=0.1,
                                        reynolds=1600.0, grid_map="sine", grid_amp=0.05),
+    # Equidistant solution DOFs on the LGL grid.
+    "vortex_p3_4x3x3_equi": cases.CaseSpec(name="vortex_p3_4x3x3_equi", kind="vortex",
+                                           n_elem=(4, 3, 3), p=3, hi=(10.0, 7.5, 7.5),
+                                           center=(5.0, 3.75, 3.75), dof_location="equidistant"),
     # A body force per unit volume (N/m^3) on the isentropic vortex, degree 3.
     "vortex_p3_4x4x2_body": cases.CaseSpec(name="vortex_p3_4x4x2_body", kind="vortex",
                                            n_elem=(4, 4, 2), p=3, hi=(10.0, 10.0, 5.0),
@@ -185,6 +189,16 @@ SYNC_SPECS = {
     # multiple of the padding, as for degree 3).
     "vortex_p3_4x3x3_vreman": (GOLDEN_SPECS["vortex_p3_4x3x3_vreman"],
                                {"Synchronization time step": "2.0e-4"}, 2),
+    # Equidistant solution DOFs of degree 5 (K^3 a multiple of the padding, see
+    # above), from the restart file at those DOFs, with the parameter file's
+    # pressure pulse.
+    "vortex_p5_equi": (cases.CaseSpec(
+        name="vortex_p5_equi", kind="vortex", n_elem=(3, 3, 2), p=5, hi=(10.0, 10.0, 6.0),
+        center=(5.0, 5.0, 3.0), beta=2.0, dof_location="equidistant"),
+        {"Synchronization time step": "2.0e-4",
+         "Fluctuations to add to initial solution": "Pressure pulse",
+         "Pressure pulse center": "4.0 5.0 3.0", "Pressure pulse strength": "1.0e-2",
+         "Pressure pulse width": "1.0"}, 2),
     "pulse_p3_6x4x2_sponge_cml": (OPEN_SPECS["pulse_p3_6x4x2_sponge_cml"],
                                   {"Synchronization time step": "5.0e-5", "Restart": "no",
                                    "Fluctuations to add to initial solution": "Pressure pulse",

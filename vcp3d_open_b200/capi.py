@@ -28,6 +28,7 @@ EXPORTED = [
     "vcpg_create", "vcpg_destroy", "vcpg_last_error", "vcpg_setup_geometry",
     "vcpg_setup_geometry_device", "vcpg_setup_nodal_metrics",
     "vcpg_set_partition", "vcpg_pack_states", "vcpg_unpack_states", "vcpg_rk_stage",
+    "vcpg_vandermonde_inverse",
     "vcpg_nodal_conservative_to_modal", "vcpg_set_state", "vcpg_get_state",
     "vcpg_get_residual", "vcpg_residual", "vcpg_get_raw_residual", "vcpg_time_step",
     "vcpg_step", "vcpg_synchronization_step", "vcpg_sync", "vcpg_stream", "vcpg_launch_count", "vcpg_stats",
@@ -113,6 +114,7 @@ def load() -> C.CDLL:
     lib.vcpg_setup_geometry_device.argtypes = [C.POINTER(Params), C.c_int32, C.c_int32, ip, dp, dp, dp,
                                         dp, dp, dp, dp, dp, dp, dp, dp, ip]
     lib.vcpg_setup_nodal_metrics.argtypes = [C.POINTER(Params), C.c_int32, C.c_int32, dp, dp, dp]
+    lib.vcpg_vandermonde_inverse.argtypes = [C.c_int32, C.c_int32, dp]
     lib.vcpg_nodal_conservative_to_modal.argtypes = [C.POINTER(Params), dp, dp, dp, C.c_int64]
     for name in ("vcpg_set_state", "vcpg_get_state", "vcpg_get_residual", "vcpg_get_raw_residual"):
         getattr(lib, name).argtypes = [hp, dp]

@@ -174,6 +174,10 @@ class CaseSpec:
     ref_area: float = 1.0
     # Body force per unit volume (N/m^3, x, y, z); None: none.
     body_force: Optional[Tuple[float, float, float]] = None
+    # "Location of the DOFs" of the solution ("lgl" or "equidistant") and whether
+    # the grid nodes sit at LGL positions (generated grids do).
+    dof_location: str = "lgl"
+    grid_lgl: bool = True
 
     def __post_init__(self):
         if self.p_grid is None:
@@ -370,17 +374,39 @@ def conservative_state(spec: CaseSpec, xyz: np.ndarray, ref: RefConditions) -> n
     return np.stack([rho, rho * u, rho * v, rho * w, rE])
 
 
-def solution_dof_coordinates(spec: CaseSpec, elem_nodes: np.ndarray) -> np.ndarray:
-    """Coordinates of the nodal solution DOFs per element, shape (nElem, 3, K^3).
+def _lagrange_1d(nodes: np.ndarray, points: np.ndarray) -> np.ndarray:
+    """L[j, i]: the Lagrange polynomial of node j at point i."""
+    L = np.ones((len(nodes), len(points)))
+    for j in range(len(nodes)):
+        for m in range(len(nodes)):
+            if m != j:
+                L[j] *= (points - nodes[m]) / (nodes[j] - nodes[m])
+    return L
 
-    The generated grids place the grid nodes of every element at the LGL points
-    of the element, and the solution DOFs are LGL points of the same degree, so
-    the DOFs coincide with the grid nodes (the reference interpolates the grid
-    with Lagrange polynomials to the DOFs, ElementClass::ComputeCoorNodalSolDOFs).
-    """
-    if spec.p_grid != spec.p:
-        raise NotImplementedError("generated cases use grid degree == solution degree")
-    return elem_nodes
+
+def dof_location_code(spec: CaseSpec) -> int:
+    """enum vcpg_dof_location of a case: solution DOF and grid node positions."""
+    sol_lgl = spec.dof_location.lower() == "lgl"
+    return {(True, True): 1, (False, False): 0, (False, True): 2, (True, False): 3}[
+        (sol_lgl, bool(spec.grid_lgl))]
+
+
+def solution_dof_coordinates(spec: CaseSpec, elem_nodes: np.ndarray) -> np.ndarray:
+    """Coordinates of the nodal solution DOFs per element, shape (nElem, 3, K^3):
+    the grid interpolated with its Lagrange polynomials to the DOF positions
+    (ElementClass::ComputeCoorNodalSolDOFs, src/ElementClass.cpp:816-918). With
+    DOFs at the grid's own positions they are the grid nodes."""
+    Kg, K = spec.p_grid + 1, spec.p + 1
+    sol_lgl = spec.dof_location.lower() == "lgl"
+    if Kg == K and sol_lgl == bool(spec.grid_lgl):
+        return elem_nodes
+    rg = lgl_points(Kg) if spec.grid_lgl else equidistant_points(Kg)
+    rs = lgl_points(K) if sol_lgl else equidistant_points(K)
+    L = _lagrange_1d(rg, rs)                                  # [Kg, K]
+    x = elem_nodes.reshape(elem_nodes.shape[0], 3, Kg, Kg, Kg)   # (k, j, i)
+    for ax in (4, 3, 2):
+        x = np.moveaxis(np.tensordot(x, L, axes=([ax], [0])), -1, ax)
+    return np.ascontiguousarray(x.reshape(elem_nodes.shape[0], 3, K ** 3))
 
 
 # ---------------------------------------------------------------------------
@@ -580,7 +606,7 @@ def param_cfg_text(spec: CaseSpec, grid_file="grid.xyz", restart_file="restart.d
 Polynomial degree grid: {spec.p_grid}
 Polynomial degree solution: {spec.p}
 Polynomial degree integration rule: {spec.n_poly_int}
-Location of the DOFs: LGL
+Location of the DOFs: {"LGL" if spec.dof_location.lower() == "lgl" else "Equidistant"}
 Grid file name: {grid_file}
 Solution file name: data/Solution
 Restart file name: {restart_file}

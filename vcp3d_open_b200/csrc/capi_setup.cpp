@@ -24,7 +24,7 @@ int vcpg_setup_geometry(const vcpg_params *params, int32_t p_grid, int32_t dof_l
     if (K < 2 || M < 1 || nI < 1 || nJ < 1 || nK < 1) return VCPG_E_INVALID;
     // The grid nodes of the generated cases sit at the LGL (or equidistant) positions
     // matching dof_location, as ElementClass::LGLDistribution detects.
-    StdElement se = vcpg::host::BuildStdElement(K, M, Kg, dof_location, dof_location);
+    StdElement se = vcpg::host::BuildStdElement(K, M, Kg, vcpg::host::SolLgl(dof_location), vcpg::host::GridLgl(dof_location));
     if (leg_int) std::memcpy(leg_int, se.leg.data(), sizeof(double) * K * M);
     if (dleg_int) std::memcpy(dleg_int, se.dleg.data(), sizeof(double) * K * M);
     if (leg_face) std::memcpy(leg_face, se.face.data(), sizeof(double) * 2 * K);
@@ -57,12 +57,25 @@ int vcpg_setup_nodal_metrics(const vcpg_params *params, int32_t p_grid, int32_t 
     const int K = params->n_poly + 1, M = params->n_int_1d, Kg = p_grid + 1;
     const int64_t nE = (int64_t)params->n_elem[0] * params->n_elem[1] * params->n_elem[2];
     if (K < 2 || M < 1 || nE < 1) return VCPG_E_INVALID;
-    StdElement se = vcpg::host::BuildStdElement(K, M, Kg, dof_location, dof_location);
+    StdElement se = vcpg::host::BuildStdElement(K, M, Kg, vcpg::host::SolLgl(dof_location), vcpg::host::GridLgl(dof_location));
     if (dleg_dofs) std::memcpy(dleg_dofs, se.dlegdof.data(), sizeof(double) * K * K);
     const int KD = K * K * K, KG3 = Kg * Kg * Kg;
     if (vol_metric_dofs)
       for (int64_t e = 0; e < nE; ++e)
         vcpg::host::NodalMetrics(se, grid_nodes + e * 3 * KG3, vol_metric_dofs + e * 10 * KD);
+  } catch (const std::exception &) {
+    return VCPG_E_INVALID;
+  }
+  return VCPG_OK;
+}
+
+int vcpg_vandermonde_inverse(int32_t n_poly, int32_t dof_location, double *vand_inv) {
+  if (n_poly < 1 || n_poly > 9 || !vand_inv) return VCPG_E_INVALID;
+  const int K = n_poly + 1;
+  try {
+    const std::vector<double> v =
+        vcpg::host::BuildStdElement(K, K, K, vcpg::host::SolLgl(dof_location), 1).vandInv;
+    std::memcpy(vand_inv, v.data(), sizeof(double) * K * K);
   } catch (const std::exception &) {
     return VCPG_E_INVALID;
   }

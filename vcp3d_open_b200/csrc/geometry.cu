@@ -214,7 +214,7 @@ int vcpg_setup_geometry_device(const vcpg_params *params, int32_t p_grid, int32_
   if (K < 2 || M < 1 || nI < 1 || nJ < 1 || nK < 1 || Kg > 10 || M > 16) return VCPG_E_INVALID;
   StdElement se;
   try {
-    se = vcpg::host::BuildStdElement(K, M, Kg, dof_location, dof_location);
+    se = vcpg::host::BuildStdElement(K, M, Kg, vcpg::host::SolLgl(dof_location), vcpg::host::GridLgl(dof_location));
   } catch (const std::exception &) {
     return VCPG_E_INVALID;
   }

@@ -7,6 +7,11 @@
 namespace vcpg {
 namespace host {
 
+// The location code of the C ABI (enum vcpg_dof_location): LGL solution DOFs and
+// LGL grid nodes.
+inline int SolLgl(int loc) { return loc == 1 || loc == 3; }
+inline int GridLgl(int loc) { return loc == 1 || loc == 2; }
+
 double NormJacobi(int n, int alpha, int beta, double x);
 double GradNormJacobi(int n, int alpha, int beta, double x);
 void GaussLegendre(int n, std::vector<double> &x, std::vector<double> &w);

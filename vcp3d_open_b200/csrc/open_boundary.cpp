@@ -186,7 +186,7 @@ int BuildOpenBoundary(const vcpg_params &prm, const vcpg_open_boundary &ob,
     // derivative at the DOFs, and the Lagrange derivative on the Gauss points.
     std::vector<double> rInt, wInt, rDof;
     host::GaussLegendre(M, rInt, wInt);
-    host::DofLocations(K, dofLocation, rDof);
+    host::DofLocations(K, host::SolLgl(dofLocation), rDof);
     std::vector<double> lqv, lqd, ldv, ldd, qqv, qqd;
     Lagrange(rDof, rInt, lqv, lqd);   // lqv[j * M + i] = L_j(q_i)
     Lagrange(rDof, rDof, ldv, ldd);   // ldd[j * K + i] = L_j'(r_i)
@@ -324,7 +324,7 @@ int BuildOpenBoundary(const vcpg_params &prm, const vcpg_open_boundary &ob,
       if (!gridNodes || pGrid < 1) { err = "sponge layers need the grid nodes"; return VCPG_E_INVALID; }
       const int Kg = pGrid + 1, KG3 = Kg * Kg * Kg;
       std::vector<double> rGrid, lgv, lgd;
-      host::DofLocations(Kg, dofLocation, rGrid);
+      host::DofLocations(Kg, host::GridLgl(dofLocation), rGrid);
       Lagrange(rGrid, rInt, lgv, lgd);
       const int n[3] = {nI, nJ, nK};
       // Layer membership per element and direction: bit 2 d = min side, 2 d + 1 = max side.

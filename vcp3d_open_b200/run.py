@@ -107,10 +107,6 @@ def load_case(pf: ParamFile) -> cases.CaseData:
     """CaseData of a parameter file: grid, reference conditions, boundary data
     and the initial nodal state (restart file or free stream, plus fluctuations)."""
     param_file.check_supported(pf)
-    if pf.dof_location != "lgl":
-        raise UnsupportedOption("Location of the DOFs: Equidistant")
-    if pf.p_grid != pf.p:
-        raise UnsupportedOption("grid degree different from the solution degree")
     ref = param_file.reference_conditions(pf)
     n_elem = param_file.n_elements(pf)
     grid = cases.read_plot3d(pf.file(pf.grid_file))
@@ -120,9 +116,13 @@ def load_case(pf: ParamFile) -> cases.CaseData:
             f"grid has {grid.shape[3]}x{grid.shape[2]}x{grid.shape[1]} nodes, the subfaces and "
             f"the grid degree give {expect[0]}x{expect[1]}x{expect[2]}")
     nodes = cases.element_nodes(grid, n_elem, pf.p_grid)
-    if not _grid_is_lgl(nodes, pf.p_grid):
-        raise UnsupportedOption("grid nodes at equidistant positions with LGL solution DOFs")
-    xyz = nodes                      # LGL DOFs of the grid's degree: the grid nodes
+    # Grid nodes at LGL or equidistant positions (detected as the reference does),
+    # solution DOFs where the parameter file puts them; their coordinates are the
+    # grid's Lagrange interpolation.
+    grid_lgl = _grid_is_lgl(nodes, pf.p_grid) if pf.p_grid > 1 else True
+    loc = cases.CaseSpec(p=pf.p, p_grid=pf.p_grid, dof_location=pf.dof_location,
+                         grid_lgl=grid_lgl)
+    xyz = cases.solution_dof_coordinates(loc, nodes)
     n_e, K3 = xyz.shape[0], (pf.p + 1) ** 3
     if pf.restart:
         names, cols = _read_su2_columns(pf.file(pf.restart_file), n_e, K3)
@@ -166,6 +166,7 @@ def load_case(pf: ParamFile) -> cases.CaseData:
         reynolds_length=pf.reynolds_length, t_inf=pf.t_inf,
         vel_dir=vel_dir, riemann="IsmailRoe" if pf.riemann == "ismailroe" else "Roe",
         sgs=pf.sgs_model, monitor_forces=pf.monitor_forces, ref_area=pf.reference_area,
+        dof_location=pf.dof_location, grid_lgl=grid_lgl,
         body_force=tuple(pf.body_force) if pf.body_force is not None else None,
         theta_sym=pf.theta_sym, penalty=pf.penalty, cfl=pf.cfl, grid_map="none",
         bc=bcs, p_inf=ref.p_ref, outlet_len=pf.outlet_len, outlet_sigma=pf.outlet_sigma,

@@ -43,6 +43,7 @@ class Discretization:
     # the metric terms at the nodal DOFs [nE][10][K^3] (vcpg_setup_nodal_metrics).
     dleg_dofs: Optional[np.ndarray] = None
     vol_metric_dofs: Optional[np.ndarray] = None
+    dof_location: int = 1          # enum vcpg_dof_location
 
     @property
     def n_elements(self) -> int:
@@ -98,9 +99,11 @@ def setup_discretization(case: CaseData, params: capi.Params,
         neighbors=np.zeros((nE, 6), dtype=np.int32))
     per = np.asarray(periodic, dtype=np.int32)
     nodes = np.ascontiguousarray(case.elem_nodes, dtype=np.float64)
+    from .cases import dof_location_code
+    d.dof_location = dof_location_code(s)
     setup = lib.vcpg_setup_geometry_device if device else lib.vcpg_setup_geometry
     rc = setup(
-        C.byref(params), s.p_grid, 1, capi.ptr(per), capi.ptr(nodes), capi.ptr(d.leg_int),
+        C.byref(params), s.p_grid, d.dof_location, capi.ptr(per), capi.ptr(nodes), capi.ptr(d.leg_int),
         capi.ptr(d.dleg_int), capi.ptr(d.leg_face), capi.ptr(d.dleg_face), capi.ptr(d.w_int),
         capi.ptr(d.leg_dofs), capi.ptr(d.basis_center), capi.ptr(d.vol_metric),
         capi.ptr(d.face_metric), capi.ptr(d.elem_scalars), capi.ptr(d.neighbors))
@@ -110,7 +113,7 @@ def setup_discretization(case: CaseData, params: capi.Params,
     if params.sgs_model != capi.SGS_NONE:
         d.dleg_dofs = np.zeros((K, K))
         d.vol_metric_dofs = np.zeros((nE, 10, K ** 3))
-        rc = lib.vcpg_setup_nodal_metrics(C.byref(params), s.p_grid, 1, capi.ptr(nodes),
+        rc = lib.vcpg_setup_nodal_metrics(C.byref(params), s.p_grid, d.dof_location, capi.ptr(nodes),
                                           capi.ptr(d.dleg_dofs), capi.ptr(d.vol_metric_dofs))
         if rc != capi.VCPG_OK:
             raise capi.VcpgError(rc, "vcpg_setup_nodal_metrics failed")
@@ -122,7 +125,16 @@ def nodal_to_modal(case: CaseData, params: capi.Params) -> np.ndarray:
     lib = capi.load()
     cons = np.ascontiguousarray(case.cons, dtype=np.float64)
     out = np.zeros_like(cons)
-    rc = lib.vcpg_nodal_conservative_to_modal(C.byref(params), None, capi.ptr(cons),
+    from .cases import dof_location_code
+    vinv = None
+    if dof_location_code(case.spec) not in (1, 3):   # equidistant solution DOFs
+        K = params.n_poly + 1
+        vinv = np.zeros((K, K))
+        rc = lib.vcpg_vandermonde_inverse(params.n_poly, dof_location_code(case.spec),
+                                          capi.ptr(vinv))
+        if rc != capi.VCPG_OK:
+            raise capi.VcpgError(rc, "vcpg_vandermonde_inverse failed")
+    rc = lib.vcpg_nodal_conservative_to_modal(C.byref(params), capi.ptr(vinv), capi.ptr(cons),
                                               capi.ptr(out), cons.shape[0])
     if rc != capi.VCPG_OK:
         raise capi.VcpgError(rc, "vcpg_nodal_conservative_to_modal failed")
@@ -213,7 +225,7 @@ class Solver:
         geom = capi.Geometry(capi.ptr(self._keep[7]), capi.ptr(self._keep[8]),
                              capi.ptr(self._keep[9]), capi.ptr(self._keep[10]))
         self._check(self.lib.vcpg_set_open_boundary(self.h, C.byref(ob), C.byref(geom),
-                                                     case.spec.p_grid, 1,
+                                                     case.spec.p_grid, self.disc.dof_location,
                                                      capi.ptr(self._keep_ob[1])),
                     "set_open_boundary")
 
