@@ -155,6 +155,14 @@ OPEN_SPECS = {
         center=(2.0, 3.3, 1.0), seed=10, riemann="Roe",
         bc=("inflow_supersonic", "outflow_supersonic", "farfield", "farfield", "periodic",
             "periodic"), **_OPEN),
+    # Degree 7 (M = 12, element arrays in global scratch): static inflow and
+    # characteristic outflow with a sponge layer and the matching layer, far field
+    # on the j faces, k periodic, uniform grid.
+    "pulse_p7_3x2x2": cases.CaseSpec(
+        name="pulse_p7_3x2x2", n_elem=(3, 2, 2), p=7, n_poly_int=22, hi=(3.0, 2.0, 2.0),
+        center=(2.4, 1.0, 1.0), sponge=(0, 1, 0, 0, 0, 0), cml=True,
+        bc=("inflow_static_nscbc", "outflow_nscbc", "farfield", "farfield", "periodic",
+            "periodic"), **dict(_OPEN, grid_map="none")),
     # WALE model with walls (isothermal on j-min, heat flux on j-max), static inflow
     # and characteristic outflow in i with a sponge layer, k periodic, degree 4; an
     # isentropic vortex next to the isothermal wall gives the wall faces velocity

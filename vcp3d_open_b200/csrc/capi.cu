@@ -639,7 +639,7 @@ int vcpg_set_open_boundary(vcpg_handle *h, const vcpg_open_boundary *ob,
   if (h->nOwned != h->nE)
     return Fail(h, VCPG_E_INVALID, "open boundaries: the block is partitioned");
   if (!SupportsOpenBoundaries(h->K, h->M))
-    return Fail(h, VCPG_E_UNSUPPORTED_KM, "open boundaries run up to degree 6");
+    return Fail(h, VCPG_E_UNSUPPORTED_KM, "no open-boundary kernels for this degree");
   OpenBoundaryHost ob_host;
   std::string err;
   int rc = BuildOpenBoundary(h->prm, *ob, *geom, p_grid, dof_location, grid_nodes, ob_host, err);

@@ -63,13 +63,24 @@ __device__ __forceinline__ bool BoundaryFaceActive(const BoundaryArgs &a, const 
 
 __device__ __forceinline__ int BFastParam(const int d) { return d == 0 ? 1 : 0; }
 
+// Shared memory of BoundaryTraceKernel in doubles; dynamic above the 48 KB of
+// static shared memory (degrees 7-9).
+template <int K, int M> struct BoundaryTraceSmem {
+  static constexpr int N = 5 * K * K * K + 10 * K * K + 15 * K * M + 21 * M * M;
+  static constexpr bool DYN = N * 8 > 48 * 1024;
+};
+
 template <int K, int M, int NT>
 __global__ void __launch_bounds__(NT) BoundaryTraceKernel(const BoundaryArgs a) {
   constexpr int SLOT = Slot<K, M>::value;
   constexpr int KD = K * K * K, K2 = K * K, M2 = M * M;
-  __shared__ double s_sol[5 * KD], s_bn[5 * K2], s_bnd[5 * K2];
-  __shared__ double s_t1a[5 * K * M], s_t1b[5 * K * M], s_t1c[5 * K * M];
-  __shared__ double s_tr[4 * 5 * M2], s_w[M2];
+  using SM = BoundaryTraceSmem<K, M>;
+  __shared__ double s_static[SM::DYN ? 1 : SM::N];
+  extern __shared__ __align__(16) double sm_bt[];
+  double *s_sol = SM::DYN ? sm_bt : s_static;
+  double *s_bn = s_sol + 5 * KD, *s_bnd = s_bn + 5 * K2;
+  double *s_t1a = s_bnd + 5 * K2, *s_t1b = s_t1a + 5 * K * M, *s_t1c = s_t1b + 5 * K * M;
+  double *s_tr = s_t1c + 5 * K * M, *s_w = s_tr + 4 * 5 * M2;
   const int b = blockIdx.x;
   if (b >= a.nB) return;
   const int *bf = a.bface + b * kBfStride;

@@ -325,8 +325,19 @@ static cudaError_t ConfigureFluxKMT() {
 }
 
 template <int K, int M>
+static cudaError_t ConfigureBoundaryKM() {
+  using SM = BoundaryTraceSmem<K, M>;
+  constexpr int NT = M * M > 64 ? 128 : 64;
+  if (!SM::DYN) return cudaSuccess;
+  return cudaFuncSetAttribute(BoundaryTraceKernel<K, M, NT>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)(sizeof(double) * SM::N));
+}
+
+template <int K, int M>
 static cudaError_t ConfigureKM() {
-  cudaError_t e = ConfigureFluxKMT<K, M, double>();
+  cudaError_t e = ConfigureBoundaryKM<K, M>();
+  if (e == cudaSuccess) e = ConfigureFluxKMT<K, M, double>();
   if (e == cudaSuccess) e = ConfigureFluxKMT<K, M, float>();
   if (e == cudaSuccess) e = ConfigureKMT<K, M, double, false>();
   if (e == cudaSuccess) e = ConfigureKMT<K, M, float, false>();
@@ -374,7 +385,8 @@ static cudaError_t LaunchResidualKM(const ResidualArgs &a, cudaStream_t st) {
 template <int K, int M>
 static cudaError_t LaunchBoundaryKM(const BoundaryArgs &a, cudaStream_t st) {
   constexpr int NT = M * M > 64 ? 128 : 64;
-  BoundaryTraceKernel<K, M, NT><<<a.nB, NT, 0, st>>>(a);
+  using SM = BoundaryTraceSmem<K, M>;
+  BoundaryTraceKernel<K, M, NT><<<a.nB, NT, SM::DYN ? sizeof(double) * SM::N : 0, st>>>(a);
   BoundaryFluxKernel<K, M, NT><<<a.nB, NT, 0, st>>>(a);
   return cudaGetLastError();
 }
@@ -409,11 +421,10 @@ static cudaError_t ConfigureTimeStepKM() {
   return e;
 }
 
-// Every supported (K, M) pair; the open-boundary kernels (static shared memory
-// sized by the pair) exist up to degree 6.
+// Every supported (K, M) pair (the open-boundary kernels exist for all of them).
 #define VCPG_PAIRS(X) \
   X(2, 2) X(2, 3) X(3, 4) X(4, 5) X(5, 7) X(6, 8) X(7, 9) X(8, 12) X(9, 13) X(10, 14)
-#define VCPG_PAIRS_OPEN(X) X(2, 2) X(2, 3) X(3, 4) X(4, 5) X(5, 7) X(6, 8) X(7, 9)
+#define VCPG_PAIRS_OPEN(X) VCPG_PAIRS(X)
 
 bool Supported(int K, int M) {
 #define VCPG_IS(K_, M_) if (K == K_ && M == M_) return true;
