@@ -91,6 +91,10 @@ GOLDEN_SPECS = {
     "tgv_p4_3x3x3_wale": cases.CaseSpec(name="tgv_p4_3x3x3_wale", kind="tgv", n_elem=(3, 3, 3),
                                         p=4, hi=(TWO_PI,) * 3, mach=0.1, reynolds=1.0e5,
                                         grid_map="random", grid_amp=0.005, seed=11, sgs="wale"),
+    # WALE at degree 9 (the time step's model arrays in global scratch).
+    "tgv_p9_2x2x2_wale": cases.CaseSpec(name="tgv_p9_2x2x2_wale", kind="tgv", n_elem=(2, 2, 2),
+                                        p=9, hi=(TWO_PI,) * 3, mach=0.1, reynolds=1.0e5,
+                                        grid_map="sine", grid_amp=0.05, sgs="wale"),
     # Vreman model, isentropic vortex, degree 3, Roe flux, anisotropic block.
     "vortex_p3_4x3x3_vreman": cases.CaseSpec(name="vortex_p3_4x3x3_vreman", kind="vortex",
                                              n_elem=(4, 3, 3), p=3, riemann="Roe",

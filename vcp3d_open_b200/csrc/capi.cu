@@ -131,6 +131,8 @@ TimeStepArgs MakeTimeStepArgs(vcpg_handle *h) {
   t.sol = h->d_sol;
   t.elem_scalars = h->d_sc;
   t.n_elem = (int)h->nOwned;
+  t.scratch = h->d_scratch;
+  t.scratch_ctas = h->scratch_ctas;
   t.n_poly = h->prm.n_poly;
   t.cfl = h->prm.cfl;
   t.mu = h->prm.mu;
@@ -292,11 +294,6 @@ int vcpg_create(const vcpg_params *params, const vcpg_operators *ops, const vcpg
       (params->sgs_model != VCPG_SGS_NONE && (!ops->dleg_dofs || !geom->vol_metric_dofs))) {
     int rc = Fail(h, VCPG_E_INVALID, "sgs_model must be VCPG_SGS_NONE, _WALE or _VREMAN; a model "
                                      "needs ops->dleg_dofs and geom->vol_metric_dofs");
-    *out = h;
-    return rc;
-  }
-  if (params->sgs_model != VCPG_SGS_NONE && h->K > 9) {
-    int rc = Fail(h, VCPG_E_UNSUPPORTED_KM, "the SGS time step runs up to degree 8");
     *out = h;
     return rc;
   }

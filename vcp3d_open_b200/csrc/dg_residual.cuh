@@ -95,6 +95,8 @@ struct TimeStepArgs {
   CaseView cases;  // several cases: per-case parameters and time steps
   int sgs;                          // enum vcpg_sgs
   const double *vol_metric_dofs;    // [nE][10][K^3] metric at the nodal DOFs (with sgs)
+  void *scratch;                    // degree 9 with a model: 32 K^3 doubles per CTA
+  int scratch_ctas;
 };
 
 template <int NT, typename T>

@@ -101,15 +101,12 @@ __global__ void __launch_bounds__(NT) TimeStepKernel(const TimeStepArgs a) {
 // Dynamic shared memory: state, nodal values, two stage buffers (5 K^3 each)
 // and the three parametric gradients of V1..V4 (12 K^3).
 template <int K, int M, int NT>
-__global__ void __launch_bounds__(NT) TimeStepSgsKernel(const TimeStepArgs a) {
+__device__ __forceinline__ void TimeStepSgsElement(const TimeStepArgs &a, const int e,
+                                                   double *sm_ts, double *s_red) {
   constexpr int SLOT = Slot<K, M>::value;
   constexpr int KD = K * K * K;
-  extern __shared__ __align__(16) double sm_ts[];
   double *s_sol = sm_ts, *s_val = s_sol + 5 * KD, *tA = s_val + 5 * KD, *tB = tA + 5 * KD;
   double *gr = tB + 5 * KD;  // [3][4][KD]: d/dr, d/ds, d/dt of V1..V4
-  __shared__ double s_red[64];
-  const int e = blockIdx.x;
-  if (e >= a.n_elem) return;
   int cs = 0;
   double cfl = a.cfl, mu = a.mu, pRef = a.p_ref, uRef = a.u_ref, rhoRef = a.rho_ref;
   if (a.cases.elem_case) {
@@ -214,6 +211,30 @@ __global__ void __launch_bounds__(NT) TimeStepSgsKernel(const TimeStepArgs a) {
     const double dtInv = f1[a.n_poly] * radInvMax + f2[a.n_poly] * radVisMax;
     const double dtElem = cfl * uRef / dtInv;
     atomicMin(a.dt_bits + cs, (unsigned long long)__double_as_longlong(dtElem));
+  }
+}
+
+// The 32 K^3 doubles of an element in shared memory, or above one CTA's shared
+// memory (degree 9) in the handle's global scratch, one area per CTA of a grid
+// that loops over the elements.
+template <int K> struct TimeStepSgsSmem {
+  static constexpr size_t BYTES = sizeof(double) * 32 * K * K * K;
+  static constexpr bool BIG = BYTES > 227 * 1024;
+};
+
+template <int K, int M, int NT>
+__global__ void __launch_bounds__(NT) TimeStepSgsKernel(const TimeStepArgs a) {
+  extern __shared__ __align__(16) double sm_ts[];
+  __shared__ double s_red[64];
+  if constexpr (TimeStepSgsSmem<K>::BIG) {
+    double *base = reinterpret_cast<double *>(a.scratch) + (size_t)blockIdx.x * 32 * K * K * K;
+    for (int e = blockIdx.x; e < a.n_elem; e += gridDim.x) {
+      TimeStepSgsElement<K, M, NT>(a, e, base, s_red);
+      __syncthreads();
+    }
+  } else {
+    if ((int)blockIdx.x >= a.n_elem) return;
+    TimeStepSgsElement<K, M, NT>(a, blockIdx.x, sm_ts, s_red);
   }
 }
 
@@ -393,12 +414,15 @@ static cudaError_t LaunchBoundaryKM(const BoundaryArgs &a, cudaStream_t st) {
 
 template <int K, int M>
 static cudaError_t LaunchTimeStepKM(const TimeStepArgs &a, cudaStream_t st) {
-  constexpr size_t sgsSmem = sizeof(double) * 32 * K * K * K;
   if (a.sgs) {
-    if constexpr (sgsSmem <= 227 * 1024)
-      TimeStepSgsKernel<K, M, 64><<<a.n_elem, 64, sgsSmem, st>>>(a);
-    else
-      return cudaErrorInvalidValue;   // no SGS time step at degree 9
+    using SG = TimeStepSgsSmem<K>;
+    if constexpr (SG::BIG) {
+      if (!a.scratch || a.scratch_ctas < 1) return cudaErrorInvalidValue;
+      TimeStepSgsKernel<K, M, 64>
+          <<<a.n_elem < a.scratch_ctas ? a.n_elem : a.scratch_ctas, 64, 0, st>>>(a);
+    } else {
+      TimeStepSgsKernel<K, M, 64><<<a.n_elem, 64, SG::BYTES, st>>>(a);
+    }
   } else {
     using SM = TimeStepSmem<K>;
     TimeStepKernel<K, M, 64><<<a.n_elem, 64, SM::DYN ? sizeof(double) * SM::N : 0, st>>>(a);
@@ -463,6 +487,7 @@ template <int K, int M> static size_t ScratchBytesKM(int ctas) {
   take(Plan<K, M, float, true>::BIG, sizeof(float) * Plan<K, M, float, true>::SCRATCH);
   take(FluxPlan<K, M, double>::BIG, sizeof(double) * FluxPlan<K, M, double>::SCRATCH);
   take(FluxPlan<K, M, float>::BIG, sizeof(float) * FluxPlan<K, M, float>::SCRATCH);
+  take(TimeStepSgsSmem<K>::BIG, TimeStepSgsSmem<K>::BYTES);
   return b;
 }
 
