@@ -177,7 +177,8 @@ class Ensemble:
         cid = C.c_int64()
         ob = C.byref(pc.ob) if pc.ob is not None else None
         rc = self.lib.vcpg_ensemble_submit(self.h, C.byref(pc.params), C.byref(ops), C.byref(geom),
-                                           capi.ptr(pc.modal), n_steps, ob, pc.spec.p_grid, 1,
+                                           capi.ptr(pc.modal), n_steps, ob, pc.spec.p_grid,
+                                           cases.dof_location_code(pc.spec),
                                            capi.ptr(pc.grid_nodes), C.byref(cid))
         if rc == 7:   # VCPG_E_ADMISSION
             return None
