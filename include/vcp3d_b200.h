@@ -272,11 +272,13 @@ int vcpg_stats(vcpg_handle *h, int64_t *cg_iterations, int64_t *element_solves);
  * VCPG_NOALLOC_MAX_ELEMS elements (2 MiB), held by every GPU that loads the
  * library until the process exits. Larger n_elem returns VCPG_E_ADMISSION
  * before any device work. The first call on each device looks up the array's
- * device address with that device current; make that first call before any
- * stream capture. All calls share the array and overwrite it: calls that
- * overlap on the GPU (different streams or host threads) race, so order them.
- * The call synchronises `stream` (a cudaStream_t, NULL = legacy default stream)
- * before returning; VCPG_E_NEG_A2 reports a negative speed of sound squared. */
+ * device address with that device current. All calls share the array and
+ * overwrite it: calls that overlap on the GPU (different streams or host
+ * threads) race, so order them. Each call uploads the operators and launches
+ * its kernels on `stream` (a cudaStream_t, NULL = legacy default stream), then
+ * reads its status back and synchronises that stream before returning, so it
+ * cannot be captured into a CUDA graph. VCPG_E_NEG_A2 reports a negative (or
+ * not-a-number) speed of sound squared in the state. */
 #define VCPG_NOALLOC_MAX_ELEMS 262144
 int vcpg_time_step_noalloc(const vcpg_params *params, const vcpg_operators *ops,
                            const double *d_sol, const double *d_elem_scalars, double *d_dt,

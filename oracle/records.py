@@ -15,6 +15,15 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_EXE = os.path.join(HERE, "_ref", "vcp3d_ref")
+# The reference's VCP3D_CurviLinear source folder (only this container has it):
+# the one variable that build recipes and CPU tests read.
+REF_SRC_ENV = "VCP3D_REF_SRC"
+REF_SRC_DEFAULT = "/root/reference/VCP3D_CurviLinear"
+
+
+def reference_source_dir() -> str:
+    """The reference source folder: $VCP3D_REF_SRC, else the default location."""
+    return os.environ.get(REF_SRC_ENV) or REF_SRC_DEFAULT
 
 
 def read_records(path: str) -> Dict[str, np.ndarray]:

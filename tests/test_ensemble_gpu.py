@@ -160,3 +160,25 @@ def test_slot_reuse_keeps_results(gpu_available):
     assert len(results) == len(prepared)
     for k in range(len(prepared)):
         np.testing.assert_array_equal(results[k][0], alone[k][0], err_msg=specs[k].name)
+
+
+def test_bucket_rejects_other_solution_dof_positions(gpu_available):
+    """The bucket's operator table (basis at the nodal DOFs of the time step) is
+    fixed by its first case: a later case of the same degree with equidistant
+    solution DOFs is refused, one with LGL DOFs is admitted."""
+    import dataclasses
+    lgl = serving.vortex_spec(3, 3, 0.4, 4.0, "lgl")
+    equi = dataclasses.replace(serving.vortex_spec(3, 3, 0.3, 3.0, "equi"),
+                               dof_location="equidistant", grid_lgl=False)
+    ens = serving.Ensemble(_caps([lgl, lgl, equi], slack=3), precision=capi.FP64, max_cases=4)
+    try:
+        ida = ens.submit(serving.prepare(lgl, capi.FP64), 2)
+        with pytest.raises(capi.VcpgError) as err:
+            ens.submit(serving.prepare(equi, capi.FP64), 2)
+        assert err.value.code == capi.VCPG_E_INVALID
+        assert "solution-DOF positions" in str(err.value)
+        idb = ens.submit(serving.prepare(dataclasses.replace(lgl, name="lgl2"), capi.FP64), 2)
+        res = _run_to_completion(ens, [ida, idb])
+        assert np.all(np.isfinite(res[idb][0]))
+    finally:
+        ens.close()

@@ -11,9 +11,10 @@ import numpy as np
 import pytest
 
 from conftest import load_golden, rel_l2, sync_golden_files, write_sync_case
+from oracle import records
 from vcp3d_open_b200 import cases, param_file, run, solver
 
-REF_TESTS = "/root/reference/VCP3D_CurviLinear/test"
+REF_TESTS = os.path.join(records.reference_source_dir(), "test")
 
 
 @pytest.mark.parametrize("path", sync_golden_files(), ids=os.path.basename)

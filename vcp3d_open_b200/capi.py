@@ -13,6 +13,7 @@ import numpy as np
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libvcp3d_b200.so")
 
 VCPG_OK = 0
+VCPG_E_NEG_A2, VCPG_E_ADMISSION, VCPG_E_INVALID = 3, 7, 8
 ERRORS = {1: "VCPG_E_CUDA", 2: "VCPG_E_CG_NOCONV", 3: "VCPG_E_NEG_A2", 4: "VCPG_E_NONFINITE",
           5: "VCPG_E_OOM", 6: "VCPG_E_UNSUPPORTED_KM", 7: "VCPG_E_ADMISSION", 8: "VCPG_E_INVALID"}
 ROE, ISMAIL_ROE = 0, 1

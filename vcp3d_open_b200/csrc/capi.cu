@@ -155,7 +155,7 @@ int CheckStatus(vcpg_handle *h) {
     VCPG_CUDA(h, cudaMemsetAsync(h->d_status, 0, sizeof(st), h->stream));
   if (st[0]) return Fail(h, VCPG_E_CG_NOCONV, "mass-matrix CG reached 100 iterations in " +
                                                   std::to_string(st[0]) + " element solve(s)");
-  if (st[2]) return Fail(h, VCPG_E_NEG_A2, "negative square speed of sound in the time step");
+  if (st[2]) return Fail(h, VCPG_E_NEG_A2, "negative or not-a-number square speed of sound in the time step");
   if (st[1]) return Fail(h, VCPG_E_INVALID, "physical boundary face without a boundary condition");
   return VCPG_OK;
 }

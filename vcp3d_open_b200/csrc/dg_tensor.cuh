@@ -67,12 +67,15 @@ VCPG_SLOTS(VCPG_SLOT_DECL)
 template <int SLOT> __device__ __forceinline__ decltype(auto) Ops() { return SlotOps<SLOT>::get(); }
 
 // Fills and uploads the table of one pair from the C-ABI operator arrays of
-// this unit's copy (legdof / dlegdof may be absent: zeros).
+// this unit's copy (legdof / dlegdof may be absent: zeros). With a stream the
+// copy is ordered on that stream (the host table is staged before the call
+// returns); without one it is a synchronous copy.
 template <int K, int M, typename Sym>
 static inline cudaError_t UploadOperatorsKM(const Sym &sym, const double *leg, const double *dleg,
                                             const double *face, const double *dface,
                                             const double *w, const double *legdof,
-                                            const double *dlegdof) {
+                                            const double *dlegdof, cudaStream_t st,
+                                            bool async) {
   OpTableKM<K, M> t{};
   for (int i = 0; i < K * M; ++i) {
     t.leg[i] = leg[i];
@@ -94,16 +97,19 @@ static inline cudaError_t UploadOperatorsKM(const Sym &sym, const double *leg, c
     t.legdof[i] = legdof ? legdof[i] : 0.0;
     t.dlegdof[i] = dlegdof ? dlegdof[i] : 0.0;
   }
+  if (async) return cudaMemcpyToSymbolAsync(sym, &t, sizeof(t), 0, cudaMemcpyHostToDevice, st);
   return cudaMemcpyToSymbol(sym, &t, sizeof(t), 0, cudaMemcpyHostToDevice);
 }
 
 static inline cudaError_t UploadOperators(int K, int M, const double *leg, const double *dleg,
                                           const double *face, const double *dface,
                                           const double *w, const double *legdof,
-                                          const double *dlegdof) {
+                                          const double *dlegdof, cudaStream_t st = nullptr,
+                                          bool async = false) {
 #define VCPG_SLOT_UPLOAD(S_, K_, M_)                                                  \
   if (K == K_ && M == M_)                                                             \
-    return UploadOperatorsKM<K_, M_>(c_ops##S_, leg, dleg, face, dface, w, legdof, dlegdof);
+    return UploadOperatorsKM<K_, M_>(c_ops##S_, leg, dleg, face, dface, w, legdof, dlegdof, \
+                                     st, async);
   VCPG_SLOTS(VCPG_SLOT_UPLOAD)
 #undef VCPG_SLOT_UPLOAD
   return cudaErrorInvalidValue;

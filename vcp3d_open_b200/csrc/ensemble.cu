@@ -131,6 +131,10 @@ struct Bucket {
   std::vector<int64_t> slotCase;  // case id per slot, -1 = free
   int resident = 0;
   bool opsReady = false, pcReady = false;
+  // Solution-DOF positions of the operator table (1 LGL, 0 equidistant; the grid
+  // node positions do not enter it): the bucket's first case fixes them, since
+  // the time step evaluates the basis at the nodal DOFs.
+  int dofLoc = -1;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int64_t graphE = -1, graphB = -1;
@@ -403,7 +407,7 @@ int CheckBucketStatus(vcpg_ensemble *e, Bucket &b) {
     ENS_CUDA(e, cudaMemsetAsync(b.status, 0, sizeof(st), b.stream));
     if (st[0]) return Fail(e, VCPG_E_CG_NOCONV, "mass-matrix CG reached 100 iterations (degree " +
                                                    std::to_string(b.deg) + ")");
-    if (st[2]) return Fail(e, VCPG_E_NEG_A2, "negative square speed of sound in the time step");
+    if (st[2]) return Fail(e, VCPG_E_NEG_A2, "negative or not-a-number square speed of sound in the time step");
     return Fail(e, VCPG_E_INVALID, "physical boundary face without a boundary condition");
   }
   return VCPG_OK;
@@ -479,6 +483,11 @@ int vcpg_ensemble_submit(vcpg_ensemble *ens, const vcpg_params *params,
       params->metric_index_compat != e->cfg.metric_index_compat ||
       params->theta_sym != e->cfg.theta_sym || params->rel_penalty != e->cfg.rel_penalty)
     return Fail(e, VCPG_E_INVALID, "case settings differ from the ensemble's shared settings");
+  const int solLgl =
+      (dof_location == VCPG_DOFS_LGL || dof_location == VCPG_DOFS_LGL_GRID_EQUI) ? 1 : 0;
+  if (b.opsReady && solLgl != b.dofLoc)
+    return Fail(e, VCPG_E_INVALID,
+                "solution-DOF positions differ from the bucket's (its first case fixed them)");
   const int64_t nE = (int64_t)params->n_elem[0] * params->n_elem[1] * params->n_elem[2];
   if (nE <= 0) return Fail(e, VCPG_E_INVALID, "invalid element count");
   const int KD = b.KD, MD = b.MD, M2 = b.M2;
@@ -549,6 +558,7 @@ int vcpg_ensemble_submit(vcpg_ensemble *ens, const vcpg_params *params,
       ce = cudaMemcpy(b.center, ops->basis_center, 8 * (size_t)b.KD, cudaMemcpyHostToDevice);
     if (ce != cudaSuccess) { rollback(); return Fail(e, VCPG_E_CUDA, cudaGetErrorString(ce)); }
     b.opsReady = true;
+    b.dofLoc = solLgl;
   }
   if (nB > 0 && !b.pcReady) {
     cudaError_t ce = cudaMemcpy(b.pc, obh.pc.data(), 8 * obh.pc.size(), cudaMemcpyHostToDevice);

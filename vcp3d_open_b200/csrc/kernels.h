@@ -14,6 +14,23 @@ struct TimeStepArgs;
 struct BoundaryArgs;
 struct CaseView;
 
+// Every supported (K, M) pair: the reference's tensor-product dispatch
+// (src/TensorProductVolumeResidualK2.cpp ... K10.cpp).
+#define VCPG_PAIRS(X) \
+  X(2, 2) X(2, 3) X(3, 4) X(4, 5) X(5, 7) X(6, 8) X(7, 9) X(8, 12) X(9, 13) X(10, 14)
+
+// Per-pair entry points, defined by the pair's own object (kernels_pair.cu).
+#define VCPG_PAIR_FN(name, K_, M_) Pair##name##_##K_##_##M_
+#define VCPG_PAIR_DECLARE(K_, M_)                                                           \
+  cudaError_t VCPG_PAIR_FN(LaunchResidual, K_, M_)(const ResidualArgs &a, cudaStream_t st); \
+  cudaError_t VCPG_PAIR_FN(LaunchBoundary, K_, M_)(const BoundaryArgs &a, cudaStream_t st); \
+  cudaError_t VCPG_PAIR_FN(LaunchTimeStep, K_, M_)(const TimeStepArgs &a, cudaStream_t st); \
+  cudaError_t VCPG_PAIR_FN(ConfigureResidual, K_, M_)();                                    \
+  cudaError_t VCPG_PAIR_FN(ConfigureTimeStep, K_, M_)();                                    \
+  cudaError_t VCPG_PAIR_FN(Upload, K_, M_)(const vcpg_operators *ops);
+VCPG_PAIRS(VCPG_PAIR_DECLARE)
+#undef VCPG_PAIR_DECLARE
+
 bool Supported(int K, int M);
 int SlotOf(int K, int M);
 size_t ResidualSmemBytes(int K, int M);

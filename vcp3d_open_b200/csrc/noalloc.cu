@@ -14,6 +14,8 @@
 // until the process exits. All calls share it and each call overwrites it, so
 // calls that overlap on the GPU (other streams, other host threads) race; the
 // caller must order them. The status slot is cleared at the start of every call.
+// Every call also reads the status back and synchronises the caller's stream,
+// so a call cannot be captured into a CUDA graph.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -22,6 +24,7 @@
 
 #include "../../include/vcp3d_b200.h"
 #include "dg_residual.cuh"
+#include "dg_timestep.cuh"
 #include "kernels.h"
 
 namespace {
@@ -51,60 +54,25 @@ int ScratchForCurrentDevice(double **out) {
   return VCPG_OK;
 }
 
-// Per-element step into scratch[e] (the arithmetic of ElementClass::ComputeTimeStep,
-// src/ElementClass.cpp:1522-1644, as in TimeStepKernel).
+// Per-element step into scratch[e]: the arithmetic of the handle's time step
+// (ElementTimeStep, dg_timestep.cuh).
 template <int K, int M, int NT>
 __global__ void __launch_bounds__(NT) NoAllocElementDtKernel(const double *sol,
                                                              const double *scalars, int n_elem,
                                                              int n_poly, double cfl, double mu,
                                                              double p_ref, double u_ref,
                                                              double rho_ref, double *scratch) {
-  constexpr int SLOT = Slot<K, M>::value;
   constexpr int KD = K * K * K;
   __shared__ double s_sol[5 * KD], s_t1[5 * KD], s_t2[5 * KD], s_red[64];
   const int e = blockIdx.x;
   if (e >= n_elem) return;
-  const double *src = sol + (size_t)e * 5 * KD;
-  for (int i = threadIdx.x; i < 5 * KD; i += NT) s_sol[i] = src[i];
-  __syncthreads();
-  Contract<NT, SLOT, K, M, kLegDof, 2, 5, K, K, K, K, K, false>(s_sol, s_t1);
-  __syncthreads();
-  Contract<NT, SLOT, K, M, kLegDof, 1, 5, K, K, K, K, K, false>(s_t1, s_t2);
-  __syncthreads();
-  Contract<NT, SLOT, K, M, kLegDof, 0, 5, K, K, K, K, K, false>(s_t2, s_t1);
-  __syncthreads();
-  const double *sc = scalars + (size_t)e * 15;
-  const double muDim = mu * p_ref / u_ref;
-  const double dliInv = 1.0 / sc[0], dljInv = 1.0 / sc[1], dlkInv = 1.0 / sc[2];
-  const double dLen2Inv = dliInv * dliInv + dljInv * dljInv + dlkInv * dlkInv;
-  const double radVisOverNuLam = fmax(fmax(1.0, 2.0 + kLamOverMu), kFactHFLam) * dLen2Inv;
-  double radInvMax = 0.0, radVisMax = 0.0, a2Min = 1.e+10;
-  for (int l = threadIdx.x; l < KD; l += NT) {
-    double rho, u, v, w, p, eKin;
-    EntropyToPrim(s_t1[l], s_t1[KD + l], s_t1[2 * KD + l], s_t1[3 * KD + l], s_t1[4 * KD + l],
-                  rho, u, v, w, p, eKin);
-    rho *= rho_ref; u *= u_ref; v *= u_ref; w *= u_ref; p *= p_ref;
-    const double rhoInv = 1.0 / rho;
-    const double a2 = kGam * p * rhoInv;
-    const double velI = u * sc[6] + v * sc[7] + w * sc[8];
-    const double velJ = u * sc[9] + v * sc[10] + w * sc[11];
-    const double velK = u * sc[12] + v * sc[13] + w * sc[14];
-    const double aa = sqrt(fabs(a2));
-    const double radInv = (fabs(velI) + aa) * dliInv + (fabs(velJ) + aa) * dljInv +
-                          (fabs(velK) + aa) * dlkInv;
-    const double radVis = rhoInv * (muDim * radVisOverNuLam + 0.0);
-    radInvMax = fmax(radInvMax, radInv);
-    radVisMax = fmax(radVisMax, radVis);
-    a2Min = fmin(a2Min, a2);
-  }
-  radInvMax = BlockMax<NT>(radInvMax, s_red);
-  radVisMax = BlockMax<NT>(radVisMax, s_red);
-  a2Min = -BlockMax<NT>(-a2Min, s_red);
+  bool bad = false;
+  const double dt = ElementTimeStep<K, M, NT>(sol + (size_t)e * 5 * KD, scalars + (size_t)e * 15,
+                                              n_poly, cfl, mu, p_ref, u_ref, rho_ref, s_sol, s_t1,
+                                              s_t2, s_red, &bad);
   if (threadIdx.x == 0) {
-    if (a2Min < 0.0) scratch[kStatusSlot] = 1.0;
-    const double f1[] = {2.0, 6.0, 12.0, 20.0, 28.0, 38.0, 50.0, 64.0, 80.0, 98.0};
-    const double f2[] = {6.0, 36.0, 150.0, 420.0, 980.0, 1975.0, 3575.0, 7000.0, 14000.0, 28000.0};
-    scratch[e] = cfl * u_ref / (f1[n_poly] * radInvMax + f2[n_poly] * radVisMax);
+    if (bad) scratch[kStatusSlot] = 1.0;
+    scratch[e] = dt;
   }
 }
 
@@ -145,9 +113,10 @@ extern "C" int vcpg_time_step_noalloc(const vcpg_params *params, const vcpg_oper
   int rc = ScratchForCurrentDevice(&scratch);
   if (rc != VCPG_OK) return rc;
   cudaStream_t st = (cudaStream_t)stream;
-  // Operators of this (K, M) pair into this file's constant memory.
+  // Operators of this (K, M) pair into this file's constant memory, ordered on
+  // the caller's stream before the kernels that read them.
   if (UploadOperators(K, M, ops->leg_int, ops->dleg_int, ops->leg_face, ops->dleg_face,
-                      ops->w_int, ops->leg_dofs, nullptr) != cudaSuccess)
+                      ops->w_int, ops->leg_dofs, nullptr, st, true) != cudaSuccess)
     return VCPG_E_CUDA;
   if (cudaMemsetAsync(scratch + kStatusSlot, 0, sizeof(double), st) != cudaSuccess)
     return VCPG_E_CUDA;
