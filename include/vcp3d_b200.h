@@ -258,6 +258,14 @@ int64_t vcpg_launch_count(const vcpg_handle *h);
  * element solves (the reference's per-element CG, src/CG_MassMatrix.cpp:395-492). */
 int vcpg_stats(vcpg_handle *h, int64_t *cg_iterations, int64_t *element_solves);
 
+/* Measurement hook (no counterpart in the reference): evaluates the residual
+ * of the current state `reps` times with CUDA events on the handle's stream
+ * around each kernel and returns the average milliseconds per launch:
+ * ms[0] the two characteristic-boundary kernels (0 without such faces),
+ * ms[1] FaceFluxKernel, ms[2] ResidualKernel. The device residual afterwards
+ * is that of the current state, as after vcpg_residual. */
+int vcpg_time_residual_kernels(vcpg_handle *h, int32_t reps, double *ms);
+
 /* Allocation-free CFL time step. This entry point has no counterpart in the
  * reference solver. It is for callers that cannot call cudaMalloc: programs
  * whose device memory all belongs to their own pool allocator (a framework's

@@ -11,6 +11,7 @@
 //   vcp3d_ref <param.cfg> residual <out.bin> [--state <in.bin>]
 //   vcp3d_ref <param.cfg> run      <out.bin> --scheme ssprk3|lsrk4 --steps N
 //                                  [--dt DT] [--state <in.bin>] [--time]
+//                                  [--every E]   (also <out.bin>.<n> every E steps)
 //   vcp3d_ref <param.cfg> sync     <out.bin> --steps N
 //
 // The residual command replicates the loop structure of SolverClass::Residual
@@ -380,7 +381,7 @@ int main(int argc, char **argv) {
   }
   std::string cfg = argv[1], cmd = argv[2], out = argv[3];
   std::string scheme = "ssprk3", statePath;
-  int steps = 1;
+  int steps = 1, every = 0;
   double fixedDt = -1.0;
   bool timeIt = false;
   for (int a = 4; a < argc; ++a) {
@@ -390,6 +391,7 @@ int main(int argc, char **argv) {
     else if (o == "--dt" && a + 1 < argc) fixedDt = std::atof(argv[++a]);
     else if (o == "--state" && a + 1 < argc) statePath = argv[++a];
     else if (o == "--time") timeIt = true;
+    else if (o == "--every" && a + 1 < argc) every = std::atoi(argv[++a]);
     else { std::fprintf(stderr, "unknown option %s\n", o.c_str()); return 2; }
   }
   // Resolve output/state paths before changing into the case directory.
@@ -476,6 +478,12 @@ int main(int argc, char **argv) {
       } else {
         std::fprintf(stderr, "unknown scheme %s\n", scheme.c_str());
         return 2;
+      }
+      // Sample files for long runs: the state and the steps so far.
+      if (every > 0 && (step + 1) % every == 0) {
+        Writer ws((out + "." + std::to_string(step + 1)).c_str());
+        ws.rec("sol", {nE, 5, nDOFsPad}, Gather(solver, &ElementClass::mSol, 5, nDOFsPad).data());
+        ws.rec("dtHist", {(int64_t)dtHist.size()}, dtHist.data());
       }
     }
     auto t1 = std::chrono::steady_clock::now();

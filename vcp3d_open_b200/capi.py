@@ -33,6 +33,7 @@ EXPORTED = [
     "vcpg_nodal_conservative_to_modal", "vcpg_set_state", "vcpg_get_state",
     "vcpg_get_residual", "vcpg_residual", "vcpg_get_raw_residual", "vcpg_time_step",
     "vcpg_step", "vcpg_synchronization_step", "vcpg_sync", "vcpg_stream", "vcpg_launch_count", "vcpg_stats",
+    "vcpg_time_residual_kernels",
     "vcpg_time_step_noalloc", "vcpg_set_open_boundary", "vcpg_ensemble_create",
     "vcpg_ensemble_destroy", "vcpg_ensemble_last_error", "vcpg_ensemble_footprint",
     "vcpg_ensemble_submit", "vcpg_ensemble_step", "vcpg_ensemble_poll", "vcpg_ensemble_retire",
@@ -134,6 +135,7 @@ def load() -> C.CDLL:
     lib.vcpg_launch_count.argtypes = [hp]
     lib.vcpg_launch_count.restype = C.c_int64
     lib.vcpg_stats.argtypes = [hp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    lib.vcpg_time_residual_kernels.argtypes = [hp, C.c_int32, dp]
     lib.vcpg_time_step_noalloc.argtypes = [C.POINTER(Params), C.POINTER(Operators), C.c_void_p,
                                            C.c_void_p, C.c_void_p, C.c_void_p]
     lib.vcpg_set_open_boundary.argtypes = [hp, C.POINTER(OpenBoundary), C.POINTER(Geometry),

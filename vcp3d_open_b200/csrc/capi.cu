@@ -452,6 +452,38 @@ int vcpg_residual(vcpg_handle *h, double *monitoring, int32_t keep_raw) {
   return rc;
 }
 
+int vcpg_time_residual_kernels(vcpg_handle *h, int32_t reps, double *ms) {
+  if (!h || reps < 1 || !ms) return VCPG_E_INVALID;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  for (auto &e : ev) VCPG_CUDA(h, cudaEventCreate(&e));
+  const ResidualArgs a = MakeResidualArgs(h, nullptr, nullptr);
+  const bool open = h->open && h->nB > 0;
+  double acc[3] = {0.0, 0.0, 0.0};
+  cudaError_t err = cudaSuccess;
+  for (int r = 0; r < reps && err == cudaSuccess; ++r) {
+    err = cudaEventRecord(ev[0], h->stream);
+    if (err == cudaSuccess && open) err = LaunchBoundary(h->K, h->M, MakeBoundaryArgs(h), h->stream);
+    if (err == cudaSuccess) err = cudaEventRecord(ev[1], h->stream);
+    if (err == cudaSuccess) err = LaunchResidual(h->K, h->M, a, h->stream, 1);
+    if (err == cudaSuccess) err = cudaEventRecord(ev[2], h->stream);
+    if (err == cudaSuccess) err = LaunchResidual(h->K, h->M, a, h->stream, 2);
+    if (err == cudaSuccess) err = cudaEventRecord(ev[3], h->stream);
+    if (err == cudaSuccess) err = cudaEventSynchronize(ev[3]);
+    for (int k = 0; k < 3 && err == cudaSuccess; ++k) {
+      float t = 0.f;
+      err = cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+      acc[k] += t;
+    }
+  }
+  for (auto &e : ev) cudaEventDestroy(e);
+  VCPG_CUDA(h, err);
+  h->launches += (int64_t)reps * ResidualLaunches(h);
+  for (int k = 0; k < 3; ++k) ms[k] = acc[k] / reps;
+  const int rc = CheckStatus(h);
+  h->res_valid = rc == VCPG_OK;
+  return rc;
+}
+
 int vcpg_time_step(vcpg_handle *h, double *dt) {
   if (!h || !dt) return VCPG_E_INVALID;
   TimeStepArgs t = MakeTimeStepArgs(h);

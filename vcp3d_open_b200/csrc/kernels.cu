@@ -144,9 +144,10 @@ size_t FaceFluxBytesPerElement(int K, int M) {
   return sizeof(double) * 3 * 20 * (size_t)M * M;
 }
 
-cudaError_t LaunchResidual(int K, int M, const ResidualArgs &a, cudaStream_t st) {
+cudaError_t LaunchResidual(int K, int M, const ResidualArgs &a, cudaStream_t st, int phase) {
   if (a.n_elem <= 0) return cudaSuccess;
-#define VCPG_LAUNCH(K_, M_) if (K == K_ && M == M_) return VCPG_PAIR_FN(LaunchResidual, K_, M_)(a, st);
+#define VCPG_LAUNCH(K_, M_) \
+  if (K == K_ && M == M_) return VCPG_PAIR_FN(LaunchResidual, K_, M_)(a, st, phase);
   VCPG_PAIRS(VCPG_LAUNCH)
 #undef VCPG_LAUNCH
   return cudaErrorInvalidValue;

@@ -22,7 +22,8 @@ struct CaseView;
 // Per-pair entry points, defined by the pair's own object (kernels_pair.cu).
 #define VCPG_PAIR_FN(name, K_, M_) Pair##name##_##K_##_##M_
 #define VCPG_PAIR_DECLARE(K_, M_)                                                           \
-  cudaError_t VCPG_PAIR_FN(LaunchResidual, K_, M_)(const ResidualArgs &a, cudaStream_t st); \
+  cudaError_t VCPG_PAIR_FN(LaunchResidual, K_, M_)(const ResidualArgs &a, cudaStream_t st,  \
+                                                    int phase);                               \
   cudaError_t VCPG_PAIR_FN(LaunchBoundary, K_, M_)(const BoundaryArgs &a, cudaStream_t st); \
   cudaError_t VCPG_PAIR_FN(LaunchTimeStep, K_, M_)(const TimeStepArgs &a, cudaStream_t st); \
   cudaError_t VCPG_PAIR_FN(ConfigureResidual, K_, M_)();                                    \
@@ -50,8 +51,9 @@ cudaError_t LaunchEnsembleFinalize(int n_cases, int *state, const int *target, i
                                    unsigned long long *dt_bits, double *dt, double *sim_time,
                                    cudaStream_t st);
 
-// One residual = FaceFluxKernel + ResidualKernel (2 launches).
-cudaError_t LaunchResidual(int K, int M, const ResidualArgs &a, cudaStream_t st);
+// One residual = FaceFluxKernel + ResidualKernel (2 launches). phase 1 launches
+// only FaceFluxKernel, phase 2 only ResidualKernel (per-kernel timing).
+cudaError_t LaunchResidual(int K, int M, const ResidualArgs &a, cudaStream_t st, int phase = 0);
 // Sets the shared-memory limits of all residual-kernel variants of a (K, M) pair;
 // call before capturing launches into a CUDA graph.
 cudaError_t ConfigureResidual(int K, int M);

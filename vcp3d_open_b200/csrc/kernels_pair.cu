@@ -69,8 +69,9 @@ static cudaError_t ConfigureKM() {
 }
 
 // One residual: the face fluxes, then the fused volume / distribution / mass-solve kernel.
+// phase 0 launches both, 1 only FaceFluxKernel, 2 only ResidualKernel (timing).
 template <int K, int M, typename T, bool OPEN>
-static cudaError_t LaunchResidualKMT(const ResidualArgs &a, cudaStream_t st) {
+static cudaError_t LaunchResidualKMT(const ResidualArgs &a, cudaStream_t st, int phase) {
   using P = Plan<K, M, T, OPEN>;
   using PF = FluxPlan<K, M, T>;
   cudaError_t err = ConfigureKMT<K, M, T, OPEN>();
@@ -80,10 +81,13 @@ static cudaError_t LaunchResidualKMT(const ResidualArgs &a, cudaStream_t st) {
   if ((P::BIG || PF::BIG) && (!a.scratch || a.scratch_ctas < 1)) return cudaErrorInvalidValue;
   const unsigned gridF = PF::BIG ? (nFace < a.scratch_ctas ? nFace : a.scratch_ctas) : nFace;
   const size_t smemF = PF::BIG ? 0 : PF::BYTES;
-  if (a.sgs)
-    FaceFluxKernel<K, M, PF::NT, T, true><<<gridF, PF::NT, smemF, st>>>(a);
-  else
-    FaceFluxKernel<K, M, PF::NT, T, false><<<gridF, PF::NT, smemF, st>>>(a);
+  if (phase != 2) {
+    if (a.sgs)
+      FaceFluxKernel<K, M, PF::NT, T, true><<<gridF, PF::NT, smemF, st>>>(a);
+    else
+      FaceFluxKernel<K, M, PF::NT, T, false><<<gridF, PF::NT, smemF, st>>>(a);
+  }
+  if (phase == 1) return cudaGetLastError();
   if constexpr (P::BIG)
     ResidualKernel<K, M, P::NT, T, OPEN>
         <<<a.n_elem < a.scratch_ctas ? a.n_elem : a.scratch_ctas, P::NT, 0, st>>>(a);
@@ -95,12 +99,12 @@ static cudaError_t LaunchResidualKMT(const ResidualArgs &a, cudaStream_t st) {
 // FP64 form or the mixed form (FP32 compute, FP64 inputs and outputs), each
 // with or without open boundaries and sponge layers.
 template <int K, int M>
-static cudaError_t LaunchResidualKM(const ResidualArgs &a, cudaStream_t st) {
+static cudaError_t LaunchResidualKM(const ResidualArgs &a, cudaStream_t st, int phase) {
   if (a.open)
-    return a.mixed ? LaunchResidualKMT<K, M, float, true>(a, st)
-                   : LaunchResidualKMT<K, M, double, true>(a, st);
-  return a.mixed ? LaunchResidualKMT<K, M, float, false>(a, st)
-                 : LaunchResidualKMT<K, M, double, false>(a, st);
+    return a.mixed ? LaunchResidualKMT<K, M, float, true>(a, st, phase)
+                   : LaunchResidualKMT<K, M, double, true>(a, st, phase);
+  return a.mixed ? LaunchResidualKMT<K, M, float, false>(a, st, phase)
+                 : LaunchResidualKMT<K, M, double, false>(a, st, phase);
 }
 
 // The two characteristic-boundary kernels (dg_boundary.cuh).
@@ -153,8 +157,9 @@ static cudaError_t PairUploadKM(const vcpg_operators *ops) {
 }
 
 #define VCPG_PAIR_DEFINE(K_, M_)                                                              \
-  cudaError_t VCPG_PAIR_FN(LaunchResidual, K_, M_)(const ResidualArgs &a, cudaStream_t st) {  \
-    return LaunchResidualKM<K_, M_>(a, st);                                                   \
+  cudaError_t VCPG_PAIR_FN(LaunchResidual, K_, M_)(const ResidualArgs &a, cudaStream_t st,  \
+                                                    int phase) {                              \
+    return LaunchResidualKM<K_, M_>(a, st, phase);                                            \
   }                                                                                           \
   cudaError_t VCPG_PAIR_FN(LaunchBoundary, K_, M_)(const BoundaryArgs &a, cudaStream_t st) {  \
     return LaunchBoundaryKM<K_, M_>(a, st);                                                   \

@@ -328,6 +328,14 @@ class Solver:
         self._check(self.lib.vcpg_stats(self.h, C.byref(it), C.byref(n)), "stats")
         return it.value, n.value
 
+    def time_residual_kernels(self, reps: int = 10):
+        """Average ms per launch of the residual's kernels, each between CUDA events
+        on the library stream: (boundary kernels, FaceFluxKernel, ResidualKernel)."""
+        ms = np.zeros(3)
+        self._check(self.lib.vcpg_time_residual_kernels(self.h, reps, capi.ptr(ms)),
+                    "time_residual_kernels")
+        return tuple(float(x) for x in ms)
+
     @property
     def launch_count(self) -> int:
         return int(self.lib.vcpg_launch_count(self.h))
