@@ -2,9 +2,10 @@
 vortex on the curvilinear 8^3 grid of degree 3, 100 time steps of low-storage
 RK4 and of SSP-RK3 at CFL 0.5 from the same files, GPU (FP64) and the
 reference build (oracle/_ref, the host's threads). The states after 100 steps
-agree to 1e-12 relative L2 and every step's Delta t to 1e-12; the conserved
-integrals of both runs drift by less than 1e-10 of their scales (the mass-matrix
-solves stop at 1e-10 relative)."""
+agree to 1e-12 relative L2 and every step's Delta t to 1e-12. The conserved
+integrals drift by ~1e-10 of their scales over 100 steps in both runs (the
+mass-matrix solves stop at 1e-10 relative, so the projected residual conserves
+only to that level); the GPU's drift equals the reference's to 1e-12."""
 from __future__ import annotations
 
 import pytest
@@ -28,5 +29,5 @@ def test_config1_vortex_100_steps_matches_reference_build(gpu_available, scheme)
     for r in rows:
         assert r["rel_l2_state_gpu_vs_reference"] < TOL_STATE, r
         assert r["max_rel_dt_diff"] < TOL_DT, r
-        assert max(abs(x) for x in r["gpu_drift"]) < 1e-10, r
-        assert max(abs(x) for x in r["reference_drift"]) < 1e-10, r
+        assert max(abs(x) for x in r["reference_drift"]) < 1e-9, r
+        assert max(abs(a - b) for a, b in zip(r["gpu_drift"], r["reference_drift"])) < 1e-12, r

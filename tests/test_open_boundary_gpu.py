@@ -88,7 +88,7 @@ def test_open_boundary_launches_and_graph(gpu_available):
         n0 = s.launch_count
         s.step(2, capi.LSRK4)
         # dt + finalize + 5 x (stage update + 4 residual launches) per step.
-        assert s.launch_count - n0 == 2 * (2 + 5 * 5)
+        assert s.launch_count - n0 == 2 * (2 + 5 * 4)
     finally:
         s.close()
 

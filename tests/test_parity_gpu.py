@@ -160,8 +160,9 @@ def test_launch_count_and_graph_reuse(gpu_available):
         n0 = s.launch_count
         s.step(2, capi.SSPRK3)
         s.step(2, capi.SSPRK3)
-        # dt + finalize + 3 x (stage update + face fluxes + residual) per step.
-        assert s.launch_count - n0 == 4 * 11
+        # dt + start of the step (first stage's update) + 3 x (face fluxes +
+        # residual with the next stage's update fused) per step.
+        assert s.launch_count - n0 == 4 * 8
     finally:
         s.close()
 
@@ -178,7 +179,33 @@ def test_step_after_set_state_evaluates_the_residual_first(gpu_available):
         s.set_state(g["sol0"])
         n0 = s.launch_count
         s.step(2, capi.LSRK4)
-        assert s.launch_count - n0 == 2 + 2 * 17
+        assert s.launch_count - n0 == 2 + 2 * 12
         np.testing.assert_array_equal(s.get_state(), want)
+    finally:
+        s.close()
+
+
+@pytest.mark.parametrize("scheme", [capi.LSRK4, capi.SSPRK3])
+def test_fused_stage_updates_equal_the_stage_kernels(gpu_available, scheme):
+    """The step graph applies each stage's update in the residual kernel's
+    epilogue; stepping stage by stage (vcpg_rk_stage, then a residual) gives the
+    same states and time steps bit for bit."""
+    g = load_golden(golden_files()[0])
+    _, _, _, s = _make(g["spec"])
+    try:
+        s.set_state(g["sol0"])
+        s.residual()
+        hist = s.step(3, scheme)
+        fused = s.get_state()
+        s.set_state(g["sol0"])
+        s.residual()
+        stages = 5 if scheme == capi.LSRK4 else 3
+        for n in range(3):
+            dt = s.time_step()
+            assert dt == hist[n]
+            for st in range(stages):
+                s.rk_stage(scheme, st, dt)
+                s.residual()
+        np.testing.assert_array_equal(s.get_state(), fused)
     finally:
         s.close()

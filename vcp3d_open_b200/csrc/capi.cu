@@ -34,6 +34,7 @@ struct vcpg_handle {
   double *d_nmetric = nullptr;   // [nE][10][K^3] metric at the nodal DOFs (SGS model)
   double *d_dt = nullptr, *d_fixed = nullptr, *d_hist = nullptr;
   int *d_status = nullptr, *d_counter = nullptr;
+  unsigned int *d_ticket = nullptr;   // last-block ticket of StartStepKernel
   unsigned long long *d_cgstats = nullptr;
   int hist_cap = 0;
   cudaGraph_t graph[2] = {nullptr, nullptr};
@@ -203,30 +204,39 @@ int EnqueueResidual(vcpg_handle *h, const ResidualArgs &a, int *launches) {
 
 int ResidualLaunches(const vcpg_handle *h) { return (h->open && h->nB > 0) ? 4 : 2; }
 
+// One time step of a single case: the CFL time step, then the first stage's
+// update together with recording the step (StartStepKernel), then per stage a
+// residual whose kernel applies the next stage's update to its element in its
+// epilogue; the last stage's residual is stored (the next step's first stage
+// uses it). SSP-RK3: 2 + 3 residuals' launches, low-storage RK4: 2 + 5.
 int EnqueueStep(vcpg_handle *h, int scheme) {
   const size_t n = (size_t)h->nOwned * 5 * h->KD;
   TimeStepArgs t = MakeTimeStepArgs(h);
   VCPG_CUDA(h, LaunchTimeStep(h->K, h->M, t, h->stream));
+  const double alphaRK[] = {1.0, 3.0 / 4.0, 1.0 / 3.0};
+  const double betaRK[] = {1.0, 1.0 / 4.0, 2.0 / 3.0};
+  const bool ssp = scheme == VCPG_SSPRK3;
+  const int stages = ssp ? 3 : 5;
+  const int kind = ssp ? kRkSsp : kRkLowStorage;
+  auto coefA = [&](int s) { return ssp ? alphaRK[s] : kLsA[s]; };
+  auto coefB = [&](int s) { return ssp ? betaRK[s] : kLsB[s]; };
   // The fixed step lives in device memory (d_fixed); a non-positive value selects the CFL step.
-  VCPG_CUDA(h, LaunchFinalizeDt(h->d_dtbits, h->d_fixed, h->d_dt, h->d_hist, h->hist_cap, h->d_counter,
-                                h->stream));
-  ResidualArgs a = MakeResidualArgs(h, nullptr, nullptr);
-  if (scheme == VCPG_SSPRK3) {
-    const double alphaRK[] = {1.0, 3.0 / 4.0, 1.0 / 3.0};
-    const double betaRK[] = {1.0, 1.0 / 4.0, 2.0 / 3.0};
-    for (int s = 0; s < 3; ++s) {
-      VCPG_CUDA(h, LaunchSspStage(h->d_sol, h->d_solOld, h->d_res, h->d_dt, alphaRK[s], betaRK[s],
-                                  s == 0, n, h->stream, CaseView{}, 5 * h->KD));
-      int rc = EnqueueResidual(h, a, nullptr);
-      if (rc) return rc;
+  VCPG_CUDA(h, LaunchStartStep(h->d_dtbits, h->d_fixed, h->d_dt, h->d_hist, h->hist_cap,
+                               h->d_counter, h->d_ticket, h->d_sol, h->d_solOld, h->d_res, kind,
+                               coefA(0), coefB(0), n, h->stream));
+  for (int s = 0; s < stages; ++s) {
+    ResidualArgs a = MakeResidualArgs(h, nullptr, nullptr);
+    if (s + 1 < stages) {
+      a.rk_kind = kind;
+      a.rk_a = coefA(s + 1);
+      a.rk_b = coefB(s + 1);
+      a.rk_dt = h->d_dt;
+      a.rk_sol = h->d_sol;
+      a.rk_reg = h->d_solOld;
+      a.rk_store_res = 0;
     }
-  } else {
-    for (int s = 0; s < 5; ++s) {
-      VCPG_CUDA(h, LaunchLsrkStage(h->d_sol, h->d_solOld, h->d_res, h->d_dt, kLsA[s], kLsB[s], n,
-                                   h->stream, CaseView{}, 5 * h->KD));
-      int rc = EnqueueResidual(h, a, nullptr);
-      if (rc) return rc;
-    }
+    int rc = EnqueueResidual(h, a, nullptr);
+    if (rc) return rc;
   }
   return VCPG_OK;
 }
@@ -245,7 +255,7 @@ int vcpg_destroy(vcpg_handle *h) {
   }
   void *bufs[] = {h->d_sol, h->d_solOld, h->d_res, h->d_resRaw, h->d_vol, h->d_face, h->d_sc,
                   h->d_nbr, h->d_dtbits, h->d_mach2, h->d_dt, h->d_fixed, h->d_hist,
-                  h->d_status, h->d_counter, h->d_cgstats, h->d_bface, h->d_bpresc, h->d_pc,
+                  h->d_status, h->d_counter, h->d_ticket, h->d_cgstats, h->d_bface, h->d_bpresc, h->d_pc,
                   h->d_dlq, h->d_btrace, h->d_bmach, h->d_bflux, h->d_sponge, h->d_dampfn,
                   h->d_dampst, h->d_cml, h->d_cfg, h->d_fflux, h->d_eddymax, h->d_nmetric,
                   h->d_bforce, h->d_center, h->d_scratch};
@@ -346,6 +356,8 @@ int vcpg_create(const vcpg_params *params, const vcpg_operators *ops, const vcpg
   if ((rc = alloc((void **)&h->d_fixed, sizeof(double)))) return rc;
   if ((rc = alloc((void **)&h->d_status, 4 * sizeof(int)))) return rc;
   if ((rc = alloc((void **)&h->d_counter, sizeof(int)))) return rc;
+  if ((rc = alloc((void **)&h->d_ticket, sizeof(unsigned int)))) return rc;
+  VCPG_CUDA(h, cudaMemsetAsync(h->d_ticket, 0, sizeof(unsigned int), h->stream));
   if ((rc = alloc((void **)&h->d_cgstats, 2 * sizeof(unsigned long long)))) return rc;
   VCPG_CUDA(h, cudaMemsetAsync(h->d_cgstats, 0, 2 * sizeof(unsigned long long), h->stream));
   h->hist_cap = 1024;
@@ -538,7 +550,7 @@ int vcpg_step(vcpg_handle *h, int32_t scheme, int32_t n_steps, double fixed_dt,
     if (e != cudaSuccess) return CudaFail(h, e, "cudaStreamEndCapture");
     h->graph[scheme] = g;
     VCPG_CUDA(h, cudaGraphInstantiate(&h->exec[scheme], g, 0));
-    h->graph_launches[scheme] = 2 + (scheme == VCPG_SSPRK3 ? 3 : 5) * (1 + ResidualLaunches(h));
+    h->graph_launches[scheme] = 2 + (scheme == VCPG_SSPRK3 ? 3 : 5) * ResidualLaunches(h);
   }
   for (int s = 0; s < n_steps; ++s) VCPG_CUDA(h, cudaGraphLaunch(h->exec[scheme], h->stream));
   h->launches += (int64_t)n_steps * h->graph_launches[scheme];

@@ -18,6 +18,7 @@
 #include <type_traits>
 
 #include "dg_physics.cuh"
+#include "dg_rk.cuh"
 #include "dg_tensor.cuh"
 
 namespace vcpg {
@@ -81,9 +82,37 @@ struct ResidualArgs {
   int scratch_ctas;            // CTAs the scratch areas hold (the grid of those degrees)
   int body_force;              // 1: the body-force source with fbody
   double fbody[3];             // body force per unit volume / p_ref
+  // Runge-Kutta stage update fused into the epilogue (enum RkKind; single-case
+  // steps): the element's residual updates its own state in place (no other CTA
+  // of the residual kernel reads it) and is written to res only with
+  // rk_store_res. kRkNone writes res.
+  int rk_kind;
+  int rk_store_res;
+  double rk_a, rk_b;           // low-storage (a, b) or SSP (alpha, beta)
+  const double *rk_dt;         // the step's time step (device)
+  double *rk_sol;              // the state (the array sol points to)
+  double *rk_reg;              // du (low-storage) or solOld (SSP)
 };
 
-// Arguments of the CFL time-step kernel (kernels.cu).
+// Final value r of residual entry gi (after the mass-matrix solve): stored, or
+// applied to the state by the fused stage update, whose inputs are the entry's
+// state sol0 and its second register reg0 (du or solOld).
+__device__ __forceinline__ void StoreResidual(const ResidualArgs &a, const size_t gi,
+                                              const double r, const double dt,
+                                              const double sol0, const double reg0) {
+  if (a.rk_kind == kRkNone || a.rk_store_res) a.res[gi] = r;
+  if (a.rk_kind == kRkNone) return;
+  double s = sol0, g = reg0;
+  if (a.rk_kind == kRkLowStorage) {
+    LsrkUpdate(s, g, r, dt, a.rk_a, a.rk_b);
+    a.rk_reg[gi] = g;
+  } else {
+    SspUpdate(s, g, r, dt, a.rk_a, a.rk_b);
+  }
+  a.rk_sol[gi] = s;
+}
+
+// Arguments of the CFL time-step kernels (dg_timestep.cuh).
 struct TimeStepArgs {
   const double *sol;
   const double *elem_scalars;
@@ -98,6 +127,15 @@ struct TimeStepArgs {
   void *scratch;                    // degree 9 with a model: 32 K^3 doubles per CTA
   int scratch_ctas;
 };
+
+// Asynchronous 8-byte copy global -> shared (cp.async; the calling thread waits
+// for its own copies with CpAsyncWaitAll).
+__device__ __forceinline__ void CpAsync8(double *dst_smem, const double *src_gmem) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src_gmem) : "memory");
+}
+__device__ __forceinline__ void CpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void CpAsyncWaitAll() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 template <int NT, typename T>
 __device__ __forceinline__ T BlockSum(T v, T *red) {
@@ -925,7 +963,8 @@ __device__ __forceinline__ void PointOperator(const T *s_cgp, const T *s_jw, con
 // (src/CG_MassMatrix.cpp:250-504): flexible PCG with the element-centre
 // dV/dU * 8/vol preconditioner, stop at ||r||_inf < 1e-10 ||r0||_inf, at most
 // 100 iterations (the cap raises a status flag instead of aborting).
-// r is s_R (dense, overwritten); the solution is written to dst (global, dense).
+// r is s_R (dense, overwritten); the solution goes through StoreResidual (the
+// residual array, or the fused Runge-Kutta stage update of the element).
 //
 // One iteration is seven barrier-separated steps: k, j transforms to the
 // integration points (the first with the search-direction update), the
@@ -936,10 +975,10 @@ __device__ __forceinline__ void PointOperator(const T *s_cgp, const T *s_jw, con
 // reductions use one barrier each and alternate their scratch areas. The CG
 // arrays use the padded layouts of CgLayout.
 // ---------------------------------------------------------------------------
-template <int NT, int K, int M, typename T>
+template <int NT, int K, int M, typename T, bool OPEN>
 __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, const T *s_sol,
                                           T *s_R, const T *s_cgp, const T *s_jw,
-                                          T *work, T *s_red, double *dst) {
+                                          T *work, T *s_red) {
   constexpr int SLOT = Slot<K, M>::value;
   using P = Plan<K, M, T>;
   using L = typename P::CL;
@@ -967,9 +1006,49 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
 #pragma unroll
     for (int q = 0; q < 5; ++q) x[q * LP::SV + off(l)] = T(0.0);
   }
+  // Inputs of a fused stage update (the state's second register, and in the
+  // mixed form the FP64 state itself; the FP64 form takes the state from s_sol)
+  // are fetched asynchronously into the part of the work area that the CG
+  // leaves free, each entry by the thread that applies the update to it.
+  const size_t g0 = (size_t)e * 5 * KD;
+  // The launched kernel's plan (its work area; shared memory unless BIG).
+  using PK = Plan<K, M, T, OPEN>;
+  constexpr bool kMixed = sizeof(T) == 4;
+  constexpr int kPrefOff = (P::CG + 1) / 2 * 2;   // in T, 8-byte aligned
+  constexpr bool kPrefetch =
+      !PK::BIG && (size_t)(PK::WORK - kPrefOff) * sizeof(T) >= (kMixed ? 2 : 1) * 5 * KD * 8;
+  double *pref = reinterpret_cast<double *>(work + kPrefOff);
+  const bool fused = a.rk_kind != kRkNone;
+  if (kPrefetch && fused) {
+    for (int l = threadIdx.x; l < KD; l += NT) {
+#pragma unroll
+      for (int q = 0; q < 5; ++q) {
+        CpAsync8(pref + q * KD + l, a.rk_reg + g0 + q * KD + l);
+        if (kMixed) CpAsync8(pref + 5 * KD + q * KD + l, a.rk_sol + g0 + q * KD + l);
+      }
+    }
+    CpAsyncCommit();
+  }
+  // Entry idx = q K^3 + l of the element: stored or applied (same thread as its prefetch).
+  auto finish = [&](const int idx, const double r, const double dt) {
+    if (!fused) { a.res[g0 + idx] = r; return; }
+    double s0, r0;
+    if constexpr (kPrefetch) {
+      r0 = pref[idx];
+      s0 = kMixed ? pref[5 * KD + idx] : double(s_sol[idx]);
+    } else {
+      r0 = a.rk_reg[g0 + idx];
+      s0 = kMixed ? a.rk_sol[g0 + idx] : double(s_sol[idx]);
+    }
+    StoreResidual(a, g0 + idx, r, dt, s0, r0);
+  };
   const T rInitMax = BlockMax<NT>(m, s_red);
   if (!(rInitMax * JacInv > T(1.e-10))) {
-    for (int i = threadIdx.x; i < 5 * KD; i += NT) dst[i] = 0.0;
+    const double dtStage = fused ? *a.rk_dt : 0.0;
+    if (kPrefetch && fused) CpAsyncWaitAll();
+    for (int l = threadIdx.x; l < KD; l += NT)
+#pragma unroll
+      for (int q = 0; q < 5; ++q) finish(q * KD + l, 0.0, dtStage);
     return;
   }
 
@@ -1133,10 +1212,12 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
     atomicAdd(a.cg_stats + 1, 1ull);
   }
   // Every thread reads back the entries it wrote itself in the last update.
+  const double dtStage = fused ? *a.rk_dt : 0.0;
+  if (kPrefetch && fused) CpAsyncWaitAll();
   for (int l = threadIdx.x; l < KD; l += NT) {
     const int o = off(l);
 #pragma unroll
-    for (int q = 0; q < 5; ++q) dst[q * KD + l] = double(x[q * LP::SV + o]);
+    for (int q = 0; q < 5; ++q) finish(q * KD + l, double(x[q * LP::SV + o]), dtStage);
   }
 }
 
@@ -1172,7 +1253,7 @@ __device__ __forceinline__ void ResidualElement(const ResidualArgs &a, const int
     for (int i = threadIdx.x; i < 5 * KD; i += NT) dst[i] = double(s_R[i]);
   }
   __syncthreads();
-  MassSolve<NT, K, M>(a, e, s_sol, s_R, s_cgp, s_jw, work, s_red, a.res + (size_t)e * 5 * KD);
+  MassSolve<NT, K, M, T, OPEN>(a, e, s_sol, s_R, s_cgp, s_jw, work, s_red);
 }
 
 template <int K, int M, int NT, typename T, bool OPEN>

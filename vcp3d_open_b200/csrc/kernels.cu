@@ -6,6 +6,7 @@
 
 #include "dg_boundary.cuh"
 #include "dg_residual.cuh"
+#include "dg_rk.cuh"
 #include "dg_timestep.cuh"
 #include "kernels.h"
 
@@ -65,12 +66,10 @@ __global__ void SspStageKernel(double *sol, double *solOld, const double *res, c
   if (i >= n) return;
   const int c = StageCase(cv, i, elemSize);
   if (c < 0) return;
-  const double betaDt = beta * d_dt[c];
-  const double oneMinAlpha = 1.0 - alpha;
-  const double s = sol[i];
-  double so;
+  double s = sol[i], so;
   if (copyOld) { so = s; solOld[i] = s; } else { so = solOld[i]; }
-  sol[i] = oneMinAlpha * s + alpha * so - betaDt * res[i];
+  SspUpdate(s, so, res[i], d_dt[c], alpha, beta);
+  sol[i] = s;
 }
 
 // Low-storage RK stage: dU = a dU - dt R; U += b dU (a == 0 starts a new step).
@@ -80,10 +79,51 @@ __global__ void LsrkStageKernel(double *sol, double *du, const double *res, cons
   if (i >= n) return;
   const int c = StageCase(cv, i, elemSize);
   if (c < 0) return;
-  const double dt = d_dt[c];
-  const double d = (ca == 0.0) ? -dt * res[i] : ca * du[i] - dt * res[i];
+  double s = sol[i], d = ca == 0.0 ? 0.0 : du[i];
+  LsrkUpdate(s, d, res[i], d_dt[c], ca, cb);
   du[i] = d;
-  sol[i] = sol[i] + cb * d;
+  sol[i] = s;
+}
+
+// The start of a single-case step: the time step (the reduced CFL step, or the
+// fixed one) and the first stage's update with it, in one grid. Every block
+// reads the reduced step first; the block that finishes last records it
+// (d_dt for the stages fused into the residual kernels, the history) and
+// re-arms the reduction. ticket: a zero-initialised counter, reset here.
+__global__ void StartStepKernel(unsigned long long *dt_bits, const double *fixed_dt, double *d_dt,
+                                double *hist, int hist_cap, int *counter, unsigned int *ticket,
+                                double *sol, double *reg, const double *res, int kind,
+                                double ca, double cb, size_t n) {
+  const double fx = *fixed_dt;
+  const double dt = fx > 0.0 ? fx : __longlong_as_double((long long)*dt_bits);
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    double s = sol[i];
+    if (kind == kRkLowStorage) {
+      double d = ca == 0.0 ? 0.0 : reg[i];
+      LsrkUpdate(s, d, res[i], dt, ca, cb);
+      reg[i] = d;
+    } else {
+      reg[i] = s;                     // solOld = sol
+      SspUpdate(s, s, res[i], dt, ca, cb);
+    }
+    sol[i] = s;
+  }
+  __shared__ bool last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    *d_dt = dt;
+    const int c = *counter;
+    if (c < hist_cap) hist[c] = dt;
+    *counter = c + 1;
+    *dt_bits = (unsigned long long)__double_as_longlong(1.e+10);
+    *ticket = 0u;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -213,6 +253,19 @@ cudaError_t LaunchLsrkStage(double *sol, double *du, const double *res, const do
   const int nt = 256;
   LsrkStageKernel<<<(unsigned)((n + nt - 1) / nt), nt, 0, st>>>(sol, du, res, d_dt, ca, cb, n,
                                                                 cv, elemSize);
+  return cudaGetLastError();
+}
+
+cudaError_t LaunchStartStep(unsigned long long *dt_bits, const double *fixed_dt, double *d_dt,
+                            double *hist, int hist_cap, int *counter, unsigned int *ticket,
+                            double *sol, double *reg, const double *res, int kind, double ca,
+                            double cb, size_t n, cudaStream_t st) {
+  // A grid of at most 8 resident blocks of 256 threads per SM (148 SMs).
+  const int nt = 256;
+  const size_t want = (n + nt - 1) / nt;
+  const unsigned grid = (unsigned)(want < 148 * 8 ? (want > 0 ? want : 1) : 148 * 8);
+  StartStepKernel<<<grid, nt, 0, st>>>(dt_bits, fixed_dt, d_dt, hist, hist_cap, counter, ticket,
+                                       sol, reg, res, kind, ca, cb, n);
   return cudaGetLastError();
 }
 

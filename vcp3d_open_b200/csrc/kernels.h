@@ -64,6 +64,13 @@ cudaError_t LaunchBoundary(int K, int M, const BoundaryArgs &a, cudaStream_t st)
 cudaError_t LaunchTimeStep(int K, int M, const TimeStepArgs &a, cudaStream_t st);
 cudaError_t LaunchFinalizeDt(unsigned long long *dt_bits, const double *fixed_dt, double *d_dt,
                              double *hist, int hist_cap, int *counter, cudaStream_t st);
+// The start of a single-case step: the reduced (or fixed) time step recorded,
+// the reduction re-armed, and the first stage's update (kind: enum RkKind,
+// coefficients (a, b) or (alpha, beta)); reg is du or solOld.
+cudaError_t LaunchStartStep(unsigned long long *dt_bits, const double *fixed_dt, double *d_dt,
+                            double *hist, int hist_cap, int *counter, unsigned int *ticket,
+                            double *sol, double *reg, const double *res, int kind, double ca,
+                            double cb, size_t n, cudaStream_t st);
 // Stage updates; d_dt holds one time step per case (one entry for a single case).
 cudaError_t LaunchSspStage(double *sol, double *solOld, const double *res, const double *d_dt,
                            double alpha, double beta, int copyOld, size_t n, cudaStream_t st,
