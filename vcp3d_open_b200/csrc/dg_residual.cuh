@@ -354,16 +354,28 @@ __device__ __forceinline__ void MatchingLayerSource(const ResidualArgs &a, const
   for (int n = 0; n < 5; ++n) bufC[n * MD + l] = out[n];
 }
 
+// The element's volume metric (10 M^3 doubles) is fetched asynchronously into
+// the part of the work area above the volume phase's arrays, while the
+// interpolation contractions run, where it fits that space (FP64 up to degree 3).
+template <int K, int M, typename T, bool OPEN> struct VolumeMetricPrefetch {
+  using P = Plan<K, M, T, OPEN>;
+  static constexpr int OFF = (P::VOL + 1) / 2 * 2;   // in T, 8-byte aligned
+  static constexpr bool value =
+      !P::BIG && (long)(P::WORK - OFF) * (long)sizeof(T) >= 10L * M * M * M * 8;
+};
+
 // ---------------------------------------------------------------------------
 // Volume phase: solution and gradients at the integration points
 // (TPSAGV), pointwise fluxes, and the three transposed contractions (TPAVR)
 // into s_R. Also stores the CG point data (rho, u, v, w, p)
 // and J*w.  Follows ElementClass::VolumeResidual, src/ElementClass.cpp:3809-4443.
 // ---------------------------------------------------------------------------
+// vms: the element's volume metric staged in shared memory (VolumeMetricPrefetch),
+// or null to read it from global memory.
 template <int NT, int K, int M, typename T, bool OPEN>
 __device__ __forceinline__ void VolumePhase(const ResidualArgs &a, const int e, const double mu,
                                             const T *s_sol, T *s_R, T *s_cgp,
-                                            T *s_jw, T *work, T *s_red) {
+                                            T *s_jw, T *work, T *s_red, const double *vms) {
   constexpr int SLOT = Slot<K, M>::value;
   using P = Plan<K, M, T, OPEN>;
   constexpr int MD = P::MD, KD = P::KD, M2 = P::M2;
@@ -391,9 +403,15 @@ __device__ __forceinline__ void VolumePhase(const ResidualArgs &a, const int e, 
   __syncthreads();
   ContractL<NT, SLOT, K, M, kLeg, 0, 5, K, M, M, K, M, false, T, typename P::VB, Dense<M, M, M>>(tJ, dZ);
   for (int i = threadIdx.x; i < 5 * KD; i += NT) s_R[i] = T(0.0);
+  if constexpr (VolumeMetricPrefetch<K, M, T, OPEN>::value) CpAsyncWaitAll();
   __syncthreads();
 
   const double *vm = a.vol_metric + (size_t)e * 10 * MD;
+  constexpr bool kVPref = VolumeMetricPrefetch<K, M, T, OPEN>::value;
+  auto Vm = [&](const int i) -> T {
+    if constexpr (kVPref) return T(vms[i]);
+    else return LdT<T>(vm + i);
+  };
   const T gm1 = T(kGam) - T(1.0), ov1mg = -T(1.0) / gm1;
   T mach2 = T(0.0), eddyMax = T(0.0);
   for (int l = threadIdx.x; l < MD; l += NT) {
@@ -405,12 +423,12 @@ __device__ __forceinline__ void VolumePhase(const ResidualArgs &a, const int e, 
     for (int n = 0; n < 5; ++n) {
       const int mi = a.metric_compat ? n : l;
       const T dvdr = dX[n * MD + l], dvds = dY[n * MD + l], dvdt = dZ[n * MD + l];
-      gx[n] = dvdr * LdT<T>(vm + 1 * MD + mi) + dvds * LdT<T>(vm + 4 * MD + mi) +
-              dvdt * LdT<T>(vm + 7 * MD + mi);
-      gy[n] = dvdr * LdT<T>(vm + 2 * MD + mi) + dvds * LdT<T>(vm + 5 * MD + mi) +
-              dvdt * LdT<T>(vm + 8 * MD + mi);
-      gz[n] = dvdr * LdT<T>(vm + 3 * MD + mi) + dvds * LdT<T>(vm + 6 * MD + mi) +
-              dvdt * LdT<T>(vm + 9 * MD + mi);
+      gx[n] = dvdr * Vm(1 * MD + mi) + dvds * Vm(4 * MD + mi) +
+              dvdt * Vm(7 * MD + mi);
+      gy[n] = dvdr * Vm(2 * MD + mi) + dvds * Vm(5 * MD + mi) +
+              dvdt * Vm(8 * MD + mi);
+      gz[n] = dvdr * Vm(3 * MD + mi) + dvds * Vm(6 * MD + mi) +
+              dvdt * Vm(9 * MD + mi);
       V[n] = Var[n * MD + l];
     }
     // Entropy -> primitive variables, velocity and internal-energy gradients
@@ -436,13 +454,13 @@ __device__ __forceinline__ void VolumePhase(const ResidualArgs &a, const int e, 
     mach2 = Fmax(mach2, rho * (u * u + v * v + w * w) / (T(kGam) * p));
     if (OPEN && cmlHere)
       MatchingLayerSource<M>(a, sp, l, V, gx, gy, gz, rho, u, v, w, p, eKin, rE,
-                             -LdT<T>(vm + l) * Weight1D<SLOT, T>(i) * Weight1D<SLOT, T>(j) *
+                             -Vm(l) * Weight1D<SLOT, T>(i) * Weight1D<SLOT, T>(j) *
                                  Weight1D<SLOT, T>(k),
                              bufC);
 
     // Inviscid + viscous fluxes times -J w and the metric (src/ElementClass.cpp:4320-4416).
     const T Wl = Weight1D<SLOT, T>(i) * Weight1D<SLOT, T>(j) * Weight1D<SLOT, T>(k);
-    const T Jl = LdT<T>(vm + l);
+    const T Jl = Vm(l);
     s_jw[l] = Wl * Jl;
     const T weight = -Jl * Wl;
     const T ru = rho * u, rv = rho * v, rw = rho * w;
@@ -470,12 +488,12 @@ __device__ __forceinline__ void VolumePhase(const ResidualArgs &a, const int e, 
                           (rE + p) * v - (u * tauxy + v * tauyy + w * tauyz - qy)};
     const T fz[5] = {rw, ru * w - tauxz, rv * w - tauyz, rw * w - tauzz + p,
                           (rE + p) * w - (u * tauxz + v * tauyz + w * tauzz - qz)};
-    const T drdx = weight * LdT<T>(vm + 1 * MD + l), drdy = weight * LdT<T>(vm + 2 * MD + l),
-                 drdz = weight * LdT<T>(vm + 3 * MD + l);
-    const T dsdx = weight * LdT<T>(vm + 4 * MD + l), dsdy = weight * LdT<T>(vm + 5 * MD + l),
-                 dsdz = weight * LdT<T>(vm + 6 * MD + l);
-    const T dtdx = weight * LdT<T>(vm + 7 * MD + l), dtdy = weight * LdT<T>(vm + 8 * MD + l),
-                 dtdz = weight * LdT<T>(vm + 9 * MD + l);
+    const T drdx = weight * Vm(1 * MD + l), drdy = weight * Vm(2 * MD + l),
+                 drdz = weight * Vm(3 * MD + l);
+    const T dsdx = weight * Vm(4 * MD + l), dsdy = weight * Vm(5 * MD + l),
+                 dsdz = weight * Vm(6 * MD + l);
+    const T dtdx = weight * Vm(7 * MD + l), dtdy = weight * Vm(8 * MD + l),
+                 dtdz = weight * Vm(9 * MD + l);
 #pragma unroll
     for (int n = 0; n < 5; ++n) {
       dX[n * MD + l] = fx[n] * drdx + fy[n] * drdy + fz[n] * drdz;
@@ -587,8 +605,11 @@ __device__ __forceinline__ int DerivSlot(const int d, const int p) {
 }
 
 // Face-normal evaluation of the six sides of a group (first stage of TPSAG[IJK]).
+// s_nb: the three neighbours' states staged in shared memory ([3][5 K^3], in
+// the order of the directions), or null to read them from gsol.
 template <int NT, int SLOT, int K, typename T>
 __device__ __forceinline__ void FaceNormalBatch(const T *s_sol, const double *gsol,
+                                                const double *s_nb,
                                                 const int nb0, const int nb1, const int nb2,
                                                 const int g, const T *s_fv, T *bn,
                                                 T *bnd) {
@@ -608,12 +629,22 @@ __device__ __forceinline__ void FaceNormalBatch(const T *s_sol, const double *gs
     if (nbr) {
       const int nb = d == 0 ? nb0 : (d == 1 ? nb1 : nb2);
       if (nb >= 0) {
-        const double *b = gsol + (size_t)nb * 5 * KD + base;
+        if (s_nb) {
+          const double *b = s_nb + d * 5 * KD + base;
 #pragma unroll
-        for (int n = 0; n < K; ++n) {
-          const T x = LdT<T>(b + n * ns);
-          a0 = Fma(fv[n], x, a0);
-          d0 = Fma(dfv[n], x, d0);
+          for (int n = 0; n < K; ++n) {
+            const T x = T(b[n * ns]);
+            a0 = Fma(fv[n], x, a0);
+            d0 = Fma(dfv[n], x, d0);
+          }
+        } else {
+          const double *b = gsol + (size_t)nb * 5 * KD + base;
+#pragma unroll
+          for (int n = 0; n < K; ++n) {
+            const T x = LdT<T>(b + n * ns);
+            a0 = Fma(fv[n], x, a0);
+            d0 = Fma(dfv[n], x, d0);
+          }
         }
       }
     } else {
@@ -753,7 +784,8 @@ __device__ __forceinline__ void FaceRoles(const ResidualArgs &a, const int g, co
 // (their fluxes come from the boundary kernels).
 template <int NT, int K, int M, typename T, bool SGS>
 __device__ __forceinline__ void MinFaceFluxes(const ResidualArgs &a, const int e, const double mu,
-                                              const T *s_sol, const T *s_fv, T *work) {
+                                              const T *s_sol, const T *s_fv, T *work,
+                                              const double *s_nb) {
   constexpr int SLOT = Slot<K, M>::value;
   constexpr int M2 = M * M, K2 = K * K;
   static_assert(K <= M, "face-flux buffer aliasing");
@@ -761,7 +793,7 @@ __device__ __forceinline__ void MinFaceFluxes(const ResidualArgs &a, const int e
   T *BN = T1c + 30 * K * M, *BND = BN + 30 * K2;  // 60 K^2
   T *TR = BN;                               // 120 M^2 (BN is dead when TR is written)
   const int nb0 = a.nbr[e * 6 + 0], nb1 = a.nbr[e * 6 + 2], nb2 = a.nbr[e * 6 + 4];
-  FaceNormalBatch<NT, SLOT, K>(s_sol, a.sol, nb0, nb1, nb2, 0, s_fv, BN, BND);
+  FaceNormalBatch<NT, SLOT, K>(s_sol, a.sol, s_nb, nb0, nb1, nb2, 0, s_fv, BN, BND);
   __syncthreads();
   Contract<NT, SLOT, K, M, kLeg, 0, 30, K, K, 1, K, M, false>(BN, T1a);
   Contract<NT, SLOT, K, M, kDLeg, 0, 30, K, K, 1, K, M, false>(BN, T1b);
@@ -1016,7 +1048,7 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
   constexpr bool kMixed = sizeof(T) == 4;
   constexpr int kPrefOff = (P::CG + 1) / 2 * 2;   // in T, 8-byte aligned
   constexpr bool kPrefetch =
-      !PK::BIG && (size_t)(PK::WORK - kPrefOff) * sizeof(T) >= (kMixed ? 2 : 1) * 5 * KD * 8;
+      !PK::BIG && (long)(PK::WORK - kPrefOff) * (long)sizeof(T) >= (kMixed ? 2L : 1L) * 5 * KD * 8;
   double *pref = reinterpret_cast<double *>(work + kPrefOff);
   const bool fused = a.rk_kind != kRkNone;
   if (kPrefetch && fused) {
@@ -1239,6 +1271,13 @@ __device__ __forceinline__ void ResidualElement(const ResidualArgs &a, const int
     if (cs < 0 || a.cases.state[cs] != a.cases.require) return;
     mu = a.cases.par[cs * kCasePar + kParMu];
   }
+  using VP = VolumeMetricPrefetch<K, M, T, OPEN>;
+  double *vms = VP::value ? reinterpret_cast<double *>(work + VP::OFF) : nullptr;
+  if constexpr (VP::value) {
+    const double *g = a.vol_metric + (size_t)e * 10 * P::MD;
+    for (int i = threadIdx.x; i < 10 * P::MD; i += NT) CpAsync8(vms + i, g + i);
+    CpAsyncCommit();
+  }
   const double *src = a.sol + (size_t)e * 5 * KD;
   for (int i = threadIdx.x; i < 5 * KD; i += NT) s_sol[i] = T(src[i]);
   if (threadIdx.x < 2 * K) {
@@ -1246,7 +1285,7 @@ __device__ __forceinline__ void ResidualElement(const ResidualArgs &a, const int
     s_fv[2 * K + threadIdx.x] = FaceDer<Slot<K, M>::value, T>(threadIdx.x);
   }
   __syncthreads();
-  VolumePhase<NT, K, M, T, OPEN>(a, e, mu, s_sol, s_R, s_cgp, s_jw, work, s_red);
+  VolumePhase<NT, K, M, T, OPEN>(a, e, mu, s_sol, s_R, s_cgp, s_jw, work, s_red, vms);
   FacePhase<NT, K, M, T, OPEN>(a, e, s_R, s_fv, work);
   if (a.res_raw) {
     double *dst = a.res_raw + (size_t)e * 5 * KD;
@@ -1277,9 +1316,9 @@ template <int K, int M, typename T = double> struct FluxPlan {
   static constexpr int KD = K * K * K, M2 = M * M;
   static constexpr int FV = 4 * (K > 7 ? K : 7);
   static constexpr int TOTAL = 5 * KD + FV + 90 * K * M + 120 * M2;
-  static constexpr size_t BYTES = sizeof(T) * (size_t)TOTAL;
+  static constexpr size_t BASE_BYTES = sizeof(T) * (size_t)TOTAL;
   // Above one CTA's shared memory: global scratch per CTA, elements in a loop.
-  static constexpr bool BIG = BYTES > 227 * 1024;
+  static constexpr bool BIG = BASE_BYTES > 227 * 1024;
   static constexpr int SCRATCH = (TOTAL + 3) / 4 * 4;
   // Launch shape measured best on B200 over 96..192 threads and 2..4 CTAs per SM:
   // 128 threads and up to 4 CTAs (<= 128 registers) for degree <= 3; from degree
@@ -1288,30 +1327,52 @@ template <int K, int M, typename T = double> struct FluxPlan {
   static constexpr bool FP64 = sizeof(T) == 8;
   static constexpr int NT = K <= 4 ? 128 : 160;
   static constexpr int CAP = K <= 4 ? 4 : (FP64 ? 2 : 3);
-  static constexpr int FIT = (int)(227 * 1024 / BYTES);
+  static constexpr int FIT = (int)(227 * 1024 / BASE_BYTES);
   static constexpr int MIN_BLOCKS = FIT < 1 ? 1 : (FIT > CAP ? CAP : FIT);
+  // The three lower neighbours' FP64 states staged in shared memory (after the
+  // T arrays, 8-byte aligned) where that keeps MIN_BLOCKS CTAs per SM: one burst
+  // of coalesced asynchronous copies instead of strided per-line global loads.
+  static constexpr int NB_OFF = (TOTAL * (int)sizeof(T) + 7) / 8;   // in doubles
+  static constexpr size_t NB_BYTES = 8 * ((size_t)NB_OFF + 15 * (size_t)KD);
+  static constexpr bool NB_PREF = !BIG && (int)(227 * 1024 / NB_BYTES) >= MIN_BLOCKS;
+  static constexpr size_t BYTES = NB_PREF ? NB_BYTES : BASE_BYTES;
 };
 
 // The fluxes of every interior face, computed once by the face's upper element
 // (its Min faces), before the residual kernel distributes them to both sides.
 template <int K, int M, int NT, typename T, bool SGS>
 __device__ __forceinline__ void FaceFluxElement(const ResidualArgs &a, const int e, T *smem) {
+  using FP = FluxPlan<K, M, T>;
   constexpr int KD = K * K * K;
-  T *s_sol = smem, *s_fv = s_sol + 5 * KD, *work = s_fv + FluxPlan<K, M, T>::FV;
+  T *s_sol = smem, *s_fv = s_sol + 5 * KD, *work = s_fv + FP::FV;
   double mu = a.mu;
   if (a.cases.elem_case) {
     const int cs = a.cases.elem_case[e];
     if (cs < 0 || a.cases.state[cs] != a.cases.require) return;
     mu = a.cases.par[cs * kCasePar + kParMu];
   }
+  // The lower neighbours' states (i, j, k), fetched asynchronously while the
+  // element's own state is converted.
+  double *s_nb = FP::NB_PREF ? reinterpret_cast<double *>(smem) + FP::NB_OFF : nullptr;
+  if constexpr (FP::NB_PREF) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const int nb = a.nbr[e * 6 + 2 * d];
+      if (nb < 0) continue;
+      const double *g = a.sol + (size_t)nb * 5 * KD;
+      for (int i = threadIdx.x; i < 5 * KD; i += NT) CpAsync8(s_nb + d * 5 * KD + i, g + i);
+    }
+    CpAsyncCommit();
+  }
   const double *src = a.sol + (size_t)e * 5 * KD;
   for (int i = threadIdx.x; i < 5 * KD; i += NT) s_sol[i] = T(src[i]);
+  if constexpr (FP::NB_PREF) CpAsyncWaitAll();
   if (threadIdx.x < 2 * K) {
     s_fv[threadIdx.x] = FaceVal<Slot<K, M>::value, T>(threadIdx.x);
     s_fv[2 * K + threadIdx.x] = FaceDer<Slot<K, M>::value, T>(threadIdx.x);
   }
   __syncthreads();
-  MinFaceFluxes<NT, K, M, T, SGS>(a, e, mu, s_sol, s_fv, work);
+  MinFaceFluxes<NT, K, M, T, SGS>(a, e, mu, s_sol, s_fv, work, s_nb);
 }
 
 // SGS: with a subgrid-scale model (without one the kernel carries none of its code).
