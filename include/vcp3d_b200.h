@@ -373,6 +373,45 @@ int vcpg_set_open_boundary(vcpg_handle *h, const vcpg_open_boundary *ob,
                            const vcpg_geometry *geom, int32_t p_grid, int32_t dof_location,
                            const double *grid_nodes);
 
+/* One subface of a block face: an entry of the reference's "Subface
+ * information" with its prescribed boundary data (InputParamClass::
+ * ReadSubfaceInformation / ReadBoundaryData, src/InputParamClass.cpp:1340-1580;
+ * element ranges as mapped by SolverClass, src/SolverClass.cpp:1640-1660). It
+ * covers the element faces of block face `face` whose in-plane element indices
+ * lie in [elem_begin, elem_end) along the face's two in-plane directions taken
+ * in i, j, k order (j and k on i faces, i and k on j faces, i and j on k faces;
+ * 0-based, end exclusive), with its own condition and prescribed data (the
+ * fields of vcpg_open_boundary for one face, same units). */
+typedef struct vcpg_subface {
+  int32_t face;                   /* block face 0 iMin .. 5 kMax                       */
+  int32_t elem_begin[2];          /* first element index, both in-plane directions    */
+  int32_t elem_end[2];            /* one past the last                                 */
+  int32_t bc;                     /* enum vcpg_bc                                      */
+  double p_out;                   /* outflow: static pressure (Pa)                     */
+  double inflow[4];               /* static inflow: density, velocity x, y, z          */
+  double inflow_total[5];         /* total inflow: p_t (Pa), T_t (K), direction x, y, z */
+  double wall_data;               /* heat flux (W/m^2) or wall temperature (K)         */
+  double inflow_super[5];         /* supersonic inflow: density, velocity, pressure    */
+} vcpg_subface;
+
+/* vcpg_set_open_boundary with several subfaces per block face. A block face
+ * named by at least one subface takes the condition and prescribed data of
+ * each element face from the subface that covers it; its subfaces must cover
+ * every one of its element faces exactly once (else VCPG_E_INVALID). The other
+ * block faces keep ob->bc and ob's per-face data. The NSCBC tuning parameters
+ * of ob apply to every characteristic subface (outlet and inlet settings
+ * separately). As in the reference, the projected Mach number of a
+ * characteristic subface is averaged over the characteristic element faces of
+ * its whole block face and divided by the area of all of that block face's
+ * physical element faces (SolverClass::InitNSCBC / AverageDataNSCBC,
+ * src/SolverClass.cpp:2447-2581; ElementClass::ComputeSurfaceAreaBoundary /
+ * AverageMachNSCBC, src/ElementClass.cpp:303-509). n_subfaces = 0 is
+ * vcpg_set_open_boundary. */
+int vcpg_set_open_boundary_subfaces(vcpg_handle *h, const vcpg_open_boundary *ob,
+                                    const vcpg_subface *subfaces, int32_t n_subfaces,
+                                    const vcpg_geometry *geom, int32_t p_grid,
+                                    int32_t dof_location, const double *grid_nodes);
+
 /* ------------------------------------------------------------------------- */
 /* Served ensemble: many cases resident on one GPU, batched by degree.        */
 /* ------------------------------------------------------------------------- */

@@ -64,8 +64,16 @@ def assert_forces_match(mon, ref, spec, rel=1e-10):
     group to rel times its largest component."""
     mon, ref = np.asarray(mon, dtype=float), np.asarray(ref, dtype=float)
     ext = np.asarray(spec.hi, dtype=float) - np.asarray(spec.lo, dtype=float)
-    area = sum(float(np.prod(np.delete(ext, f // 2))) for f, b in enumerate(spec.bc)
-               if b.startswith("wall_"))
+    area = 0.0
+    for f, b in enumerate(spec.bc):
+        if b == "periodic":
+            continue
+        d = f // 2
+        a0, a1 = (1, 2) if d == 0 else ((0, 2) if d == 1 else (0, 1))
+        for (b0, e0, b1, e1), sbc, _ in spec.face_subfaces(f):
+            if sbc.startswith("wall_"):
+                area += float(ext[a0] * ext[a1]) * (e0 - b0) / spec.n_elem[a0] * \
+                    (e1 - b1) / spec.n_elem[a1]
     if not (spec.monitor_forces and area > 0.0):
         assert np.all(mon[:6] == 0.0)
         return

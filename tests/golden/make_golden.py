@@ -177,6 +177,20 @@ OPEN_SPECS = {
         wall_data=(0.0, 0.0, 310.0, 20.0, 0.0, 0.0), sponge=(0, 1, 0, 0, 0, 0),
         bc=("inflow_static_nscbc", "outflow_nscbc", "wall_isothermal", "wall_heat_flux",
             "periodic", "periodic"), **dict(_OPEN, kind="vortex", beta=2.0)),
+    # Several subfaces per block face: i-min holds a static-inflow patch (j < 2)
+    # beside an isothermal wall (j >= 2); i-max a characteristic outflow (j < 3,
+    # its Mach average over the block face's characteristic faces divided by the
+    # area of the whole face) beside a heat-flux wall; far field on the j faces,
+    # sponge with the matching layer on i-max, k periodic; forces monitored.
+    "subfaces_p3_4x4x2": cases.CaseSpec(
+        name="subfaces_p3_4x4x2", n_elem=(4, 4, 2), p=3, hi=(4.0, 4.0, 2.0),
+        center=(3.2, 1.2, 1.0), seed=15, monitor_forces=True, sponge=(0, 1, 0, 0, 0, 0),
+        cml=True, wall_data=(330.0, 25.0, 0.0, 0.0, 0.0, 0.0),
+        bc=("inflow_static_nscbc", "outflow_nscbc", "farfield", "farfield", "periodic",
+            "periodic"),
+        subfaces=((0, (0, 2, 0, 2), "inflow_static_nscbc"), (0, (2, 4, 0, 2), "wall_isothermal"),
+                  (1, (0, 3, 0, 2), "outflow_nscbc"), (1, (3, 4, 0, 2), "wall_heat_flux")),
+        **_OPEN),
     # Vreman model with the subsonic inflow / outflow states and far field, a
     # vortex next to the j-max far field.
     "vreman_p3_4x4x2_farfield": cases.CaseSpec(
@@ -217,6 +231,22 @@ SYNC_SPECS = {
                                    "Pressure pulse center": "5.2 0.8 1.0",
                                    "Pressure pulse strength": "1.0e-2",
                                    "Pressure pulse width": "0.5"}, 2),
+    # Several subfaces per face from the parameter file, each with its own data:
+    # i-min a static inflow beside an isothermal wall at 320 K, i-max two
+    # characteristic outflows at different pressures, far field on the j faces.
+    "subfaces_p3_4x4x2": (cases.CaseSpec(
+        name="subfaces_p3_4x4x2_sync", n_elem=(4, 4, 2), p=3, hi=(4.0, 4.0, 2.0),
+        center=(3.2, 1.2, 1.0), seed=15, sponge=(0, 1, 0, 0, 0, 0), cml=True,
+        bc=("inflow_static_nscbc", "outflow_nscbc", "farfield", "farfield", "periodic",
+            "periodic"),
+        subfaces=((0, (0, 2, 0, 2), "inflow_static_nscbc"),
+                  (0, (2, 4, 0, 2), "wall_isothermal", (320.0,)),
+                  (1, (0, 1, 0, 2), "outflow_nscbc", (101000.0,)),
+                  (1, (1, 4, 0, 2), "outflow_nscbc", (101325.0,))), **_OPEN),
+        {"Synchronization time step": "5.0e-5", "Restart": "no",
+         "Fluctuations to add to initial solution": "Pressure pulse",
+         "Pressure pulse center": "3.2 1.2 1.0", "Pressure pulse strength": "1.0e-2",
+         "Pressure pulse width": "0.5"}, 2),
     # The configuration of the reference's own total-inflow test case (8x4x4
     # elements of degree 3 on [0,2]x[0,1]x[0,1], total inflow / outflow in i,
     # periodic in j and k, a pressure pulse on the free stream), generated here.

@@ -31,6 +31,14 @@ def test_reference_conditions_and_initial_state(path, tmp_path):
     assert ref.mu_nondim == pytest.approx(mu, rel=1e-13)
     case = run.load_case(pf)
     assert case.spec.bc == g["spec"].bc
+    # Several subfaces per face: element ranges, conditions and the subfaces' own
+    # prescribed data read back from the file.
+    want = g["spec"].subfaces or ()
+    got = case.spec.subfaces or ()
+    assert [e[:3] for e in got] == [e[:3] for e in want]
+    for a, b in zip(got, want):
+        if b[3] is not None:
+            assert a[3] == pytest.approx(b[3], rel=1e-15)
     params = solver.make_params(case)
     sol0 = solver.nodal_to_modal(case, params)     # host code of the library
     assert rel_l2(sol0, g["sol0"]) < 1e-13

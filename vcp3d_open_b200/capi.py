@@ -34,7 +34,7 @@ EXPORTED = [
     "vcpg_get_residual", "vcpg_residual", "vcpg_get_raw_residual", "vcpg_time_step",
     "vcpg_step", "vcpg_synchronization_step", "vcpg_sync", "vcpg_stream", "vcpg_launch_count", "vcpg_stats",
     "vcpg_time_residual_kernels",
-    "vcpg_time_step_noalloc", "vcpg_set_open_boundary", "vcpg_ensemble_create",
+    "vcpg_time_step_noalloc", "vcpg_set_open_boundary", "vcpg_set_open_boundary_subfaces", "vcpg_ensemble_create",
     "vcpg_ensemble_destroy", "vcpg_ensemble_last_error", "vcpg_ensemble_footprint",
     "vcpg_ensemble_submit", "vcpg_ensemble_step", "vcpg_ensemble_poll", "vcpg_ensemble_retire",
     "vcpg_ensemble_sync", "vcpg_ensemble_stats",
@@ -76,6 +76,14 @@ class OpenBoundary(C.Structure):
                 ("cml", C.c_int32), ("sponge_state", C.c_double * 5),
                 ("inflow_total", (C.c_double * 5) * 6), ("wall_data", C.c_double * 6),
                 ("inflow_super", (C.c_double * 5) * 6), ("free_stream", C.c_double * 5)]
+
+
+class Subface(C.Structure):
+    """vcpg_subface: one subface of a block face with its condition and data."""
+    _fields_ = [("face", C.c_int32), ("elem_begin", C.c_int32 * 2), ("elem_end", C.c_int32 * 2),
+                ("bc", C.c_int32), ("p_out", C.c_double), ("inflow", C.c_double * 4),
+                ("inflow_total", C.c_double * 5), ("wall_data", C.c_double),
+                ("inflow_super", C.c_double * 5)]
 
 
 class EnsembleConfig(C.Structure):
@@ -138,6 +146,10 @@ def load() -> C.CDLL:
     lib.vcpg_time_residual_kernels.argtypes = [hp, C.c_int32, dp]
     lib.vcpg_time_step_noalloc.argtypes = [C.POINTER(Params), C.POINTER(Operators), C.c_void_p,
                                            C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.vcpg_set_open_boundary_subfaces.argtypes = [hp, C.POINTER(OpenBoundary),
+                                                    C.POINTER(Subface), C.c_int32,
+                                                    C.POINTER(Geometry), C.c_int32, C.c_int32,
+                                                    dp]
     lib.vcpg_set_open_boundary.argtypes = [hp, C.POINTER(OpenBoundary), C.POINTER(Geometry),
                                            C.c_int32, C.c_int32, dp]
     lib.vcpg_ensemble_create.argtypes = [C.POINTER(EnsembleConfig), C.POINTER(C.c_void_p)]

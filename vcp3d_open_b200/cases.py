@@ -178,6 +178,16 @@ class CaseSpec:
     # the grid nodes sit at LGL positions (generated grids do).
     dof_location: str = "lgl"
     grid_lgl: bool = True
+    # Several subfaces per block face: entries (face, (b0, e0, b1, e1), bc) or
+    # (face, (b0, e0, b1, e1), bc, data), the element rectangle [b0, e0) x [b1, e1)
+    # of block face `face` along its two in-plane directions in i, j, k order. A
+    # block face named here takes its conditions from its subfaces, which must
+    # cover it (its bc entry then only marks it as non-periodic). data, when
+    # given, is the subface's prescribed data (dimensional): (p,) for outflows,
+    # (rho, u, v, w) for the static inflow, (p_t, T_t, dir x, y, z) for total
+    # inflows, (value,) for walls, (rho, u, v, w, p) for the supersonic inflow;
+    # otherwise the face's data apply.
+    subfaces: Optional[Tuple[tuple, ...]] = None
 
     def __post_init__(self):
         if self.p_grid is None:
@@ -196,6 +206,23 @@ class CaseSpec:
                 raise ValueError(f"unknown boundary condition {b!r}")
         if self.cml and not any(self.sponge):
             raise ValueError("the matching layer needs sponge layers")
+        if self.subfaces is not None:
+            self.subfaces = tuple(
+                (int(e[0]), tuple(int(v) for v in e[1]), str(e[2]),
+                 tuple(float(v) for v in e[3]) if len(e) > 3 and e[3] is not None else None)
+                for e in self.subfaces)
+            for f, r, b, _ in self.subfaces:
+                if b not in BC_NAMES or b == "periodic" or self.bc[f] == "periodic":
+                    raise ValueError(f"subface on face {f}: {b!r} on a non-periodic face only")
+
+    def face_subfaces(self, f: int):
+        """The subfaces of block face f as (range, bc, data); one covering the whole
+        face with bc[f] and the face's data when none are given."""
+        if self.subfaces and any(sf[0] == f for sf in self.subfaces):
+            return [(r, b, dat) for g, r, b, dat in self.subfaces if g == f]
+        d = f // 2
+        a0, a1 = (1, 2) if d == 0 else ((0, 2) if d == 1 else (0, 1))
+        return [((0, self.n_elem[a0], 0, self.n_elem[a1]), self.bc[f], None)]
 
     @property
     def is_open(self) -> bool:
@@ -476,8 +503,10 @@ def read_su2_restart(path: str, n_elem: int, n_dofs: int):
 
 
 def _subfaces(spec: CaseSpec) -> str:
-    """Subface table: one subface per block face, periodic (1-to-1 with a
-    translation) or a physical boundary condition over the whole face."""
+    """Subface table: periodic faces (1-to-1 with a translation) over the whole
+    face; physical faces as one subface or as the spec's subfaces, with node
+    index ranges (the elements [b, e) of an in-plane direction span the nodes
+    b + 1 .. e + 1)."""
     nI, nJ, nK = spec.n_elem
     L = [spec.hi[d] - spec.lo[d] for d in range(3)]
     I, J, K = nI + 1, nJ + 1, nK + 1
@@ -489,15 +518,26 @@ def _subfaces(spec: CaseSpec) -> str:
         (f"1 {I} 1 {J} 1 1", f"1 {I} 1 {J} {K} {K}", (0.0, 0.0, L[2])),
         (f"1 {I} 1 {J} {K} {K}", f"1 {I} 1 {J} 1 1", (0.0, 0.0, -L[2])),
     ]
+    nodes = (I, J, K)
     out = []
     for face, (own, donor, t) in enumerate(rows, start=1):
-        out.append(f"    {face}    1")
         bc = spec.bc[face - 1]
         if bc == "periodic":
+            out.append(f"    {face}    1")
             out.append(f"        Periodic1to1Trans  {own}   {donor}   1 2 3   "
                        f"{t[0]!r} {t[1]!r} {t[2]!r}")
-        else:
-            out.append(f"        {BC_NAMES[bc]}  {own}")
+            continue
+        subs = spec.face_subfaces(face - 1)
+        out.append(f"    {face}    {len(subs)}")
+        d = (face - 1) // 2
+        plane = 1 if (face - 1) % 2 == 0 else nodes[d]
+        a0, a1 = (1, 2) if d == 0 else ((0, 2) if d == 1 else (0, 1))
+        for (b0, e0, b1, e1), sbc, _ in subs:
+            rng = [None] * 3
+            rng[d] = (plane, plane)
+            rng[a0] = (b0 + 1, e0 + 1)
+            rng[a1] = (b1 + 1, e1 + 1)
+            out.append(f"        {BC_NAMES[sbc]}  " + " ".join(f"{x} {y}" for x, y in rng))
     return "\n".join(out)
 
 
@@ -531,35 +571,56 @@ Sponge layer information
 """
     p_out, rho_in, vel_in = prescribed_values(spec, ref)
     lines = []
-    for f, bc in enumerate(spec.bc):
-        if bc == "outflow_nscbc":
-            lines.append(f"    {f + 1}    1    1    Pressure")
-            lines.append(f"        {p_out!r}")
-        elif bc == "inflow_static_nscbc":
-            lines.append(f"    {f + 1}    1    1    Density VelocityX VelocityY VelocityZ")
-            lines.append(f"        {rho_in!r} {vel_in[0]!r} {vel_in[1]!r} {vel_in[2]!r}")
-        elif bc == "outflow_subsonic":
-            lines.append(f"    {f + 1}    1    1    Pressure")
-            lines.append(f"        {p_out!r}")
-        elif bc in ("wall_heat_flux", "wall_isothermal"):
-            val = spec.wall_data[f] if spec.wall_data else (
-                0.0 if bc == "wall_heat_flux" else spec.t_inf)
-            name = "HeatFlux" if bc == "wall_heat_flux" else "Temperature"
-            lines.append(f"    {f + 1}    1    1    {name}")
-            lines.append(f"        {float(val)!r}")
-        elif bc == "inflow_supersonic":
-            q = spec.prescribed_super[f] if spec.prescribed_super else (rho_in, *vel_in, p_out)
-            lines.append(f"    {f + 1}    1    1    Density VelocityX VelocityY VelocityZ Pressure")
-            lines.append("        " + " ".join(repr(float(v)) for v in q))
-        elif bc in ("inflow_total_nscbc", "inflow_subsonic"):
-            t = total_inflow_values(spec)
-            lines.append(f"    {f + 1}    1    1    TotalPressure TotalTemperature VelocityDirX "
-                         "VelocityDirY VelocityDirZ")
-            lines.append("        " + " ".join(repr(float(v)) for v in t))
+    for f, fbc in enumerate(spec.bc):
+        if fbc == "periodic":
+            continue
+        for si, (_, bc, dat) in enumerate(spec.face_subfaces(f), start=1):
+            head = f"    {f + 1}    {si}    1    "
+            names = _DATA_NAMES.get(bc)
+            if dat is not None and names:
+                lines.append(head + " ".join(names))
+                lines.append("        " + " ".join(repr(float(v)) for v in dat))
+            elif bc == "outflow_nscbc":
+                lines.append(head + "Pressure")
+                lines.append(f"        {p_out!r}")
+            elif bc == "inflow_static_nscbc":
+                lines.append(head + "Density VelocityX VelocityY VelocityZ")
+                lines.append(f"        {rho_in!r} {vel_in[0]!r} {vel_in[1]!r} {vel_in[2]!r}")
+            elif bc == "outflow_subsonic":
+                lines.append(head + "Pressure")
+                lines.append(f"        {p_out!r}")
+            elif bc in ("wall_heat_flux", "wall_isothermal"):
+                val = spec.wall_data[f] if spec.wall_data else (
+                    0.0 if bc == "wall_heat_flux" else spec.t_inf)
+                name = "HeatFlux" if bc == "wall_heat_flux" else "Temperature"
+                lines.append(head + name)
+                lines.append(f"        {float(val)!r}")
+            elif bc == "inflow_supersonic":
+                q = spec.prescribed_super[f] if spec.prescribed_super else (rho_in, *vel_in, p_out)
+                lines.append(head + "Density VelocityX VelocityY VelocityZ Pressure")
+                lines.append("        " + " ".join(repr(float(v)) for v in q))
+            elif bc in ("inflow_total_nscbc", "inflow_subsonic"):
+                t = total_inflow_values(spec)
+                lines.append(head + "TotalPressure TotalTemperature VelocityDirX "
+                             "VelocityDirY VelocityDirZ")
+                lines.append("        " + " ".join(repr(float(v)) for v in t))
     presc = ""
     if lines:
         presc = "\nPrescribed boundary data\n" + "\n".join(lines) + "\n"
     return params, sponge, presc
+
+
+# Prescribed-data variable names of a subface's data tuple, per condition.
+_DATA_NAMES = {
+    "outflow_nscbc": ("Pressure",), "outflow_subsonic": ("Pressure",),
+    "inflow_static_nscbc": ("Density", "VelocityX", "VelocityY", "VelocityZ"),
+    "inflow_total_nscbc": ("TotalPressure", "TotalTemperature", "VelocityDirX", "VelocityDirY",
+                           "VelocityDirZ"),
+    "inflow_subsonic": ("TotalPressure", "TotalTemperature", "VelocityDirX", "VelocityDirY",
+                        "VelocityDirZ"),
+    "wall_heat_flux": ("HeatFlux",), "wall_isothermal": ("Temperature",),
+    "inflow_supersonic": ("Density", "VelocityX", "VelocityY", "VelocityZ", "Pressure"),
+}
 
 
 def total_inflow_values(spec: CaseSpec):

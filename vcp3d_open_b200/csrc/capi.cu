@@ -675,7 +675,16 @@ int vcpg_stats(vcpg_handle *h, int64_t *cg_iterations, int64_t *element_solves) 
 int vcpg_set_open_boundary(vcpg_handle *h, const vcpg_open_boundary *ob,
                            const vcpg_geometry *geom, int32_t p_grid, int32_t dof_location,
                            const double *grid_nodes) {
-  if (!h || !ob || !geom) return VCPG_E_INVALID;
+  return vcpg_set_open_boundary_subfaces(h, ob, nullptr, 0, geom, p_grid, dof_location,
+                                         grid_nodes);
+}
+
+int vcpg_set_open_boundary_subfaces(vcpg_handle *h, const vcpg_open_boundary *ob,
+                                    const vcpg_subface *subfaces, int32_t n_subfaces,
+                                    const vcpg_geometry *geom, int32_t p_grid,
+                                    int32_t dof_location, const double *grid_nodes) {
+  if (!h || !ob || !geom || n_subfaces < 0 || (n_subfaces > 0 && !subfaces))
+    return VCPG_E_INVALID;
   if (h->open) return Fail(h, VCPG_E_INVALID, "open boundaries are already configured");
   if (h->nOwned != h->nE)
     return Fail(h, VCPG_E_INVALID, "open boundaries: the block is partitioned");
@@ -683,7 +692,8 @@ int vcpg_set_open_boundary(vcpg_handle *h, const vcpg_open_boundary *ob,
     return Fail(h, VCPG_E_UNSUPPORTED_KM, "no open-boundary kernels for this degree");
   OpenBoundaryHost ob_host;
   std::string err;
-  int rc = BuildOpenBoundary(h->prm, *ob, *geom, p_grid, dof_location, grid_nodes, ob_host, err);
+  int rc = BuildOpenBoundary(h->prm, *ob, *geom, p_grid, dof_location, grid_nodes, ob_host, err,
+                             subfaces, n_subfaces);
   if (rc != VCPG_OK) return Fail(h, rc, err);
   const int M2 = h->M2, MD = h->MD;
   auto upload = [&](void **dst, const void *src, size_t bytes) -> int {

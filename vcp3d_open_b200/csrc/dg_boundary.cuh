@@ -138,9 +138,11 @@ __global__ void __launch_bounds__(NT) BoundaryTraceKernel(const BoundaryArgs a) 
   }
   __syncthreads();
   if (threadIdx.x == 0) {
+    // Only characteristic faces enter the boundary average (the weighted Mach
+    // number of the other subfaces is zero, SubfaceBaseClass::WeightedMachElement).
     double m = 0.0;
     for (int l = 0; l < M2; ++l) m += s_w[l];
-    a.bmach[b] = m;
+    a.bmach[b] = bf[kBfType] < VCPG_BC_WALL_HEAT_FLUX ? m : 0.0;
   }
 }
 
@@ -471,7 +473,7 @@ __global__ void __launch_bounds__(NT) BoundaryFluxKernel(const BoundaryArgs a) {
       // elimination in the order of the reference (E, F, G, H coefficients). The
       // eigenvalues use the unit normal here.
       const int iPsi = c.iPhi == 0 ? 4 : 0;
-      const double kk = -c.sigma / c.len;
+      const double kk = -c.inSigma / c.inLen;
       const double urn = u * rn[0] + v * rn[1] + w * rn[2];
       const double l1 = urn - aa, l3 = urn + aa;
       ov1 = 1.0 / l1;
@@ -536,8 +538,8 @@ __global__ void __launch_bounds__(NT) BoundaryFluxKernel(const BoundaryArgs a) {
       // BCInflowStaticCharacteristicSubfaceClass::ComputeBoundaryState
       // (src/BoundaryState.cpp:1579-1847).
       const double sign = (factNorm > 0.0) ? -1.0 : 1.0;
-      const double ka = sign * 0.5 * c.sigma * (1.0 - Mavg2) / c.len;
-      const double ku = c.sigma / c.len;
+      const double ka = sign * 0.5 * c.inSigma * (1.0 - Mavg2) / c.inLen;
+      const double ku = c.inSigma / c.inLen;
       const double ovlmb2 = 1.0 / ur;
       if (c.incoming) {
         LL[0] = 0.5 * lmb1 * (ovrhoa * dpdr - durdr);

@@ -170,17 +170,70 @@ static void WeakBoundaryData(int type, const vcpg_open_boundary &ob, int f,
 
 int BuildOpenBoundary(const vcpg_params &prm, const vcpg_open_boundary &ob,
                       const vcpg_geometry &geom, int pGrid, int dofLocation,
-                      const double *gridNodes, OpenBoundaryHost &out, std::string &err) {
+                      const double *gridNodes, OpenBoundaryHost &out, std::string &err,
+                      const vcpg_subface *subfaces, int nSubfaces) {
   try {
     const int K = prm.n_poly + 1, M = prm.n_int_1d, M2 = M * M, MD = M * M * M;
     const int nI = prm.n_elem[0], nJ = prm.n_elem[1], nK = prm.n_elem[2];
     const int64_t nE = (int64_t)nI * nJ * nK;
     if (!geom.face_metric || !geom.neighbors) { err = "geometry arrays missing"; return VCPG_E_INVALID; }
+    auto badBc = [](int bc) { return bc < VCPG_BC_NONE || bc > VCPG_BC_OUTFLOW_SUPERSONIC; };
     for (int f = 0; f < 6; ++f)
-      if (ob.bc[f] < VCPG_BC_NONE || ob.bc[f] > VCPG_BC_OUTFLOW_SUPERSONIC) {
+      if (badBc(ob.bc[f])) {
         err = "unknown boundary condition on face " + std::to_string(f);
         return VCPG_E_INVALID;
       }
+    // Subfaces: per subface a copy of ob carrying the subface's condition and
+    // prescribed data in its block face's slots, so that every element face reads
+    // its settings from one vcpg_open_boundary.
+    if (nSubfaces < 0 || (nSubfaces > 0 && !subfaces)) { err = "invalid subface list"; return VCPG_E_INVALID; }
+    std::vector<vcpg_open_boundary> subOb((size_t)nSubfaces, ob);
+    bool faceHasSub[6] = {false, false, false, false, false, false};
+    const int nIdx[3] = {nI, nJ, nK};
+    for (int s2 = 0; s2 < nSubfaces; ++s2) {
+      const vcpg_subface &sf = subfaces[s2];
+      if (sf.face < 0 || sf.face > 5 || badBc(sf.bc)) {
+        err = "subface " + std::to_string(s2) + ": invalid block face or boundary condition";
+        return VCPG_E_INVALID;
+      }
+      const int fd = sf.face / 2, a0 = fd == 0 ? 1 : 0, a1 = fd == 2 ? 1 : 2;
+      if (sf.elem_begin[0] < 0 || sf.elem_begin[1] < 0 || sf.elem_end[0] > nIdx[a0] ||
+          sf.elem_end[1] > nIdx[a1] || sf.elem_begin[0] >= sf.elem_end[0] ||
+          sf.elem_begin[1] >= sf.elem_end[1]) {
+        err = "subface " + std::to_string(s2) + ": element range outside its block face";
+        return VCPG_E_INVALID;
+      }
+      faceHasSub[sf.face] = true;
+      vcpg_open_boundary &o = subOb[s2];
+      const int f = sf.face;
+      o.bc[f] = sf.bc;
+      o.p_out[f] = sf.p_out;
+      for (int q = 0; q < 4; ++q) o.inflow[f][q] = sf.inflow[q];
+      for (int q = 0; q < 5; ++q) o.inflow_total[f][q] = sf.inflow_total[q];
+      o.wall_data[f] = sf.wall_data;
+      for (int q = 0; q < 5; ++q) o.inflow_super[f][q] = sf.inflow_super[q];
+    }
+    // The settings of element e's block face f: its subface's, or ob's.
+    auto settingsOf = [&](int64_t e, int f, std::string &why) -> const vcpg_open_boundary * {
+      if (!faceHasSub[f]) return &ob;
+      const int64_t idx[3] = {e % nI, (e / nI) % nJ, e / ((int64_t)nI * nJ)};
+      const int fd = f / 2, a0 = fd == 0 ? 1 : 0, a1 = fd == 2 ? 1 : 2;
+      const vcpg_open_boundary *hit = nullptr;
+      int hits = 0;
+      for (int s2 = 0; s2 < nSubfaces; ++s2) {
+        const vcpg_subface &sf = subfaces[s2];
+        if (sf.face != f) continue;
+        if (idx[a0] >= sf.elem_begin[0] && idx[a0] < sf.elem_end[0] &&
+            idx[a1] >= sf.elem_begin[1] && idx[a1] < sf.elem_end[1]) {
+          hit = &subOb[s2];
+          ++hits;
+        }
+      }
+      if (hits != 1)
+        why = "element " + std::to_string(e) + " face " + std::to_string(f) + " is covered by " +
+              std::to_string(hits) + " subfaces (exactly one expected)";
+      return hits == 1 ? hit : nullptr;
+    };
 
     // 1-D operators: Lagrange basis of the solution DOFs at the Gauss points, its
     // derivative at the DOFs, and the Lagrange derivative on the Gauss points.
@@ -237,36 +290,38 @@ int BuildOpenBoundary(const vcpg_params &prm, const vcpg_open_boundary &ob,
     for (int f = 0; f < 6; ++f) {
       BlockFaceCfg &c = out.cfg[f];
       c = BlockFaceCfg{};
-      c.type = ob.bc[f];
+      c.type = faceHasSub[f] ? -1 : ob.bc[f];
       c.first = out.nB;
       const double factNorm = (f % 2 == 0) ? -1.0 : 1.0;
       c.dell = factNorm * c0;
       c.iPhi = factNorm > 0.0 ? 0 : 4;
-      if (c.type == VCPG_BC_OUTFLOW_NSCBC) {
-        c.sigma = ob.outlet_sigma; c.len = ob.outlet_len;
-        c.betaL = ob.outlet_beta_l; c.betaT = ob.outlet_beta_t;
-        c.oneMinusBeta = ob.outlet_one_minus_beta ? 1 : 0;
-      } else if (c.type == VCPG_BC_INFLOW_STATIC_NSCBC || c.type == VCPG_BC_INFLOW_TOTAL_NSCBC) {
-        c.sigma = ob.inlet_sigma; c.len = ob.inlet_len;
-        c.incoming = ob.inlet_incoming ? 1 : 0;
-      }
-      if (c.type == VCPG_BC_INFLOW_TOTAL_NSCBC || c.type == VCPG_BC_INFLOW_SUBSONIC) {
-        const double *t = ob.inflow_total[f];
-        const double dl = std::sqrt(t[2] * t[2] + t[3] * t[3] + t[4] * t[4]);
-        if (!(t[0] > 0.0) || !(t[1] > 0.0) || !(dl > 0.0)) {
-          err = "total inflow needs a positive total pressure, total temperature and a "
-                "velocity direction on face " + std::to_string(f);
-          return VCPG_E_INVALID;
-        }
-      }
-      const bool weak = c.type >= VCPG_BC_WALL_HEAT_FLUX;
-      if (c.type != VCPG_BC_NONE && !weak && !(c.len > 0.0)) {
-        err = "characteristic length must be positive on face " + std::to_string(f);
-        return VCPG_E_INVALID;
-      }
+      c.sigma = ob.outlet_sigma; c.len = ob.outlet_len;
+      c.betaL = ob.outlet_beta_l; c.betaT = ob.outlet_beta_t;
+      c.oneMinusBeta = ob.outlet_one_minus_beta ? 1 : 0;
+      c.inSigma = ob.inlet_sigma; c.inLen = ob.inlet_len;
+      c.incoming = ob.inlet_incoming ? 1 : 0;
       for (int64_t e = 0; e < nE; ++e) {
         if (geom.neighbors[e * 6 + f] >= 0) continue;
-        if (c.type == VCPG_BC_NONE) continue;  // stays -1: flagged by the residual kernel
+        std::string why;
+        const vcpg_open_boundary *o = settingsOf(e, f, why);
+        if (!o) { err = why; return VCPG_E_INVALID; }
+        const int type = o->bc[f];
+        if (type == VCPG_BC_NONE) continue;  // stays -1: flagged by the residual kernel
+        if (type == VCPG_BC_INFLOW_TOTAL_NSCBC || type == VCPG_BC_INFLOW_SUBSONIC) {
+          const double *t = o->inflow_total[f];
+          const double dl = std::sqrt(t[2] * t[2] + t[3] * t[3] + t[4] * t[4]);
+          if (!(t[0] > 0.0) || !(t[1] > 0.0) || !(dl > 0.0)) {
+            err = "total inflow needs a positive total pressure, total temperature and a "
+                  "velocity direction on face " + std::to_string(f);
+            return VCPG_E_INVALID;
+          }
+        }
+        const bool weak = type >= VCPG_BC_WALL_HEAT_FLUX;
+        const double len = type == VCPG_BC_OUTFLOW_NSCBC ? c.len : c.inLen;
+        if (!weak && !(len > 0.0)) {
+          err = "characteristic length must be positive on face " + std::to_string(f);
+          return VCPG_E_INVALID;
+        }
         const double *fm = geom.face_metric + ((size_t)e * 6 + f) * 13 * M2;
         const int fd = f / 2;
         int grad[3] = {fd, fd == 0 ? 1 : 0, fd == 2 ? 1 : 2};
@@ -277,21 +332,21 @@ int BuildOpenBoundary(const vcpg_params &prm, const vcpg_open_boundary &ob,
           return VCPG_E_INVALID;
         }
         const int b = out.nB++;
-        int row[kBfStride] = {(int)e, f, c.type, grad[0], grad[1], grad[2], 0, 0};
+        int row[kBfStride] = {(int)e, f, type, grad[0], grad[1], grad[2], 0, 0};
         out.bface.insert(out.bface.end(), row, row + kBfStride);
         double pres[kPrescStride] = {0.0, 0.0, 0.0, 0.0, 0.0};
-        if (c.type == VCPG_BC_OUTFLOW_NSCBC) {
-          pres[0] = ob.p_out[f] / prm.p_ref;
-        } else if (c.type == VCPG_BC_INFLOW_STATIC_NSCBC) {
-          pres[0] = ob.inflow[f][0] / prm.rho_ref;
-          pres[1] = ob.inflow[f][1] / prm.u_ref;
-          pres[2] = ob.inflow[f][2] / prm.u_ref;
-          pres[3] = ob.inflow[f][3] / prm.u_ref;
-        } else if (c.type == VCPG_BC_INFLOW_TOTAL_NSCBC) {
+        if (type == VCPG_BC_OUTFLOW_NSCBC) {
+          pres[0] = o->p_out[f] / prm.p_ref;
+        } else if (type == VCPG_BC_INFLOW_STATIC_NSCBC) {
+          pres[0] = o->inflow[f][0] / prm.rho_ref;
+          pres[1] = o->inflow[f][1] / prm.u_ref;
+          pres[2] = o->inflow[f][2] / prm.u_ref;
+          pres[3] = o->inflow[f][3] / prm.u_ref;
+        } else if (type == VCPG_BC_INFLOW_TOTAL_NSCBC) {
           // BCInflowTotalCharacteristicSubfaceClass::ConvertPrescribedData
           // (src/SubfaceClasses.cpp:1577-1608): p_t / p_ref, T_t / (p_ref / rho_ref)
           // (the gas constant stays in the boundary formulas), unit direction.
-          const double *t = ob.inflow_total[f];
+          const double *t = o->inflow_total[f];
           const double dl = std::sqrt(t[2] * t[2] + t[3] * t[3] + t[4] * t[4]);
           pres[0] = t[0] / prm.p_ref;
           pres[1] = t[1] / (prm.p_ref / prm.rho_ref);
@@ -299,7 +354,7 @@ int BuildOpenBoundary(const vcpg_params &prm, const vcpg_open_boundary &ob,
           pres[3] = t[3] / dl;
           pres[4] = t[4] / dl;
         } else {
-          WeakBoundaryData(c.type, ob, f, prm, pres);
+          WeakBoundaryData(type, *o, f, prm, pres);
         }
         out.bpresc.insert(out.bpresc.end(), pres, pres + kPrescStride);
         out.nbrCode[e * 6 + f] = -2 - b;

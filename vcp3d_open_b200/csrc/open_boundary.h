@@ -11,17 +11,21 @@
 
 namespace vcpg {
 
-// Per block face (0 iMin .. 5 kMax) settings of a characteristic boundary.
+// Per block face (0 iMin .. 5 kMax) settings of the characteristic boundaries
+// on it (the element faces' conditions are in the boundary-face list; a block
+// face with several subfaces may hold outlets and inlets).
 struct BlockFaceCfg {
-  int type;            // enum vcpg_bc
+  int type;            // enum vcpg_bc of the whole face, -1 with several conditions
   int first, count;    // range of this block face's entries in the boundary-face list
   int iPhi;            // index of the incoming acoustic wave amplitude (0 or 4)
   int oneMinusBeta;    // outlet: transverse terms weighted by (1 - beta)
   int incoming;        // inlet: keep the outgoing acoustic amplitudes of the interior
   double dell;         // factNorm * (-dL_0(r_0)): Lagrange derivative at the boundary DOF
-  double area;         // sum of w * area over the block face (SolverClass::InitNSCBC)
-  double sigma, len;   // normal relaxation coefficient and characteristic length
+  double area;         // sum of w * area over the block face's physical element faces
+                       // (SolverClass::InitNSCBC)
+  double sigma, len;   // outlet: normal relaxation coefficient and characteristic length
   double betaL, betaT; // outlet transverse relaxation coefficients
+  double inSigma, inLen;  // inlet: normal relaxation coefficient and characteristic length
 };
 
 // Entries of one boundary face in the boundary-face list (ints).
@@ -56,9 +60,11 @@ struct OpenBoundaryHost {
   int cmlOn = 0;
 };
 
-// Builds the open-boundary data of a block. Returns a vcpg status and sets err.
+// Builds the open-boundary data of a block (optionally with several subfaces
+// per block face, vcpg_subface). Returns a vcpg status and sets err.
 int BuildOpenBoundary(const vcpg_params &prm, const vcpg_open_boundary &ob,
                       const vcpg_geometry &geom, int pGrid, int dofLocation,
-                      const double *gridNodes, OpenBoundaryHost &out, std::string &err);
+                      const double *gridNodes, OpenBoundaryHost &out, std::string &err,
+                      const vcpg_subface *subfaces = nullptr, int nSubfaces = 0);
 
 }  // namespace vcpg

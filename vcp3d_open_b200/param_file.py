@@ -547,11 +547,13 @@ def check_supported(pf: ParamFile) -> None:
     if pf.outlet_local_mach:
         raise UnsupportedOption("Outlet use local (element) averaged Mach number")
     for face, subs in enumerate(pf.subfaces):
-        if len(subs) != 1:
-            raise UnsupportedOption(f"face {face + 1}: {len(subs)} subfaces (one per face runs)")
-        if subs[0].kind not in _BC_TO_CASE:
-            why = _WHY_NOT.get(subs[0].kind, subs[0].bc)
-            raise UnsupportedOption(f"face {face + 1}: boundary condition {why}")
+        for sub in subs:
+            if sub.kind not in _BC_TO_CASE:
+                why = _WHY_NOT.get(sub.kind, sub.bc)
+                raise UnsupportedOption(f"face {face + 1}: boundary condition {why}")
+        if len(subs) > 1 and any(sub.kind == "periodic1to1trans" for sub in subs):
+            raise UnsupportedOption(f"face {face + 1}: a periodic subface beside others "
+                                    "(periodic connections cover whole faces here)")
     for d in range(3):
         a, b = pf.subfaces[2 * d][0].kind, pf.subfaces[2 * d + 1][0].kind
         if (a == "periodic1to1trans") != (b == "periodic1to1trans"):
@@ -566,41 +568,77 @@ def n_elements(pf: ParamFile) -> Tuple[int, int, int]:
 
 
 def case_bcs(pf: ParamFile) -> Tuple[str, ...]:
+    """The condition of each block face (its first subface's)."""
     return tuple(_BC_TO_CASE[pf.subfaces[f][0].kind] for f in range(6))
 
 
-def outflow_pressure(pf: ParamFile, face: int) -> float:
-    return _need(pf, face, ("Pressure",), pf.subfaces[face][0].bc)[0]
+def subface_data(pf: ParamFile, face: int, sub: int, bc: str) -> Tuple[float, ...]:
+    """Prescribed data of one subface as the data tuple of a case subface."""
+    if bc in ("outflow_nscbc", "outflow_subsonic"):
+        return (outflow_pressure(pf, face, sub),)
+    if bc == "inflow_static_nscbc":
+        return inflow_static(pf, face, sub)
+    if bc in ("inflow_total_nscbc", "inflow_subsonic"):
+        return inflow_total(pf, face, sub)
+    if bc in ("wall_heat_flux", "wall_isothermal"):
+        return (wall_value(pf, face, sub),)
+    if bc == "inflow_supersonic":
+        return inflow_supersonic(pf, face, sub)
+    return ()
 
 
-def _need(pf: ParamFile, face: int, names: Sequence[str], what: str) -> Tuple[float, ...]:
-    data = pf.prescribed.get((face, 0), {})
+def case_subfaces(pf: ParamFile):
+    """Subfaces of the block faces that have more than one, as case subfaces
+    (face, element range, condition, data): the node-index ranges of the file
+    (1-based) give the elements [min - 1, max - 1) of each in-plane direction
+    (SolverClass, src/SolverClass.cpp:1640-1660). None when every face has one."""
+    out = []
+    for face, subs in enumerate(pf.subfaces):
+        if len(subs) < 2:
+            continue
+        d = face // 2
+        a0, a1 = (1, 2) if d == 0 else ((0, 2) if d == 1 else (0, 1))
+        for si, sub in enumerate(subs):
+            lo = [min(sub.own[2 * a], sub.own[2 * a + 1]) - 1 for a in (a0, a1)]
+            hi = [max(sub.own[2 * a], sub.own[2 * a + 1]) - 1 for a in (a0, a1)]
+            bc = _BC_TO_CASE[sub.kind]
+            out.append((face, (lo[0], hi[0], lo[1], hi[1]), bc, subface_data(pf, face, si, bc)))
+    return tuple(out) if out else None
+
+
+def outflow_pressure(pf: ParamFile, face: int, sub: int = 0) -> float:
+    return _need(pf, face, ("Pressure",), pf.subfaces[face][sub].bc, sub)[0]
+
+
+def _need(pf: ParamFile, face: int, names: Sequence[str], what: str,
+          sub: int = 0) -> Tuple[float, ...]:
+    data = pf.prescribed.get((face, sub), {})
     if not all(nm in data for nm in names):
-        raise ParamFileError(f"face {face + 1}: {what} needs the prescribed data "
-                             + ", ".join(names))
+        raise ParamFileError(f"face {face + 1} subface {sub + 1}: {what} needs the prescribed "
+                             "data " + ", ".join(names))
     return tuple(data[nm] for nm in names)
 
 
-def inflow_total(pf: ParamFile, face: int) -> Tuple[float, float, float, float, float]:
+def inflow_total(pf: ParamFile, face: int, sub: int = 0) -> Tuple[float, float, float, float, float]:
     """Total conditions of BCInflowTotalNSCBC or BCInflowSubsonic (the latter's
     density/velocity data set is not run: its boundary state uses the totals)."""
     return _need(pf, face, ("TotalPressure", "TotalTemperature", "VelocityDirX",
-                            "VelocityDirY", "VelocityDirZ"), pf.subfaces[face][0].bc)
+                            "VelocityDirY", "VelocityDirZ"), pf.subfaces[face][sub].bc, sub)
 
 
-def wall_value(pf: ParamFile, face: int) -> float:
-    kind = pf.subfaces[face][0].kind
+def wall_value(pf: ParamFile, face: int, sub: int = 0) -> float:
+    kind = pf.subfaces[face][sub].kind
     name = "HeatFlux" if kind == "bcwallheatflux" else "Temperature"
-    return _need(pf, face, (name,), pf.subfaces[face][0].bc)[0]
+    return _need(pf, face, (name,), pf.subfaces[face][sub].bc, sub)[0]
 
 
-def inflow_supersonic(pf: ParamFile, face: int) -> Tuple[float, ...]:
+def inflow_supersonic(pf: ParamFile, face: int, sub: int = 0) -> Tuple[float, ...]:
     return _need(pf, face, ("Density", "VelocityX", "VelocityY", "VelocityZ", "Pressure"),
-                 "BCInflowSupersonic")
+                 "BCInflowSupersonic", sub)
 
 
-def inflow_static(pf: ParamFile, face: int) -> Tuple[float, float, float, float]:
-    data = pf.prescribed.get((face, 0), {})
+def inflow_static(pf: ParamFile, face: int, sub: int = 0) -> Tuple[float, float, float, float]:
+    data = pf.prescribed.get((face, sub), {})
     names = ("Density", "VelocityX", "VelocityY", "VelocityZ")
     if not all(nm in data for nm in names):
         raise ParamFileError(f"face {face + 1}: BCInflowStaticNSCBC needs Density and "

@@ -12,6 +12,7 @@ time-to-completion (arrival -> result on the host) beside the aggregate
 DOF-updates/s.
 
     python -m vcp3d_open_b200.serving [--cases 256] [--steps 300] [--precision mixed]
+    python -m vcp3d_open_b200.serving --cases 128 --offered-load 0.5,0.8,0.95
 """
 from __future__ import annotations
 
@@ -346,6 +347,38 @@ def serve(requests: List[Request], ens: Ensemble, prepare_workers: int = 8,
     return out
 
 
+def offered_load_sweep(requests: List[Request], loads: List[float], caps: Dict[int, tuple],
+                       precision: int, max_cases: int, workers: int) -> dict:
+    """Latency against offered load. The capacity C (DOF-updates/s) is measured
+    first with every request arriving at t = 0 (the GPU never idles); then for
+    each offered load rho the same requests arrive in the same order with their
+    inter-arrival times scaled so that the stream offers rho C on average
+    (mean inter-arrival = total work / (cases rho C)). Below capacity the
+    latency reflects admission and co-scheduling rather than a backlog."""
+    work = float(sum(r.spec.n_dofs * r.steps for r in requests))
+    t_last = max(r.arrival for r in requests)
+    rows = []
+
+    def one(reqs):
+        ens = Ensemble(caps, precision=precision, max_cases=max_cases)
+        try:
+            return serve(reqs, ens, prepare_workers=workers)
+        finally:
+            ens.close()
+
+    rep = one([dataclasses.replace(r, arrival=0.0) for r in requests])
+    cap = rep["dof_updates_per_s"]
+    rows.append(dict(rep, offered_load=None, mean_interarrival_s=0.0))
+    for rho in loads:
+        mean_ia = work / (len(requests) * rho * cap)
+        scale = mean_ia * len(requests) / t_last   # t_last ~ n * mean of the unscaled stream
+        reqs = [dataclasses.replace(r, arrival=r.arrival * scale) for r in requests]
+        rep = one(reqs)
+        rows.append(dict(rep, offered_load=rho, mean_interarrival_s=mean_ia,
+                         last_arrival_s=max(r.arrival for r in reqs)))
+    return {"capacity_dof_updates_per_s": cap, "total_dof_updates": work, "rows": rows}
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--cases", type=int, default=256)
@@ -357,11 +390,26 @@ def main(argv=None) -> int:
     ap.add_argument("--max-cases", type=int, default=8,
                     help="case slots per degree bucket: the cases stepped together")
     ap.add_argument("--progress", type=float, default=0.0, help="seconds between progress lines")
+    ap.add_argument("--offered-load", default=None,
+                    help="comma-separated fractions of the measured capacity: sweep the "
+                         "arrival rate (offered_load_sweep) instead of one run")
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
     reqs = request_stream(a.cases, a.seed, steps=a.steps)
     caps = plan_capacities(reqs, int(a.budget_gb * 1e9))
     prec = capi.MIXED if a.precision == "mixed" else capi.FP64
+    if a.offered_load:
+        loads = [float(x) for x in a.offered_load.split(",")]
+        rep = offered_load_sweep(reqs, loads, caps, prec, a.max_cases, a.workers)
+        rep.update({"precision": a.precision, "steps_per_case": a.steps, "seed": a.seed,
+                    "cases": a.cases, "max_cases_per_bucket": a.max_cases,
+                    "capacities": {str(k): list(v) for k, v in caps.items()}})
+        line = json.dumps(rep)
+        print(line)
+        if a.out:
+            with open(a.out, "w") as f:
+                f.write(line + "\n")
+        return 0
     ens = Ensemble(caps, precision=prec, max_cases=a.max_cases)
     rep = serve(reqs, ens, prepare_workers=a.workers, progress_every=a.progress)
     rep.update({"precision": a.precision, "steps_per_case": a.steps, "seed": a.seed,

@@ -68,7 +68,8 @@ def make_params(case: CaseData, metric_compat: bool = True,
     p.sgs_model = SGS_CODES[s.sgs.lower()]
     # The reference monitors forces only where wall faces exist
     # (src/InputParamClass.cpp:1574-1575).
-    walls = any(b.startswith("wall_") for b in s.bc)
+    walls = any(b.startswith("wall_") for b in s.bc) or any(
+        e[2].startswith("wall_") for e in (s.subfaces or ()))
     p.monitor_forces = 1 if (s.monitor_forces and walls) else 0
     p.mach, p.ref_area = s.mach, s.ref_area
     if s.body_force is not None:
@@ -141,39 +142,50 @@ def nodal_to_modal(case: CaseData, params: capi.Params) -> np.ndarray:
     return out
 
 
+BC_CODES = {"periodic": capi.BC_NONE, "outflow_nscbc": capi.BC_OUTFLOW_NSCBC,
+            "inflow_static_nscbc": capi.BC_INFLOW_STATIC_NSCBC,
+            "inflow_total_nscbc": capi.BC_INFLOW_TOTAL_NSCBC,
+            "wall_heat_flux": capi.BC_WALL_HEAT_FLUX, "wall_isothermal": capi.BC_WALL_ISOTHERMAL,
+            "wall_inviscid": capi.BC_WALL_INVISCID, "farfield": capi.BC_FARFIELD,
+            "inflow_subsonic": capi.BC_INFLOW_SUBSONIC,
+            "inflow_supersonic": capi.BC_INFLOW_SUPERSONIC,
+            "outflow_subsonic": capi.BC_OUTFLOW_SUBSONIC,
+            "outflow_supersonic": capi.BC_OUTFLOW_SUPERSONIC}
+
+
+def _face_data(s, f: int, bc: str, p_out, rho_in, vel_in):
+    """Prescribed data of condition bc on block face f (dimensional): outflow
+    pressure, static inflow (rho, u, v, w), total inflow, wall value, supersonic
+    inflow state."""
+    from .cases import total_inflow_values
+    po = s.prescribed_p[f] if s.prescribed_p else p_out
+    inflow = tuple(s.prescribed_inflow[f]) if s.prescribed_inflow else (rho_in, *vel_in)
+    total = ((s.prescribed_total[f] if s.prescribed_total else total_inflow_values(s))
+             if bc in ("inflow_total_nscbc", "inflow_subsonic") else (0.0,) * 5)
+    wall = ((s.wall_data[f] if s.wall_data else (0.0 if bc == "wall_heat_flux" else s.t_inf))
+            if bc in ("wall_heat_flux", "wall_isothermal") else 0.0)
+    sup = ((s.prescribed_super[f] if s.prescribed_super else (rho_in, *vel_in, p_out))
+           if bc == "inflow_supersonic" else (0.0,) * 5)
+    return po, inflow, total, wall, sup
+
+
 def open_boundary(case: CaseData) -> capi.OpenBoundary:
     """vcpg_open_boundary of a case: its boundary conditions with the free stream
     as prescribed data, NSCBC tuning parameters, sponge layers and matching layer."""
-    from .cases import free_stream_values, prescribed_values, total_inflow_values
+    from .cases import free_stream_values, prescribed_values
     s, ref = case.spec, case.ref
     ob = capi.OpenBoundary()
-    codes = {"periodic": capi.BC_NONE, "outflow_nscbc": capi.BC_OUTFLOW_NSCBC,
-             "inflow_static_nscbc": capi.BC_INFLOW_STATIC_NSCBC,
-             "inflow_total_nscbc": capi.BC_INFLOW_TOTAL_NSCBC,
-             "wall_heat_flux": capi.BC_WALL_HEAT_FLUX, "wall_isothermal": capi.BC_WALL_ISOTHERMAL,
-             "wall_inviscid": capi.BC_WALL_INVISCID, "farfield": capi.BC_FARFIELD,
-             "inflow_subsonic": capi.BC_INFLOW_SUBSONIC,
-             "inflow_supersonic": capi.BC_INFLOW_SUPERSONIC,
-             "outflow_subsonic": capi.BC_OUTFLOW_SUBSONIC,
-             "outflow_supersonic": capi.BC_OUTFLOW_SUPERSONIC}
     p_out, rho_in, vel_in = prescribed_values(s, ref)
     per_face = lambda v, f: v[f] if isinstance(v, (tuple, list)) else v
     for f, bc in enumerate(s.bc):
-        ob.bc[f] = codes[bc]
-        ob.p_out[f] = s.prescribed_p[f] if s.prescribed_p else p_out
-        inflow = s.prescribed_inflow[f] if s.prescribed_inflow else (rho_in, *vel_in)
+        ob.bc[f] = BC_CODES[bc]
+        po, inflow, total, wall, sup = _face_data(s, f, bc, p_out, rho_in, vel_in)
+        ob.p_out[f] = po
         ob.inflow[f][0], ob.inflow[f][1], ob.inflow[f][2], ob.inflow[f][3] = inflow
-        if bc in ("inflow_total_nscbc", "inflow_subsonic"):
-            total = s.prescribed_total[f] if s.prescribed_total else total_inflow_values(s)
-            for q in range(5):
-                ob.inflow_total[f][q] = total[q]
-        if bc in ("wall_heat_flux", "wall_isothermal"):
-            ob.wall_data[f] = (s.wall_data[f] if s.wall_data else
-                               (0.0 if bc == "wall_heat_flux" else s.t_inf))
-        if bc == "inflow_supersonic":
-            sup = s.prescribed_super[f] if s.prescribed_super else (rho_in, *vel_in, p_out)
-            for q in range(5):
-                ob.inflow_super[f][q] = sup[q]
+        for q in range(5):
+            ob.inflow_total[f][q] = total[q]
+            ob.inflow_super[f][q] = sup[q]
+        ob.wall_data[f] = wall
         ob.sponge_elems[f] = s.sponge[f]
         ob.sponge_sigma[f] = per_face(s.sponge_sigma, f)
         ob.sponge_alpha[f] = per_face(s.sponge_alpha, f)
@@ -187,6 +199,38 @@ def open_boundary(case: CaseData) -> capi.OpenBoundary:
                           [rho_in, vel_in[0], vel_in[1], vel_in[2], p_out])
     ob.free_stream[:] = list(s.free_stream if s.free_stream else free_stream_values(s))
     return ob
+
+
+def subfaces(case: CaseData):
+    """vcpg_subface array of a case with several subfaces per block face (None
+    without): each subface with its condition and its block face's data."""
+    from .cases import prescribed_values
+    s = case.spec
+    if not s.subfaces:
+        return None
+    p_out, rho_in, vel_in = prescribed_values(s, case.ref)
+    arr = (capi.Subface * len(s.subfaces))()
+    for i, (f, (b0, e0, b1, e1), bc, dat) in enumerate(s.subfaces):
+        sf = arr[i]
+        sf.face, sf.bc = f, BC_CODES[bc]
+        sf.elem_begin[0], sf.elem_end[0], sf.elem_begin[1], sf.elem_end[1] = b0, e0, b1, e1
+        po, inflow, total, wall, sup = _face_data(s, f, bc, p_out, rho_in, vel_in)
+        if dat is not None:       # the subface's own prescribed data
+            if bc in ("outflow_nscbc", "outflow_subsonic"):
+                po = dat[0]
+            elif bc == "inflow_static_nscbc":
+                inflow = tuple(dat)
+            elif bc in ("inflow_total_nscbc", "inflow_subsonic"):
+                total = tuple(dat)
+            elif bc in ("wall_heat_flux", "wall_isothermal"):
+                wall = dat[0]
+            elif bc == "inflow_supersonic":
+                sup = tuple(dat)
+        sf.p_out, sf.wall_data = po, wall
+        sf.inflow[:] = list(inflow)
+        sf.inflow_total[:] = list(total)
+        sf.inflow_super[:] = list(sup)
+    return arr
 
 
 class Solver:
@@ -224,10 +268,12 @@ class Solver:
         self._keep_ob = (ob, np.ascontiguousarray(case.elem_nodes, dtype=np.float64))
         geom = capi.Geometry(capi.ptr(self._keep[7]), capi.ptr(self._keep[8]),
                              capi.ptr(self._keep[9]), capi.ptr(self._keep[10]))
-        self._check(self.lib.vcpg_set_open_boundary(self.h, C.byref(ob), C.byref(geom),
-                                                     case.spec.p_grid, self.disc.dof_location,
-                                                     capi.ptr(self._keep_ob[1])),
-                    "set_open_boundary")
+        sfs = subfaces(case)
+        self._keep_sf = sfs
+        self._check(self.lib.vcpg_set_open_boundary_subfaces(
+            self.h, C.byref(ob), sfs, len(sfs) if sfs is not None else 0, C.byref(geom),
+            case.spec.p_grid, self.disc.dof_location, capi.ptr(self._keep_ob[1])),
+            "set_open_boundary")
 
     def _check(self, rc: int, what: str):
         if rc != capi.VCPG_OK:
