@@ -231,8 +231,8 @@ void *vcpg_stream(vcpg_handle *h);
  * [0, n_owned) owned: residual, time step (local minimum) and stages run on
  * them. Elements [n_owned, n_owned + n_face_ghost) are ghosts whose Min faces
  * towards owned elements are evaluated here (their other lower neighbours -1);
- * the remaining elements are ghosts that only provide their state. Periodic
- * blocks only (open boundaries are rejected); vcpg_step and
+ * the remaining elements are ghosts that only provide their state. Open
+ * boundaries of a partitioned block: vcpg_set_open_boundary_partition; vcpg_step and
  * vcpg_synchronization_step are rejected, a step being: vcpg_time_step, the
  * minimum over ranks, then per stage vcpg_rk_stage, the exchange of the ghost
  * states (vcpg_pack_states / vcpg_unpack_states around the transport) and
@@ -411,6 +411,47 @@ int vcpg_set_open_boundary_subfaces(vcpg_handle *h, const vcpg_open_boundary *ob
                                     const vcpg_subface *subfaces, int32_t n_subfaces,
                                     const vcpg_geometry *geom, int32_t p_grid,
                                     int32_t dof_location, const double *grid_nodes);
+
+/* Open boundaries of a partitioned block (after vcpg_set_partition): the
+ * set-up of the whole block (ob and the subfaces as for
+ * vcpg_set_open_boundary_subfaces; block_n_elem, block_geom and
+ * block_grid_nodes describe the whole block), of which the handle keeps the
+ * boundary faces and sponge elements of its owned elements. local_to_global
+ * gives the block index of each of the handle's elements. Boundary areas and
+ * sponge extents are those of the whole block, as the reference's rank sums
+ * and minima / maxima make them (src/SolverClass.cpp:2478-2481,
+ * src/SpongeLayer.cpp:135-136). The boundary-averaged Mach number spans the
+ * ranks: before each residual the caller gathers every rank's
+ * vcpg_boundary_mach_weights, sums each block face's weights in block element
+ * order (rank order along k) and passes the sums to
+ * vcpg_set_boundary_mach_sums (src/SolverClass.cpp:2556-2560). */
+int vcpg_set_open_boundary_partition(vcpg_handle *h, const vcpg_open_boundary *ob,
+                                     const vcpg_subface *subfaces, int32_t n_subfaces,
+                                     const int32_t *block_n_elem, const vcpg_geometry *block_geom,
+                                     int32_t p_grid, int32_t dof_location,
+                                     const double *block_grid_nodes,
+                                     const int64_t *local_to_global);
+
+/* The area-weighted projected Mach numbers of the handle's characteristic
+ * boundary faces for its current state (ElementClass::AverageMachNSCBC,
+ * src/ElementClass.cpp:357-509; zero on other boundary faces), in the handle's
+ * boundary-face order: counts[f] faces of block face f, f = 0..5 in turn;
+ * weights needs their total. Synchronises the handle's stream. */
+int vcpg_boundary_mach_weights(vcpg_handle *h, double *weights, int32_t *counts);
+
+/* Per block face, the sum of the Mach weights over the whole block, which the
+ * next residuals divide by the block face's area in place of summing the
+ * handle's own faces; NULL returns to the handle's own sums. */
+int vcpg_set_boundary_mach_sums(vcpg_handle *h, const double *sums);
+
+/* A residual of a partitioned handle in two parts, so that the halo exchange
+ * can run meanwhile: part 0 needs no ghost state (the boundary kernels, the
+ * face fluxes of the owned layers above the first, the residuals of the layers
+ * between the first and the last); part 1, after the ghost layers are
+ * unpacked, completes the residual (the first layer's and the upper ghost
+ * layer's face fluxes, the first and the last layer's residuals). Part 0 then
+ * part 1 equals vcpg_residual without monitoring data. */
+int vcpg_residual_part(vcpg_handle *h, int32_t part);
 
 /* ------------------------------------------------------------------------- */
 /* Served ensemble: many cases resident on one GPU, batched by degree.        */

@@ -56,6 +56,52 @@ def test_slab_split_and_limits():
     wall[0, 4] = -1
     with pytest.raises(ValueError, match="periodic in k"):
         partition.local_neighbors(partition.slabs((3, 2, 5), 2)[0], wall)
+    inner = np.array(disc.neighbors)
+    inner[7, 4] = inner[7, 5] = -1       # element 7 lies in layer 1, inside the block
+    with pytest.raises(ValueError, match="inside the block"):
+        partition.local_neighbors(partition.slabs((3, 2, 5), 2, periodic_k=False)[0], inner)
+
+
+@pytest.mark.parametrize("world", [1, 2, 3])
+def test_local_tables_with_open_faces(world):
+    """A block with boundary faces in i and k (not periodic there): boundary
+    faces stay -1, the first slab has no lower and the last no upper exchange."""
+    n_elem = (3, 2, 5)
+    spec = cases.CaseSpec(name="open", kind="pulse", n_elem=n_elem, p=2, hi=(3.0, 2.0, 5.0),
+                          mach=0.3, grid_map="none", center=(1.5, 1.0, 2.5),
+                          bc=("inflow_static_nscbc", "outflow_nscbc", "periodic", "periodic",
+                              "inflow_static_nscbc", "outflow_nscbc"))
+    case = cases.build_case(spec)
+    prm = solver.make_params(case)
+    nbr = solver.setup_discretization(case, prm).neighbors
+    for sl in partition.slabs(n_elem, world, periodic_k=False):
+        ln = partition.local_neighbors(sl, nbr)
+        l2g = sl.local_to_global()
+        own = l2g[:sl.n_owned]
+        for f in range(6):
+            want = nbr[own, f]
+            got = ln[:sl.n_owned, f]
+            assert np.array_equal(got < 0, want < 0)
+            assert np.array_equal(l2g[got[got >= 0]], want[want >= 0])
+        assert sl.has_down == (sl.rank > 0) and sl.has_up == (sl.rank < world - 1)
+        up = slice(sl.upper_ghost, sl.upper_ghost + sl.layer)
+        assert np.all(ln[up, 4] == (-1 if not sl.has_up else ln[up, 4]))
+        assert np.all(ln[up][:, [0, 1, 2, 3, 5]] == -1)
+
+
+def test_block_mach_sums_in_block_order():
+    """The slabs' per-face weights summed one after the other in rank order is
+    the sequential sum over the block's list."""
+    rng = np.random.default_rng(4)
+    block = [rng.standard_normal(n) for n in (7, 0, 5, 5, 3, 0)]
+    cuts = [(0, 3, 7), (0, 0, 0), (0, 2, 5), (0, 4, 5), (0, 0, 3), (0, 0, 0)]
+    ranks = [[block[f][c[r]:c[r + 1]] for f, c in enumerate(cuts)] for r in range(2)]
+    got = partition.block_mach_sums(ranks)
+    for f in range(6):
+        m = 0.0
+        for x in block[f]:
+            m += float(x)
+        assert got[f] == m
 
 
 class HostShard:
@@ -81,7 +127,7 @@ class HostShard:
         pass
 
 
-def _rank_main(rank, world, port, n_elem, out):
+def _rank_main(rank, world, port, n_elem, out, periodic_k=True):
     import torch.distributed as dist
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world)
@@ -89,11 +135,17 @@ def _rank_main(rank, world, port, n_elem, out):
         kd5 = 7
         rng = np.random.default_rng(3)
         block = rng.standard_normal((int(np.prod(n_elem)), kd5))
-        sl = partition.slabs(n_elem, world)[rank]
+        sl = partition.slabs(n_elem, world, periodic_k=periodic_k)[rank]
         sh = HostShard(sl, kd5, block)
         t = partition.DistTransport(sh)
         t.exchange()
-        ok = np.array_equal(sh.state, block[sl.local_to_global()])
+        want = block[sl.local_to_global()].copy()
+        if not sl.has_up:     # no slab above: that ghost layer stays as it was
+            want[sl.upper_ghost:sl.upper_ghost + sl.layer] = 0.0
+        if not sl.has_down:
+            want[sl.lower_ghost:sl.lower_ghost + sl.layer] = 0.0
+        ok = np.array_equal(sh.state, want)
+        ok = ok and t.gather([rank * 10])[:world] == [r * 10 for r in range(world)]
         lo = t.reduce([float(rank) + 0.5, 10.0], "min")
         hi = t.reduce([-1.0, float(rank)], "max")
         out.put((rank, ok, lo, hi))
@@ -107,14 +159,15 @@ def _free_port():
         return s.getsockname()[1]
 
 
+@pytest.mark.parametrize("periodic_k", [True, False])
 @pytest.mark.parametrize("world", [2, 3])
-def test_exchange_over_gloo(world):
+def test_exchange_over_gloo(world, periodic_k):
     import torch.multiprocessing as mp
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
     n_elem = (2, 3, 4)
-    procs = [ctx.Process(target=_rank_main, args=(r, world, port, n_elem, q))
+    procs = [ctx.Process(target=_rank_main, args=(r, world, port, n_elem, q, periodic_k))
              for r in range(world)]
     for p in procs:
         p.start()

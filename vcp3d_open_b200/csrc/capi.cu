@@ -26,6 +26,7 @@ struct vcpg_handle {
   // Partition (vcpg_set_partition): residual, time step and stages run on the
   // first nOwned elements, face fluxes on the first nFace; both nE otherwise.
   int64_t nOwned = 0, nFace = 0;
+  int64_t layer = 0;   // elements per ghost layer (n_face_ghost of vcpg_set_partition)
   cudaStream_t stream = nullptr;
   double *d_sol = nullptr, *d_solOld = nullptr, *d_res = nullptr, *d_resRaw = nullptr;
   double *d_vol = nullptr, *d_face = nullptr, *d_sc = nullptr;
@@ -58,6 +59,9 @@ struct vcpg_handle {
   double *d_dampfn = nullptr, *d_dampst = nullptr, *d_cml = nullptr;
   int cml_on = 0;
   BlockFaceCfg cfg[6] = {};
+  // Block-wide Mach sums per block face (vcpg_set_boundary_mach_sums).
+  double *d_bmachsums = nullptr;
+  bool use_bmach_sums = false;
   std::string err;
 };
 
@@ -172,6 +176,7 @@ BoundaryArgs MakeBoundaryArgs(vcpg_handle *h) {
   b.dlq = h->d_dlq;
   b.btrace = h->d_btrace;
   b.bmach = h->d_bmach;
+  b.bmach_sums = h->use_bmach_sums ? h->d_bmachsums : nullptr;
   b.bflux = h->d_bflux;
   b.nB = h->nB;
   b.mu = h->prm.mu;
@@ -199,6 +204,51 @@ int EnqueueResidual(vcpg_handle *h, const ResidualArgs &a, int *launches) {
   VCPG_CUDA(h, LaunchResidual(h->K, h->M, a, h->stream));
   n += 2;
   if (launches) *launches = n;
+  return VCPG_OK;
+}
+
+// Uploads a block's (or slab's) open-boundary data to the handle.
+int InstallOpenBoundary(vcpg_handle *h, const OpenBoundaryHost &ob_host) {
+  int rc = VCPG_OK;
+  const int M2 = h->M2, MD = h->MD;
+  auto upload = [&](void **dst, const void *src, size_t bytes) -> int {
+    if (bytes == 0) return VCPG_OK;
+    cudaError_t e = cudaMalloc(dst, bytes);
+    if (e != cudaSuccess) return Fail(h, VCPG_E_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    if (src) {
+      e = cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) return CudaFail(h, e, "cudaMemcpy open boundary");
+    }
+    return VCPG_OK;
+  };
+  const size_t nB = (size_t)ob_host.nB, nS = (size_t)ob_host.nS;
+  if ((rc = upload((void **)&h->d_bface, ob_host.bface.data(), sizeof(int) * ob_host.bface.size())) ||
+      (rc = upload((void **)&h->d_bpresc, ob_host.bpresc.data(), sizeof(double) * ob_host.bpresc.size())) ||
+      (rc = upload((void **)&h->d_pc, ob_host.pc.data(), sizeof(double) * ob_host.pc.size())) ||
+      (rc = upload((void **)&h->d_dlq, ob_host.dlq.data(), sizeof(double) * ob_host.dlq.size())) ||
+      (rc = upload((void **)&h->d_btrace, nullptr, sizeof(double) * nB * 4 * 5 * M2)) ||
+      (rc = upload((void **)&h->d_bmach, nullptr, sizeof(double) * nB)) ||
+      (rc = upload((void **)&h->d_bforce, nullptr, sizeof(double) * nB * 6)) ||
+      (rc = upload((void **)&h->d_bflux, nullptr, sizeof(double) * nB * 4 * 5 * M2)) ||
+      (rc = upload((void **)&h->d_sponge, ob_host.spongeIdx.data(), sizeof(int) * ob_host.spongeIdx.size())) ||
+      (rc = upload((void **)&h->d_dampfn, ob_host.dampFn.data(), sizeof(double) * nS * 3 * MD)) ||
+      (rc = upload((void **)&h->d_dampst, ob_host.dampState.data(), sizeof(double) * nS * 5 * MD)) ||
+      (rc = upload((void **)&h->d_cml, ob_host.cml.data(), sizeof(double) * nS * 6)) ||
+      (rc = upload((void **)&h->d_cfg, ob_host.cfg, sizeof(BlockFaceCfg) * 6)))
+    return rc;
+  // Boundary faces are coded in the neighbour table as -2 - (boundary-face index).
+  VCPG_CUDA(h, cudaMemcpy(h->d_nbr, ob_host.nbrCode.data(), sizeof(int32_t) * ob_host.nbrCode.size(),
+                          cudaMemcpyHostToDevice));
+  h->nB = ob_host.nB;
+  h->cml_on = ob_host.cmlOn;
+  for (int f = 0; f < 6; ++f) h->cfg[f] = ob_host.cfg[f];
+  h->open = true;
+  h->res_valid = false;
+  // Captured steps hold the previous launch sequence.
+  for (int s = 0; s < 2; ++s) {
+    if (h->exec[s]) { cudaGraphExecDestroy(h->exec[s]); h->exec[s] = nullptr; }
+    if (h->graph[s]) { cudaGraphDestroy(h->graph[s]); h->graph[s] = nullptr; }
+  }
   return VCPG_OK;
 }
 
@@ -258,7 +308,7 @@ int vcpg_destroy(vcpg_handle *h) {
                   h->d_status, h->d_counter, h->d_ticket, h->d_cgstats, h->d_bface, h->d_bpresc, h->d_pc,
                   h->d_dlq, h->d_btrace, h->d_bmach, h->d_bflux, h->d_sponge, h->d_dampfn,
                   h->d_dampst, h->d_cml, h->d_cfg, h->d_fflux, h->d_eddymax, h->d_nmetric,
-                  h->d_bforce, h->d_center, h->d_scratch};
+                  h->d_bforce, h->d_center, h->d_scratch, h->d_bmachsums};
   for (void *p : bufs)
     if (p) cudaFree(p);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -606,9 +656,11 @@ int vcpg_set_partition(vcpg_handle *h, int32_t n_owned, int32_t n_face_ghost) {
     return Fail(h, VCPG_E_INVALID, "partition: need 1 <= n_owned and n_owned + n_face_ghost "
                                    "<= the handle's elements");
   if (h->open)
-    return Fail(h, VCPG_E_INVALID, "partition: blocks with open boundaries are not partitioned");
+    return Fail(h, VCPG_E_INVALID, "partition: declare the partition before the open boundaries "
+                                   "(vcpg_set_open_boundary_partition)");
   h->nOwned = n_owned;
   h->nFace = (int64_t)n_owned + n_face_ghost;
+  h->layer = n_face_ghost;
   h->res_valid = false;
   for (int s = 0; s < 2; ++s) {
     if (h->exec[s]) { cudaGraphExecDestroy(h->exec[s]); h->exec[s] = nullptr; }
@@ -687,7 +739,8 @@ int vcpg_set_open_boundary_subfaces(vcpg_handle *h, const vcpg_open_boundary *ob
     return VCPG_E_INVALID;
   if (h->open) return Fail(h, VCPG_E_INVALID, "open boundaries are already configured");
   if (h->nOwned != h->nE)
-    return Fail(h, VCPG_E_INVALID, "open boundaries: the block is partitioned");
+    return Fail(h, VCPG_E_INVALID, "open boundaries of a partitioned block: "
+                                   "vcpg_set_open_boundary_partition");
   if (!SupportsOpenBoundaries(h->K, h->M))
     return Fail(h, VCPG_E_UNSUPPORTED_KM, "no open-boundary kernels for this degree");
   OpenBoundaryHost ob_host;
@@ -695,46 +748,108 @@ int vcpg_set_open_boundary_subfaces(vcpg_handle *h, const vcpg_open_boundary *ob
   int rc = BuildOpenBoundary(h->prm, *ob, *geom, p_grid, dof_location, grid_nodes, ob_host, err,
                              subfaces, n_subfaces);
   if (rc != VCPG_OK) return Fail(h, rc, err);
-  const int M2 = h->M2, MD = h->MD;
-  auto upload = [&](void **dst, const void *src, size_t bytes) -> int {
-    if (bytes == 0) return VCPG_OK;
-    cudaError_t e = cudaMalloc(dst, bytes);
-    if (e != cudaSuccess) return Fail(h, VCPG_E_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-    if (src) {
-      e = cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice);
-      if (e != cudaSuccess) return CudaFail(h, e, "cudaMemcpy open boundary");
-    }
+  return InstallOpenBoundary(h, ob_host);
+}
+
+int vcpg_set_open_boundary_partition(vcpg_handle *h, const vcpg_open_boundary *ob,
+                                     const vcpg_subface *subfaces, int32_t n_subfaces,
+                                     const int32_t *block_n_elem, const vcpg_geometry *block_geom,
+                                     int32_t p_grid, int32_t dof_location,
+                                     const double *block_grid_nodes,
+                                     const int64_t *local_to_global) {
+  if (!h || !ob || !block_n_elem || !block_geom || !local_to_global || n_subfaces < 0 ||
+      (n_subfaces > 0 && !subfaces))
+    return VCPG_E_INVALID;
+  if (h->open) return Fail(h, VCPG_E_INVALID, "open boundaries are already configured");
+  if (h->nOwned == h->nE)
+    return Fail(h, VCPG_E_INVALID, "declare the partition first (vcpg_set_partition)");
+  if (!SupportsOpenBoundaries(h->K, h->M))
+    return Fail(h, VCPG_E_UNSUPPORTED_KM, "no open-boundary kernels for this degree");
+  vcpg_params bp = h->prm;
+  for (int d = 0; d < 3; ++d) bp.n_elem[d] = block_n_elem[d];
+  const int64_t nBlock = (int64_t)bp.n_elem[0] * bp.n_elem[1] * bp.n_elem[2];
+  for (int64_t l = 0; l < h->nE; ++l)
+    if (local_to_global[l] < 0 || local_to_global[l] >= nBlock)
+      return Fail(h, VCPG_E_INVALID, "local_to_global: element index outside the block");
+  OpenBoundaryHost block, local;
+  std::string err;
+  int rc = BuildOpenBoundary(bp, *ob, *block_geom, p_grid, dof_location, block_grid_nodes, block,
+                             err, subfaces, n_subfaces);
+  if (rc != VCPG_OK) return Fail(h, rc, err);
+  std::vector<int32_t> nbr((size_t)h->nE * 6);
+  VCPG_CUDA(h, cudaMemcpy(nbr.data(), h->d_nbr, sizeof(int32_t) * nbr.size(),
+                          cudaMemcpyDeviceToHost));
+  SliceOpenBoundary(block, local_to_global, h->nE, h->nOwned, nbr.data(), h->MD, local);
+  return InstallOpenBoundary(h, local);
+}
+
+int vcpg_boundary_mach_weights(vcpg_handle *h, double *weights, int32_t *counts) {
+  if (!h || !counts) return VCPG_E_INVALID;
+  for (int f = 0; f < 6; ++f) counts[f] = h->open ? h->cfg[f].count : 0;
+  if (!h->open || h->nB == 0) return VCPG_OK;
+  if (!weights) return VCPG_E_INVALID;
+  VCPG_CUDA(h, LaunchBoundary(h->K, h->M, MakeBoundaryArgs(h), h->stream, 1));
+  h->launches += 1;
+  VCPG_CUDA(h, cudaMemcpyAsync(weights, h->d_bmach, sizeof(double) * h->nB,
+                               cudaMemcpyDeviceToHost, h->stream));
+  VCPG_CUDA(h, cudaStreamSynchronize(h->stream));
+  return VCPG_OK;
+}
+
+int vcpg_set_boundary_mach_sums(vcpg_handle *h, const double *sums) {
+  if (!h) return VCPG_E_INVALID;
+  if (!sums) { h->use_bmach_sums = false; return VCPG_OK; }
+  if (!h->d_bmachsums) {
+    cudaError_t e = cudaMalloc((void **)&h->d_bmachsums, 6 * sizeof(double));
+    if (e != cudaSuccess) return Fail(h, VCPG_E_OOM, "cudaMalloc Mach sums");
+  }
+  VCPG_CUDA(h, cudaMemcpyAsync(h->d_bmachsums, sums, 6 * sizeof(double), cudaMemcpyHostToDevice,
+                               h->stream));
+  VCPG_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->use_bmach_sums = true;
+  return VCPG_OK;
+}
+
+int vcpg_residual_part(vcpg_handle *h, int32_t part) {
+  if (!h || (part != 0 && part != 1)) return VCPG_E_INVALID;
+  if (h->nOwned == h->nE)
+    return Fail(h, VCPG_E_INVALID, "residual parts: a partitioned handle only");
+  const int64_t L = h->layer, nO = h->nOwned, nF = h->nFace;
+  int n = 0;
+  auto launch = [&](int phase, int64_t first, int64_t count) -> int {
+    if (count <= 0) return VCPG_OK;
+    ResidualArgs a = MakeResidualArgs(h, nullptr, nullptr);
+    a.n_elem = a.n_face_elem = (int)count;
+    if (phase == 1) a.face_first = (int)first; else a.res_first = (int)first;
+    VCPG_CUDA(h, LaunchResidual(h->K, h->M, a, h->stream, phase));
+    ++n;
     return VCPG_OK;
   };
-  const size_t nB = (size_t)ob_host.nB, nS = (size_t)ob_host.nS;
-  if ((rc = upload((void **)&h->d_bface, ob_host.bface.data(), sizeof(int) * ob_host.bface.size())) ||
-      (rc = upload((void **)&h->d_bpresc, ob_host.bpresc.data(), sizeof(double) * ob_host.bpresc.size())) ||
-      (rc = upload((void **)&h->d_pc, ob_host.pc.data(), sizeof(double) * ob_host.pc.size())) ||
-      (rc = upload((void **)&h->d_dlq, ob_host.dlq.data(), sizeof(double) * ob_host.dlq.size())) ||
-      (rc = upload((void **)&h->d_btrace, nullptr, sizeof(double) * nB * 4 * 5 * M2)) ||
-      (rc = upload((void **)&h->d_bmach, nullptr, sizeof(double) * nB)) ||
-      (rc = upload((void **)&h->d_bforce, nullptr, sizeof(double) * nB * 6)) ||
-      (rc = upload((void **)&h->d_bflux, nullptr, sizeof(double) * nB * 4 * 5 * M2)) ||
-      (rc = upload((void **)&h->d_sponge, ob_host.spongeIdx.data(), sizeof(int) * ob_host.spongeIdx.size())) ||
-      (rc = upload((void **)&h->d_dampfn, ob_host.dampFn.data(), sizeof(double) * nS * 3 * MD)) ||
-      (rc = upload((void **)&h->d_dampst, ob_host.dampState.data(), sizeof(double) * nS * 5 * MD)) ||
-      (rc = upload((void **)&h->d_cml, ob_host.cml.data(), sizeof(double) * nS * 6)) ||
-      (rc = upload((void **)&h->d_cfg, ob_host.cfg, sizeof(BlockFaceCfg) * 6)))
-    return rc;
-  // Boundary faces are coded in the neighbour table as -2 - (boundary-face index).
-  VCPG_CUDA(h, cudaMemcpy(h->d_nbr, ob_host.nbrCode.data(), sizeof(int32_t) * ob_host.nbrCode.size(),
-                          cudaMemcpyHostToDevice));
-  h->nB = ob_host.nB;
-  h->cml_on = ob_host.cmlOn;
-  for (int f = 0; f < 6; ++f) h->cfg[f] = ob_host.cfg[f];
-  h->open = true;
-  h->res_valid = false;
-  // Captured steps hold the previous launch sequence.
-  for (int s = 0; s < 2; ++s) {
-    if (h->exec[s]) { cudaGraphExecDestroy(h->exec[s]); h->exec[s] = nullptr; }
-    if (h->graph[s]) { cudaGraphDestroy(h->graph[s]); h->graph[s] = nullptr; }
+  int rc = VCPG_OK;
+  if (part == 0) {
+    // No ghost state needed: the boundary kernels (the slab's own faces), the face
+    // fluxes of owned layers 1.., the residuals of the layers between the first
+    // and the last.
+    if (h->open && h->nB > 0) {
+      VCPG_CUDA(h, LaunchBoundary(h->K, h->M, MakeBoundaryArgs(h), h->stream));
+      n += 2;
+    }
+    if ((rc = launch(1, L, nO - L)) || (rc = launch(2, L, nO - 2 * L))) return rc;
+    h->launches += n;
+    h->res_valid = false;
+    return VCPG_OK;
   }
-  return VCPG_OK;
+  // After the ghost layers are in: the first layer's and the upper ghost layer's
+  // face fluxes, the first and the last layer's residuals.
+  const int64_t firstEnd = L < nO ? L : nO;
+  const int64_t lastBegin = (nO - L > L) ? nO - L : L;
+  if ((rc = launch(1, 0, firstEnd)) || (rc = launch(1, nO, nF - nO)) ||
+      (rc = launch(2, 0, firstEnd)) || (rc = launch(2, lastBegin, nO - lastBegin)))
+    return rc;
+  h->launches += n;
+  rc = CheckStatus(h);
+  h->res_valid = rc == VCPG_OK;
+  return rc;
 }
 
 }  // extern "C"

@@ -38,6 +38,9 @@ struct BoundaryArgs {
   const double *dlq;           // [M][M]
   double *btrace;              // [nB][4][5][M^2]: value, d/dr, d/ds, d/dt
   double *bmach;               // [nB] area-weighted projected Mach number
+  // Optional [6]: per block face, the sum of the weights over the whole block
+  // (a partitioned block sums across its slabs); null: this list's own faces.
+  const double *bmach_sums;
   double *bflux;               // [nB][4][5][M^2]
   int nB;
   double mu, tau_num, theta_sym;
@@ -370,7 +373,11 @@ __global__ void __launch_bounds__(NT) BoundaryFluxKernel(const BoundaryArgs a) {
   // Boundary-averaged projected Mach number of this block face (sum in element order).
   if (threadIdx.x == 0) {
     double m = 0.0;
-    for (int i = 0; i < c.count; ++i) m += a.bmach[c.first + i];
+    if (a.bmach_sums) {
+      m = a.bmach_sums[f];
+    } else {
+      for (int i = 0; i < c.count; ++i) m += a.bmach[c.first + i];
+    }
     if (fabs(c.area) > 1.e-30) m /= c.area;
     s_mach = m;
   }

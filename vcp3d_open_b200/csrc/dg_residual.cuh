@@ -50,6 +50,11 @@ struct ResidualArgs {
   // Elements whose Min-face fluxes FaceFluxKernel computes (0: n_elem). More than
   // n_elem in a partitioned block: the ghost elements above the owned ones.
   int n_face_elem;
+  // First element of the launch's range: FaceFluxKernel covers elements
+  // [face_first, face_first + n_face_elem), ResidualKernel [res_first,
+  // res_first + n_elem) (0 and the counts above for a whole block; ranges split
+  // a partitioned residual around the halo exchange).
+  int face_first, res_first;
   double mu;                   // non-dimensional viscosity
   double tau_num;              // (p+1)^2 * relative penalty parameter
   double theta_sym;
@@ -1301,13 +1306,14 @@ __global__ void __launch_bounds__(NT, (Plan<K, M, T, OPEN>::MIN_BLOCKS)) Residua
   extern __shared__ __align__(16) unsigned char smem_raw[];
   if constexpr (P::BIG) {
     T *base = reinterpret_cast<T *>(a.scratch) + (size_t)blockIdx.x * P::SCRATCH;
-    for (int e = blockIdx.x; e < a.n_elem; e += gridDim.x) {
-      ResidualElement<K, M, NT, T, OPEN>(a, e, base);
+    for (int i = blockIdx.x; i < a.n_elem; i += gridDim.x) {
+      ResidualElement<K, M, NT, T, OPEN>(a, a.res_first + i, base);
       __syncthreads();
     }
   } else {
     if ((int)blockIdx.x >= a.n_elem) return;
-    ResidualElement<K, M, NT, T, OPEN>(a, blockIdx.x, reinterpret_cast<T *>(smem_raw));
+    ResidualElement<K, M, NT, T, OPEN>(a, a.res_first + (int)blockIdx.x,
+                                       reinterpret_cast<T *>(smem_raw));
   }
 }
 
@@ -1383,13 +1389,14 @@ __global__ void __launch_bounds__(NT, (FluxPlan<K, M, T>::MIN_BLOCKS)) FaceFluxK
   const int n = a.n_face_elem > 0 ? a.n_face_elem : a.n_elem;
   if constexpr (P::BIG) {
     T *base = reinterpret_cast<T *>(a.scratch) + (size_t)blockIdx.x * P::SCRATCH;
-    for (int e = blockIdx.x; e < n; e += gridDim.x) {
-      FaceFluxElement<K, M, NT, T, SGS>(a, e, base);
+    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+      FaceFluxElement<K, M, NT, T, SGS>(a, a.face_first + i, base);
       __syncthreads();
     }
   } else {
     if ((int)blockIdx.x >= n) return;
-    FaceFluxElement<K, M, NT, T, SGS>(a, blockIdx.x, reinterpret_cast<T *>(smem_raw));
+    FaceFluxElement<K, M, NT, T, SGS>(a, a.face_first + (int)blockIdx.x,
+                                      reinterpret_cast<T *>(smem_raw));
   }
 }
 

@@ -207,9 +207,10 @@ cudaError_t ConfigureResidual(int K, int M) {
   return cudaErrorInvalidValue;
 }
 
-cudaError_t LaunchBoundary(int K, int M, const BoundaryArgs &a, cudaStream_t st) {
+cudaError_t LaunchBoundary(int K, int M, const BoundaryArgs &a, cudaStream_t st, int phase) {
   if (a.nB <= 0) return cudaSuccess;
-#define VCPG_LAUNCH(K_, M_) if (K == K_ && M == M_) return VCPG_PAIR_FN(LaunchBoundary, K_, M_)(a, st);
+#define VCPG_LAUNCH(K_, M_) \
+  if (K == K_ && M == M_) return VCPG_PAIR_FN(LaunchBoundary, K_, M_)(a, st, phase);
   VCPG_PAIRS_OPEN(VCPG_LAUNCH)
 #undef VCPG_LAUNCH
   return cudaErrorInvalidValue;

@@ -24,7 +24,8 @@ struct CaseView;
 #define VCPG_PAIR_DECLARE(K_, M_)                                                           \
   cudaError_t VCPG_PAIR_FN(LaunchResidual, K_, M_)(const ResidualArgs &a, cudaStream_t st,  \
                                                     int phase);                               \
-  cudaError_t VCPG_PAIR_FN(LaunchBoundary, K_, M_)(const BoundaryArgs &a, cudaStream_t st); \
+  cudaError_t VCPG_PAIR_FN(LaunchBoundary, K_, M_)(const BoundaryArgs &a, cudaStream_t st,  \
+                                                    int phase);                               \
   cudaError_t VCPG_PAIR_FN(LaunchTimeStep, K_, M_)(const TimeStepArgs &a, cudaStream_t st); \
   cudaError_t VCPG_PAIR_FN(ConfigureResidual, K_, M_)();                                    \
   cudaError_t VCPG_PAIR_FN(ConfigureTimeStep, K_, M_)();                                    \
@@ -60,7 +61,8 @@ cudaError_t ConfigureResidual(int K, int M);
 // Dynamic shared memory of the time-step kernels (with an SGS model, or degree >= 7).
 cudaError_t ConfigureTimeStep(int K, int M);
 // Boundary traces + Mach weights, then the boundary states and fluxes (2 launches).
-cudaError_t LaunchBoundary(int K, int M, const BoundaryArgs &a, cudaStream_t st);
+// phase 1: the trace kernel only (traces and Mach weights).
+cudaError_t LaunchBoundary(int K, int M, const BoundaryArgs &a, cudaStream_t st, int phase = 0);
 cudaError_t LaunchTimeStep(int K, int M, const TimeStepArgs &a, cudaStream_t st);
 cudaError_t LaunchFinalizeDt(unsigned long long *dt_bits, const double *fixed_dt, double *d_dt,
                              double *hist, int hist_cap, int *counter, cudaStream_t st);

@@ -109,11 +109,11 @@ static cudaError_t LaunchResidualKM(const ResidualArgs &a, cudaStream_t st, int 
 
 // The two characteristic-boundary kernels (dg_boundary.cuh).
 template <int K, int M>
-static cudaError_t LaunchBoundaryKM(const BoundaryArgs &a, cudaStream_t st) {
+static cudaError_t LaunchBoundaryKM(const BoundaryArgs &a, cudaStream_t st, int phase) {
   constexpr int NT = M * M > 64 ? 128 : 64;
   using SM = BoundaryTraceSmem<K, M>;
   BoundaryTraceKernel<K, M, NT><<<a.nB, NT, SM::DYN ? sizeof(double) * SM::N : 0, st>>>(a);
-  BoundaryFluxKernel<K, M, NT><<<a.nB, NT, 0, st>>>(a);
+  if (phase != 1) BoundaryFluxKernel<K, M, NT><<<a.nB, NT, 0, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -161,8 +161,9 @@ static cudaError_t PairUploadKM(const vcpg_operators *ops) {
                                                     int phase) {                              \
     return LaunchResidualKM<K_, M_>(a, st, phase);                                            \
   }                                                                                           \
-  cudaError_t VCPG_PAIR_FN(LaunchBoundary, K_, M_)(const BoundaryArgs &a, cudaStream_t st) {  \
-    return LaunchBoundaryKM<K_, M_>(a, st);                                                   \
+  cudaError_t VCPG_PAIR_FN(LaunchBoundary, K_, M_)(const BoundaryArgs &a, cudaStream_t st,  \
+                                                    int phase) {                              \
+    return LaunchBoundaryKM<K_, M_>(a, st, phase);                                            \
   }                                                                                           \
   cudaError_t VCPG_PAIR_FN(LaunchTimeStep, K_, M_)(const TimeStepArgs &a, cudaStream_t st) {  \
     return LaunchTimeStepKM<K_, M_>(a, st);                                                   \

@@ -457,4 +457,54 @@ int BuildOpenBoundary(const vcpg_params &prm, const vcpg_open_boundary &ob,
   }
 }
 
+void SliceOpenBoundary(const OpenBoundaryHost &block, const int64_t *localToGlobal, int64_t nLocal,
+                       int64_t nOwned, const int32_t *localNbr, int MD, OpenBoundaryHost &out) {
+  std::vector<int64_t> localOf(block.nbrCode.size() / 6, -1);   // block element -> owned local
+  for (int64_t l = 0; l < nOwned; ++l) localOf[localToGlobal[l]] = l;
+  out = OpenBoundaryHost{};
+  out.pc = block.pc;
+  out.dlq = block.dlq;
+  out.cmlOn = block.cmlOn;
+  // Boundary faces of owned elements, block order kept (per block face, element order).
+  std::vector<int> newIndex((size_t)block.nB, -1);
+  for (int f = 0; f < 6; ++f) {
+    out.cfg[f] = block.cfg[f];            // areas and settings of the whole block face
+    out.cfg[f].first = out.nB;
+    for (int b = block.cfg[f].first; b < block.cfg[f].first + block.cfg[f].count; ++b) {
+      const int *row = &block.bface[(size_t)b * kBfStride];
+      const int64_t l = localOf[row[kBfElem]];
+      if (l < 0) continue;
+      newIndex[b] = out.nB++;
+      out.bface.insert(out.bface.end(), row, row + kBfStride);
+      out.bface[out.bface.size() - kBfStride + kBfElem] = (int)l;
+      out.bpresc.insert(out.bpresc.end(), block.bpresc.begin() + (size_t)b * kPrescStride,
+                        block.bpresc.begin() + (size_t)(b + 1) * kPrescStride);
+    }
+    out.cfg[f].count = out.nB - out.cfg[f].first;
+  }
+  // Neighbour table: the handle's, with the owned elements' boundary faces coded.
+  out.nbrCode.assign(localNbr, localNbr + nLocal * 6);
+  for (int64_t l = 0; l < nOwned; ++l) {
+    const int64_t g = localToGlobal[l];
+    for (int f = 0; f < 6; ++f) {
+      const int c = block.nbrCode[g * 6 + f];
+      if (c <= -2) out.nbrCode[l * 6 + f] = -2 - newIndex[-2 - c];
+      else if (c == -1) out.nbrCode[l * 6 + f] = -1;
+    }
+  }
+  // Sponge elements among the owned ones, in local order.
+  out.spongeIdx.assign(nLocal, -1);
+  for (int64_t l = 0; l < nOwned; ++l) {
+    const int s = block.spongeIdx[localToGlobal[l]];
+    if (s < 0) continue;
+    out.spongeIdx[l] = out.nS++;
+    out.dampFn.insert(out.dampFn.end(), block.dampFn.begin() + (size_t)s * 3 * MD,
+                      block.dampFn.begin() + (size_t)(s + 1) * 3 * MD);
+    out.dampState.insert(out.dampState.end(), block.dampState.begin() + (size_t)s * 5 * MD,
+                         block.dampState.begin() + (size_t)(s + 1) * 5 * MD);
+    out.cml.insert(out.cml.end(), block.cml.begin() + (size_t)s * 6,
+                   block.cml.begin() + (size_t)(s + 1) * 6);
+  }
+}
+
 }  // namespace vcpg
