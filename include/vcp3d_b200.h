@@ -436,7 +436,8 @@ int vcpg_set_open_boundary_partition(vcpg_handle *h, const vcpg_open_boundary *o
  * boundary faces for its current state (ElementClass::AverageMachNSCBC,
  * src/ElementClass.cpp:357-509; zero on other boundary faces), in the handle's
  * boundary-face order: counts[f] faces of block face f, f = 0..5 in turn;
- * weights needs their total. Synchronises the handle's stream. */
+ * weights needs their total (NULL: only the counts are returned).
+ * Synchronises the handle's stream. */
 int vcpg_boundary_mach_weights(vcpg_handle *h, double *weights, int32_t *counts);
 
 /* Per block face, the sum of the Mach weights over the whole block, which the

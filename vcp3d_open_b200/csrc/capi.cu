@@ -786,8 +786,7 @@ int vcpg_set_open_boundary_partition(vcpg_handle *h, const vcpg_open_boundary *o
 int vcpg_boundary_mach_weights(vcpg_handle *h, double *weights, int32_t *counts) {
   if (!h || !counts) return VCPG_E_INVALID;
   for (int f = 0; f < 6; ++f) counts[f] = h->open ? h->cfg[f].count : 0;
-  if (!h->open || h->nB == 0) return VCPG_OK;
-  if (!weights) return VCPG_E_INVALID;
+  if (!h->open || h->nB == 0 || !weights) return VCPG_OK;   // NULL weights: the counts only
   VCPG_CUDA(h, LaunchBoundary(h->K, h->M, MakeBoundaryArgs(h), h->stream, 1));
   h->launches += 1;
   VCPG_CUDA(h, cudaMemcpyAsync(weights, h->d_bmach, sizeof(double) * h->nB,
