@@ -266,6 +266,21 @@ int vcpg_stats(vcpg_handle *h, int64_t *cg_iterations, int64_t *element_solves);
  * is that of the current state, as after vcpg_residual. */
 int vcpg_time_residual_kernels(vcpg_handle *h, int32_t reps, double *ms);
 
+/* Measurement hook (no counterpart in the reference): the line contraction of
+ * one sum-factorisation stage, 128 lines per tile, run `reps` times per tile
+ * from shared memory to shared memory, with variant 0 FP32 fused multiply-adds
+ * (the mixed form's residual kernel), 1 TF32 tensor-core tiles (tcgen05.mma
+ * kind::tf32, accumulator in tensor memory), 2 the same with the operands split
+ * into TF32 high and low parts (three MMAs, FP32-level accuracy). K inputs and
+ * M outputs per line, (K, M) = (5, 7) or (6, 8); x [n_lines][K], op [K][M]
+ * (op[k * M + m]), y [n_lines][M] receives the last stage's outputs (each
+ * stage's next inputs are its first K outputs times scale). n_lines a multiple
+ * of 128; ms receives the device time of the timed launch (after a warm-up
+ * launch). Allocates its own device buffers. */
+int vcpg_line_contraction_probe(int32_t variant, int32_t K, int32_t M, int64_t n_lines,
+                                int32_t reps, float scale, const float *x, const float *op,
+                                float *y, double *ms);
+
 /* Allocation-free CFL time step. This entry point has no counterpart in the
  * reference solver. It is for callers that cannot call cudaMalloc: programs
  * whose device memory all belongs to their own pool allocator (a framework's

@@ -17,7 +17,7 @@ BUILD = os.path.join(ROOT, "_build")
 LIB = os.path.join(PKG, "libvcp3d_b200.so")
 SOURCES = ["kernels.cu", "capi.cu", "capi_setup.cpp", "host_setup.cpp", "open_boundary.cpp",
            "ensemble.cu", "geometry.cu",
-           "noalloc.cu"]
+           "noalloc.cu", "tc_contract.cu"]
 # kernels_pair.cu is compiled once per supported (K, M) pair (the reference's
 # tensor-product dispatch), so that the pairs compile in parallel.
 PAIRS = [(2, 2), (2, 3), (3, 4), (4, 5), (5, 7), (6, 8), (7, 9), (8, 12), (9, 13), (10, 14)]

@@ -35,6 +35,7 @@ EXPORTED = [
     "vcpg_step", "vcpg_synchronization_step", "vcpg_sync", "vcpg_stream", "vcpg_launch_count", "vcpg_stats",
     "vcpg_time_residual_kernels", "vcpg_set_open_boundary_partition",
     "vcpg_boundary_mach_weights", "vcpg_set_boundary_mach_sums", "vcpg_residual_part",
+    "vcpg_line_contraction_probe",
     "vcpg_time_step_noalloc", "vcpg_set_open_boundary", "vcpg_set_open_boundary_subfaces", "vcpg_ensemble_create",
     "vcpg_ensemble_destroy", "vcpg_ensemble_last_error", "vcpg_ensemble_footprint",
     "vcpg_ensemble_submit", "vcpg_ensemble_step", "vcpg_ensemble_poll", "vcpg_ensemble_retire",
@@ -151,6 +152,9 @@ def load() -> C.CDLL:
         hp, C.POINTER(OpenBoundary), C.POINTER(Subface), C.c_int32, ip, C.POINTER(Geometry),
         C.c_int32, C.c_int32, dp, C.POINTER(C.c_int64)]
     lib.vcpg_boundary_mach_weights.argtypes = [hp, dp, ip]
+    fp = C.POINTER(C.c_float)
+    lib.vcpg_line_contraction_probe.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int64,
+                                                C.c_int32, C.c_float, fp, fp, fp, dp]
     lib.vcpg_set_boundary_mach_sums.argtypes = [hp, dp]
     lib.vcpg_residual_part.argtypes = [hp, C.c_int32]
     lib.vcpg_set_open_boundary_subfaces.argtypes = [hp, C.POINTER(OpenBoundary),
