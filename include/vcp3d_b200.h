@@ -271,7 +271,8 @@ int vcpg_time_residual_kernels(vcpg_handle *h, int32_t reps, double *ms);
  * from shared memory to shared memory, with variant 0 FP32 fused multiply-adds
  * (the mixed form's residual kernel), 1 TF32 tensor-core tiles (tcgen05.mma
  * kind::tf32, accumulator in tensor memory), 2 the same with the operands split
- * into TF32 high and low parts (three MMAs, FP32-level accuracy). K inputs and
+ * into TF32 high and low parts (three MMAs, FP32-level accuracy), 3 the FP32
+ * lines with the operator in constant memory instead of shared memory. K inputs and
  * M outputs per line, (K, M) = (5, 7) or (6, 8); x [n_lines][K], op [K][M]
  * (op[k * M + m]), y [n_lines][M] receives the last stage's outputs (each
  * stage's next inputs are its first K outputs times scale). n_lines a multiple

@@ -15,7 +15,8 @@
 // is the split "3xTF32" form, X B ~ Xhi Bhi + Xhi Blo + Xlo Bhi with hi =
 // tf32(v), lo = tf32(v - hi), three MMAs into one accumulator. Variant 0 is the
 // FMA path: one thread per line, its K inputs read from shared memory, M
-// sequential FMA chains.
+// sequential FMA chains, the operator from shared memory; variant 3 is the same
+// with the operator in constant memory, as the residual kernel holds it.
 //
 // Every variant runs `reps` chained stages per tile inside shared memory, as a
 // residual kernel does between its global loads and stores: the stage writes its
@@ -220,8 +221,13 @@ __global__ void __launch_bounds__(128) TcContractKernel(const float *x, const fl
                  : "memory");
 }
 
-// FMA stages: one thread per line, inputs and outputs in shared memory.
-template <int K, int M>
+// The operator in constant memory (variant 3: the residual kernel's operand source).
+__constant__ float c_probe_op[kKPad * kN];
+
+// FMA stages: one thread per line, inputs and outputs in shared memory; the
+// operator read from shared memory (variant 0, as a TMA- or bulk-copied operator
+// table would be) or from the constant bank (variant 3, uniform operands).
+template <int K, int M, bool CONST_OP>
 __global__ void __launch_bounds__(128) FmaContractKernel(const float *x, const float *op,
                                                          float *y, int n_tiles, int reps,
                                                          float scale) {
@@ -246,7 +252,8 @@ __global__ void __launch_bounds__(128) FmaContractKernel(const float *x, const f
       for (int m = 0; m < M; ++m) {
         float acc = 0.0f;
 #pragma unroll
-        for (int k = 0; k < K; ++k) acc = fmaf(s_op[k * M + m], xv[k], acc);
+        for (int k = 0; k < K; ++k)
+          acc = fmaf(CONST_OP ? c_probe_op[k * M + m] : s_op[k * M + m], xv[k], acc);
         d[m] = acc;
         s_out[tid][m] = acc;
       }
@@ -266,7 +273,9 @@ template <int K, int M>
 cudaError_t Launch(int variant, const float *x, const float *op, float *y, int n_tiles,
                    int reps, float scale, int *err, int grid, cudaStream_t st) {
   if (variant == 0)
-    FmaContractKernel<K, M><<<grid, 128, 0, st>>>(x, op, y, n_tiles, reps, scale);
+    FmaContractKernel<K, M, false><<<grid, 128, 0, st>>>(x, op, y, n_tiles, reps, scale);
+  else if (variant == 3)
+    FmaContractKernel<K, M, true><<<grid, 128, 0, st>>>(x, op, y, n_tiles, reps, scale);
   else if (variant == 1)
     TcContractKernel<K, M, false><<<grid, 128, 0, st>>>(x, op, y, n_tiles, reps, scale, err);
   else
@@ -280,7 +289,7 @@ extern "C" int vcpg_line_contraction_probe(int32_t variant, int32_t K, int32_t M
                                            int64_t n_lines, int32_t reps, float scale,
                                            const float *x, const float *op, float *y,
                                            double *ms) {
-  if (variant < 0 || variant > 2 || reps < 1 || n_lines < kTile || n_lines % kTile || !x ||
+  if (variant < 0 || variant > 3 || reps < 1 || n_lines < kTile || n_lines % kTile || !x ||
       !op || !y || !ms)
     return VCPG_E_INVALID;
   if (!((K == 5 && M == 7) || (K == 6 && M == 8))) return VCPG_E_UNSUPPORTED_KM;
@@ -301,6 +310,7 @@ extern "C" int vcpg_line_contraction_probe(int32_t variant, int32_t K, int32_t M
       ok(cudaMalloc((void **)&derr, sizeof(int))) && ok(cudaMemset(derr, 0, sizeof(int))) &&
       ok(cudaMemcpy(dx, x, sizeof(float) * n_lines * K, cudaMemcpyHostToDevice)) &&
       ok(cudaMemcpy(dop, op, sizeof(float) * K * M, cudaMemcpyHostToDevice)) &&
+      ok(cudaMemcpyToSymbol(c_probe_op, op, sizeof(float) * K * M)) &&
       ok(cudaEventCreate(&e0)) && ok(cudaEventCreate(&e1))) {
     // Four resident CTAs per SM (tensor memory: 4 x 32 of 512 columns).
     const int grid = n_tiles < 4 * sms ? n_tiles : 4 * sms;

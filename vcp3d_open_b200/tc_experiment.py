@@ -4,9 +4,10 @@ One sum-factorisation stage maps lines of K modal coefficients to M Gauss
 points with the 1-D Legendre operator (degree 4: K = 5, M = 7; degree 5: K = 6,
 M = 8). vcpg_line_contraction_probe runs it from shared memory to shared memory
 as the residual kernel does, 128 lines per tile and `reps` chained stages per
-tile, with FP32 fused multiply-adds (the mixed form's current path), TF32
-tensor-core tiles (tcgen05.mma kind::tf32, accumulator in tensor memory) and the
-split 3xTF32 form. Reported per variant: stage throughput (lines x stages per
+tile, with FP32 fused multiply-adds (operator in shared memory, as a TMA- or
+bulk-copied table would be, and in constant memory, as the residual kernel
+holds it), TF32 tensor-core tiles (tcgen05.mma kind::tf32, accumulator in tensor
+memory) and the split 3xTF32 form. Reported per variant: stage throughput (lines x stages per
 second) and the error of one stage against FP64 on the same FP32 inputs.
 
     python -m vcp3d_open_b200.tc_experiment [--lines 1048576] [--reps 64]
@@ -24,7 +25,8 @@ import numpy as np
 
 from . import capi, cases, solver
 
-VARIANTS = {0: "fp32 fma", 1: "tf32 tcgen05", 2: "3xtf32 tcgen05"}
+VARIANTS = {0: "fp32 fma", 1: "tf32 tcgen05", 2: "3xtf32 tcgen05",
+            3: "fp32 fma, constant operator"}
 
 
 def operator(p: int) -> np.ndarray:
