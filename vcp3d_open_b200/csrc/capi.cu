@@ -254,11 +254,18 @@ int InstallOpenBoundary(vcpg_handle *h, const OpenBoundaryHost &ob_host) {
 
 int ResidualLaunches(const vcpg_handle *h) { return (h->open && h->nB > 0) ? 4 : 2; }
 
+bool FusedSteps(const vcpg_handle *h) {
+  return FusedStageUpdate(h->K, h->M, h->prm.precision == VCPG_MIXED, h->open);
+}
+
 // One time step of a single case: the CFL time step, then the first stage's
 // update together with recording the step (StartStepKernel), then per stage a
 // residual whose kernel applies the next stage's update to its element in its
 // epilogue; the last stage's residual is stored (the next step's first stage
-// uses it). SSP-RK3: 2 + 3 residuals' launches, low-storage RK4: 2 + 5.
+// uses it). SSP-RK3: 2 + 3 residuals' launches, low-storage RK4: 2 + 5. Where
+// the residual kernel cannot prefetch the update's inputs (FusedStageUpdate),
+// the step records the time step (FinalizeDtKernel) and runs a stage kernel
+// before each residual instead.
 int EnqueueStep(vcpg_handle *h, int scheme) {
   const size_t n = (size_t)h->nOwned * 5 * h->KD;
   TimeStepArgs t = MakeTimeStepArgs(h);
@@ -270,7 +277,23 @@ int EnqueueStep(vcpg_handle *h, int scheme) {
   const int kind = ssp ? kRkSsp : kRkLowStorage;
   auto coefA = [&](int s) { return ssp ? alphaRK[s] : kLsA[s]; };
   auto coefB = [&](int s) { return ssp ? betaRK[s] : kLsB[s]; };
-  // The fixed step lives in device memory (d_fixed); a non-positive value selects the CFL step.
+  if (!FusedSteps(h)) {
+    // The fixed step lives in device memory (d_fixed); a non-positive value selects the CFL step.
+    VCPG_CUDA(h, LaunchFinalizeDt(h->d_dtbits, h->d_fixed, h->d_dt, h->d_hist, h->hist_cap,
+                                  h->d_counter, h->stream));
+    const ResidualArgs a = MakeResidualArgs(h, nullptr, nullptr);
+    for (int s = 0; s < stages; ++s) {
+      if (ssp)
+        VCPG_CUDA(h, LaunchSspStage(h->d_sol, h->d_solOld, h->d_res, h->d_dt, alphaRK[s],
+                                    betaRK[s], s == 0, n, h->stream, CaseView{}, 5 * h->KD));
+      else
+        VCPG_CUDA(h, LaunchLsrkStage(h->d_sol, h->d_solOld, h->d_res, h->d_dt, kLsA[s], kLsB[s],
+                                     n, h->stream, CaseView{}, 5 * h->KD));
+      int rc = EnqueueResidual(h, a, nullptr);
+      if (rc) return rc;
+    }
+    return VCPG_OK;
+  }
   VCPG_CUDA(h, LaunchStartStep(h->d_dtbits, h->d_fixed, h->d_dt, h->d_hist, h->hist_cap,
                                h->d_counter, h->d_ticket, h->d_sol, h->d_solOld, h->d_res, kind,
                                coefA(0), coefB(0), n, h->stream));
@@ -600,7 +623,8 @@ int vcpg_step(vcpg_handle *h, int32_t scheme, int32_t n_steps, double fixed_dt,
     if (e != cudaSuccess) return CudaFail(h, e, "cudaStreamEndCapture");
     h->graph[scheme] = g;
     VCPG_CUDA(h, cudaGraphInstantiate(&h->exec[scheme], g, 0));
-    h->graph_launches[scheme] = 2 + (scheme == VCPG_SSPRK3 ? 3 : 5) * ResidualLaunches(h);
+    h->graph_launches[scheme] = 2 + (scheme == VCPG_SSPRK3 ? 3 : 5) *
+                                        (ResidualLaunches(h) + (FusedSteps(h) ? 0 : 1));
   }
   for (int s = 0; s < n_steps; ++s) VCPG_CUDA(h, cudaGraphLaunch(h->exec[scheme], h->stream));
   h->launches += (int64_t)n_steps * h->graph_launches[scheme];

@@ -99,6 +99,13 @@ struct ResidualArgs {
   double *rk_reg;              // du (low-storage) or solOld (SSP)
 };
 
+// Whether the residual kernel of (K, M, T, OPEN) fetches the fused stage update's
+// inputs asynchronously into its free work area (MassSolve); without that the
+// epilogue's dependent loads lengthen every element (degrees 7-9 with their
+// element arrays in global scratch, and the mixed form of degrees 5 and 6), and a
+// step there applies the updates with the separate stage kernels.
+template <int K, int M, typename T, bool OPEN> struct FusedUpdatePrefetch;
+
 // Final value r of residual entry gi (after the mass-matrix solve): stored, or
 // applied to the state by the fused stage update, whose inputs are the entry's
 // state sol0 and its second register reg0 (du or solOld).
@@ -268,6 +275,15 @@ template <int K, int M, typename T = double, bool OPEN = false> struct Plan {
   static constexpr int MIN_BLOCKS = FIT < 1 ? 1 : (FIT > CAP ? CAP : FIT);
 };
 
+
+template <int K, int M, typename T, bool OPEN> struct FusedUpdatePrefetch {
+  using PK = Plan<K, M, T, OPEN>;
+  static constexpr int KD = K * K * K;
+  static constexpr int OFF = (Plan<K, M, T>::CG + 1) / 2 * 2;   // in T, 8-byte aligned
+  static constexpr bool value =
+      !PK::BIG && (long)(PK::WORK - OFF) * (long)sizeof(T) >=
+                      (sizeof(T) == 4 ? 2L : 1L) * 5 * KD * 8;
+};
 
 // ---------------------------------------------------------------------------
 // Characteristic matching layer source of one integration point
@@ -1049,11 +1065,9 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
   // leaves free, each entry by the thread that applies the update to it.
   const size_t g0 = (size_t)e * 5 * KD;
   // The launched kernel's plan (its work area; shared memory unless BIG).
-  using PK = Plan<K, M, T, OPEN>;
   constexpr bool kMixed = sizeof(T) == 4;
-  constexpr int kPrefOff = (P::CG + 1) / 2 * 2;   // in T, 8-byte aligned
-  constexpr bool kPrefetch =
-      !PK::BIG && (long)(PK::WORK - kPrefOff) * (long)sizeof(T) >= (kMixed ? 2L : 1L) * 5 * KD * 8;
+  constexpr int kPrefOff = FusedUpdatePrefetch<K, M, T, OPEN>::OFF;
+  constexpr bool kPrefetch = FusedUpdatePrefetch<K, M, T, OPEN>::value;
   double *pref = reinterpret_cast<double *>(work + kPrefOff);
   const bool fused = a.rk_kind != kRkNone;
   if (kPrefetch && fused) {
@@ -1317,6 +1331,12 @@ __global__ void __launch_bounds__(NT, (Plan<K, M, T, OPEN>::MIN_BLOCKS)) Residua
   }
 }
 
+// Staging of the lower neighbours' states in the face-flux kernel's shared
+// memory (FluxPlan::NB_PREF); 0 reads them per line from global memory.
+#ifndef VCPG_FACE_NB_STAGING
+#define VCPG_FACE_NB_STAGING 1
+#endif
+
 // Shared memory (in T) and launch shape of the face-flux kernel.
 template <int K, int M, typename T = double> struct FluxPlan {
   static constexpr int KD = K * K * K, M2 = M * M;
@@ -1340,7 +1360,8 @@ template <int K, int M, typename T = double> struct FluxPlan {
   // of coalesced asynchronous copies instead of strided per-line global loads.
   static constexpr int NB_OFF = (TOTAL * (int)sizeof(T) + 7) / 8;   // in doubles
   static constexpr size_t NB_BYTES = 8 * ((size_t)NB_OFF + 15 * (size_t)KD);
-  static constexpr bool NB_PREF = !BIG && (int)(227 * 1024 / NB_BYTES) >= MIN_BLOCKS;
+  static constexpr bool NB_PREF = VCPG_FACE_NB_STAGING && !BIG &&
+                                  (int)(227 * 1024 / NB_BYTES) >= MIN_BLOCKS;
   static constexpr size_t BYTES = NB_PREF ? NB_BYTES : BASE_BYTES;
 };
 

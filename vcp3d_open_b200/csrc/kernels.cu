@@ -152,6 +152,25 @@ int SlotOf(int K, int M) {
   return -1;
 }
 
+// Stage updates fused into the residual kernel where it prefetches their inputs
+// (0: always the separate stage kernels).
+#ifndef VCPG_FUSED_STAGES
+#define VCPG_FUSED_STAGES 1
+#endif
+
+bool FusedStageUpdate(int K, int M, bool mixed, bool open) {
+  if (!VCPG_FUSED_STAGES) return false;
+#define VCPG_FUSED(K_, M_)                                                                   \
+  if (K == K_ && M == M_)                                                                    \
+    return mixed ? (open ? FusedUpdatePrefetch<K_, M_, float, true>::value                   \
+                         : FusedUpdatePrefetch<K_, M_, float, false>::value)                 \
+                 : (open ? FusedUpdatePrefetch<K_, M_, double, true>::value                  \
+                         : FusedUpdatePrefetch<K_, M_, double, false>::value);
+  VCPG_PAIRS(VCPG_FUSED)
+#undef VCPG_FUSED
+  return false;
+}
+
 size_t ResidualSmemBytes(int K, int M) {
 #define VCPG_SMEM(K_, M_) if (K == K_ && M == M_) return Plan<K_, M_>::BIG ? 0 : Plan<K_, M_>::BYTES;
   VCPG_PAIRS(VCPG_SMEM)

@@ -34,6 +34,10 @@ VCPG_PAIRS(VCPG_PAIR_DECLARE)
 #undef VCPG_PAIR_DECLARE
 
 bool Supported(int K, int M);
+// Whether a step applies the Runge-Kutta stage updates inside the residual
+// kernel (its inputs prefetched into free shared memory) for this variant;
+// otherwise the separate stage kernels apply them.
+bool FusedStageUpdate(int K, int M, bool mixed, bool open);
 int SlotOf(int K, int M);
 size_t ResidualSmemBytes(int K, int M);
 // Device bytes per element of the face-flux buffer (ResidualArgs::face_flux).
