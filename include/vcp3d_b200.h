@@ -372,6 +372,15 @@ typedef struct vcpg_open_boundary {
                                      pressure                                          */
   double free_stream[5];          /* far field: density, velocity x, y, z, pressure
                                      (the reference's free stream, dimensional)        */
+  int32_t outlet_local_mach;      /* "Outlet use local (element) averaged Mach number":
+                                     the characteristic outflow of a subface uses the
+                                     projected Mach number averaged over one element
+                                     face -- as in the reference run on one thread, the
+                                     face of the subface's last element in element order,
+                                     whose value the reference's subface-wide member
+                                     holds when the residual runs
+                                     (src/BoundaryState.cpp:990, 1327). Not with
+                                     vcpg_set_open_boundary_partition.                 */
 } vcpg_open_boundary;
 
 /* Configures open boundaries on a handle whose geometry has boundary faces

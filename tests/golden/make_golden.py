@@ -131,6 +131,15 @@ OPEN_SPECS = {
         outlet_beta_t=-1.0, outlet_one_minus_beta=False,
         bc=("periodic", "periodic", "periodic", "periodic", "inflow_static_nscbc",
             "outflow_nscbc"), sponge=(0, 0, 0, 0, 0, 1), **_OPEN),
+    # The same with "Outlet use local (element) averaged Mach number": every outlet
+    # face takes the projected Mach number averaged over the last outlet element's
+    # face (the value the reference's subface member holds after its averaging loop).
+    "pulse_p3_3x3x4_kfaces_local": cases.CaseSpec(
+        name="pulse_p3_3x3x4_kfaces_local", n_elem=(3, 3, 4), p=3, hi=(3.0, 3.0, 4.0),
+        center=(1.5, 1.5, 3.3), vel_dir=(0.0, 0.0, 1.0), seed=16, outlet_beta_l=-1.0,
+        outlet_beta_t=-1.0, outlet_one_minus_beta=False, outlet_local_mach=True,
+        bc=("periodic", "periodic", "periodic", "periodic", "inflow_static_nscbc",
+            "outflow_nscbc"), sponge=(0, 0, 0, 0, 0, 1), **_OPEN),
     # Total-condition inflow (relaxing total pressure, total temperature and the
     # flow direction) with the outgoing amplitude kept, outflow on i-max with a
     # sponge and the matching layer, flow at an angle in the x-y plane.

@@ -38,26 +38,14 @@ sys.path.insert(0, ROOT)
 from oracle import records  # noqa: E402
 from vcp3d_open_b200 import capi, cases, pulse_report, solver, tgv_report, workloads  # noqa: E402
 
-GAMMA = 1.4
 CONFIGS = {"vortex": "vortex8_p3_lsrk4", "tgv": "tgv32_p3_lsrk4", "pulse": "pulse40_p4_lsrk4"}
 SCHEMES = {"lsrk4": capi.LSRK4, "ssprk3": capi.SSPRK3}
 
 
 def conserved_integrals(modal: np.ndarray, disc: solver.Discretization) -> np.ndarray:
-    """Integrals of (rho, rho u, rho v, rho w, rho E) over the block (non-dimensional),
-    by the Gauss quadrature of the elements."""
-    V = tgv_report._to_points(modal, disc.leg_int)
-    V4Inv = 1.0 / V[:, 4]
-    u, v, w = -V4Inv * V[:, 1], -V4Inv * V[:, 2], -V4Inv * V[:, 3]
-    q2 = u * u + v * v + w * w
-    s = GAMMA - (GAMMA - 1.0) * (V[:, 0] - 0.5 * V[:, 4] * q2)
-    rho = (-V[:, 4] * np.exp(s)) ** (-1.0 / (GAMMA - 1.0))
-    p = -V4Inv * rho
-    rE = p / (GAMMA - 1.0) + 0.5 * rho * q2
-    w1 = disc.w_int
-    W = (w1[None, None, :] * w1[None, :, None] * w1[:, None, None]).reshape(-1)
-    JW = disc.vol_metric[:, 0] * W[None, :]
-    return np.array([np.sum(JW * q) for q in (rho, rho * u, rho * v, rho * w, rE)])
+    """Integrals of (rho, rho u, rho v, rho w, rho E) over the block by the elements'
+    Gauss quadrature (vcp3d_open_b200.tgv_report.conserved_integrals)."""
+    return tgv_report.conserved_integrals(modal, disc)
 
 
 def _rel(a, b) -> float:

@@ -77,7 +77,8 @@ class OpenBoundary(C.Structure):
                 ("sponge_sigma", C.c_double * 6), ("sponge_alpha", C.c_double * 6),
                 ("cml", C.c_int32), ("sponge_state", C.c_double * 5),
                 ("inflow_total", (C.c_double * 5) * 6), ("wall_data", C.c_double * 6),
-                ("inflow_super", (C.c_double * 5) * 6), ("free_stream", C.c_double * 5)]
+                ("inflow_super", (C.c_double * 5) * 6), ("free_stream", C.c_double * 5),
+                ("outlet_local_mach", C.c_int32)]
 
 
 class Subface(C.Structure):

@@ -188,6 +188,8 @@ class CaseSpec:
     # inflows, (value,) for walls, (rho, u, v, w, p) for the supersonic inflow;
     # otherwise the face's data apply.
     subfaces: Optional[Tuple[tuple, ...]] = None
+    # "Outlet use local (element) averaged Mach number".
+    outlet_local_mach: bool = False
 
     def __post_init__(self):
         if self.p_grid is None:
@@ -549,7 +551,7 @@ def _open_blocks(spec: CaseSpec, ref: "RefConditions") -> Tuple[str, str, str]:
     params = f"""Outlet characteristic length: {spec.outlet_len!r}
 Outlet normal relaxation (sigma): {spec.outlet_sigma!r}
 Outlet use one minus beta transverse relaxation: {yn(spec.outlet_one_minus_beta)}
-Outlet use local (element) averaged Mach number: no
+Outlet use local (element) averaged Mach number: {yn(spec.outlet_local_mach)}
 Outlet coupled   transverse relaxation (beta_l): {spec.outlet_beta_l!r}
 Outlet uncoupled transverse relaxation (beta_t): {spec.outlet_beta_t!r}
 Inlet characteristic length: {spec.inlet_len!r}

@@ -176,6 +176,7 @@ BoundaryArgs MakeBoundaryArgs(vcpg_handle *h) {
   b.dlq = h->d_dlq;
   b.btrace = h->d_btrace;
   b.bmach = h->d_bmach;
+  b.bmach_local = h->d_bmach ? h->d_bmach + h->nB : nullptr;   // [nB, 2 nB)
   b.bmach_sums = h->use_bmach_sums ? h->d_bmachsums : nullptr;
   b.bflux = h->d_bflux;
   b.nB = h->nB;
@@ -227,7 +228,7 @@ int InstallOpenBoundary(vcpg_handle *h, const OpenBoundaryHost &ob_host) {
       (rc = upload((void **)&h->d_pc, ob_host.pc.data(), sizeof(double) * ob_host.pc.size())) ||
       (rc = upload((void **)&h->d_dlq, ob_host.dlq.data(), sizeof(double) * ob_host.dlq.size())) ||
       (rc = upload((void **)&h->d_btrace, nullptr, sizeof(double) * nB * 4 * 5 * M2)) ||
-      (rc = upload((void **)&h->d_bmach, nullptr, sizeof(double) * nB)) ||
+      (rc = upload((void **)&h->d_bmach, nullptr, sizeof(double) * nB * 2)) ||
       (rc = upload((void **)&h->d_bforce, nullptr, sizeof(double) * nB * 6)) ||
       (rc = upload((void **)&h->d_bflux, nullptr, sizeof(double) * nB * 4 * 5 * M2)) ||
       (rc = upload((void **)&h->d_sponge, ob_host.spongeIdx.data(), sizeof(int) * ob_host.spongeIdx.size())) ||
@@ -789,6 +790,10 @@ int vcpg_set_open_boundary_partition(vcpg_handle *h, const vcpg_open_boundary *o
     return Fail(h, VCPG_E_INVALID, "declare the partition first (vcpg_set_partition)");
   if (!SupportsOpenBoundaries(h->K, h->M))
     return Fail(h, VCPG_E_UNSUPPORTED_KM, "no open-boundary kernels for this degree");
+  if (ob->outlet_local_mach)
+    return Fail(h, VCPG_E_INVALID, "the outlet's element-local Mach number takes the last "
+                                   "element of a subface, which a partitioned block does not "
+                                   "hold on every rank");
   vcpg_params bp = h->prm;
   for (int d = 0; d < 3; ++d) bp.n_elem[d] = block_n_elem[d];
   const int64_t nBlock = (int64_t)bp.n_elem[0] * bp.n_elem[1] * bp.n_elem[2];

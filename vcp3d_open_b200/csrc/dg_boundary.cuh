@@ -38,6 +38,7 @@ struct BoundaryArgs {
   const double *dlq;           // [M][M]
   double *btrace;              // [nB][4][5][M^2]: value, d/dr, d/ds, d/dt
   double *bmach;               // [nB] area-weighted projected Mach number
+  double *bmach_local;         // [nB] the same averaged over the face's own area
   // Optional [6]: per block face, the sum of the weights over the whole block
   // (a partitioned block sums across its slabs); null: this list's own faces.
   const double *bmach_sums;
@@ -69,7 +70,7 @@ __device__ __forceinline__ int BFastParam(const int d) { return d == 0 ? 1 : 0; 
 // Shared memory of BoundaryTraceKernel in doubles; dynamic above the 48 KB of
 // static shared memory (degrees 7-9).
 template <int K, int M> struct BoundaryTraceSmem {
-  static constexpr int N = 5 * K * K * K + 10 * K * K + 15 * K * M + 21 * M * M;
+  static constexpr int N = 5 * K * K * K + 10 * K * K + 15 * K * M + 22 * M * M;
   static constexpr bool DYN = N * 8 > 48 * 1024;
 };
 
@@ -124,7 +125,9 @@ __global__ void __launch_bounds__(NT) BoundaryTraceKernel(const BoundaryArgs a) 
   __syncthreads();
   double *dst = a.btrace + (size_t)b * 4 * 5 * M2;
   for (int i = threadIdx.x; i < 4 * 5 * M2; i += NT) dst[i] = s_tr[i];
-  // Area-weighted Mach number projected on the normal parametric direction.
+  // Area-weighted Mach number projected on the normal parametric direction, and
+  // its average over the element face (BCStandardCharacteristicSubfaceClass::
+  // WeightedMachElement, src/BoundaryState.cpp:935-994).
   const double *fm = a.face_metric + ((size_t)e * 6 + f) * 13 * M2;
   const int I0 = 4 + 3 * bf[kBfGrad];
   for (int l = threadIdx.x; l < M2; l += NT) {
@@ -138,14 +141,19 @@ __global__ void __launch_bounds__(NT) BoundaryTraceKernel(const BoundaryArgs a) 
     const double aa = sqrt(-kGam * V4Inv);
     const double urr = (u * rrx + v * rry + w * rrz) / magrr;
     s_w[l] = wts * magn * (urr / aa);
+    s_w[M2 + l] = wts * magn;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
     // Only characteristic faces enter the boundary average (the weighted Mach
     // number of the other subfaces is zero, SubfaceBaseClass::WeightedMachElement).
-    double m = 0.0;
-    for (int l = 0; l < M2; ++l) m += s_w[l];
+    double m = 0.0, area = 0.0;
+    for (int l = 0; l < M2; ++l) {
+      m += s_w[l];
+      area += s_w[M2 + l];
+    }
     a.bmach[b] = bf[kBfType] < VCPG_BC_WALL_HEAT_FLUX ? m : 0.0;
+    if (a.bmach_local) a.bmach_local[b] = m / area;
   }
 }
 
@@ -382,7 +390,14 @@ __global__ void __launch_bounds__(NT) BoundaryFluxKernel(const BoundaryArgs a) {
     s_mach = m;
   }
   __syncthreads();
-  const double Mach = s_mach, Mavg2 = Mach * Mach;
+  // The outlet's Mach number: the boundary average, or with "Outlet use local
+  // (element) averaged Mach number" the average over the element face of the
+  // subface's last element (the value the reference's subface member holds,
+  // src/BoundaryState.cpp:1327); the inlets always take the boundary average.
+  const double Mach = (type == VCPG_BC_OUTFLOW_NSCBC && c.localMach && a.bmach_local)
+                          ? a.bmach_local[bf[kBfLast]]
+                          : s_mach;
+  const double Mavg2 = Mach * Mach;
   const double gm1 = kGam - 1.0, ovgm1 = 1.0 / gm1;
   const int I0 = 4 + 3 * ig[0], J0 = 4 + 3 * ig[1], K0 = 4 + 3 * ig[2];
 

@@ -182,7 +182,7 @@ int64_t ElementBytes(int K, int M) {
   return 8 * (3 * 5 * KD + 10 * MD + 6 * 13 * M2 + 15 + 3 * 20 * M2) + 4 * (6 + 2);
 }
 
-int64_t BFaceBytes(int M) { return 8 * (4 + 2 * 4 * 5 * (int64_t)M * M + 1) + 4 * kBfStride; }
+int64_t BFaceBytes(int M) { return 8 * (4 + 2 * 4 * 5 * (int64_t)M * M + 2) + 4 * kBfStride; }
 
 int64_t SpongeBytes(int M) { return 8 * (8 * (int64_t)M * M * M + 6); }
 
@@ -243,7 +243,7 @@ int AllocBucket(vcpg_ensemble *e, Bucket &b, int deg, int64_t capE, int64_t capB
       (rc = alloc((void **)&b.bface, 4 * B * kBfStride)) ||
       (rc = alloc((void **)&b.bpresc, 8 * B * kPrescStride)) ||
       (rc = alloc((void **)&b.btrace, 8 * B * 4 * 5 * b.M2)) ||
-      (rc = alloc((void **)&b.bmach, 8 * B)) ||
+      (rc = alloc((void **)&b.bmach, 8 * 2 * B)) ||
       (rc = alloc((void **)&b.bflux, 8 * B * 4 * 5 * b.M2)) ||
       (rc = alloc((void **)&b.pc, 8 * (size_t)b.M2 * b.M2)) ||
       (rc = alloc((void **)&b.dlq, 8 * (size_t)b.M * b.M)) ||
@@ -318,6 +318,7 @@ BoundaryArgs BucketBoundaryArgs(const vcpg_ensemble *e, const Bucket &b, int req
   a.dlq = b.dlq;
   a.btrace = b.btrace;
   a.bmach = b.bmach;
+  a.bmach_local = b.bmach + b.capB;   // [capB, 2 capB)
   a.bflux = b.bflux;
   a.nB = (int)b.bfaces.HighWater();
   a.tau_num = (double)(b.K * b.K) * e->cfg.rel_penalty;
@@ -580,6 +581,7 @@ int vcpg_ensemble_submit(vcpg_ensemble *ens, const vcpg_params *params,
   for (int64_t r = 0; r < nB; ++r) {
     brows[r * kBfStride + kBfElem] += (int)eFirst;
     brows[r * kBfStride + kBfCase] = slot;
+    if (brows[r * kBfStride + kBfLast] >= 0) brows[r * kBfStride + kBfLast] += (int)bFirst;
   }
   BlockFaceCfg cfgs[6];
   for (int f = 0; f < 6; ++f) {

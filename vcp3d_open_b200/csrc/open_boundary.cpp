@@ -213,8 +213,11 @@ int BuildOpenBoundary(const vcpg_params &prm, const vcpg_open_boundary &ob,
       o.wall_data[f] = sf.wall_data;
       for (int q = 0; q < 5; ++q) o.inflow_super[f][q] = sf.inflow_super[q];
     }
-    // The settings of element e's block face f: its subface's, or ob's.
-    auto settingsOf = [&](int64_t e, int f, std::string &why) -> const vcpg_open_boundary * {
+    // The settings of element e's block face f: its subface's, or ob's (which
+    // subface in *which: -1 for ob).
+    auto settingsOf = [&](int64_t e, int f, std::string &why,
+                          int *which) -> const vcpg_open_boundary * {
+      *which = -1;
       if (!faceHasSub[f]) return &ob;
       const int64_t idx[3] = {e % nI, (e / nI) % nJ, e / ((int64_t)nI * nJ)};
       const int fd = f / 2, a0 = fd == 0 ? 1 : 0, a1 = fd == 2 ? 1 : 2;
@@ -226,6 +229,7 @@ int BuildOpenBoundary(const vcpg_params &prm, const vcpg_open_boundary &ob,
         if (idx[a0] >= sf.elem_begin[0] && idx[a0] < sf.elem_end[0] &&
             idx[a1] >= sf.elem_begin[1] && idx[a1] < sf.elem_end[1]) {
           hit = &subOb[s2];
+          *which = s2;
           ++hits;
         }
       }
@@ -300,10 +304,13 @@ int BuildOpenBoundary(const vcpg_params &prm, const vcpg_open_boundary &ob,
       c.oneMinusBeta = ob.outlet_one_minus_beta ? 1 : 0;
       c.inSigma = ob.inlet_sigma; c.inLen = ob.inlet_len;
       c.incoming = ob.inlet_incoming ? 1 : 0;
+      c.localMach = ob.outlet_local_mach ? 1 : 0;
+      std::vector<int> rowSub;   // subface of each of this block face's rows
       for (int64_t e = 0; e < nE; ++e) {
         if (geom.neighbors[e * 6 + f] >= 0) continue;
         std::string why;
-        const vcpg_open_boundary *o = settingsOf(e, f, why);
+        int which = -1;
+        const vcpg_open_boundary *o = settingsOf(e, f, why, &which);
         if (!o) { err = why; return VCPG_E_INVALID; }
         const int type = o->bc[f];
         if (type == VCPG_BC_NONE) continue;  // stays -1: flagged by the residual kernel
@@ -332,7 +339,8 @@ int BuildOpenBoundary(const vcpg_params &prm, const vcpg_open_boundary &ob,
           return VCPG_E_INVALID;
         }
         const int b = out.nB++;
-        int row[kBfStride] = {(int)e, f, type, grad[0], grad[1], grad[2], 0, 0};
+        rowSub.push_back(which);
+        int row[kBfStride] = {(int)e, f, type, grad[0], grad[1], grad[2], 0, b};
         out.bface.insert(out.bface.end(), row, row + kBfStride);
         double pres[kPrescStride] = {0.0, 0.0, 0.0, 0.0, 0.0};
         if (type == VCPG_BC_OUTFLOW_NSCBC) {
@@ -361,6 +369,12 @@ int BuildOpenBoundary(const vcpg_params &prm, const vcpg_open_boundary &ob,
         for (int l = 0; l < M2; ++l) c.area += wInt[l % M] * wInt[l / M] * fm[3 * M2 + l];
       }
       c.count = out.nB - c.first;
+      // The last face of each subface (rows are in element order): index by
+      // subface (+1, so that the whole-face settings -1 take slot 0).
+      std::vector<int> lastOf((size_t)nSubfaces + 1, -1);
+      for (int r = 0; r < c.count; ++r) lastOf[(size_t)(rowSub[r] + 1)] = c.first + r;
+      for (int r = 0; r < c.count; ++r)
+        out.bface[(size_t)(c.first + r) * kBfStride + kBfLast] = lastOf[(size_t)(rowSub[r] + 1)];
     }
 
     // Sponge layers and the characteristic matching layer.
@@ -477,10 +491,17 @@ void SliceOpenBoundary(const OpenBoundaryHost &block, const int64_t *localToGlob
       newIndex[b] = out.nB++;
       out.bface.insert(out.bface.end(), row, row + kBfStride);
       out.bface[out.bface.size() - kBfStride + kBfElem] = (int)l;
+      out.bface[out.bface.size() - kBfStride + kBfLast] = -1;   // remapped below
       out.bpresc.insert(out.bpresc.end(), block.bpresc.begin() + (size_t)b * kPrescStride,
                         block.bpresc.begin() + (size_t)(b + 1) * kPrescStride);
     }
     out.cfg[f].count = out.nB - out.cfg[f].first;
+  }
+  for (int b = 0; b < block.nB; ++b) {
+    const int nb = newIndex[b];
+    const int last = block.bface[(size_t)b * kBfStride + kBfLast];
+    if (nb >= 0 && last >= 0 && newIndex[last] >= 0)
+      out.bface[(size_t)nb * kBfStride + kBfLast] = newIndex[last];
   }
   // Neighbour table: the handle's, with the owned elements' boundary faces coded.
   out.nbrCode.assign(localNbr, localNbr + nLocal * 6);

@@ -26,6 +26,7 @@ struct BlockFaceCfg {
   double sigma, len;   // outlet: normal relaxation coefficient and characteristic length
   double betaL, betaT; // outlet transverse relaxation coefficients
   double inSigma, inLen;  // inlet: normal relaxation coefficient and characteristic length
+  int localMach;          // outlet: the element-local averaged Mach number (kBfLast's face)
 };
 
 // Entries of one boundary face in the boundary-face list (ints).
@@ -35,6 +36,7 @@ enum BFaceField {
   kBfType = 2,   // enum vcpg_bc
   kBfGrad = 3,   // 3 entries: parametric axis of the normal, first and second transverse
   kBfCase = 6,   // case slot when a launch holds several cases (0 for one case)
+  kBfLast = 7,   // list index of the last face (in element order) of this face's subface
   kBfStride = 8
 };
 

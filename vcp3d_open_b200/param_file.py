@@ -544,8 +544,6 @@ def check_supported(pf: ParamFile) -> None:
         raise UnsupportedOption(f"Fluctuations to add to initial solution: {pf.fluctuations}")
     if pf.compute_average:
         raise UnsupportedOption("Compute average solution")
-    if pf.outlet_local_mach:
-        raise UnsupportedOption("Outlet use local (element) averaged Mach number")
     for face, subs in enumerate(pf.subfaces):
         for sub in subs:
             if sub.kind not in _BC_TO_CASE:

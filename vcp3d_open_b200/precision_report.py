@@ -10,6 +10,8 @@ Every `--every` steps it reports, per the mixed-precision configuration
   rel_l2_state   ||U_mixed - U_fp64|| / ||U_fp64||         (modal entropy variables)
   rel_l2_change  ||U_mixed - U_fp64|| / ||U_fp64 - U_0||   (stricter: error of the change)
   rel_l2_res     ||R_mixed - R_fp64|| / ||R_fp64||         (one residual at the final FP64 state)
+  drift_fp64, drift_mixed  (integral - integral at step 0) / scale of mass, x, y, z
+                 momentum (scale: the mass) and total energy, Gauss quadrature
 
 Prints one JSON line.
 
@@ -25,7 +27,7 @@ import time
 
 import numpy as np
 
-from . import capi, cases, solver, workloads
+from . import capi, cases, solver, tgv_report, workloads
 
 
 def _rel(a: np.ndarray, b: np.ndarray) -> float:
@@ -51,6 +53,7 @@ def run(workload: str, steps: int, every: int, scheme: int = capi.LSRK4) -> dict
     s64 = solver.create(case, precision=capi.FP64, disc=disc)
     s32 = solver.create(case, precision=capi.MIXED, disc=disc)
     u0 = s64.get_state()
+    i0 = tgv_report.conserved_integrals(u0, disc)
     rows = []
     t_wall = time.time()
     done = 0
@@ -65,7 +68,9 @@ def run(workload: str, steps: int, every: int, scheme: int = capi.LSRK4) -> dict
         u64, u32 = s64.get_state(), s32.get_state()
         rows.append({"step": done, "time": sim_time,
                      "rel_l2_state": _rel(u32, u64),
-                     "rel_l2_change": _rel(u32 - u0, u64 - u0)})
+                     "rel_l2_change": _rel(u32 - u0, u64 - u0),
+                     "drift_fp64": tgv_report.drift(tgv_report.conserved_integrals(u64, disc), i0),
+                     "drift_mixed": tgv_report.drift(tgv_report.conserved_integrals(u32, disc), i0)})
     u64, u32 = s64.get_state(), s32.get_state()
     rows[-1]["rel_l2_res"] = residual_difference(s64, s32, u64)
     s64.close()

@@ -178,7 +178,7 @@ def load_case(pf: ParamFile) -> cases.CaseData:
         cml=pf.cml and any(sponge), prescribed_p=prescribed_p, prescribed_inflow=prescribed_in,
         prescribed_total=prescribed_tot, sponge_state=sponge_state, wall_data=wall_data,
         prescribed_super=prescribed_sup, free_stream=tuple(ref.free_stream),
-        subfaces=param_file.case_subfaces(pf))
+        subfaces=param_file.case_subfaces(pf), outlet_local_mach=bool(pf.outlet_local_mach))
     refc = cases.RefConditions(ref.p_ref, ref.rho_ref, ref.u_ref, ref.mu_nondim, speed, vel_dir)
     return cases.CaseData(spec, refc, grid, nodes, xyz, np.ascontiguousarray(cons))
 

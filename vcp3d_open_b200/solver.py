@@ -195,6 +195,7 @@ def open_boundary(case: CaseData) -> capi.OpenBoundary:
     ob.inlet_len, ob.inlet_sigma = s.inlet_len, s.inlet_sigma
     ob.inlet_incoming = 1 if s.inlet_incoming else 0
     ob.cml = 1 if s.cml else 0
+    ob.outlet_local_mach = 1 if s.outlet_local_mach else 0
     ob.sponge_state[:] = (list(s.sponge_state) if s.sponge_state else
                           [rho_in, vel_in[0], vel_in[1], vel_in[2], p_out])
     ob.free_stream[:] = list(s.free_stream if s.free_stream else free_stream_values(s))

@@ -51,6 +51,34 @@ def kinetic_energy(modal: np.ndarray, disc: solver.Discretization) -> float:
     return float(np.sum(JW * 0.5 * rho * q2) / np.sum(JW))
 
 
+def conserved_integrals(modal: np.ndarray, disc: solver.Discretization,
+                        chunk: int = 8192) -> np.ndarray:
+    """Integrals of (rho, rho u, rho v, rho w, rho E) over the block (non-dimensional),
+    by the Gauss quadrature of the elements, in element chunks."""
+    w1 = disc.w_int
+    W = (w1[None, None, :] * w1[None, :, None] * w1[:, None, None]).reshape(-1)
+    out = np.zeros(5)
+    for e0 in range(0, modal.shape[0], chunk):
+        V = _to_points(modal[e0:e0 + chunk], disc.leg_int)
+        V4Inv = 1.0 / V[:, 4]
+        u, v, w = -V4Inv * V[:, 1], -V4Inv * V[:, 2], -V4Inv * V[:, 3]
+        q2 = u * u + v * v + w * w
+        s = GAMMA - (GAMMA - 1.0) * (V[:, 0] - 0.5 * V[:, 4] * q2)
+        rho = (-V[:, 4] * np.exp(s)) ** (-1.0 / (GAMMA - 1.0))
+        p = -V4Inv * rho
+        rE = p / (GAMMA - 1.0) + 0.5 * rho * q2
+        JW = disc.vol_metric[e0:e0 + chunk, 0] * W[None, :]
+        out += np.array([np.sum(JW * q) for q in (rho, rho * u, rho * v, rho * w, rE)])
+    return out
+
+
+def drift(integrals: np.ndarray, initial: np.ndarray) -> list:
+    """(integral - initial) / scale: mass, x, y, z momentum (scale: the mass) and
+    total energy."""
+    scl = np.array([abs(initial[0])] * 4 + [abs(initial[4])])
+    return [float(x) for x in (integrals - initial) / scl]
+
+
 def initial_dissipation(reynolds: float, n: int = 64) -> float:
     """nu <|omega|^2> of u = (sin x cos y cos z, -cos x sin y cos z, 0) on the
     periodic cube (midpoint rule, exact for these trigonometric products)."""
