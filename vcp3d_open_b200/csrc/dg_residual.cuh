@@ -234,7 +234,8 @@ template <int K, int M, typename T = double, bool OPEN = false> struct Plan {
   using CL = CgLayout<K, M, (int)sizeof(T)>;
   static constexpr int CG_TK = 5 * (CL::A::SV > CL::E::SV ? CL::A::SV : CL::E::SV);
   static constexpr int CG_TJ = 5 * (CL::B::SV > CL::D::SV ? CL::B::SV : CL::D::SV);
-  static constexpr int CG = 20 * CL::P::SV + 5 * CL::C::SV + CG_TK + CG_TJ;
+  // The last 32 entries hold the preconditioner and the centre's entropy variables.
+  static constexpr int CG = 20 * CL::P::SV + 5 * CL::C::SV + CG_TK + CG_TJ + 32;
   // Volume phase: tK, tJ, Var, dX, dY, dZ (+ the matching-layer source when
   // OPEN). tK and tJ take the CG's padded layouts where that does not enlarge
   // the shared memory of the kernel.
@@ -968,7 +969,7 @@ __device__ __forceinline__ void KForwardUpdate(T *__restrict__ p, const T *__res
   }
 }
 
-template <int NT, int SLOT, int K, int M, typename T, typename LI, typename LP>
+template <int NT, int SLOT, int K, int M, typename T, typename LI, typename LP, bool DOT = true>
 __device__ __forceinline__ T IBackwardDot(const T *__restrict__ in, const T *__restrict__ p,
                                           T *__restrict__ Ap) {
   constexpr int K2 = K * K, NLINES = 5 * K2;
@@ -987,7 +988,7 @@ __device__ __forceinline__ T IBackwardDot(const T *__restrict__ in, const T *__r
 #pragma unroll
       for (int c = 0; c < M; ++c) acc = fma(Coef<SLOT, K, M, kLegT, T>(c, o), xv[c], acc);
       Ap[ob + o] = acc;
-      part = Fma(p[ob + o], acc, part);
+      if constexpr (DOT) part = Fma(p[ob + o], acc, part);
     }
   }
   return part;
@@ -1026,7 +1027,13 @@ __device__ __forceinline__ void PointOperator(const T *s_cgp, const T *s_jw, con
 // k, j, i transforms back (the last with the partial sums of p . Ap), and the
 // update of x, r and z with the three sums that close the iteration. The two
 // reductions use one barrier each and alternate their scratch areas. The CG
-// arrays use the padded layouts of CgLayout.
+// arrays use the padded layouts of CgLayout. The update is DOF-local.
+// Where every thread owns at most one DOF (K^3 <= threads) the iteration has
+// nine steps: the owner keeps x, r and the search direction p in registers,
+// forms p = z + beta p itself and stores it for the forward transforms (one more
+// barrier), and forms the partial sums of p . Ap from its registers after the
+// backward i transform (one more barrier); z then never passes through shared
+// memory and the first and last transforms read only their lines.
 // ---------------------------------------------------------------------------
 template <int NT, int K, int M, typename T, bool OPEN>
 __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, const T *s_sol,
@@ -1043,9 +1050,10 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
   // Point operators held in registers: one point per thread, or two when the
   // launch bounds leave at least 168 registers per thread.
   constexpr bool kRegD = PP == 1 || (PP == 2 && 65536 / (NT * P::MIN_BLOCKS) >= 168);
+  constexpr bool kOwn = KD <= NT;   // x, r and p of the owned DOF in registers
   T *z = work, *p = z + 5 * LP::SV, *Ap = p + 5 * LP::SV, *x = Ap + 5 * LP::SV;
   T *pInt = x + 5 * LP::SV, *tK = pInt + 5 * LC::SV, *tJ = tK + P::CG_TK;
-  T *dvdu = s_red + 32;  // 15 preconditioner entries
+  T *dvdu = tJ + P::CG_TJ;  // 15 preconditioner entries, then V at the centre
   T *redA = s_red, *redB = s_red + 32;
   T *r = s_R;
   const T volElem = a.elem_scalars[(size_t)e * 15 + 5];
@@ -1053,11 +1061,24 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
   // Padded offset of DOF l = (k K + j) K + i.
   auto off = [](const int l) { return (l / K2) * LP::S2 + ((l / K) % K) * LP::S1 + l % K; };
 
+  // The owned DOF's iterate, residual and search direction (kOwn).
+  T xo[5], ro[5], po[5];
   T m = T(0.0);
-  for (int i = threadIdx.x; i < 5 * KD; i += NT) m = Fmax(m, Fabs(r[i]));
-  for (int l = threadIdx.x; l < KD; l += NT) {
+  if constexpr (kOwn) {
+    const int l = threadIdx.x;
 #pragma unroll
-    for (int q = 0; q < 5; ++q) x[q * LP::SV + off(l)] = T(0.0);
+    for (int q = 0; q < 5; ++q) {
+      ro[q] = l < KD ? r[q * KD + l] : T(0.0);
+      xo[q] = T(0.0);
+      po[q] = T(0.0);
+      m = Fmax(m, Fabs(ro[q]));
+    }
+  } else {
+    for (int i = threadIdx.x; i < 5 * KD; i += NT) m = Fmax(m, Fabs(r[i]));
+    for (int l = threadIdx.x; l < KD; l += NT) {
+#pragma unroll
+      for (int q = 0; q < 5; ++q) x[q * LP::SV + off(l)] = T(0.0);
+    }
   }
   // Inputs of a fused stage update (the state's second register, and in the
   // mixed form the FP64 state itself; the FP64 form takes the state from s_sol)
@@ -1140,9 +1161,17 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
     dvdu[14] = JacInv * abv1;
   }
   __syncthreads();
-  T D[15];
+  // The preconditioner: read as shared-memory broadcasts where it is applied
+  // when x, r and p take registers, else held in registers.
+  T Dr[kOwn ? 1 : 15];
+  if constexpr (!kOwn) {
 #pragma unroll
-  for (int q = 0; q < 15; ++q) D[q] = dvdu[q];
+    for (int q = 0; q < 15; ++q) Dr[q] = dvdu[q];
+  }
+  auto D = [&](const int q) -> T {
+    if constexpr (kOwn) return dvdu[q];
+    else return Dr[q];
+  };
   // The i-direction basis values and the point operators of this thread's points.
   T lc[PP][K];
   T dd[kRegD ? PP : 1][16];
@@ -1157,19 +1186,21 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
   }
   T part = T(0.0);
   for (int l = threadIdx.x; l < KD; l += NT) {
-    const T r0 = r[l], r1 = r[KD + l], r2 = r[2 * KD + l], r3 = r[3 * KD + l],
-            r4 = r[4 * KD + l];
-    const T zz[5] = {D[0] * r0 + D[1] * r1 + D[2] * r2 + D[3] * r3 + D[4] * r4,
-                     D[1] * r0 + D[5] * r1 + D[6] * r2 + D[7] * r3 + D[8] * r4,
-                     D[2] * r0 + D[6] * r1 + D[9] * r2 + D[10] * r3 + D[11] * r4,
-                     D[3] * r0 + D[7] * r1 + D[10] * r2 + D[12] * r3 + D[13] * r4,
-                     D[4] * r0 + D[8] * r1 + D[11] * r2 + D[13] * r3 + D[14] * r4};
-    const T rr[5] = {r0, r1, r2, r3, r4};
+    T rr[5];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) rr[q] = kOwn ? ro[q] : r[q * KD + l];
+    const T zz[5] = {
+        D(0) * rr[0] + D(1) * rr[1] + D(2) * rr[2] + D(3) * rr[3] + D(4) * rr[4],
+        D(1) * rr[0] + D(5) * rr[1] + D(6) * rr[2] + D(7) * rr[3] + D(8) * rr[4],
+        D(2) * rr[0] + D(6) * rr[1] + D(9) * rr[2] + D(10) * rr[3] + D(11) * rr[4],
+        D(3) * rr[0] + D(7) * rr[1] + D(10) * rr[2] + D(12) * rr[3] + D(13) * rr[4],
+        D(4) * rr[0] + D(8) * rr[1] + D(11) * rr[2] + D(13) * rr[3] + D(14) * rr[4]};
     const int o = off(l);
 #pragma unroll
     for (int q = 0; q < 5; ++q) {
-      z[q * LP::SV + o] = zz[q];
+      if constexpr (!kOwn) z[q * LP::SV + o] = zz[q];
       p[q * LP::SV + o] = zz[q];
+      if constexpr (kOwn) po[q] = zz[q];
       part = Fma(rr[q], zz[q], part);
     }
   }
@@ -1183,7 +1214,7 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
       break;
     }
     // Ap = Leg^T3 (w J dU/dV (Leg3 p)) (src/CG_MassMatrix.cpp:408-443).
-    KForwardUpdate<NT, SLOT, K, M, T, LP, typename L::A>(p, z, beta, iter > 0, tK);
+    KForwardUpdate<NT, SLOT, K, M, T, LP, typename L::A>(p, z, beta, !kOwn && iter > 0, tK);
     __syncthreads();
     ContractL<NT, SLOT, K, M, kLeg, 1, 5, K, K, M, K, M, false, T, typename L::A, LB>(tK, tJ);
     __syncthreads();
@@ -1224,31 +1255,52 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
     ContractL<NT, SLOT, K, M, kLegT, 1, 5, M, M, K, M, K, false, T, typename L::D,
               typename L::E>(tJ, tK);
     __syncthreads();
-    const T alpha =
-        dotrz / BlockSum1<NT>(IBackwardDot<NT, SLOT, K, M, T, typename L::E, LP>(tK, p, Ap), redA);
+    T alpha;
+    if constexpr (kOwn) {
+      IBackwardDot<NT, SLOT, K, M, T, typename L::E, LP, false>(tK, p, Ap);
+      __syncthreads();
+      T pAp = T(0.0);
+      if (threadIdx.x < KD) {
+        const int o = off(threadIdx.x);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) pAp = Fma(po[q], Ap[q * LP::SV + o], pAp);
+      }
+      alpha = dotrz / BlockSum1<NT>(pAp, redA);
+    } else {
+      alpha = dotrz /
+              BlockSum1<NT>(IBackwardDot<NT, SLOT, K, M, T, typename L::E, LP>(tK, p, Ap), redA);
+    }
     // Each thread owns whole DOFs: update x and r, precondition, and form the
     // partial sums of the three reductions that close the iteration.
     T zAp = T(0.0), rzNew = T(0.0), rMax = T(0.0);
+    T zn[5] = {T(0.0), T(0.0), T(0.0), T(0.0), T(0.0)};
     for (int l = threadIdx.x; l < KD; l += NT) {
       const int o = off(l);
       T rr[5], ap[5];
 #pragma unroll
       for (int q = 0; q < 5; ++q) {
         ap[q] = Ap[q * LP::SV + o];
-        x[q * LP::SV + o] = Fma(alpha, p[q * LP::SV + o], x[q * LP::SV + o]);
-        rr[q] = Fma(-alpha, ap[q], r[q * KD + l]);
-        r[q * KD + l] = rr[q];
+        if constexpr (kOwn) {
+          xo[q] = Fma(alpha, po[q], xo[q]);
+          rr[q] = Fma(-alpha, ap[q], ro[q]);
+          ro[q] = rr[q];
+        } else {
+          x[q * LP::SV + o] = Fma(alpha, p[q * LP::SV + o], x[q * LP::SV + o]);
+          rr[q] = Fma(-alpha, ap[q], r[q * KD + l]);
+          r[q * KD + l] = rr[q];
+        }
         rMax = Fmax(rMax, Fabs(rr[q]));
       }
       const T zz[5] = {
-          D[0] * rr[0] + D[1] * rr[1] + D[2] * rr[2] + D[3] * rr[3] + D[4] * rr[4],
-          D[1] * rr[0] + D[5] * rr[1] + D[6] * rr[2] + D[7] * rr[3] + D[8] * rr[4],
-          D[2] * rr[0] + D[6] * rr[1] + D[9] * rr[2] + D[10] * rr[3] + D[11] * rr[4],
-          D[3] * rr[0] + D[7] * rr[1] + D[10] * rr[2] + D[12] * rr[3] + D[13] * rr[4],
-          D[4] * rr[0] + D[8] * rr[1] + D[11] * rr[2] + D[13] * rr[3] + D[14] * rr[4]};
+          D(0) * rr[0] + D(1) * rr[1] + D(2) * rr[2] + D(3) * rr[3] + D(4) * rr[4],
+          D(1) * rr[0] + D(5) * rr[1] + D(6) * rr[2] + D(7) * rr[3] + D(8) * rr[4],
+          D(2) * rr[0] + D(6) * rr[1] + D(9) * rr[2] + D(10) * rr[3] + D(11) * rr[4],
+          D(3) * rr[0] + D(7) * rr[1] + D(10) * rr[2] + D(12) * rr[3] + D(13) * rr[4],
+          D(4) * rr[0] + D(8) * rr[1] + D(11) * rr[2] + D(13) * rr[3] + D(14) * rr[4]};
 #pragma unroll
       for (int q = 0; q < 5; ++q) {
-        z[q * LP::SV + o] = zz[q];
+        if constexpr (!kOwn) z[q * LP::SV + o] = zz[q];
+        zn[q] = zz[q];
         zAp = Fma(zz[q], ap[q], zAp);
         rzNew = Fma(rr[q], zz[q], rzNew);
       }
@@ -1257,18 +1309,33 @@ __device__ __forceinline__ void MassSolve(const ResidualArgs &a, const int e, co
     if (rMax < T(a.cg_tol) * rInitMax) break;
     beta = -alpha * zAp / dotrz;
     dotrz = rzNew;
+    // The owner forms the next search direction p = z + beta p and stores it
+    // for the forward transforms.
+    if constexpr (kOwn) {
+      if (threadIdx.x < KD) {
+        const int o = off(threadIdx.x);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+          po[q] = Fma(beta, po[q], zn[q]);
+          p[q * LP::SV + o] = po[q];
+        }
+      }
+      __syncthreads();
+    }
   }
   if (threadIdx.x == 0 && a.cg_stats) {
     atomicAdd(a.cg_stats, (unsigned long long)(iter + 1));
     atomicAdd(a.cg_stats + 1, 1ull);
   }
-  // Every thread reads back the entries it wrote itself in the last update.
+  // Every thread stores the iterate of the DOFs it owns (it wrote their
+  // entries of x itself in the last update).
   const double dtStage = fused ? *a.rk_dt : 0.0;
   if (kPrefetch && fused) CpAsyncWaitAll();
   for (int l = threadIdx.x; l < KD; l += NT) {
     const int o = off(l);
 #pragma unroll
-    for (int q = 0; q < 5; ++q) finish(q * KD + l, double(x[q * LP::SV + o]), dtStage);
+    for (int q = 0; q < 5; ++q)
+      finish(q * KD + l, double(kOwn ? xo[q] : x[q * LP::SV + o]), dtStage);
   }
 }
 

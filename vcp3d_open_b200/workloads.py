@@ -31,6 +31,10 @@ WORKLOADS = {
     "tgv16_p6_lsrk4": dict(_TGV, n_elem=(16, 16, 16), p=6, n_poly_int=16, grid_map="sine",
                            grid_amp=0.05),
     "tgv12_p9_lsrk4": dict(_TGV, n_elem=(12, 12, 12), p=9, grid_map="sine", grid_amp=0.05),
+    # Degrees 2 and 5 (the other degrees of the served ensemble's cases): 40^3 elements
+    # of degree 2 (1.7M DOFs) and 24^3 of degree 5 (3.0M DOFs).
+    "tgv40_p2_lsrk4": dict(_TGV, n_elem=(40, 40, 40), p=2),
+    "tgv24_p5_lsrk4": dict(_TGV, n_elem=(24, 24, 24), p=5),
     # Degree 4 on 16^3 elements: the mixed-versus-FP64 test case (fits a test's time).
     "tgv16_p4_lsrk4": dict(_TGV, n_elem=(16, 16, 16), p=4),
     # Acoustic pulse with open boundaries: [0,20]x[0,10]x[0,10], 40x20x20 elements of
