@@ -235,8 +235,9 @@ void *vcpg_stream(vcpg_handle *h);
  * boundaries of a partitioned block: vcpg_set_open_boundary_partition; vcpg_step and
  * vcpg_synchronization_step are rejected, a step being: vcpg_time_step, the
  * minimum over ranks, then per stage vcpg_rk_stage, the exchange of the ghost
- * states (vcpg_pack_states / vcpg_unpack_states around the transport) and
- * vcpg_residual. */
+ * states (vcpg_pack_send_list or vcpg_pack_states, the transport, then
+ * vcpg_unpack_states) and vcpg_residual (or vcpg_residual_part 0 and 1 around
+ * the exchange). */
 int vcpg_set_partition(vcpg_handle *h, int32_t n_owned, int32_t n_face_ghost);
 
 /* Device-to-device copies, on the handle's stream, between the states of
@@ -472,12 +473,30 @@ int vcpg_set_boundary_mach_sums(vcpg_handle *h, const double *sums);
 
 /* A residual of a partitioned handle in two parts, so that the halo exchange
  * can run meanwhile: part 0 needs no ghost state (the boundary kernels, the
- * face fluxes of the owned layers above the first, the residuals of the layers
- * between the first and the last); part 1, after the ghost layers are
- * unpacked, completes the residual (the first layer's and the upper ghost
- * layer's face fluxes, the first and the last layer's residuals). Part 0 then
- * part 1 equals vcpg_residual without monitoring data. */
+ * face fluxes of elements [0, flux_ready) and the residuals of elements
+ * [0, res_ready) of vcpg_set_partition_parts); part 1, after the ghost states
+ * are unpacked, completes the residual (the face fluxes of the remaining owned
+ * elements and of the face ghosts, the remaining residuals). Part 0 then part
+ * 1 equals vcpg_residual without monitoring data. The overlap of the
+ * reference's Residual (src/SolverClass.cpp:3428-3611). */
 int vcpg_residual_part(vcpg_handle *h, int32_t part);
+
+/* What part 0 of vcpg_residual_part computes, for a handle whose owned
+ * elements are ordered so that [0, flux_ready) have only owned lower
+ * neighbours and [0, res_ready) have no ghost neighbour at all
+ * (0 <= res_ready <= flux_ready <= n_owned). vcpg_set_partition resets both to
+ * 0: part 0 then runs the boundary kernels only. */
+int vcpg_set_partition_parts(vcpg_handle *h, int32_t flux_ready, int32_t res_ready);
+
+/* The owned elements whose states go to a neighbouring rank, as list
+ * `list` (0 <= list < 6: per direction, towards the rank below and above);
+ * vcpg_pack_send_list gathers their states in list order, on the handle's
+ * stream, into a device buffer of count * 5 K^3 doubles (the neighbour's ghost
+ * elements, unpacked there with vcpg_unpack_states). The reference's
+ * DistributeGrid halo (src/SolverClass.cpp:1537-1584) between the blocks of a
+ * 3-D split. */
+int vcpg_set_send_list(vcpg_handle *h, int32_t list, const int32_t *elems, int32_t count);
+int vcpg_pack_send_list(vcpg_handle *h, int32_t list, double *d_buf);
 
 /* ------------------------------------------------------------------------- */
 /* Served ensemble: many cases resident on one GPU, batched by degree.        */

@@ -1,12 +1,13 @@
-"""A block split into k slabs, all slabs driven by one process on one GPU
-(LocalTransport): residuals and steps of the partitioned block against the
-single-handle path on the same block, for periodic blocks and for blocks with
-open boundaries (characteristic conditions, sponge and matching layers,
-subfaces, k boundary faces). Every face is evaluated from the same inputs in
+"""A block split into Cartesian parts (k slabs, i or j splits, 2x2 and 2x2x2
+grids), all parts driven by one process on one GPU (LocalTransport):
+residuals and steps of the partitioned block against the single-handle path on
+the same block, for periodic blocks and for blocks with open boundaries
+(characteristic conditions, sponge and matching layers, subfaces, boundary
+faces in the split directions). Every face is evaluated from the same inputs in
 both and the boundary-averaged Mach number is summed in the same order, so the
 results are equal bit for bit. The residual computes the part that needs no
-ghost state before the ghost layers are written (LocalTransport unpacks them
-only afterwards), so a dependence on a stale ghost would show."""
+ghost state before the ghosts are written (LocalTransport unpacks them only
+afterwards), so a dependence on a stale ghost would show."""
 from __future__ import annotations
 
 import numpy as np
@@ -35,7 +36,7 @@ OPEN = [OPEN_SPECS["pulse_p3_6x4x2_sponge_cml"], OPEN_SPECS["pulse_p3_3x3x4_kfac
         OPEN_SPECS["subfaces_p3_4x4x2"]]
 
 
-def _setup(spec, world, precision=capi.FP64):
+def _setup(spec, grid, precision=capi.FP64):
     case = cases.build_case(spec)
     prm = solver.make_params(case, precision=precision)
     disc = solver.setup_discretization(case, prm)
@@ -44,25 +45,32 @@ def _setup(spec, world, precision=capi.FP64):
     if spec.is_open:
         whole.set_open_boundary(case)
     whole.set_state(modal)
-    shards = [partition.Shard(sl, prm, disc, modal, case=case)
-              for sl in partition.slabs(spec.n_elem, world, periodic_k=spec.periodic[2] == 1)]
+    shards = [partition.Shard(pt, prm, disc, modal, case=case)
+              for pt in partition.parts(spec.n_elem, grid, [v == 1 for v in spec.periodic])]
     return whole, partition.ShardedSolver(partition.LocalTransport(shards))
 
 
 def _gather(sharded, what):
-    out = []
+    """The owned parts in block element order."""
+    n = sum(s.part.n_owned for s in sharded.shards)
+    out = None
     for s in sharded.shards:
         a = s.solver.get_residual() if what == "res" else s.solver.get_state()
-        out.append(a[:s.slab.n_owned])
-    return np.concatenate(out)
+        if out is None:
+            out = np.zeros((n,) + a.shape[1:])
+        out[s.part.local_to_global()[:s.part.n_owned]] = a[:s.part.n_owned]
+    return out
 
 
-@pytest.mark.parametrize("world", [2, 3])
+GRIDS = [(1, 1, 2), (1, 1, 3), (2, 1, 1), (1, 2, 1), (2, 2, 1), (2, 2, 2)]
+
+
+@pytest.mark.parametrize("grid", GRIDS, ids=lambda g: "x".join(map(str, g)))
 @pytest.mark.parametrize("spec", SPECS + OPEN, ids=lambda s: s.name)
-def test_partitioned_residual_and_steps_equal_the_block(gpu_available, spec, world):
-    if world > spec.n_elem[2]:
-        pytest.skip("more slabs than k layers")
-    whole, sharded = _setup(spec, world)
+def test_partitioned_residual_and_steps_equal_the_block(gpu_available, spec, grid):
+    if any(g > n for g, n in zip(grid, spec.n_elem)):
+        pytest.skip("more parts than elements in a direction")
+    whole, sharded = _setup(spec, grid)
     try:
         mon_w = whole.residual(monitoring=True)
         mon_s = sharded.residual(monitoring=True)
@@ -81,7 +89,7 @@ def test_partitioned_residual_and_steps_equal_the_block(gpu_available, spec, wor
 
 
 def test_partitioned_mixed_form(gpu_available):
-    whole, sharded = _setup(SPECS[0], 2, precision=capi.MIXED)
+    whole, sharded = _setup(SPECS[0], (1, 2, 2), precision=capi.MIXED)
     try:
         hw = whole.step(3, capi.LSRK4)
         hs = sharded.step(3, capi.LSRK4)
@@ -94,7 +102,7 @@ def test_partitioned_mixed_form(gpu_available):
 
 
 def test_partitioned_handle_refuses_whole_block_calls(gpu_available):
-    _, sharded = _setup(SPECS[1], 2)
+    _, sharded = _setup(SPECS[1], (1, 1, 2))
     try:
         s = sharded.shards[0].solver
         with pytest.raises(capi.VcpgError, match="stage by stage"):

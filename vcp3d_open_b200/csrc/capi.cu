@@ -19,6 +19,8 @@
 
 using namespace vcpg;
 
+constexpr int kSendLists = 6;   // per direction, towards the rank below and above
+
 struct vcpg_handle {
   vcpg_params prm{};
   int K = 0, M = 0, KD = 0, MD = 0, M2 = 0;
@@ -26,7 +28,12 @@ struct vcpg_handle {
   // Partition (vcpg_set_partition): residual, time step and stages run on the
   // first nOwned elements, face fluxes on the first nFace; both nE otherwise.
   int64_t nOwned = 0, nFace = 0;
-  int64_t layer = 0;   // elements per ghost layer (n_face_ghost of vcpg_set_partition)
+  // vcpg_residual_part: part 0 computes the face fluxes of [0, fluxReady) and the
+  // residuals of [0, resReady) (vcpg_set_partition_parts), part 1 the rest.
+  int64_t fluxReady = 0, resReady = 0;
+  // Owned elements sent to neighbouring ranks (vcpg_set_send_list).
+  int *d_send[kSendLists] = {};
+  int32_t nSend[kSendLists] = {};
   cudaStream_t stream = nullptr;
   double *d_sol = nullptr, *d_solOld = nullptr, *d_res = nullptr, *d_resRaw = nullptr;
   double *d_vol = nullptr, *d_face = nullptr, *d_sc = nullptr;
@@ -334,6 +341,8 @@ int vcpg_destroy(vcpg_handle *h) {
                   h->d_dampst, h->d_cml, h->d_cfg, h->d_fflux, h->d_eddymax, h->d_nmetric,
                   h->d_bforce, h->d_center, h->d_scratch, h->d_bmachsums};
   for (void *p : bufs)
+    if (p) cudaFree(p);
+  for (int *p : h->d_send)
     if (p) cudaFree(p);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -685,12 +694,55 @@ int vcpg_set_partition(vcpg_handle *h, int32_t n_owned, int32_t n_face_ghost) {
                                    "(vcpg_set_open_boundary_partition)");
   h->nOwned = n_owned;
   h->nFace = (int64_t)n_owned + n_face_ghost;
-  h->layer = n_face_ghost;
+  h->fluxReady = h->resReady = 0;   // no overlap until vcpg_set_partition_parts
   h->res_valid = false;
   for (int s = 0; s < 2; ++s) {
     if (h->exec[s]) { cudaGraphExecDestroy(h->exec[s]); h->exec[s] = nullptr; }
     if (h->graph[s]) { cudaGraphDestroy(h->graph[s]); h->graph[s] = nullptr; }
   }
+  return VCPG_OK;
+}
+
+int vcpg_set_partition_parts(vcpg_handle *h, int32_t flux_ready, int32_t res_ready) {
+  if (!h) return VCPG_E_INVALID;
+  if (h->nOwned == h->nE)
+    return Fail(h, VCPG_E_INVALID, "partition parts: a partitioned handle only");
+  if (res_ready < 0 || res_ready > flux_ready || flux_ready > h->nOwned)
+    return Fail(h, VCPG_E_INVALID, "partition parts: need 0 <= res_ready <= flux_ready <= "
+                                   "n_owned");
+  h->fluxReady = flux_ready;
+  h->resReady = res_ready;
+  return VCPG_OK;
+}
+
+int vcpg_set_send_list(vcpg_handle *h, int32_t list, const int32_t *elems, int32_t count) {
+  if (!h || list < 0 || list >= kSendLists || count < 0 || (count > 0 && !elems))
+    return VCPG_E_INVALID;
+  for (int32_t i = 0; i < count; ++i)
+    if (elems[i] < 0 || elems[i] >= h->nOwned)
+      return Fail(h, VCPG_E_INVALID, "send list: elements must be owned");
+  if (h->d_send[list]) {
+    VCPG_CUDA(h, cudaStreamSynchronize(h->stream));
+    cudaFree(h->d_send[list]);
+    h->d_send[list] = nullptr;
+  }
+  h->nSend[list] = count;
+  if (count == 0) return VCPG_OK;
+  cudaError_t e = cudaMalloc((void **)&h->d_send[list], sizeof(int32_t) * count);
+  if (e != cudaSuccess) return Fail(h, VCPG_E_OOM, "cudaMalloc send list");
+  VCPG_CUDA(h, cudaMemcpyAsync(h->d_send[list], elems, sizeof(int32_t) * count,
+                               cudaMemcpyHostToDevice, h->stream));
+  VCPG_CUDA(h, cudaStreamSynchronize(h->stream));
+  return VCPG_OK;
+}
+
+int vcpg_pack_send_list(vcpg_handle *h, int32_t list, double *d_buf) {
+  if (!h || list < 0 || list >= kSendLists) return VCPG_E_INVALID;
+  if (h->nSend[list] == 0) return VCPG_OK;
+  if (!d_buf) return VCPG_E_INVALID;
+  VCPG_CUDA(h, LaunchGatherStates(h->d_sol, h->d_send[list], h->nSend[list], 5 * h->KD, d_buf,
+                                  h->stream));
+  h->launches += 1;
   return VCPG_OK;
 }
 
@@ -842,7 +894,7 @@ int vcpg_residual_part(vcpg_handle *h, int32_t part) {
   if (!h || (part != 0 && part != 1)) return VCPG_E_INVALID;
   if (h->nOwned == h->nE)
     return Fail(h, VCPG_E_INVALID, "residual parts: a partitioned handle only");
-  const int64_t L = h->layer, nO = h->nOwned, nF = h->nFace;
+  const int64_t nO = h->nOwned, nF = h->nFace, fR = h->fluxReady, rR = h->resReady;
   int n = 0;
   auto launch = [&](int phase, int64_t first, int64_t count) -> int {
     if (count <= 0) return VCPG_OK;
@@ -855,25 +907,21 @@ int vcpg_residual_part(vcpg_handle *h, int32_t part) {
   };
   int rc = VCPG_OK;
   if (part == 0) {
-    // No ghost state needed: the boundary kernels (the slab's own faces), the face
-    // fluxes of owned layers 1.., the residuals of the layers between the first
-    // and the last.
+    // No ghost state needed: the boundary kernels (the handle's own boundary
+    // faces), the face fluxes of the owned elements whose lower neighbours are
+    // owned, the residuals of the owned elements without ghost neighbours.
     if (h->open && h->nB > 0) {
       VCPG_CUDA(h, LaunchBoundary(h->K, h->M, MakeBoundaryArgs(h), h->stream));
       n += 2;
     }
-    if ((rc = launch(1, L, nO - L)) || (rc = launch(2, L, nO - 2 * L))) return rc;
+    if ((rc = launch(1, 0, fR)) || (rc = launch(2, 0, rR))) return rc;
     h->launches += n;
     h->res_valid = false;
     return VCPG_OK;
   }
-  // After the ghost layers are in: the first layer's and the upper ghost layer's
-  // face fluxes, the first and the last layer's residuals.
-  const int64_t firstEnd = L < nO ? L : nO;
-  const int64_t lastBegin = (nO - L > L) ? nO - L : L;
-  if ((rc = launch(1, 0, firstEnd)) || (rc = launch(1, nO, nF - nO)) ||
-      (rc = launch(2, 0, firstEnd)) || (rc = launch(2, lastBegin, nO - lastBegin)))
-    return rc;
+  // After the ghost states are in: the remaining owned and the face ghosts' face
+  // fluxes, the remaining residuals.
+  if ((rc = launch(1, fR, nF - fR)) || (rc = launch(2, rR, nO - rR))) return rc;
   h->launches += n;
   rc = CheckStatus(h);
   h->res_valid = rc == VCPG_OK;

@@ -276,6 +276,28 @@ cudaError_t LaunchLsrkStage(double *sol, double *du, const double *res, const do
   return cudaGetLastError();
 }
 
+// The states of listed elements, packed element after element for a neighbouring
+// rank (vcpg_pack_send_list).
+__global__ void GatherStatesKernel(const double *__restrict__ sol, const int *__restrict__ idx,
+                                   const int count, const int per, double *__restrict__ out) {
+  const size_t n = (size_t)count * per;
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const size_t e = t / per;
+    out[t] = sol[(size_t)idx[e] * per + (t - e * per)];
+  }
+}
+
+cudaError_t LaunchGatherStates(const double *sol, const int *idx, int count, int per, double *out,
+                               cudaStream_t st) {
+  const int nt = 256;
+  const size_t n = (size_t)count * per;
+  const size_t blocks = (n + nt - 1) / nt;
+  GatherStatesKernel<<<(unsigned)(blocks < 148 * 8 ? blocks : 148 * 8), nt, 0, st>>>(
+      sol, idx, count, per, out);
+  return cudaGetLastError();
+}
+
 cudaError_t LaunchStartStep(unsigned long long *dt_bits, const double *fixed_dt, double *d_dt,
                             double *hist, int hist_cap, int *counter, unsigned int *ticket,
                             double *sol, double *reg, const double *res, int kind, double ca,

@@ -77,6 +77,10 @@ cudaError_t LaunchStartStep(unsigned long long *dt_bits, const double *fixed_dt,
                             double *hist, int hist_cap, int *counter, unsigned int *ticket,
                             double *sol, double *reg, const double *res, int kind, double ca,
                             double cb, size_t n, cudaStream_t st);
+// out[i][:] = sol[idx[i]][:] for i < count, per doubles per element (the
+// indices are checked on the host when the list is set).
+cudaError_t LaunchGatherStates(const double *sol, const int *idx, int count, int per, double *out,
+                               cudaStream_t st);
 // Stage updates; d_dt holds one time step per case (one entry for a single case).
 cudaError_t LaunchSspStage(double *sol, double *solOld, const double *res, const double *d_dt,
                            double alpha, double beta, int copyOld, size_t n, cudaStream_t st,

@@ -361,6 +361,21 @@ class Solver:
         self._check(self.lib.vcpg_unpack_states(self.h, int(first), int(count),
                                                 C.c_void_p(d_buf)), "unpack_states")
 
+    def set_partition_parts(self, flux_ready: int, res_ready: int):
+        self._check(self.lib.vcpg_set_partition_parts(self.h, int(flux_ready), int(res_ready)),
+                    "set_partition_parts")
+
+    def set_send_list(self, lst: int, elems):
+        a = np.ascontiguousarray(elems, dtype=np.int32)
+        self._check(self.lib.vcpg_set_send_list(self.h, int(lst),
+                                                a.ctypes.data_as(C.POINTER(C.c_int32)), len(a)),
+                    "set_send_list")
+
+    def pack_send_list(self, lst: int, d_buf: int):
+        """States of send list lst's elements, in list order, into the device buffer d_buf."""
+        self._check(self.lib.vcpg_pack_send_list(self.h, int(lst), C.c_void_p(d_buf)),
+                    "pack_send_list")
+
     def rk_stage(self, scheme: int, stage: int, dt: float):
         self._check(self.lib.vcpg_rk_stage(self.h, int(scheme), int(stage), float(dt)),
                     "rk_stage")
