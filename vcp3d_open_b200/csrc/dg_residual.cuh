@@ -214,11 +214,47 @@ __device__ __forceinline__ void BlockReduce3(T &a, T &b, T &c, T *red) {
   }
 }
 
-// Upper bound of the CTAs per SM that __launch_bounds__ asks the register
-// allocator for in the FP64 form (a higher value caps the registers per thread
-// lower: 4 CTAs of 128 threads allow 128).
-#ifndef VCPG_FP64_MAX_MIN_BLOCKS
-#define VCPG_FP64_MAX_MIN_BLOCKS 4
+// Upper bounds of the CTAs per SM that __launch_bounds__ asks the register
+// allocator for (a higher value caps the registers per thread lower: 4 CTAs of
+// 128 threads allow 128 registers, 6 allow 80, 8 allow 64), where the shared
+// memory would allow more. Chosen by measurement on B200 (bench.py, TGV and
+// pulse workloads, degrees 2-5): more, smaller-register CTAs pay for the FP32
+// form of degrees 2 and 3 (16-44 % per step despite small spills) and for the
+// face-flux kernel of every degree up to 5 except FP64 degree 3, whose shared
+// memory allows no more; the FP64 residual kernel of degree 2 and the FP32
+// one of degrees 4-5 lose with more.
+#ifndef VCPG_CAP_RES_FP64
+#define VCPG_CAP_RES_FP64 4          // FP64 residual kernel, 128-thread CTAs
+#endif
+#ifndef VCPG_CAP_RES_FP64_SMALL
+#define VCPG_CAP_RES_FP64_SMALL 4    // the same, degrees <= 2
+#endif
+#ifndef VCPG_CAP_RES_FP32_K4
+#define VCPG_CAP_RES_FP32_K4 6       // FP32 residual kernel, degree 3
+#endif
+#ifndef VCPG_CAP_RES_FP32_SMALL
+#define VCPG_CAP_RES_FP32_SMALL 8    // FP32 residual kernel, degrees <= 2
+#endif
+#ifndef VCPG_CAP_RES_FP32_256
+#define VCPG_CAP_RES_FP32_256 3      // FP32 residual kernel, 256-thread CTAs (degrees >= 4)
+#endif
+#ifndef VCPG_CAP_FLUX_FP64_SMALL
+#define VCPG_CAP_FLUX_FP64_SMALL 6   // FP64 face-flux kernel, degrees <= 2
+#endif
+#ifndef VCPG_CAP_FLUX_FP64_K4
+#define VCPG_CAP_FLUX_FP64_K4 4      // FP64 face-flux kernel, degree 3
+#endif
+#ifndef VCPG_CAP_FLUX_FP32_K4
+#define VCPG_CAP_FLUX_FP32_K4 8      // FP32 face-flux kernel, degree 3
+#endif
+#ifndef VCPG_CAP_FLUX_FP32_SMALL
+#define VCPG_CAP_FLUX_FP32_SMALL 8   // FP32 face-flux kernel, degrees <= 2
+#endif
+#ifndef VCPG_CAP_FLUX_FP64_BIG
+#define VCPG_CAP_FLUX_FP64_BIG 2     // FP64 face-flux kernel, 160-thread CTAs (degrees >= 4)
+#endif
+#ifndef VCPG_CAP_FLUX_FP32_BIG
+#define VCPG_CAP_FLUX_FP32_BIG 4     // FP32 face-flux kernel, 160-thread CTAs
 #endif
 
 // Shared-memory plan (doubles) of the fused kernel for a (K, M) pair.
@@ -262,17 +298,19 @@ template <int K, int M, typename T = double, bool OPEN = false> struct Plan {
   // loops over the elements.
   static constexpr bool BIG = BYTES > 227 * 1024;
   static constexpr int SCRATCH = (TOTAL + 3) / 4 * 4;
-  // Threads per CTA and the CTAs per SM that the shared memory allows (227 KB).
   // Threads per CTA and CTAs per SM (through __launch_bounds__ they bound the
   // registers per thread). FP64: 128 threads cover the widest contraction stage
   // of degrees <= 4 in one or two passes; two CTAs of 128 threads are used
   // whenever two fit the 227 KB of shared memory (up to 255 registers per thread
-  // then), else one CTA of 256 threads. FP32: 256 threads from degree 4 up, as
-  // many CTAs as the shared memory allows (at most 3 of 256 or 4 of 128 threads).
+  // then), else one CTA of 256 threads. FP32: 256 threads from degree 4 up. As
+  // many CTAs as the shared memory allows, up to the VCPG_CAP_RES_* bounds.
   static constexpr int FIT = (int)(227 * 1024 / BYTES);
   static constexpr bool FP64 = sizeof(T) == 8;
   static constexpr int NT = FP64 ? ((K <= 4 || FIT >= 2) ? 128 : 256) : (K >= 5 ? 256 : 128);
-  static constexpr int CAP = FP64 ? VCPG_FP64_MAX_MIN_BLOCKS : (NT == 256 ? 3 : 4);
+  static constexpr int CAP =
+      FP64 ? (K <= 3 ? VCPG_CAP_RES_FP64_SMALL : VCPG_CAP_RES_FP64)
+           : (NT == 256 ? VCPG_CAP_RES_FP32_256
+                        : (K == 4 ? VCPG_CAP_RES_FP32_K4 : VCPG_CAP_RES_FP32_SMALL));
   static constexpr int MIN_BLOCKS = FIT < 1 ? 1 : (FIT > CAP ? CAP : FIT);
 };
 
@@ -1413,13 +1451,15 @@ template <int K, int M, typename T = double> struct FluxPlan {
   // Above one CTA's shared memory: global scratch per CTA, elements in a loop.
   static constexpr bool BIG = BASE_BYTES > 227 * 1024;
   static constexpr int SCRATCH = (TOTAL + 3) / 4 * 4;
-  // Launch shape measured best on B200 over 96..192 threads and 2..4 CTAs per SM:
-  // 128 threads and up to 4 CTAs (<= 128 registers) for degree <= 3; from degree
-  // 4 on, 160 threads (the 3 M^2 face points of a group in one pass) with up to
-  // 2 CTAs (FP64) or 3 CTAs (FP32).
+  // Launch shape measured on B200: 128 threads for degree <= 3; from degree 4
+  // on, 160 threads (the 3 M^2 face points of a group in one pass); CTAs per SM
+  // up to the VCPG_CAP_FLUX_* bounds.
   static constexpr bool FP64 = sizeof(T) == 8;
   static constexpr int NT = K <= 4 ? 128 : 160;
-  static constexpr int CAP = K <= 4 ? 4 : (FP64 ? 2 : 3);
+  static constexpr int CAP =
+      K <= 3 ? (FP64 ? VCPG_CAP_FLUX_FP64_SMALL : VCPG_CAP_FLUX_FP32_SMALL)
+      : K == 4 ? (FP64 ? VCPG_CAP_FLUX_FP64_K4 : VCPG_CAP_FLUX_FP32_K4)
+               : (FP64 ? VCPG_CAP_FLUX_FP64_BIG : VCPG_CAP_FLUX_FP32_BIG);
   static constexpr int FIT = (int)(227 * 1024 / BASE_BYTES);
   static constexpr int MIN_BLOCKS = FIT < 1 ? 1 : (FIT > CAP ? CAP : FIT);
   // The three lower neighbours' FP64 states staged in shared memory (after the
