@@ -220,9 +220,9 @@ __device__ __forceinline__ void BlockReduce3(T &a, T &b, T &c, T *red) {
 // memory would allow more. Chosen by measurement on B200 (bench.py, TGV and
 // pulse workloads, degrees 2-5): more, smaller-register CTAs pay for the FP32
 // form of degrees 2 and 3 (16-44 % per step despite small spills) and for the
-// face-flux kernel of every degree up to 5 except FP64 degree 3, whose shared
-// memory allows no more; the FP64 residual kernel of degree 2 and the FP32
-// one of degrees 4-5 lose with more.
+// face-flux kernel of every degree up to 5 (FP64 degree 3: 5 CTAs without the
+// neighbour staging, which leaves room for 4 only, +5 %); the FP64 residual
+// kernel of degree 2 and the FP32 one of degrees 4-5 lose with more.
 #ifndef VCPG_CAP_RES_FP64
 #define VCPG_CAP_RES_FP64 4          // FP64 residual kernel, 128-thread CTAs
 #endif
@@ -242,7 +242,7 @@ __device__ __forceinline__ void BlockReduce3(T &a, T &b, T &c, T *red) {
 #define VCPG_CAP_FLUX_FP64_SMALL 6   // FP64 face-flux kernel, degrees <= 2
 #endif
 #ifndef VCPG_CAP_FLUX_FP64_K4
-#define VCPG_CAP_FLUX_FP64_K4 4      // FP64 face-flux kernel, degree 3
+#define VCPG_CAP_FLUX_FP64_K4 5      // FP64 face-flux kernel, degree 3 (no neighbour staging then)
 #endif
 #ifndef VCPG_CAP_FLUX_FP32_K4
 #define VCPG_CAP_FLUX_FP32_K4 8      // FP32 face-flux kernel, degree 3
