@@ -290,7 +290,9 @@ template <int K, int M, typename T = double, bool OPEN = false> struct Plan {
   // face vectors (basis and derivative at r = -1, +1).
   // Face vectors: basis and derivative at r = -1, +1 (4 K values, room for 28 at least).
   static constexpr int FV = 4 * (K > 7 ? K : 7);
-  static constexpr int PERSIST = 10 * KD + 6 * MD + 64 + FV;
+  // Reduction scratch: two areas of 3 values per warp of up to 512 threads.
+  static constexpr int RED = 96;
+  static constexpr int PERSIST = 10 * KD + 6 * MD + RED + FV;
   static constexpr int TOTAL = PERSIST + WORK;
   static constexpr size_t BYTES = sizeof(T) * (size_t)TOTAL;
   // Above the 227 KB of one CTA (degrees 7-9 in FP64): the arrays live in a
@@ -300,13 +302,14 @@ template <int K, int M, typename T = double, bool OPEN = false> struct Plan {
   static constexpr int SCRATCH = (TOTAL + 3) / 4 * 4;
   // Threads per CTA and CTAs per SM (through __launch_bounds__ they bound the
   // registers per thread). FP64: 128 threads cover the widest contraction stage
-  // of degrees <= 4 in one or two passes; two CTAs of 128 threads are used
-  // whenever two fit the 227 KB of shared memory (up to 255 registers per thread
-  // then), else one CTA of 256 threads. FP32: 256 threads from degree 4 up. As
-  // many CTAs as the shared memory allows, up to the VCPG_CAP_RES_* bounds.
+  // of degrees <= 3 in one or two passes; from degree 4 on 256 threads (degree
+  // 4 at 2 CTAs of 256 against 2 of 128: ResidualKernel 1.59 -> 1.41 ms on the
+  // 40x20x20 pulse, 21.2 -> 20.5 ms on TGV 48^3, measured on B200). FP32: 256
+  // threads from degree 4 up. As many CTAs as the shared memory allows, up to
+  // the VCPG_CAP_RES_* bounds.
   static constexpr int FIT = (int)(227 * 1024 / BYTES);
   static constexpr bool FP64 = sizeof(T) == 8;
-  static constexpr int NT = FP64 ? ((K <= 4 || FIT >= 2) ? 128 : 256) : (K >= 5 ? 256 : 128);
+  static constexpr int NT = K <= 4 ? 128 : 256;
   static constexpr int CAP =
       FP64 ? (K <= 3 ? VCPG_CAP_RES_FP64_SMALL : VCPG_CAP_RES_FP64)
            : (NT == 256 ? VCPG_CAP_RES_FP32_256
@@ -1387,7 +1390,7 @@ __device__ __forceinline__ void ResidualElement(const ResidualArgs &a, const int
   using P = Plan<K, M, T, OPEN>;
   constexpr int KD = P::KD, MD = P::MD;
   T *s_sol = smem, *s_R = s_sol + 5 * KD, *s_cgp = s_R + 5 * KD, *s_jw = s_cgp + 5 * MD;
-  T *s_red = s_jw + MD, *s_fv = s_red + 64, *work = s_fv + P::FV;
+  T *s_red = s_jw + MD, *s_fv = s_red + P::RED, *work = s_fv + P::FV;
   // Several cases per launch: skip unused elements and cases in another state.
   double mu = a.mu;
   if (a.cases.elem_case) {
