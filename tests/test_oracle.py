@@ -14,7 +14,7 @@ from oracle import records
 from vcp3d_open_b200 import cases, solver
 
 # Tolerances (FP64): states after N steps and time steps are compared at the
-# north-star bar of 1e-12 relative L2; single residuals carry the ~1e-14
+# stated FP64 bar of 1e-12 relative L2; single residuals carry the ~1e-14
 # relative differences of independently computed metric terms, amplified by
 # the cancellation inside the residual, so they are held to 1e-10.
 TOL_STATE = 1e-12

@@ -1,6 +1,6 @@
 """Parity of the CUDA path (through the C ABI) with the reference and with the
 CPU restatement. Tolerances: states and time steps after N steps 1e-12
-relative L2; single residuals 1e-10 (see test_oracle.py);
+relative L2 (the stated FP64 bar); single residuals 1e-10 (see test_oracle.py);
 CUDA vs the restatement on identical inputs 1e-12."""
 from __future__ import annotations
 

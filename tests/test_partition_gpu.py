@@ -1,5 +1,6 @@
 """A block split into Cartesian parts (k slabs, i or j splits, 2x2 and 2x2x2
-grids), all parts driven by one process on one GPU (LocalTransport):
+grids, and the unsplit block through the same stage-wise loop), all parts
+driven by one process on one GPU (LocalTransport):
 residuals and steps of the partitioned block against the single-handle path on
 the same block, for periodic blocks and for blocks with open boundaries
 (characteristic conditions, sponge and matching layers, subfaces, boundary
@@ -62,7 +63,7 @@ def _gather(sharded, what):
     return out
 
 
-GRIDS = [(1, 1, 2), (1, 1, 3), (2, 1, 1), (1, 2, 1), (2, 2, 1), (2, 2, 2)]
+GRIDS = [(1, 1, 1), (1, 1, 2), (1, 1, 3), (2, 1, 1), (1, 2, 1), (2, 2, 1), (2, 2, 2)]
 
 
 @pytest.mark.parametrize("grid", GRIDS, ids=lambda g: "x".join(map(str, g)))
