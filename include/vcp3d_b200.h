@@ -553,6 +553,16 @@ int vcpg_ensemble_submit(vcpg_ensemble *ens, const vcpg_params *params,
                          const vcpg_open_boundary *ob, int32_t p_grid, int32_t dof_location,
                          const double *grid_nodes, int64_t *case_id);
 
+/* vcpg_ensemble_submit for a case with several subfaces per block face (as
+ * vcpg_set_open_boundary_subfaces): the reference's mSubfaces[f][l]
+ * (src/SolverClass.cpp:1646-1652) for a served case. */
+int vcpg_ensemble_submit_subfaces(vcpg_ensemble *ens, const vcpg_params *params,
+                                  const vcpg_operators *ops, const vcpg_geometry *geom,
+                                  const double *modal_state, int32_t n_steps,
+                                  const vcpg_open_boundary *ob, const vcpg_subface *subfaces,
+                                  int32_t n_subfaces, int32_t p_grid, int32_t dof_location,
+                                  const double *grid_nodes, int64_t *case_id);
+
 /* Enqueues one time step of every bucket with resident cases; does not wait. */
 int vcpg_ensemble_step(vcpg_ensemble *ens);
 

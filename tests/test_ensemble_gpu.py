@@ -97,6 +97,27 @@ def test_ensemble_matches_single_case_path(gpu_available):
             h.close()
 
 
+def test_subface_case_matches_single_case_path(gpu_available):
+    """A served case with several subfaces on a block face (an inflow and an
+    isothermal wall on i-min, an outflow and a heat-flux wall on i-max) takes
+    the same steps as the single-case handle, alone and beside a pulse case."""
+    from make_golden import OPEN_SPECS
+    spec = OPEN_SPECS["subfaces_p3_4x4x2"]
+    other = serving.pulse_spec(5, 3, 0.4, "p")
+    ens = serving.Ensemble(_caps([spec, other]), precision=capi.FP64, max_cases=4)
+    ids = [ens.submit(serving.prepare(s, capi.FP64), STEPS) for s in (spec, other)]
+    res = _run_to_completion(ens, ids)
+    ens.close()
+    h = solver.create(cases.build_case(spec))
+    try:
+        hist = h.step(STEPS, capi.LSRK4)
+        state, t = res[ids[0]]
+        assert rel_l2(state, h.get_state()) < 1e-13
+        assert t == pytest.approx(float(np.sum(hist)), rel=1e-13)
+    finally:
+        h.close()
+
+
 def test_admission_by_footprint(gpu_available):
     specs = [serving.vortex_spec(4, 3, 0.4, 4.0, "a"), serving.vortex_spec(4, 3, 0.3, 3.0, "b")]
     ne = serving.case_sizes(specs[0])[0]

@@ -39,7 +39,7 @@ EXPORTED = [
     "vcpg_line_contraction_probe",
     "vcpg_time_step_noalloc", "vcpg_set_open_boundary", "vcpg_set_open_boundary_subfaces", "vcpg_ensemble_create",
     "vcpg_ensemble_destroy", "vcpg_ensemble_last_error", "vcpg_ensemble_footprint",
-    "vcpg_ensemble_submit", "vcpg_ensemble_step", "vcpg_ensemble_poll", "vcpg_ensemble_retire",
+    "vcpg_ensemble_submit", "vcpg_ensemble_submit_subfaces", "vcpg_ensemble_step", "vcpg_ensemble_poll", "vcpg_ensemble_retire",
     "vcpg_ensemble_sync", "vcpg_ensemble_stats",
 ]
 
@@ -178,6 +178,10 @@ def load() -> C.CDLL:
                                          C.POINTER(Geometry), dp, C.c_int32,
                                          C.POINTER(OpenBoundary), C.c_int32, C.c_int32, dp,
                                          C.POINTER(C.c_int64)]
+    lib.vcpg_ensemble_submit_subfaces.argtypes = [
+        hp, C.POINTER(Params), C.POINTER(Operators), C.POINTER(Geometry), dp, C.c_int32,
+        C.POINTER(OpenBoundary), C.POINTER(Subface), C.c_int32, C.c_int32, C.c_int32, dp,
+        C.POINTER(C.c_int64)]
     lib.vcpg_ensemble_step.argtypes = [hp]
     lib.vcpg_ensemble_poll.argtypes = [hp, C.POINTER(C.c_int64), C.c_int32, C.POINTER(C.c_int32)]
     lib.vcpg_ensemble_retire.argtypes = [hp, C.c_int64, dp, dp]

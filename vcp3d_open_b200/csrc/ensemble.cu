@@ -469,7 +469,18 @@ int vcpg_ensemble_submit(vcpg_ensemble *ens, const vcpg_params *params,
                          const double *modal_state, int32_t n_steps,
                          const vcpg_open_boundary *ob, int32_t p_grid, int32_t dof_location,
                          const double *grid_nodes, int64_t *case_id) {
-  if (!ens || !params || !ops || !geom || !modal_state || !case_id || n_steps < 0)
+  return vcpg_ensemble_submit_subfaces(ens, params, ops, geom, modal_state, n_steps, ob, nullptr,
+                                       0, p_grid, dof_location, grid_nodes, case_id);
+}
+
+int vcpg_ensemble_submit_subfaces(vcpg_ensemble *ens, const vcpg_params *params,
+                                  const vcpg_operators *ops, const vcpg_geometry *geom,
+                                  const double *modal_state, int32_t n_steps,
+                                  const vcpg_open_boundary *ob, const vcpg_subface *subfaces,
+                                  int32_t n_subfaces, int32_t p_grid, int32_t dof_location,
+                                  const double *grid_nodes, int64_t *case_id) {
+  if (!ens || !params || !ops || !geom || !modal_state || !case_id || n_steps < 0 ||
+      n_subfaces < 0 || (n_subfaces > 0 && (!subfaces || !ob)))
     return VCPG_E_INVALID;
   vcpg_ensemble *e = ens;
   if (params->sgs_model != VCPG_SGS_NONE)
@@ -496,9 +507,13 @@ int vcpg_ensemble_submit(vcpg_ensemble *ens, const vcpg_params *params,
   // Sizes first (cheap), so that a refused case costs no set-up work.
   int64_t nB = 0, nS = 0;
   if (ob) {
+    // A block face with subfaces takes its conditions from them (none periodic).
+    bool sub[6] = {false, false, false, false, false, false};
+    for (int32_t s = 0; s < n_subfaces; ++s)
+      if (subfaces[s].face >= 0 && subfaces[s].face < 6) sub[subfaces[s].face] = true;
     for (int64_t e2 = 0; e2 < nE; ++e2)
       for (int f = 0; f < 6; ++f)
-        if (geom->neighbors[e2 * 6 + f] < 0 && ob->bc[f] != VCPG_BC_NONE) ++nB;
+        if (geom->neighbors[e2 * 6 + f] < 0 && (ob->bc[f] != VCPG_BC_NONE || sub[f])) ++nB;
     const int n3[3] = {params->n_elem[0], params->n_elem[1], params->n_elem[2]};
     for (int k = 0; k < n3[2]; ++k)
       for (int j = 0; j < n3[1]; ++j)
@@ -544,7 +559,8 @@ int vcpg_ensemble_submit(vcpg_ensemble *ens, const vcpg_params *params,
   OpenBoundaryHost obh;
   if (ob) {
     std::string err;
-    int rc = BuildOpenBoundary(*params, *ob, *geom, p_grid, dof_location, grid_nodes, obh, err);
+    int rc = BuildOpenBoundary(*params, *ob, *geom, p_grid, dof_location, grid_nodes, obh, err,
+                               subfaces, n_subfaces);
     if (rc) { rollback(); return Fail(e, rc, err); }
     if (obh.nB != nB || obh.nS != nS) {
       rollback();

@@ -99,6 +99,7 @@ class PreparedCase:
     grid_nodes: Optional[np.ndarray]
     n_bfaces: int
     n_sponge: int
+    subfaces: Optional[object] = None   # vcpg_subface array (several per block face)
 
     @property
     def n_dofs(self) -> int:
@@ -110,14 +111,15 @@ def prepare(spec: cases.CaseSpec, precision: int) -> PreparedCase:
     params = solver.make_params(case, metric_compat=True, precision=precision)
     disc = solver.setup_discretization(case, params)
     modal = np.ascontiguousarray(solver.nodal_to_modal(case, params))
-    ob, nodes, nb, ns = None, None, 0, 0
+    ob, nodes, nb, ns, sfs = None, None, 0, 0, None
     if spec.is_open:
         ob = solver.open_boundary(case)
+        sfs = solver.subfaces(case)
         nodes = np.ascontiguousarray(case.elem_nodes, dtype=np.float64)
         nbr = disc.neighbors
         nb = int(sum(np.count_nonzero(nbr[:, f] < 0) for f in range(6) if spec.bc[f] != "periodic"))
         ns = _sponge_elements(spec)
-    return PreparedCase(spec, params, disc, modal, ob, nodes, nb, ns)
+    return PreparedCase(spec, params, disc, modal, ob, nodes, nb, ns, sfs)
 
 
 def _sponge_elements(spec: cases.CaseSpec) -> int:
@@ -177,10 +179,16 @@ class Ensemble:
         geom = capi.Geometry(capi.ptr(arrs[7]), capi.ptr(arrs[8]), capi.ptr(arrs[9]), capi.ptr(nbr))
         cid = C.c_int64()
         ob = C.byref(pc.ob) if pc.ob is not None else None
-        rc = self.lib.vcpg_ensemble_submit(self.h, C.byref(pc.params), C.byref(ops), C.byref(geom),
-                                           capi.ptr(pc.modal), n_steps, ob, pc.spec.p_grid,
-                                           cases.dof_location_code(pc.spec),
-                                           capi.ptr(pc.grid_nodes), C.byref(cid))
+        if pc.subfaces is not None:
+            rc = self.lib.vcpg_ensemble_submit_subfaces(
+                self.h, C.byref(pc.params), C.byref(ops), C.byref(geom), capi.ptr(pc.modal),
+                n_steps, ob, pc.subfaces, len(pc.subfaces), pc.spec.p_grid,
+                cases.dof_location_code(pc.spec), capi.ptr(pc.grid_nodes), C.byref(cid))
+        else:
+            rc = self.lib.vcpg_ensemble_submit(self.h, C.byref(pc.params), C.byref(ops),
+                                               C.byref(geom), capi.ptr(pc.modal), n_steps, ob,
+                                               pc.spec.p_grid, cases.dof_location_code(pc.spec),
+                                               capi.ptr(pc.grid_nodes), C.byref(cid))
         if rc == 7:   # VCPG_E_ADMISSION
             return None
         if rc != capi.VCPG_OK:
