@@ -380,8 +380,9 @@ typedef struct vcpg_open_boundary {
                                      face of the subface's last element in element order,
                                      whose value the reference's subface-wide member
                                      holds when the residual runs
-                                     (src/BoundaryState.cpp:990, 1327). Not with
-                                     vcpg_set_open_boundary_partition.                 */
+                                     (src/BoundaryState.cpp:990, 1327); in a
+                                     partitioned block see
+                                     vcpg_set_boundary_outlet_mach.                    */
 } vcpg_open_boundary;
 
 /* Configures open boundaries on a handle whose geometry has boundary faces
@@ -449,7 +450,7 @@ int vcpg_set_open_boundary_subfaces(vcpg_handle *h, const vcpg_open_boundary *ob
  * src/SpongeLayer.cpp:135-136). The boundary-averaged Mach number spans the
  * ranks: before each residual the caller gathers every rank's
  * vcpg_boundary_mach_weights, sums each block face's weights in block element
- * order (rank order along k) and passes the sums to
+ * order (the ranks' lists merged by element index) and passes the sums to
  * vcpg_set_boundary_mach_sums (src/SolverClass.cpp:2556-2560). */
 int vcpg_set_open_boundary_partition(vcpg_handle *h, const vcpg_open_boundary *ob,
                                      const vcpg_subface *subfaces, int32_t n_subfaces,
@@ -470,6 +471,22 @@ int vcpg_boundary_mach_weights(vcpg_handle *h, double *weights, int32_t *counts)
  * next residuals divide by the block face's area in place of summing the
  * handle's own faces; NULL returns to the handle's own sums. */
 int vcpg_set_boundary_mach_sums(vcpg_handle *h, const double *sums);
+
+/* The outlet's element-local averaged Mach number ("Outlet use local averaged
+ * Mach number") in a partitioned block: the reference's subface member holds the
+ * value of the subface's last element face (src/BoundaryState.cpp:990, 1327),
+ * which may lie on another rank. vcpg_boundary_rows gives per boundary row of
+ * the handle its row in the whole block's boundary-face list (block face by
+ * block face, element order) and the block row of its subface's last face (-1
+ * without); vcpg_boundary_local_mach the rows' face-averaged Mach numbers of the
+ * last boundary trace (vcpg_boundary_mach_weights runs one); with these the
+ * ranks exchange the last faces' values and vcpg_set_boundary_outlet_mach sets
+ * per row the value its outlet uses (NULL: the handle's own last face). A
+ * partitioned handle whose last faces lie elsewhere refuses residuals until it
+ * is set. */
+int vcpg_boundary_rows(vcpg_handle *h, int32_t *block_rows, int32_t *block_last);
+int vcpg_boundary_local_mach(vcpg_handle *h, double *values);
+int vcpg_set_boundary_outlet_mach(vcpg_handle *h, const double *values);
 
 /* A residual of a partitioned handle in two parts, so that the halo exchange
  * can run meanwhile: part 0 needs no ghost state (the boundary kernels, the

@@ -4,7 +4,8 @@ driven by one process on one GPU (LocalTransport):
 residuals and steps of the partitioned block against the single-handle path on
 the same block, for periodic blocks and for blocks with open boundaries
 (characteristic conditions, sponge and matching layers, subfaces, boundary
-faces in the split directions). Every face is evaluated from the same inputs in
+faces in the split directions, the outlet's element-local Mach number taken
+from a subface's last face in another part). Every face is evaluated from the same inputs in
 both and the boundary-averaged Mach number is summed in the same order, so the
 results are equal bit for bit. The residual computes the part that needs no
 ghost state before the ghosts are written (LocalTransport unpacks them only
@@ -34,7 +35,7 @@ SPECS = [
 
 
 OPEN = [OPEN_SPECS["pulse_p3_6x4x2_sponge_cml"], OPEN_SPECS["pulse_p3_3x3x4_kfaces"],
-        OPEN_SPECS["subfaces_p3_4x4x2"]]
+        OPEN_SPECS["subfaces_p3_4x4x2"], OPEN_SPECS["pulse_p3_3x3x4_kfaces_local"]]
 
 
 def _setup(spec, grid, precision=capi.FP64):

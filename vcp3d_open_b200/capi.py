@@ -36,6 +36,7 @@ EXPORTED = [
     "vcpg_time_residual_kernels", "vcpg_set_open_boundary_partition",
     "vcpg_boundary_mach_weights", "vcpg_set_boundary_mach_sums", "vcpg_residual_part",
     "vcpg_set_partition_parts", "vcpg_set_send_list", "vcpg_pack_send_list",
+    "vcpg_boundary_rows", "vcpg_boundary_local_mach", "vcpg_set_boundary_outlet_mach",
     "vcpg_line_contraction_probe",
     "vcpg_time_step_noalloc", "vcpg_set_open_boundary", "vcpg_set_open_boundary_subfaces", "vcpg_ensemble_create",
     "vcpg_ensemble_destroy", "vcpg_ensemble_last_error", "vcpg_ensemble_footprint",
@@ -160,6 +161,9 @@ def load() -> C.CDLL:
     lib.vcpg_set_boundary_mach_sums.argtypes = [hp, dp]
     lib.vcpg_residual_part.argtypes = [hp, C.c_int32]
     lib.vcpg_set_partition_parts.argtypes = [hp, C.c_int32, C.c_int32]
+    lib.vcpg_boundary_rows.argtypes = [hp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+    lib.vcpg_boundary_local_mach.argtypes = [hp, dp]
+    lib.vcpg_set_boundary_outlet_mach.argtypes = [hp, dp]
     lib.vcpg_set_send_list.argtypes = [hp, C.c_int32, C.POINTER(C.c_int32), C.c_int32]
     lib.vcpg_pack_send_list.argtypes = [hp, C.c_int32, C.c_void_p]
     lib.vcpg_set_open_boundary_subfaces.argtypes = [hp, C.POINTER(OpenBoundary),

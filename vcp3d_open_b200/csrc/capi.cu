@@ -69,6 +69,14 @@ struct vcpg_handle {
   // Block-wide Mach sums per block face (vcpg_set_boundary_mach_sums).
   double *d_bmachsums = nullptr;
   bool use_bmach_sums = false;
+  // Partitioned blocks: per boundary row its row in the block's list and the
+  // block row of its subface's last face; the outlets' element-local Mach
+  // numbers set per residual (vcpg_set_boundary_outlet_mach) where a last face
+  // lies on another rank.
+  std::vector<int> bBlockRow, bBlockLast;
+  bool remoteLast = false;
+  double *d_bmachlast = nullptr;
+  bool use_bmachlast = false;
   std::string err;
 };
 
@@ -185,6 +193,7 @@ BoundaryArgs MakeBoundaryArgs(vcpg_handle *h) {
   b.bmach = h->d_bmach;
   b.bmach_local = h->d_bmach ? h->d_bmach + h->nB : nullptr;   // [nB, 2 nB)
   b.bmach_sums = h->use_bmach_sums ? h->d_bmachsums : nullptr;
+  b.bmach_last = h->use_bmachlast ? h->d_bmachlast : nullptr;
   b.bflux = h->d_bflux;
   b.nB = h->nB;
   b.mu = h->prm.mu;
@@ -249,6 +258,14 @@ int InstallOpenBoundary(vcpg_handle *h, const OpenBoundaryHost &ob_host) {
                           cudaMemcpyHostToDevice));
   h->nB = ob_host.nB;
   h->cml_on = ob_host.cmlOn;
+  h->bBlockRow = ob_host.blockRow;
+  h->bBlockLast = ob_host.blockLast;
+  h->remoteLast = false;
+  for (int f = 0; f < 6; ++f) {
+    const BlockFaceCfg &c = ob_host.cfg[f];
+    for (int r = c.first; r < c.first + c.count; ++r)
+      if (c.localMach && ob_host.bface[(size_t)r * kBfStride + kBfLast] < 0) h->remoteLast = true;
+  }
   for (int f = 0; f < 6; ++f) h->cfg[f] = ob_host.cfg[f];
   h->open = true;
   h->res_valid = false;
@@ -339,7 +356,7 @@ int vcpg_destroy(vcpg_handle *h) {
                   h->d_status, h->d_counter, h->d_ticket, h->d_cgstats, h->d_bface, h->d_bpresc, h->d_pc,
                   h->d_dlq, h->d_btrace, h->d_bmach, h->d_bflux, h->d_sponge, h->d_dampfn,
                   h->d_dampst, h->d_cml, h->d_cfg, h->d_fflux, h->d_eddymax, h->d_nmetric,
-                  h->d_bforce, h->d_center, h->d_scratch, h->d_bmachsums};
+                  h->d_bforce, h->d_center, h->d_scratch, h->d_bmachsums, h->d_bmachlast};
   for (void *p : bufs)
     if (p) cudaFree(p);
   for (int *p : h->d_send)
@@ -501,6 +518,9 @@ int vcpg_get_raw_residual(vcpg_handle *h, double *res) {
 
 int vcpg_residual(vcpg_handle *h, double *monitoring, int32_t keep_raw) {
   if (!h) return VCPG_E_INVALID;
+  if (h->remoteLast && !h->use_bmachlast)
+    return Fail(h, VCPG_E_INVALID, "outlet Mach numbers of subfaces whose last face lies on "
+                                   "another rank: vcpg_set_boundary_outlet_mach first");
   if (keep_raw && !h->d_resRaw) {
     cudaError_t e = cudaMalloc((void **)&h->d_resRaw, (size_t)h->nE * 5 * h->KD * 8);
     if (e != cudaSuccess) return Fail(h, VCPG_E_OOM, "cudaMalloc raw residual");
@@ -842,10 +862,6 @@ int vcpg_set_open_boundary_partition(vcpg_handle *h, const vcpg_open_boundary *o
     return Fail(h, VCPG_E_INVALID, "declare the partition first (vcpg_set_partition)");
   if (!SupportsOpenBoundaries(h->K, h->M))
     return Fail(h, VCPG_E_UNSUPPORTED_KM, "no open-boundary kernels for this degree");
-  if (ob->outlet_local_mach)
-    return Fail(h, VCPG_E_INVALID, "the outlet's element-local Mach number takes the last "
-                                   "element of a subface, which a partitioned block does not "
-                                   "hold on every rank");
   vcpg_params bp = h->prm;
   for (int d = 0; d < 3; ++d) bp.n_elem[d] = block_n_elem[d];
   const int64_t nBlock = (int64_t)bp.n_elem[0] * bp.n_elem[1] * bp.n_elem[2];
@@ -876,6 +892,41 @@ int vcpg_boundary_mach_weights(vcpg_handle *h, double *weights, int32_t *counts)
   return VCPG_OK;
 }
 
+int vcpg_boundary_rows(vcpg_handle *h, int32_t *block_rows, int32_t *block_last) {
+  if (!h || !block_rows || !block_last) return VCPG_E_INVALID;
+  if (!h->open) return Fail(h, VCPG_E_INVALID, "no open boundaries");
+  for (int b = 0; b < h->nB; ++b) {
+    const bool sliced = (size_t)b < h->bBlockRow.size();
+    block_rows[b] = sliced ? h->bBlockRow[b] : b;
+    block_last[b] = sliced ? h->bBlockLast[b] : -1;
+  }
+  return VCPG_OK;
+}
+
+int vcpg_boundary_local_mach(vcpg_handle *h, double *values) {
+  if (!h || !values) return VCPG_E_INVALID;
+  if (!h->open || h->nB == 0) return VCPG_OK;
+  VCPG_CUDA(h, cudaMemcpyAsync(values, h->d_bmach + h->nB, sizeof(double) * h->nB,
+                               cudaMemcpyDeviceToHost, h->stream));
+  VCPG_CUDA(h, cudaStreamSynchronize(h->stream));
+  return VCPG_OK;
+}
+
+int vcpg_set_boundary_outlet_mach(vcpg_handle *h, const double *values) {
+  if (!h) return VCPG_E_INVALID;
+  if (!values) { h->use_bmachlast = false; return VCPG_OK; }
+  if (!h->open || h->nB == 0) return VCPG_OK;
+  if (!h->d_bmachlast) {
+    cudaError_t e = cudaMalloc((void **)&h->d_bmachlast, sizeof(double) * h->nB);
+    if (e != cudaSuccess) return Fail(h, VCPG_E_OOM, "cudaMalloc outlet Mach numbers");
+  }
+  VCPG_CUDA(h, cudaMemcpyAsync(h->d_bmachlast, values, sizeof(double) * h->nB,
+                               cudaMemcpyHostToDevice, h->stream));
+  VCPG_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->use_bmachlast = true;
+  return VCPG_OK;
+}
+
 int vcpg_set_boundary_mach_sums(vcpg_handle *h, const double *sums) {
   if (!h) return VCPG_E_INVALID;
   if (!sums) { h->use_bmach_sums = false; return VCPG_OK; }
@@ -892,6 +943,9 @@ int vcpg_set_boundary_mach_sums(vcpg_handle *h, const double *sums) {
 
 int vcpg_residual_part(vcpg_handle *h, int32_t part) {
   if (!h || (part != 0 && part != 1)) return VCPG_E_INVALID;
+  if (h->remoteLast && !h->use_bmachlast)
+    return Fail(h, VCPG_E_INVALID, "outlet Mach numbers of subfaces whose last face lies on "
+                                   "another rank: vcpg_set_boundary_outlet_mach first");
   if (h->nOwned == h->nE)
     return Fail(h, VCPG_E_INVALID, "residual parts: a partitioned handle only");
   const int64_t nO = h->nOwned, nF = h->nFace, fR = h->fluxReady, rR = h->resReady;

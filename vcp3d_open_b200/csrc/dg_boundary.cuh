@@ -39,6 +39,10 @@ struct BoundaryArgs {
   double *btrace;              // [nB][4][5][M^2]: value, d/dr, d/ds, d/dt
   double *bmach;               // [nB] area-weighted projected Mach number
   double *bmach_local;         // [nB] the same averaged over the face's own area
+  // Optional [nB]: per face, the outlet's element-local Mach number (the value of
+  // its subface's last face, which a partitioned block may hold on another
+  // rank); null: bmach_local of the face's kBfLast row.
+  const double *bmach_last;
   // Optional [6]: per block face, the sum of the weights over the whole block
   // (a partitioned block sums across its slabs); null: this list's own faces.
   const double *bmach_sums;
@@ -395,7 +399,7 @@ __global__ void __launch_bounds__(NT) BoundaryFluxKernel(const BoundaryArgs a) {
   // subface's last element (the value the reference's subface member holds,
   // src/BoundaryState.cpp:1327); the inlets always take the boundary average.
   const double Mach = (type == VCPG_BC_OUTFLOW_NSCBC && c.localMach && a.bmach_local)
-                          ? a.bmach_local[bf[kBfLast]]
+                          ? (a.bmach_last ? a.bmach_last[b] : a.bmach_local[bf[kBfLast]])
                           : s_mach;
   const double Mavg2 = Mach * Mach;
   const double gm1 = kGam - 1.0, ovgm1 = 1.0 / gm1;

@@ -489,6 +489,8 @@ void SliceOpenBoundary(const OpenBoundaryHost &block, const int64_t *localToGlob
       const int64_t l = localOf[row[kBfElem]];
       if (l < 0) continue;
       newIndex[b] = out.nB++;
+      out.blockRow.push_back(b);
+      out.blockLast.push_back(row[kBfLast]);
       out.bface.insert(out.bface.end(), row, row + kBfStride);
       out.bface[out.bface.size() - kBfStride + kBfElem] = (int)l;
       out.bface[out.bface.size() - kBfStride + kBfLast] = -1;   // remapped below

@@ -52,6 +52,9 @@ struct OpenBoundaryHost {
   std::vector<double> dlq;          // [M][M]: dlq[i * M + k] = dL_k(q_i), Lagrange basis
                                     // on the Gauss points
   BlockFaceCfg cfg[6] = {};
+  // Sliced lists (SliceOpenBoundary): per row, its row in the whole block's list
+  // and the block row of its subface's last face (-1 without).
+  std::vector<int> blockRow, blockLast;
   std::vector<int32_t> nbrCode;     // [nE][6] neighbour table with boundary faces coded
                                     // as -2 - (index in the boundary-face list)
   int nS = 0;                       // sponge elements

@@ -331,6 +331,9 @@ class Shard:
         self.kd5 = 5 * (params.n_poly + 1) ** 3
         self.device = torch.device("cuda", torch.cuda.current_device())
         self.open = case is not None and case.spec.is_open
+        # The outlet's element-local Mach number: the value of each subface's last
+        # face, which may lie in another part.
+        self.outlet_local = self.open and self.ghosts and bool(case.spec.outlet_local_mach)
         if self.open:
             self._set_open_boundary(case, disc)
         if modal is not None:
@@ -381,6 +384,32 @@ class Shard:
             out.append((w[o:o + int(c)].copy(), ids))
             o += int(c)
         return out
+
+    def outlet_mach_inputs(self):
+        """(block rows, block rows of the subfaces' last faces, face-averaged Mach
+        numbers) of this part's boundary rows, from the last boundary trace."""
+        counts = np.zeros(6, dtype=np.int32)
+        lib = self.solver.lib
+        self.solver._check(lib.vcpg_boundary_mach_weights(self.solver.h, None, capi.ptr(counts)),
+                           "boundary_mach_weights")
+        nB = int(counts.sum())
+        rows = np.zeros(max(nB, 1), dtype=np.int32)
+        last = np.zeros(max(nB, 1), dtype=np.int32)
+        vals = np.zeros(max(nB, 1))
+        if nB:
+            self.solver._check(lib.vcpg_boundary_rows(self.solver.h, capi.ptr(rows),
+                                                      capi.ptr(last)), "boundary_rows")
+            self.solver._check(lib.vcpg_boundary_local_mach(self.solver.h, capi.ptr(vals)),
+                               "boundary_local_mach")
+        return rows[:nB].copy(), last[:nB].copy(), vals[:nB].copy()
+
+    def set_outlet_mach(self, values):
+        a = np.ascontiguousarray(values, dtype=np.float64)
+        if len(a) == 0:
+            a = np.zeros(1)
+        self.solver._check(self.solver.lib.vcpg_set_boundary_outlet_mach(self.solver.h,
+                                                                          capi.ptr(a)),
+                           "set_boundary_outlet_mach")
 
     def set_mach_sums(self, sums):
         a = np.ascontiguousarray(sums, dtype=np.float64)
@@ -611,6 +640,15 @@ class ShardedSolver:
         sums = block_mach_sums(self.t.gather([s.mach_weights() for s in self.shards]))
         for s in self.shards:
             s.set_mach_sums(sums)
+        if any(s.outlet_local for s in self.shards):
+            # Every rank's face values by block row; each outlet row takes its
+            # subface's last face's value, wherever that face lies.
+            mine = [s.outlet_mach_inputs() for s in self.shards]
+            by_row = {}
+            for rows, vals in self.t.gather([(m[0], m[2]) for m in mine]):
+                by_row.update(zip(rows.tolist(), vals.tolist()))
+            for s, (_, last, _) in zip(self.shards, mine):
+                s.set_outlet_mach([by_row[int(r)] if r >= 0 else 0.0 for r in last])
 
     def residual(self, monitoring: bool = False):
         if monitoring:
