@@ -285,21 +285,6 @@ template <int K, int M, typename T = double, bool OPEN = false> struct Plan {
   using VB = std::conditional_t<PADVOL, typename CL::B, Dense<K, M, M>>;
   using VD = std::conditional_t<PADVOL, typename CL::D, Dense<M, M, K>>;
   using VE = std::conditional_t<PADVOL, typename CL::E, Dense<M, K, K>>;
-  static constexpr int WORK = VOL > OTHER ? VOL : OTHER;
-  // Persistent: sol, R, CG point data (rho, u, v, w, p per point), J*w, reduction scratch,
-  // face vectors (basis and derivative at r = -1, +1).
-  // Face vectors: basis and derivative at r = -1, +1 (4 K values, room for 28 at least).
-  static constexpr int FV = 4 * (K > 7 ? K : 7);
-  // Reduction scratch: two areas of 3 values per warp of up to 512 threads.
-  static constexpr int RED = 96;
-  static constexpr int PERSIST = 10 * KD + 6 * MD + RED + FV;
-  static constexpr int TOTAL = PERSIST + WORK;
-  static constexpr size_t BYTES = sizeof(T) * (size_t)TOTAL;
-  // Above the 227 KB of one CTA (degrees 7-9 in FP64): the arrays live in a
-  // global scratch area per CTA (stride SCRATCH, 16-byte aligned) of a grid that
-  // loops over the elements.
-  static constexpr bool BIG = BYTES > 227 * 1024;
-  static constexpr int SCRATCH = (TOTAL + 3) / 4 * 4;
   // Threads per CTA and CTAs per SM (through __launch_bounds__ they bound the
   // registers per thread). FP64: 128 threads cover the widest contraction stage
   // of degrees <= 3 in one or two passes; from degree 4 on 256 threads (degree
@@ -307,13 +292,38 @@ template <int K, int M, typename T = double, bool OPEN = false> struct Plan {
   // 40x20x20 pulse, 21.2 -> 20.5 ms on TGV 48^3, measured on B200). FP32: 256
   // threads from degree 4 up. As many CTAs as the shared memory allows, up to
   // the VCPG_CAP_RES_* bounds.
-  static constexpr int FIT = (int)(227 * 1024 / BYTES);
   static constexpr bool FP64 = sizeof(T) == 8;
   static constexpr int NT = K <= 4 ? 128 : 256;
   static constexpr int CAP =
       FP64 ? (K <= 3 ? VCPG_CAP_RES_FP64_SMALL : VCPG_CAP_RES_FP64)
            : (NT == 256 ? VCPG_CAP_RES_FP32_256
                         : (K == 4 ? VCPG_CAP_RES_FP32_K4 : VCPG_CAP_RES_FP32_SMALL));
+  // Persistent: sol, R, CG point data (rho, u, v, w, p per point), J*w, reduction scratch,
+  // face vectors (basis and derivative at r = -1, +1).
+  // Face vectors: basis and derivative at r = -1, +1 (4 K values, room for 28 at least).
+  static constexpr int FV = 4 * (K > 7 ? K : 7);
+  // Reduction scratch: two areas of 3 values per warp of up to 512 threads.
+  static constexpr int RED = 96;
+  static constexpr int PERSIST = 10 * KD + 6 * MD + RED + FV;
+  // The work area: the largest phase, widened to hold the volume metric (10 M^3
+  // FP64 values) after the volume phase's arrays for VolumeMetricPrefetch where
+  // that keeps the CTAs per SM (228 KB per SM, 1 KB reserved per CTA).
+  static constexpr int WORK0 = VOL > OTHER ? VOL : OTHER;
+  static constexpr int VPF = (VOL + 1) / 2 * 2 + (int)((80 * (size_t)MD + sizeof(T) - 1) / sizeof(T));
+  static constexpr size_t B0 = sizeof(T) * (size_t)(PERSIST + WORK0);
+  static constexpr size_t B1 = sizeof(T) * (size_t)(PERSIST + VPF);
+  static constexpr int F0 = (int)(233472 / (B0 + 1024)), F1 = (int)(233472 / (B1 + 1024));
+  static constexpr int L0 = F0 < CAP ? F0 : CAP, L1 = F1 < CAP ? F1 : CAP;
+  static constexpr bool WIDEN = VPF > WORK0 && L1 >= 1 && L1 >= L0 && B1 <= 227 * 1024;
+  static constexpr int WORK = WIDEN ? VPF : WORK0;
+  static constexpr int TOTAL = PERSIST + WORK;
+  static constexpr size_t BYTES = sizeof(T) * (size_t)TOTAL;
+  // Above the 227 KB of one CTA (degrees 7-9 in FP64): the arrays live in a
+  // global scratch area per CTA (stride SCRATCH, 16-byte aligned) of a grid that
+  // loops over the elements.
+  static constexpr bool BIG = BYTES > 227 * 1024;
+  static constexpr int SCRATCH = (TOTAL + 3) / 4 * 4;
+  static constexpr int FIT = (int)(227 * 1024 / BYTES);
   static constexpr int MIN_BLOCKS = FIT < 1 ? 1 : (FIT > CAP ? CAP : FIT);
 };
 
