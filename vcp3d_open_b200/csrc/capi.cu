@@ -177,6 +177,8 @@ int CheckStatus(vcpg_handle *h) {
                                                   std::to_string(st[0]) + " element solve(s)");
   if (st[2]) return Fail(h, VCPG_E_NEG_A2, "negative or not-a-number square speed of sound in the time step");
   if (st[1]) return Fail(h, VCPG_E_INVALID, "physical boundary face without a boundary condition");
+  if (st[3]) return Fail(h, VCPG_E_CUDA, "an asynchronous copy into shared memory did not complete "
+                                          "within its wait bound");
   return VCPG_OK;
 }
 

@@ -146,6 +146,37 @@ __device__ __forceinline__ void CpAsync8(double *dst_smem, const double *src_gme
   const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src_gmem) : "memory");
 }
+// One bulk copy (the TMA engine's 1-D form, no multicast) of `bytes` from global
+// to this CTA's shared memory, completing on the mbarrier `bar` (both 16-byte
+// aligned, bytes a multiple of 16); issued by one thread after
+// BulkBarrierInit and an arrive that expects the bytes.
+__device__ __forceinline__ void BulkBarrierInit(unsigned long long *bar) {
+  const unsigned b = static_cast<unsigned>(__cvta_generic_to_shared(bar));
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(b) : "memory");
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+__device__ __forceinline__ void BulkCopyToShared(void *dst_smem, const void *src_gmem,
+                                                 const unsigned bytes,
+                                                 unsigned long long *bar) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst_smem));
+  const unsigned b = static_cast<unsigned>(__cvta_generic_to_shared(bar));
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n"
+               ::"r"(b), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+               ::"r"(d), "l"(src_gmem), "r"(bytes), "r"(b) : "memory");
+}
+// Waits for phase 0 of the mbarrier with a bounded number of polls; false when
+// the bound ran out (the caller records it).
+__device__ __forceinline__ bool BulkWait(unsigned long long *bar) {
+  const unsigned b = static_cast<unsigned>(__cvta_generic_to_shared(bar));
+  for (int i = 0; i < (1 << 24); ++i) {
+    unsigned done;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n"
+                 " selp.u32 %0, 1, 0, p;\n}\n" : "=r"(done) : "r"(b) : "memory");
+    if (done) return true;
+  }
+  return false;
+}
 __device__ __forceinline__ void CpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void CpAsyncWaitAll() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
@@ -309,7 +340,9 @@ template <int K, int M, typename T = double, bool OPEN = false> struct Plan {
   // FP64 values) after the volume phase's arrays for VolumeMetricPrefetch where
   // that keeps the CTAs per SM (228 KB per SM, 1 KB reserved per CTA).
   static constexpr int WORK0 = VOL > OTHER ? VOL : OTHER;
-  static constexpr int VPF = (VOL + 1) / 2 * 2 + (int)((80 * (size_t)MD + sizeof(T) - 1) / sizeof(T));
+  static constexpr int A16 = 16 / (int)sizeof(T);   // values per 16 bytes
+  static constexpr int VPF_OFF = ((PERSIST + VOL + A16 - 1) / A16) * A16 - PERSIST;
+  static constexpr int VPF = VPF_OFF + (int)(80 * (size_t)MD / sizeof(T));
   static constexpr size_t B0 = sizeof(T) * (size_t)(PERSIST + WORK0);
   static constexpr size_t B1 = sizeof(T) * (size_t)(PERSIST + VPF);
   static constexpr int F0 = (int)(233472 / (B0 + 1024)), F1 = (int)(233472 / (B1 + 1024));
@@ -432,9 +465,12 @@ __device__ __forceinline__ void MatchingLayerSource(const ResidualArgs &a, const
 // interpolation contractions run, where it fits that space (FP64 up to degree 3).
 template <int K, int M, typename T, bool OPEN> struct VolumeMetricPrefetch {
   using P = Plan<K, M, T, OPEN>;
-  static constexpr int OFF = (P::VOL + 1) / 2 * 2;   // in T, 8-byte aligned
+  // In T from the work area, 16-byte aligned in shared memory (the work area
+  // starts PERSIST values after the 16-byte aligned base).
+  static constexpr int OFF = P::VPF_OFF;
+  static constexpr unsigned BYTES = 80u * M * M * M;   // 10 M^3 FP64 values
   static constexpr bool value =
-      !P::BIG && (long)(P::WORK - OFF) * (long)sizeof(T) >= 10L * M * M * M * 8;
+      !P::BIG && (long)(P::WORK - OFF) * (long)sizeof(T) >= (long)BYTES;
 };
 
 // ---------------------------------------------------------------------------
@@ -448,7 +484,8 @@ template <int K, int M, typename T, bool OPEN> struct VolumeMetricPrefetch {
 template <int NT, int K, int M, typename T, bool OPEN>
 __device__ __forceinline__ void VolumePhase(const ResidualArgs &a, const int e, const double mu,
                                             const T *s_sol, T *s_R, T *s_cgp,
-                                            T *s_jw, T *work, T *s_red, const double *vms) {
+                                            T *s_jw, T *work, T *s_red, const double *vms,
+                                            unsigned long long *bar) {
   constexpr int SLOT = Slot<K, M>::value;
   using P = Plan<K, M, T, OPEN>;
   constexpr int MD = P::MD, KD = P::KD, M2 = P::M2;
@@ -476,7 +513,14 @@ __device__ __forceinline__ void VolumePhase(const ResidualArgs &a, const int e, 
   __syncthreads();
   ContractL<NT, SLOT, K, M, kLeg, 0, 5, K, M, M, K, M, false, T, typename P::VB, Dense<M, M, M>>(tJ, dZ);
   for (int i = threadIdx.x; i < 5 * KD; i += NT) s_R[i] = T(0.0);
-  if constexpr (VolumeMetricPrefetch<K, M, T, OPEN>::value) CpAsyncWaitAll();
+  if constexpr (VolumeMetricPrefetch<K, M, T, OPEN>::value) {
+    // A wait that runs out is recorded and followed by one more bounded wait for
+    // the copy, which must not land after the work area is reused.
+    if (!BulkWait(bar)) {
+      if (threadIdx.x == 0) atomicAdd(a.status + 3, 1);
+      BulkWait(bar);
+    }
+  }
   __syncthreads();
 
   const double *vm = a.vol_metric + (size_t)e * 10 * MD;
@@ -1410,10 +1454,14 @@ __device__ __forceinline__ void ResidualElement(const ResidualArgs &a, const int
   }
   using VP = VolumeMetricPrefetch<K, M, T, OPEN>;
   double *vms = VP::value ? reinterpret_cast<double *>(work + VP::OFF) : nullptr;
+  // The element's volume metric: one bulk copy into the work area above the
+  // volume phase's arrays, in flight during the interpolation contractions.
+  __shared__ __align__(8) unsigned long long s_bar;
   if constexpr (VP::value) {
-    const double *g = a.vol_metric + (size_t)e * 10 * P::MD;
-    for (int i = threadIdx.x; i < 10 * P::MD; i += NT) CpAsync8(vms + i, g + i);
-    CpAsyncCommit();
+    if (threadIdx.x == 0) {
+      BulkBarrierInit(&s_bar);
+      BulkCopyToShared(vms, a.vol_metric + (size_t)e * 10 * P::MD, VP::BYTES, &s_bar);
+    }
   }
   const double *src = a.sol + (size_t)e * 5 * KD;
   for (int i = threadIdx.x; i < 5 * KD; i += NT) s_sol[i] = T(src[i]);
@@ -1422,7 +1470,7 @@ __device__ __forceinline__ void ResidualElement(const ResidualArgs &a, const int
     s_fv[2 * K + threadIdx.x] = FaceDer<Slot<K, M>::value, T>(threadIdx.x);
   }
   __syncthreads();
-  VolumePhase<NT, K, M, T, OPEN>(a, e, mu, s_sol, s_R, s_cgp, s_jw, work, s_red, vms);
+  VolumePhase<NT, K, M, T, OPEN>(a, e, mu, s_sol, s_R, s_cgp, s_jw, work, s_red, vms, &s_bar);
   FacePhase<NT, K, M, T, OPEN>(a, e, s_R, s_fv, work);
   if (a.res_raw) {
     double *dst = a.res_raw + (size_t)e * 5 * KD;

@@ -404,8 +404,10 @@ int CheckBucketStatus(vcpg_ensemble *e, Bucket &b) {
   int st[4] = {0, 0, 0, 0};
   ENS_CUDA(e, cudaMemcpyAsync(st, b.status, sizeof(st), cudaMemcpyDeviceToHost, b.stream));
   ENS_CUDA(e, cudaStreamSynchronize(b.stream));
-  if (st[0] || st[1] || st[2]) {
+  if (st[0] || st[1] || st[2] || st[3]) {
     ENS_CUDA(e, cudaMemsetAsync(b.status, 0, sizeof(st), b.stream));
+    if (st[3]) return Fail(e, VCPG_E_CUDA, "an asynchronous copy into shared memory did not "
+                                           "complete within its wait bound");
     if (st[0]) return Fail(e, VCPG_E_CG_NOCONV, "mass-matrix CG reached 100 iterations (degree " +
                                                    std::to_string(b.deg) + ")");
     if (st[2]) return Fail(e, VCPG_E_NEG_A2, "negative or not-a-number square speed of sound in the time step");
