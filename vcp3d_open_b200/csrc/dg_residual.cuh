@@ -1528,8 +1528,9 @@ template <int K, int M, typename T = double> struct FluxPlan {
   // of coalesced asynchronous copies instead of strided per-line global loads.
   static constexpr int NB_OFF = (TOTAL * (int)sizeof(T) + 7) / 8;   // in doubles
   static constexpr size_t NB_BYTES = 8 * ((size_t)NB_OFF + 15 * (size_t)KD);
+  // (228 KB per SM with 1 KB reserved per CTA.)
   static constexpr bool NB_PREF = VCPG_FACE_NB_STAGING && !BIG &&
-                                  (int)(227 * 1024 / NB_BYTES) >= MIN_BLOCKS;
+                                  (int)(233472 / (NB_BYTES + 1024)) >= MIN_BLOCKS;
   static constexpr size_t BYTES = NB_PREF ? NB_BYTES : BASE_BYTES;
 };
 
