@@ -1528,8 +1528,10 @@ template <int K, int M, typename T = double> struct FluxPlan {
   // of coalesced asynchronous copies instead of strided per-line global loads.
   static constexpr int NB_OFF = (TOTAL * (int)sizeof(T) + 7) / 8;   // in doubles
   static constexpr size_t NB_BYTES = 8 * ((size_t)NB_OFF + 15 * (size_t)KD);
-  // (228 KB per SM with 1 KB reserved per CTA.)
-  static constexpr bool NB_PREF = VCPG_FACE_NB_STAGING && !BIG &&
+  // (228 KB per SM with 1 KB reserved per CTA), from degree 4 on: measured on B200,
+  // the staging takes FaceFluxKernel from 4.62 to 4.50 ms at degree 4 (TGV 48^3,
+  // FP64) but from 0.75 to 0.80 ms at degree 2 (TGV 40^3, FP64; FP32 0.52 to 0.55).
+  static constexpr bool NB_PREF = VCPG_FACE_NB_STAGING && !BIG && K >= 5 &&
                                   (int)(233472 / (NB_BYTES + 1024)) >= MIN_BLOCKS;
   static constexpr size_t BYTES = NB_PREF ? NB_BYTES : BASE_BYTES;
 };
