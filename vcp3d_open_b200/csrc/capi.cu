@@ -226,7 +226,7 @@ int EnqueueResidual(vcpg_handle *h, const ResidualArgs &a, int *launches) {
   return VCPG_OK;
 }
 
-// Uploads a block's (or slab's) open-boundary data to the handle.
+// Uploads a block's (or a part's) open-boundary data to the handle.
 int InstallOpenBoundary(vcpg_handle *h, const OpenBoundaryHost &ob_host) {
   int rc = VCPG_OK;
   const int M2 = h->M2, MD = h->MD;

@@ -72,7 +72,7 @@ int BuildOpenBoundary(const vcpg_params &prm, const vcpg_open_boundary &ob,
                       const double *gridNodes, OpenBoundaryHost &out, std::string &err,
                       const vcpg_subface *subfaces = nullptr, int nSubfaces = 0);
 
-// The part of a block's open-boundary data that a slab handle needs: boundary
+// The part of a block's open-boundary data that a partitioned handle needs: boundary
 // faces and sponge elements of its owned local elements (local_to_global[l]:
 // block index of local element l, the first nOwned owned), in block order, the
 // block faces' areas of the whole block, and the handle's neighbour table
