@@ -90,3 +90,27 @@ def test_request_loop_admits_within_capacity_and_completes(monkeypatch):
     assert 1 <= ens.max_resident < 30                      # capacity limited the batch
     assert rep["latency_p99_s"] >= rep["latency_p50_s"] >= 0.0
     assert rep["dof_updates"] == sum(r.spec.n_dofs * r.steps for r in reqs)
+
+
+def test_stream_shards_across_ranks_and_reports_merge(monkeypatch):
+    """Several GPUs: every rank serves every world-th request; the merged report
+    sums the DOF-updates over the longest rank's wall time and takes the
+    percentiles over all requests."""
+    reqs = serving.request_stream(23, seed=9, mean_interarrival=0.001, steps=3, n_range=(3, 5))
+    world = 3
+    parts = [serving.shard_requests(reqs, r, world) for r in range(world)]
+    assert sorted(r.rid for p in parts for r in p) == sorted(r.rid for r in reqs)
+    assert [len(p) for p in parts] == [8, 8, 7]
+    monkeypatch.setattr(serving, "prepare", lambda spec, precision: _Prepared(spec))
+    reports = []
+    for p in parts:
+        ens = FakeEnsemble(3 * max(r.spec.n_elements for r in p))
+        reports.append(serving.serve(p, ens, prepare_workers=2, keep_latencies=True))
+    out = serving.merge_reports(reports)
+    assert out["cases"] == 23 and out["ranks"] == world
+    assert out["dof_updates"] == sum(r.spec.n_dofs * r.steps for r in reqs)
+    wall = max(r["wall_seconds"] for r in reports)
+    assert out["wall_seconds"] == wall and out["dof_updates_per_s"] == out["dof_updates"] / wall
+    lat = np.concatenate([r["latency_s"] for r in reports])
+    assert out["latency_p50_s"] == float(np.percentile(lat, 50))
+    assert out["latency_max_s"] == float(lat.max())

@@ -13,6 +13,13 @@ DOF-updates/s.
 
     python -m vcp3d_open_b200.serving [--cases 256] [--steps 300] [--precision mixed]
     python -m vcp3d_open_b200.serving --cases 128 --offered-load 0.5,0.8,0.95
+
+Several GPUs (one process each, torchrun): every rank serves every world-th
+request of the stream on its own GPU, the cases being independent, and rank 0
+prints one report for the job (summed DOF-updates over the longest rank's wall
+time, percentiles over all requests):
+
+    torchrun --nproc-per-node N --master-addr 127.0.0.1 -m vcp3d_open_b200.serving
 """
 from __future__ import annotations
 
@@ -22,6 +29,7 @@ import concurrent.futures as cf
 import ctypes as C
 import dataclasses
 import json
+import os
 import sys
 import time
 from typing import Dict, List, Optional
@@ -278,7 +286,8 @@ def plan_capacities(requests: List[Request], budget_bytes: int) -> Dict[int, tup
 
 
 def serve(requests: List[Request], ens: Ensemble, prepare_workers: int = 8,
-          keep_results: bool = False, progress_every: float = 0.0) -> dict:
+          keep_results: bool = False, progress_every: float = 0.0,
+          keep_latencies: bool = False) -> dict:
     """Continuous batching: admit arrived requests whenever their bucket has room,
     step every bucket with resident cases, retire finished cases."""
     t0 = time.perf_counter()
@@ -352,7 +361,38 @@ def serve(requests: List[Request], ens: Ensemble, prepare_workers: int = 8,
     }
     if keep_results:
         out["results"] = results
+    if keep_latencies:
+        out["latency_s"] = lat.tolist()
+        out["admission_wait_s"] = qwait.tolist()
     return out
+
+
+def shard_requests(requests: List[Request], rank: int, world: int) -> List[Request]:
+    """The requests rank serves when world GPUs share the stream: every world-th
+    request in arrival order, starting at rank (the cases are independent, so the
+    ranks exchange nothing while they serve)."""
+    ordered = sorted(requests, key=lambda r: (r.arrival, r.rid))
+    return ordered[rank::world]
+
+
+def merge_reports(reports: List[dict]) -> dict:
+    """One report for the whole job from the ranks' reports (each with its raw
+    latencies): DOF-updates summed over ranks per the longest rank's wall time,
+    percentiles over all requests."""
+    wall = max(r["wall_seconds"] for r in reports)
+    dof = sum(r["dof_updates"] for r in reports)
+    lat = np.concatenate([np.asarray(r["latency_s"], dtype=float) for r in reports])
+    qwait = np.concatenate([np.asarray(r["admission_wait_s"], dtype=float) for r in reports])
+    return {
+        "cases": int(sum(r["cases"] for r in reports)), "wall_seconds": wall,
+        "dof_updates": float(dof), "dof_updates_per_s": dof / wall,
+        "latency_p50_s": float(np.percentile(lat, 50)),
+        "latency_p99_s": float(np.percentile(lat, 99)), "latency_max_s": float(lat.max()),
+        "admission_wait_p50_s": float(np.percentile(qwait, 50)),
+        "admission_wait_p99_s": float(np.percentile(qwait, 99)),
+        "loop_iterations_with_steps": [r["loop_iterations_with_steps"] for r in reports],
+        "ranks": len(reports),
+    }
 
 
 def offered_load_sweep(requests: List[Request], loads: List[float], caps: Dict[int, tuple],
@@ -404,8 +444,11 @@ def main(argv=None) -> int:
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
     reqs = request_stream(a.cases, a.seed, steps=a.steps)
-    caps = plan_capacities(reqs, int(a.budget_gb * 1e9))
     prec = capi.MIXED if a.precision == "mixed" else capi.FP64
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1:
+        return _serve_ranks(a, reqs, prec, world)
+    caps = plan_capacities(reqs, int(a.budget_gb * 1e9))
     if a.offered_load:
         loads = [float(x) for x in a.offered_load.split(",")]
         rep = offered_load_sweep(reqs, loads, caps, prec, a.max_cases, a.workers)
@@ -429,6 +472,42 @@ def main(argv=None) -> int:
     if a.out:
         with open(a.out, "w") as f:
             f.write(line + "\n")
+    return 0
+
+
+def _serve_ranks(a, reqs, prec, world) -> int:
+    """Under torchrun, one process per GPU: each rank serves its share of the
+    stream (shard_requests) on its own GPU; rank 0 prints the job's report."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    if a.offered_load:
+        raise SystemExit("the offered-load sweep runs on one GPU")
+    rank, local = int(os.environ["RANK"]), int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=1800))
+    try:
+        mine = shard_requests(reqs, rank, world)
+        caps = plan_capacities(mine, int(a.budget_gb * 1e9))
+        ens = Ensemble(caps, precision=prec, max_cases=a.max_cases)
+        try:
+            rep = serve(mine, ens, prepare_workers=a.workers, progress_every=a.progress,
+                        keep_latencies=True)
+        finally:
+            ens.close()
+        reports = [None] * world
+        dist.all_gather_object(reports, rep)
+    finally:
+        dist.destroy_process_group()
+    if rank == 0:
+        out = merge_reports(reports)
+        out.update({"precision": a.precision, "steps_per_case": a.steps, "seed": a.seed,
+                    "max_cases_per_bucket": a.max_cases, "gpus": world})
+        line = json.dumps(out)
+        print(line)
+        if a.out:
+            with open(a.out, "w") as f:
+                f.write(line + "\n")
     return 0
 
 
