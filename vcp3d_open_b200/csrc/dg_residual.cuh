@@ -1579,14 +1579,31 @@ __device__ __forceinline__ void FaceFluxElement(const ResidualArgs &a, const int
     }
     CpAsyncCommit();
   }
+  // The element's own state: one bulk copy where it is FP64 in shared memory and
+  // its size a multiple of 16 bytes (even K), else converted value by value.
   const double *src = a.sol + (size_t)e * 5 * KD;
-  for (int i = threadIdx.x; i < 5 * KD; i += NT) s_sol[i] = T(src[i]);
+  constexpr bool kBulkState = !FP::BIG && sizeof(T) == 8 && (40 * KD) % 16 == 0;
+  __shared__ __align__(8) unsigned long long s_bar_state;
+  if constexpr (kBulkState) {
+    if (threadIdx.x == 0) {
+      BulkBarrierInit(&s_bar_state);
+      BulkCopyToShared(s_sol, src, 40u * KD, &s_bar_state);
+    }
+  } else {
+    for (int i = threadIdx.x; i < 5 * KD; i += NT) s_sol[i] = T(src[i]);
+  }
   if constexpr (FP::NB_PREF) CpAsyncWaitAll();
   if (threadIdx.x < 2 * K) {
     s_fv[threadIdx.x] = FaceVal<Slot<K, M>::value, T>(threadIdx.x);
     s_fv[2 * K + threadIdx.x] = FaceDer<Slot<K, M>::value, T>(threadIdx.x);
   }
-  __syncthreads();
+  __syncthreads();   // also orders the barrier's initialisation before the waits
+  if constexpr (kBulkState) {
+    if (!BulkWait(&s_bar_state)) {
+      if (threadIdx.x == 0) atomicAdd(a.status + 3, 1);
+      BulkWait(&s_bar_state);
+    }
+  }
   MinFaceFluxes<NT, K, M, T, SGS>(a, e, mu, s_sol, s_fv, work, s_nb);
 }
 
